@@ -1,0 +1,596 @@
+// The exported C ABI of libcharm.so (declared in include/charm_b200.h).
+//
+// Argument checks, error reporting and output conventions restate CHarm
+// 0.4.9 (files cited per function) so that callers see the same behaviour;
+// the numerical work is delegated to the GPU engine (engine.cpp).
+#include <cfloat>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "../../include/charm_b200.h"
+#include "engine.h"
+
+extern "C"
+{
+
+// src/glob/glob.c:16-23
+CHARM_EXTERN double charm_glob_threshold = 100.0 * DBL_EPSILON;
+CHARM_EXTERN double charm_glob_threshold2 = 100000.0 * DBL_EPSILON;
+CHARM_EXTERN unsigned long charm_glob_polar_optimization_a1 = 100;
+CHARM_EXTERN double charm_glob_polar_optimization_a2 = -1.0;
+
+// ---------------------------------------------------------------------------
+// Error object, src/err/err_init.c, err_free.c, err_reset.c, err_isempty.c,
+// err_handler.c, err_set.c
+// ---------------------------------------------------------------------------
+charm_err *charm_err_init(void)
+{
+    charm_err *err = (charm_err *)malloc(sizeof(charm_err));
+    if (!err)
+        return NULL;
+    err->file = (char **)calloc(CHARM_ERR_MAX_LEVEL, sizeof(char *));
+    err->line = (size_t *)calloc(CHARM_ERR_MAX_LEVEL, sizeof(size_t));
+    err->func = (char **)calloc(CHARM_ERR_MAX_LEVEL, sizeof(char *));
+    err->msg = (char *)calloc(CHARM_ERR_MAX_MSG, 1);
+    bool ok = err->file && err->line && err->func && err->msg;
+    for (size_t e = 0; ok && e < CHARM_ERR_MAX_LEVEL; e++)
+    {
+        err->file[e] = (char *)calloc(CHARM_ERR_MAX_FILE, 1);
+        err->func[e] = (char *)calloc(CHARM_ERR_MAX_FUNC, 1);
+        ok = err->file[e] && err->func[e];
+    }
+    if (!ok)
+    {
+        charm_err_free(err);
+        return NULL;
+    }
+    err->distributed = 0;
+    charm_err_reset(err);
+    return err;
+}
+
+void charm_err_free(charm_err *err)
+{
+    if (!err)
+        return;
+    for (size_t e = 0; e < CHARM_ERR_MAX_LEVEL; e++)
+    {
+        if (err->file)
+            free(err->file[e]);
+        if (err->func)
+            free(err->func[e]);
+    }
+    free(err->file);
+    free(err->func);
+    free(err->line);
+    free(err->msg);
+    free(err);
+}
+
+void charm_err_reset(charm_err *err)
+{
+    if (!err)
+        return;
+    err->level = 0;
+    for (size_t e = 0; e < CHARM_ERR_MAX_LEVEL; e++)
+    {
+        memset(err->file[e], 0, CHARM_ERR_MAX_FILE);
+        memset(err->func[e], 0, CHARM_ERR_MAX_FUNC);
+    }
+    memset(err->line, 0, CHARM_ERR_MAX_LEVEL * sizeof(size_t));
+    err->code = CHARM_SUCCESS;
+    memset(err->msg, 0, CHARM_ERR_MAX_MSG);
+    err->saturated = 0;
+}
+
+_Bool charm_err_isempty(const charm_err *err)
+{
+    if (!err)
+        return 0;
+    return err->code == CHARM_SUCCESS;
+}
+
+// src/err/err_inc_level.c
+static void err_inc_level(charm_err *err)
+{
+    if (err->saturated)
+        return;
+    err->level += 1;
+    if (err->level >= CHARM_ERR_MAX_LEVEL)
+        err->saturated = 1;
+}
+
+static void err_set(charm_err *err, const char *file, size_t line,
+                    const char *func, int code, const char *msg)
+{
+    if (!err || err->saturated)
+        return;
+    size_t l = err->level;
+    snprintf(err->file[l], CHARM_ERR_MAX_FILE, "%s", file);
+    err->line[l] = line;
+    snprintf(err->func[l], CHARM_ERR_MAX_FUNC, "%s", func);
+    err->code = code;
+    snprintf(err->msg, CHARM_ERR_MAX_MSG, "%s", msg);
+    err_inc_level(err);
+}
+
+void charm_err_handler(charm_err *err, _Bool terminate)
+{
+    if (!err || charm_err_isempty(err))
+        return;
+    fprintf(stderr, "\n-----------\nCHarm ERROR\n-----------\n"
+                    "Error code: %u                   Traceback (most recent "
+                    "call last)\n\n",
+            err->code);
+    for (size_t e = err->level - 1; e != (size_t)(-1); e--)
+        fprintf(stderr, "    File \"%s\", line: %zu, function: \"%s\"\n\n",
+                err->file[e], err->line[e], err->func[e]);
+    if (err->saturated)
+        fprintf(stderr, "%s", "    Warning: The error structure is saturated.  "
+                              "Most recent function calls may therefore not be "
+                              "reported.\n\n");
+    fprintf(stderr, "Error message: %s\n-----------\n", err->msg);
+    if (terminate)
+        exit(CHARM_FAILURE);
+    charm_err_reset(err);
+}
+
+// src/misc/misc_is_nearly_equal.c:20-31
+static bool nearly_equal(double a, double b, double eps)
+{
+    double aa = a < 0 ? -a : a, ba = b < 0 ? -b : b;
+    double d = a > b ? a - b : b - a, s = aa + ba;
+    if (a == b)
+        return true;
+    if (a == 0.0 || b == 0.0 || s == aa || s == ba)
+        return d <= eps;
+    return d / (aa > ba ? aa : ba) <= eps;
+}
+
+#define SET_ERR(err, code, msg) err_set((err), __FILE__, __LINE__, __func__, \
+                                        (code), (msg))
+
+// ---------------------------------------------------------------------------
+// Points, src/crd/crd_point_alloc.c, crd_point_init.c, crd_point_free.c,
+// crd_point_check_inputs.c, crd_point_npoint.c
+// ---------------------------------------------------------------------------
+static bool is_point_type(int t)
+{
+    return t == CHARM_CRD_POINT_SCATTERED || t == CHARM_CRD_POINT_GRID ||
+           t == CHARM_CRD_POINT_GRID_GL || t == CHARM_CRD_POINT_GRID_DH1 ||
+           t == CHARM_CRD_POINT_GRID_DH2;
+}
+
+static bool is_quad_type(int t)
+{
+    return t == CHARM_CRD_POINT_GRID_GL || t == CHARM_CRD_POINT_GRID_DH1 ||
+           t == CHARM_CRD_POINT_GRID_DH2;
+}
+
+static bool is_grid_type(int t)
+{
+    return t == CHARM_CRD_POINT_GRID || is_quad_type(t);
+}
+
+charm_point *charm_crd_point_init(int type, size_t nlat, size_t nlon,
+                                  double *lat, double *lon, double *r)
+{
+    if (!is_point_type(type))
+        return NULL;
+    if (type == CHARM_CRD_POINT_SCATTERED && nlat != nlon)
+        return NULL;
+    charm_point *p = (charm_point *)malloc(sizeof(charm_point));
+    if (!p)
+        return NULL;
+    p->lat = p->lon = p->r = p->w = NULL;
+    if (nlat > 0)
+    {
+        p->lat = lat;
+        p->r = r;
+    }
+    if (nlon > 0)
+        p->lon = lon;
+    p->nlat = nlat;
+    p->nlon = nlon;
+    p->npoint = type == CHARM_CRD_POINT_SCATTERED ? nlat
+                                                  : (is_grid_type(type)
+                                                         ? nlat * nlon
+                                                         : 0);
+    p->type = type;
+    p->owner = 0;
+    p->distributed = 0;
+    return p;
+}
+
+static charm_point *point_alloc(int type, size_t nlat, size_t nlon, bool zero)
+{
+    if (!is_point_type(type))
+        return NULL;
+    if (type == CHARM_CRD_POINT_SCATTERED && nlat != nlon)
+        return NULL;
+    double *lat = NULL, *lon = NULL, *r = NULL, *w = NULL;
+    auto al = [&](size_t n) -> double * {
+        return zero ? (double *)calloc(n, sizeof(double))
+                    : (double *)malloc(n * sizeof(double));
+    };
+    charm_point *p = NULL;
+    if (nlat > 0)
+    {
+        lat = al(nlat);
+        r = al(nlat);
+        if (!lat || !r)
+            goto FAIL;
+    }
+    if (nlon > 0)
+    {
+        lon = al(nlon);
+        if (!lon)
+            goto FAIL;
+    }
+    p = charm_crd_point_init(type, nlat, nlon, lat, lon, r);
+    if (!p)
+        goto FAIL;
+    if (is_quad_type(type))
+    {
+        w = al(nlat > 0 ? nlat : 1);
+        if (!w)
+            goto FAIL;
+        p->w = w;
+    }
+    p->owner = 1;
+    return p;
+FAIL:
+    free(lat);
+    free(lon);
+    free(r);
+    free(w);
+    free(p);
+    return NULL;
+}
+
+charm_point *charm_crd_point_malloc(int type, size_t nlat, size_t nlon)
+{
+    return point_alloc(type, nlat, nlon, false);
+}
+
+charm_point *charm_crd_point_calloc(int type, size_t nlat, size_t nlon)
+{
+    return point_alloc(type, nlat, nlon, true);
+}
+
+void charm_crd_point_free(charm_point *pnt)
+{
+    if (!pnt)
+        return;
+    if (pnt->owner)
+    {
+        free(pnt->lat);
+        free(pnt->lon);
+        free(pnt->r);
+        free(pnt->w);
+    }
+    free(pnt);
+}
+
+// src/crd/crd_point_gl_shape.c, crd_point_dh1_shape.c, crd_point_dh2_shape.c
+void charm_crd_point_gl_shape(unsigned long nmax, size_t *nlat, size_t *nlon)
+{
+    *nlat = nmax + 1;
+    *nlon = 2 * (nmax + 1);
+}
+
+void charm_crd_point_dh1_shape(unsigned long nmax, size_t *nlat, size_t *nlon)
+{
+    *nlat = 2 * (nmax + 1);
+    *nlon = 2 * (nmax + 1);
+}
+
+void charm_crd_point_dh2_shape(unsigned long nmax, size_t *nlat, size_t *nlon)
+{
+    *nlat = 2 * (nmax + 1);
+    *nlon = 4 * (nmax + 1);
+}
+
+// src/crd/crd_point_quad.c, crd_point_gl_chunk.c, crd_point_dh_chunk.c:
+// NULL on any error (CHarm does not propagate the error object here).
+static charm_point *quad_grid(int type, unsigned long nmax, double r)
+{
+    if (r <= 0.0)
+        return NULL;
+    size_t nlat, nlon;
+    if (type == CHARM_CRD_POINT_GRID_GL)
+        charm_crd_point_gl_shape(nmax, &nlat, &nlon);
+    else if (type == CHARM_CRD_POINT_GRID_DH1)
+        charm_crd_point_dh1_shape(nmax, &nlat, &nlon);
+    else
+        charm_crd_point_dh2_shape(nmax, &nlat, &nlon);
+    charm_point *p = charm_crd_point_calloc(type, nlat, nlon);
+    if (!p)
+        return NULL;
+    cb::Status st = cb::quad_nodes(type, nmax, p->lat, p->w);
+    if (!st.ok())
+    {
+        charm_crd_point_free(p);
+        return NULL;
+    }
+    for (size_t i = 0; i < nlat; i++)
+        p->r[i] = r;
+    const double PI = 3.14159265358979323846;
+    double c = (type == CHARM_CRD_POINT_GRID_DH2) ? PI / (double)(2 * (nmax + 1))
+                                                  : PI / (double)(nmax + 1);
+    for (size_t j = 0; j < nlon; j++)
+        p->lon[j] = c * (double)j;
+    return p;
+}
+
+charm_point *charm_crd_point_gl(unsigned long nmax, double r)
+{
+    return quad_grid(CHARM_CRD_POINT_GRID_GL, nmax, r);
+}
+
+charm_point *charm_crd_point_dh1(unsigned long nmax, double r)
+{
+    return quad_grid(CHARM_CRD_POINT_GRID_DH1, nmax, r);
+}
+
+charm_point *charm_crd_point_dh2(unsigned long nmax, double r)
+{
+    return quad_grid(CHARM_CRD_POINT_GRID_DH2, nmax, r);
+}
+
+// ---------------------------------------------------------------------------
+// Coefficients, src/shc/shc_alloc.c, shc_init.c, shc_init_chunk.c,
+// shc_free.c
+// ---------------------------------------------------------------------------
+charm_shc *charm_shc_init(unsigned long nmax, double mu, double r, double *c,
+                          double *s)
+{
+    if (r <= 0.0)
+        return NULL;
+    charm_shc *h = (charm_shc *)malloc(sizeof(charm_shc));
+    if (!h)
+        return NULL;
+    h->nmax = nmax;
+    h->mu = mu;
+    h->r = r;
+    size_t nmax1 = (size_t)nmax + 1;
+    size_t len = ((nmax1 + 1) * nmax1) / 2;
+    h->nc = h->ns = len;
+    h->owner = 0;
+    h->distributed = 0;
+    h->c = (double **)malloc(nmax1 * sizeof(double *));
+    h->s = (double **)malloc(nmax1 * sizeof(double *));
+    if (!h->c || !h->s)
+    {
+        free(h->c);
+        free(h->s);
+        free(h);
+        return NULL;
+    }
+    size_t idx = 0;
+    for (size_t m = 0; m <= nmax; m++)
+    {
+        h->c[m] = c + idx;
+        h->s[m] = s + idx;
+        idx += nmax1 - m;
+    }
+    return h;
+}
+
+static charm_shc *shc_alloc(unsigned long nmax, double mu, double r, bool zero)
+{
+    size_t nmax1 = (size_t)nmax + 1;
+    size_t len = ((nmax1 + 1) * nmax1) / 2;
+    double *c = zero ? (double *)calloc(len, sizeof(double))
+                     : (double *)malloc(len * sizeof(double));
+    double *s = zero ? (double *)calloc(len, sizeof(double))
+                     : (double *)malloc(len * sizeof(double));
+    charm_shc *h = NULL;
+    if (!c || !s)
+        goto FAIL;
+    h = charm_shc_init(nmax, mu, r, c, s);
+    if (!h)
+        goto FAIL;
+    h->owner = 1;
+    return h;
+FAIL:
+    free(c);
+    free(s);
+    return NULL;
+}
+
+charm_shc *charm_shc_malloc(unsigned long nmax, double mu, double r)
+{
+    return shc_alloc(nmax, mu, r, false);
+}
+
+charm_shc *charm_shc_calloc(unsigned long nmax, double mu, double r)
+{
+    return shc_alloc(nmax, mu, r, true);
+}
+
+void charm_shc_free(charm_shc *shcs)
+{
+    if (!shcs)
+        return;
+    if (shcs->owner && shcs->c && shcs->s)
+    {
+        free(shcs->c[0]);
+        free(shcs->s[0]);
+    }
+    free(shcs->c);
+    free(shcs->s);
+    free(shcs);
+}
+
+// ---------------------------------------------------------------------------
+// Synthesis, src/shs/shs_point.c:26-129, shs_point_gradn.c:32-165,
+// shs_point_guru.c:21-119
+// ---------------------------------------------------------------------------
+static void report(charm_err *err, const char *func, const cb::Status &st)
+{
+    if (!st.ok())
+        err_set(err, __FILE__, __LINE__, func, st.code, st.msg.c_str());
+}
+
+static bool check_nmax(const charm_shc *shcs, unsigned long nmax,
+                       charm_err *err, const char *what)
+{
+    if (nmax > shcs->nmax)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg,
+                 "Maximum harmonic degree of the %s \"nmax = %lu\" cannot be "
+                 "larger than maximum harmonic degree of spherical harmonic "
+                 "coefficients \"shcs->nmax = %lu\".",
+                 what, nmax, shcs->nmax);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return false;
+    }
+    return true;
+}
+
+static bool check_type_shs(const charm_point *pnt, charm_err *err)
+{
+    if (pnt->type != CHARM_CRD_POINT_SCATTERED && !is_grid_type(pnt->type))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic synthesis "
+                "of point values.");
+        return false;
+    }
+    if (pnt->type == CHARM_CRD_POINT_SCATTERED && pnt->nlat != pnt->nlon)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The number of latitudes and longitudes in the \"pnt\" "
+                "structure must be the same to perform point-wise spherical "
+                "harmonic synthesis.");
+        return false;
+    }
+    return true;
+}
+
+void charm_shs_point(const charm_point *pnt, const charm_shc *shcs,
+                     unsigned long nmax, double *f, charm_err *err)
+{
+    if (!check_nmax(shcs, nmax, err, "synthesis"))
+        return;
+    if (!check_type_shs(pnt, err))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    double *fp[1] = {f};
+    report(err, __func__, cb::shs_point(pnt, shcs, nmax, 0, 0, 0, 0, fp));
+}
+
+void charm_shs_point_grad1(const charm_point *pnt, const charm_shc *shcs,
+                           unsigned long nmax, double **f, charm_err *err)
+{
+    if (!check_nmax(shcs, nmax, err, "synthesis"))
+        return;
+    if (!check_type_shs(pnt, err))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    cb::Status st = cb::shs_point(pnt, shcs, nmax, 1, 1, 1, 1, f);
+    report(err, __func__, st);
+    if (!st.ok())
+        return;
+    // src/shs/shs_point_gradn.c:133-145: f holds l, r, p; reorder to x, y, z
+    double *fx = f[2], *fy = f[0], *fz = f[1];
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = fz;
+}
+
+void charm_shs_point_grad2(const charm_point *pnt, const charm_shc *shcs,
+                           unsigned long nmax, double **f, charm_err *err)
+{
+    if (!check_nmax(shcs, nmax, err, "synthesis"))
+        return;
+    if (!check_type_shs(pnt, err))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    cb::Status st = cb::shs_point(pnt, shcs, nmax, 2, 2, 2, 2, f);
+    report(err, __func__, st);
+    if (!st.ok())
+        return;
+    // src/shs/shs_point_gradn.c:146-165: ll lr lp rr rp pp -> xx xy xz yy yz zz
+    double *fxx = f[5], *fxy = f[2], *fxz = f[4];
+    double *fyy = f[0], *fyz = f[1], *fzz = f[3];
+    f[0] = fxx;
+    f[1] = fxy;
+    f[2] = fxz;
+    f[3] = fyy;
+    f[4] = fyz;
+    f[5] = fzz;
+}
+
+void charm_shs_point_guru(const charm_point *pnt, const charm_shc *shcs,
+                          unsigned long nmax, unsigned dr, unsigned dlat,
+                          unsigned dlon, double *f, charm_err *err)
+{
+    if (!check_nmax(shcs, nmax, err, "synthesis"))
+        return;
+    // src/shs/shs_check_single_derivative.c
+    if ((int)dr < 0 || (int)dlat < 0 || (int)dlon < 0 || dr + dlat + dlon > 2)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg,
+                 "The sum \"dr + dlat + dlon\" is \"%d\", but it cannot be "
+                 "larger than \"%d\".",
+                 (int)(dr + dlat + dlon), 2);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (pnt->npoint == 0)
+        return;
+    if (!check_type_shs(pnt, err))
+        return;
+    double *fp[1] = {f};
+    report(err, __func__,
+           cb::shs_point(pnt, shcs, nmax, 0, (int)dr, (int)dlat, (int)dlon, fp));
+}
+
+// ---------------------------------------------------------------------------
+// Analysis, src/sha/sha_point.c:124-206
+// ---------------------------------------------------------------------------
+void charm_sha_point(const charm_point *pnt, const double *f,
+                     unsigned long nmax, charm_shc *shcs, charm_err *err)
+{
+    if (!check_nmax(shcs, nmax, err, "analysis"))
+        return;
+    if (!is_quad_type(pnt->type))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic analysis of "
+                "point data values.");
+        return;
+    }
+    const double r0 = pnt->r[0];
+    for (size_t i = 1; i < pnt->nlat; i++)
+    {
+        if (!nearly_equal(pnt->r[i], r0, charm_glob_threshold))
+        {
+            SET_ERR(err, CHARM_EFUNCARG,
+                    "All spherical radii in \"pnt->r\" must be equal.");
+            return;
+        }
+    }
+    unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                 ? (unsigned long)pnt->nlat - 1
+                                 : ((unsigned long)pnt->nlat - 2) / 2;
+    if (nmax > nmax_grd)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The input data grid \"pnt\" was created for a maximum degree "
+                "that is not high enough to recover harmonics up to the "
+                "specified maximum degree of the analysis.");
+        return;
+    }
+    report(err, __func__, cb::sha_point(pnt, f, nmax, shcs));
+}
+
+} // extern "C"

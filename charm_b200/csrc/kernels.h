@@ -1,0 +1,115 @@
+// Kernel argument blocks and launchers of charm_b200 (host <-> device
+// boundary inside the library; no torch types anywhere).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace cb
+{
+
+// Grid synthesis: lumped coefficients out[q][row][m] of every output
+// component q, row and order m (see shs_grid.cu).
+struct ShsGridArgs
+{
+    long long nmax;
+    int npairs;            // evaluated latitudes (north rows of the pairs)
+    int ntiles;            // latitude tiles per order
+    long long nitems;      // (nmax + 1) * ntiles
+    const double2 *ab;     // (a_nm, b_nm), order-major triangle
+    const double2 *cs;     // (C_nm, S_nm)
+    const double2 *en;     // (e_nm, n), derivatives only
+    const double *psx;     // sectorial seeds [m][pair] mantissa
+    const int *pse;        // sectorial seeds [m][pair] binary exponent
+    const double *t;       // sin(lat) per pair
+    const double *u;       // cos(lat) per pair
+    const double *rho;     // R / r per pair (r != R only)
+    const int *row_n;      // row index of the pair's latitude
+    const int *row_s;      // row index of its mirror, or -1
+    int nlat;              // rows of the output
+    int ldf;               // leading dimension of the output rows (double2)
+    double2 *out;          // [npar][nlat][ldf]
+    double mur;            // GM / R^(dorder + 1)
+    int fft_pack;          // 1: FFTW c2r packing (c a, -c b), c = 1/2 for m > 0
+    int dlon;              // longitudinal derivative order (single quantity)
+    double polar_thr;      // polar optimisation threshold, < 0 when off
+    unsigned long long *counter;
+    unsigned *status;
+};
+
+// Grid analysis: C_nm, S_nm partial sums per latitude group (sha_grid.cu).
+struct ShaGridArgs
+{
+    long long nmax;
+    int npairs;
+    int ntiles;            // latitude tiles per order
+    int ngroups;           // tile groups per order (partial sums)
+    int tiles_per_group;
+    long long nitems;      // (nmax + 1) * ngroups
+    const double2 *ab;
+    const double *psx;
+    const int *pse;
+    const double *t;
+    const double *u;
+    const int *row_n;
+    const int *row_s;
+    const double *cw_n;    // quadrature weight times constant, north row
+    const double *cw_s;    // same for the mirror row (0 when none)
+    const double2 *F;      // r2c output [nlat][ldF]
+    int ldF;
+    double2 *part;         // [ngroups][T] (C, S) partial sums
+    double polar_thr;
+    unsigned long long *counter;
+    unsigned *status;
+};
+
+// Scattered-point synthesis (sctr.cu).
+struct SctrArgs
+{
+    long long nmax;
+    long long npoint;
+    long long ntiles;
+    const double2 *ab;
+    const double2 *cs;
+    const double2 *en;
+    const double *dm;
+    const double *lat;
+    const double *lon;
+    const double *r;       // radius per point (read when r != R)
+    double R;              // reference radius of the coefficients
+    double *f;             // [npar][npoint]
+    double mur;
+    int dlon;
+    double polar_thr;
+    unsigned long long *counter;
+    unsigned *status;
+};
+
+cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
+                          double2 *ab, double2 *en, cudaStream_t st);
+cudaError_t launch_interleave(long long nmax, long long shc_nmax,
+                              const double *c, const double *s, double2 *cs,
+                              cudaStream_t st);
+cudaError_t launch_sectorial(long long nmax, int np, const double *u,
+                             const double *rho, int use_rho, int dorder,
+                             const double *dm, double *psx, int *pse,
+                             cudaStream_t st);
+cudaError_t launch_shs_grid(const ShsGridArgs &A, int kgrad, int dr,
+                            int dlat, bool rr, int K, int grid,
+                            cudaStream_t st);
+cudaError_t launch_lon_direct(int npar, int nlat, int nlon, long long nmax,
+                              const double2 *lc, int ldf, const double *lon,
+                              double *f, cudaStream_t st);
+cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
+                            cudaStream_t st);
+cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
+                              long long T, const double2 *part,
+                              const double *rescale, double *c, double *s,
+                              cudaStream_t st);
+cudaError_t launch_gl_nodes(unsigned long nmax, double *lat, double *w,
+                            unsigned *status, cudaStream_t st);
+cudaError_t launch_dh_nodes(unsigned long nmax, double *lat, double *w,
+                            cudaStream_t st);
+cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
+                        bool rr, int K, int grid, cudaStream_t st);
+
+} // namespace cb

@@ -1,0 +1,346 @@
+// Analysis on quadrature grids: the per-order Legendre contraction of
+// CHarm's sha_point (src/sha/sha_point.c:713-980), after the r2c transform of
+// the grid rows.
+//
+// Work item = (order m, group g of latitude tiles); one warp per item.  For
+// each tile of 32*K latitude pairs the warp runs the recurrence over n and
+// forms, per degree, the lane partial sum over its K pairs of
+// P_nm(t) * {a, b}^(n+m parity).  Every 32 degrees the warp transpose-reduce
+// leaves lane l with the warp total of degree n0 + l, which is added to the
+// group's partial column (plain read-modify-write: the warp owns it).  A
+// second kernel sums the groups in a fixed order, so results are
+// deterministic.
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "leg.cuh"
+
+namespace cb
+{
+
+namespace
+{
+
+struct PairA
+{
+    double ae, ao, be, bo;
+};
+
+__device__ __forceinline__ PairA load_pair_A(const ShaGridArgs &A, int p,
+                                             long long m)
+{
+    PairA r{0.0, 0.0, 0.0, 0.0};
+    if (p >= A.npairs)
+        return r;
+    int rn = A.row_n[p], rs = A.row_s[p];
+    double2 Fn = A.F[(size_t)rn * A.ldF + m];
+    double a = A.cw_n[p] * Fn.x;
+    double b = -A.cw_n[p] * Fn.y;
+    double a2 = 0.0, b2 = 0.0;
+    if (rs >= 0)
+    {
+        double2 Fs = A.F[(size_t)rs * A.ldF + m];
+        a2 = A.cw_s[p] * Fs.x;
+        b2 = -A.cw_s[p] * Fs.y;
+    }
+    // sha_point.c:740-747 (symm = 1 when a mirror row exists)
+    r.ae = a + a2;
+    r.ao = a - a2;
+    r.be = b + b2;
+    r.bo = b - b2;
+    return r;
+}
+
+} // namespace
+
+template <int K>
+__global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned warp = threadIdx.x >> 5;
+    const size_t stage_bytes = LEG_CHUNK * sizeof(double2);
+    unsigned char *wbase =
+        smem_raw + (size_t)warp * (2 * stage_bytes + 2 * sizeof(uint64_t));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + 2 * stage_bytes);
+    double2 *stg[2] = {reinterpret_cast<double2 *>(wbase),
+                       reinterpret_cast<double2 *>(wbase + stage_bytes)};
+    if (lane == 0)
+    {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    unsigned phase[2] = {0u, 0u};
+    const long long N = A.nmax;
+    const int np = A.npairs;
+    bool failed = false;
+
+    for (;;)
+    {
+        unsigned long long item = 0;
+        if (lane == 0)
+            item = atomicAdd(A.counter, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= (unsigned long long)A.nitems)
+            break;
+        const long long m = (long long)(item / (unsigned long long)A.ngroups);
+        const int g = (int)(item % (unsigned long long)A.ngroups);
+        const long long c0 = tri_col0(N, m);
+        const long long ncol = N - m + 1;
+        const int nchunks = (int)((ncol + LEG_CHUNK - 1) / LEG_CHUNK);
+        double2 *col = A.part + (size_t)g * (size_t)tri_size(N) + c0;
+        const int tile0 = g * A.tiles_per_group;
+        int tile1 = tile0 + A.tiles_per_group;
+        if (tile1 > A.ntiles)
+            tile1 = A.ntiles;
+        bool stored = false;
+
+        for (int tile = tile0; tile < tile1 && !failed; tile++)
+        {
+            double t[K], x[K], y[K];
+            int E[K];
+            PairA pa[K];
+            bool skip = A.polar_thr >= 0.0;
+#pragma unroll
+            for (int k = 0; k < K; k++)
+            {
+                int p = tile * (32 * K) + k * 32 + (int)lane;
+                bool valid = p < np;
+                t[k] = valid ? A.t[p] : 0.0;
+                double u = valid ? A.u[p] : 1.0;
+                x[k] = valid ? A.psx[(size_t)m * np + p] : 0.0;
+                E[k] = valid ? A.pse[(size_t)m * np + p] : 0;
+                y[k] = 0.0;
+                if (valid && !((double)m - (double)N * u > A.polar_thr))
+                    skip = false;
+                leg_seed_normalise(x[k], E[k]);
+                // scaled latitudes contribute nothing until they switch
+                pa[k] = (E[k] == 0) ? load_pair_A(A, p, m)
+                                    : PairA{0.0, 0.0, 0.0, 0.0};
+            }
+            if (__all_sync(0xffffffffu, skip))
+                continue;
+            bool any_scaled = false;
+#pragma unroll
+            for (int k = 0; k < K; k++)
+                any_scaled |= (E[k] != 0);
+            any_scaled = __any_sync(0xffffffffu, any_scaled);
+
+            auto issue = [&](int j, int s) {
+                if (lane == 0)
+                {
+                    long long cnt = ncol - (long long)j * LEG_CHUNK;
+                    if (cnt > LEG_CHUNK)
+                        cnt = LEG_CHUNK;
+                    unsigned bytes = (unsigned)(cnt * sizeof(double2));
+                    mbar_arrive_expect_tx(&bar[s], bytes);
+                    bulk_g2s(stg[s], A.ab + c0 + (long long)j * LEG_CHUNK,
+                             bytes, &bar[s]);
+                }
+            };
+            issue(0, 0);
+            if (nchunks > 1)
+                issue(1, 1);
+
+            for (int j = 0; j < nchunks; j++)
+            {
+                const int s = j & 1;
+                if (!mbar_wait_bounded(&bar[s], phase[s], A.status))
+                {
+                    failed = true;
+                    break;
+                }
+                phase[s] ^= 1u;
+                long long cntl = ncol - (long long)j * LEG_CHUNK;
+                const int cnt = cntl > LEG_CHUNK ? LEG_CHUNK : (int)cntl;
+                double2 *sab = stg[s];
+                // degrees beyond nmax read zero coefficients
+                if (cnt < LEG_CHUNK)
+                {
+                    if ((int)lane >= cnt)
+                        sab[lane] = make_double2(0.0, 0.0);
+                    if ((int)lane + 32 >= cnt)
+                        sab[lane + 32] = make_double2(0.0, 0.0);
+                    __syncwarp();
+                }
+#pragma unroll 1
+                for (int half = 0; half < 2; half++)
+                {
+                    const long long n0 = m + (long long)j * LEG_CHUNK + 32 * half;
+                    if (n0 > N)
+                        break;
+                    const double2 *blk = sab + 32 * half;
+                    const bool first = (j == 0 && half == 0);
+                    double pc[5], ps[5];
+                    double outc = 0.0, outs = 0.0;
+#pragma unroll
+                    for (int jj = 0; jj < 32; jj++)
+                    {
+                        double vc = 0.0, vs = 0.0;
+                        if (first && jj == 0)
+                        {
+#pragma unroll
+                            for (int k = 0; k < K; k++)
+                            {
+                                vc = fma(x[k], pa[k].ae, vc);
+                                vs = fma(x[k], pa[k].be, vs);
+                            }
+                        }
+                        else
+                        {
+                            double2 ab = blk[jj];
+#pragma unroll
+                            for (int k = 0; k < K; k++)
+                            {
+                                double z = fma(ab.x * t[k], x[k], -(ab.y * y[k]));
+                                y[k] = x[k];
+                                x[k] = z;
+                                if ((jj & 1) == 0)
+                                {
+                                    vc = fma(z, pa[k].ae, vc);
+                                    vs = fma(z, pa[k].be, vs);
+                                }
+                                else
+                                {
+                                    vc = fma(z, pa[k].ao, vc);
+                                    vs = fma(z, pa[k].bo, vs);
+                                }
+                            }
+                        }
+                        // streaming transpose-reduce (static levels)
+                        double wc = vc, ws = vs;
+                        bool done = false;
+#pragma unroll
+                        for (int L = 0; L < 5; L++)
+                        {
+                            if (done)
+                                break;
+                            if (((jj >> L) & 1) == 0)
+                            {
+                                pc[L] = wc;
+                                ps[L] = ws;
+                                done = true;
+                            }
+                            else
+                            {
+                                wc = tr_combine(pc[L], wc, 1 << L, lane);
+                                ws = tr_combine(ps[L], ws, 1 << L, lane);
+                                if (L == 4)
+                                {
+                                    outc = wc;
+                                    outs = ws;
+                                }
+                            }
+                        }
+                        if ((jj & 15) == 15 && any_scaled)
+                        {
+                            bool still = false;
+#pragma unroll
+                            for (int k = 0; k < K; k++)
+                            {
+                                if (leg_fixup(x[k], y[k], E[k]))
+                                {
+                                    int p = tile * (32 * K) + k * 32 + (int)lane;
+                                    pa[k] = load_pair_A(A, p, m);
+                                }
+                                still |= (E[k] != 0);
+                            }
+                            any_scaled = __any_sync(0xffffffffu, still);
+                        }
+                    }
+                    const long long n = n0 + lane;
+                    if (n <= N)
+                    {
+                        double2 *dst = col + (n - m);
+                        if (stored)
+                        {
+                            double2 o = *dst;
+                            *dst = make_double2(o.x + outc, o.y + outs);
+                        }
+                        else
+                            *dst = make_double2(outc, outs);
+                    }
+                }
+                __syncwarp();
+                if (j + 2 < nchunks)
+                {
+                    fence_proxy_async_smem();
+                    issue(j + 2, s);
+                }
+            }
+            stored = true;
+        }
+        if (failed)
+            break;
+        if (!stored)
+        {
+            for (long long n = m + lane; n <= N; n += 32)
+                col[n - m] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+// Sums the group partials and writes C, S in the caller's layout (degree
+// shc_nmax triangle), zero above nmax, with the degree-wise rescaling of
+// src/shc/shc_rescale.c applied (rescale[n], or none when null).
+__global__ void k_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
+                             long long T, const double2 *__restrict__ part,
+                             const double *__restrict__ rescale, double *c,
+                             double *s)
+{
+    long long m = blockIdx.x;
+    if (m > shc_nmax)
+        return;
+    long long d0 = tri_col0(shc_nmax, m);
+    long long c0 = tri_col0(nmax, m);
+    for (long long n = m + threadIdx.x; n <= shc_nmax; n += blockDim.x)
+    {
+        double vc = 0.0, vs = 0.0;
+        if (m <= nmax && n <= nmax)
+        {
+            for (int g = 0; g < ngroups; g++)
+            {
+                double2 v = part[(size_t)g * T + c0 + n - m];
+                vc += v.x;
+                vs += v.y;
+            }
+            if (rescale)
+            {
+                vc *= rescale[n];
+                vs *= rescale[n];
+            }
+        }
+        c[d0 + n - m] = vc;
+        s[d0 + n - m] = vs;
+    }
+}
+
+cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
+                            cudaStream_t st)
+{
+    const int warps = 4;
+    size_t smem = (size_t)warps *
+                  (2 * LEG_CHUNK * sizeof(double2) + 2 * sizeof(uint64_t));
+    if (K == 4)
+        k_sha_grid<4><<<grid, warps * 32, smem, st>>>(A);
+    else if (K == 2)
+        k_sha_grid<2><<<grid, warps * 32, smem, st>>>(A);
+    else
+        k_sha_grid<1><<<grid, warps * 32, smem, st>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
+                              long long T, const double2 *part,
+                              const double *rescale, double *c, double *s,
+                              cudaStream_t st)
+{
+    k_sha_reduce<<<(int)(shc_nmax + 1), 128, 0, st>>>(nmax, shc_nmax, ngroups,
+                                                       T, part, rescale, c, s);
+    return cudaGetLastError();
+}
+
+} // namespace cb

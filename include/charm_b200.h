@@ -1,0 +1,213 @@
+/* charm_b200.h -- C interface of the B200 (sm_100a) implementation of CHarm's
+ * point spherical-harmonic synthesis and analysis.
+ *
+ * This header mirrors, symbol for symbol, the part of CHarm 0.4.9's public C
+ * API that the point-synthesis/analysis path needs, with the same struct
+ * layouts (non-MPI build), enum values, argument meaning and error
+ * behaviour, so that C code and PyHarm's ctypes bindings written against
+ * CHarm link against libcharm.so from this project unchanged.  Each
+ * declaration cites the CHarm header line it replaces.  All arrays are host
+ * memory owned by the caller; the library stages them to the GPU internally.
+ *
+ * Threading: calls are serialised on one CUDA stream per process and device;
+ * concurrent calls from several host threads must use distinct charm_err
+ * objects and are executed one after another.
+ */
+#ifndef CHARM_B200_H
+#define CHARM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+/* C's _Bool and C++'s bool share size and representation on the supported
+ * platforms, so the struct layouts are identical in both languages. */
+#   ifndef _Bool
+#       define _Bool bool
+#   endif
+extern "C"
+{
+#endif
+
+#ifndef CHARM_EXTERN
+#   define CHARM_EXTERN __attribute__((visibility("default")))
+#endif
+#ifndef CHARM_CDECL
+#   define CHARM_CDECL
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Errors: src/err/err.h.in:80-130 (enum), :159-222 (struct)                  */
+/* ------------------------------------------------------------------------- */
+enum
+{
+    CHARM_FAILURE = -1,
+    CHARM_SUCCESS,
+    CHARM_EMEM,
+    CHARM_EFUNCARG,
+    CHARM_EFILEIO,
+    CHARM_EFFTWINIT,
+    CHARM_EMPIPROCESS
+};
+
+#define CHARM_ERR_MAX_FILE 4096U    /* err.h.in:58 */
+#define CHARM_ERR_MAX_FUNC 256U     /* err.h.in:65 */
+#define CHARM_ERR_MAX_MSG 4096U     /* err.h.in:71 */
+#define CHARM_ERR_MAX_LEVEL 10U     /* err.h.in:77 */
+#define CHARM_ERR_MALLOC_FAILURE "Memory allocation failure."  /* :137 */
+
+typedef struct
+{
+    size_t level;
+    char **file;
+    size_t *line;
+    char **func;
+    int code;
+    char *msg;
+    _Bool saturated;
+    _Bool distributed;
+} charm_err;
+
+/* err.h.in:236-294 */
+CHARM_EXTERN charm_err * CHARM_CDECL charm_err_init(void);
+CHARM_EXTERN void CHARM_CDECL charm_err_free(charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_err_reset(charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_err_handler(charm_err *err,
+                                                 _Bool terminate);
+CHARM_EXTERN _Bool CHARM_CDECL charm_err_isempty(const charm_err *err);
+
+/* ------------------------------------------------------------------------- */
+/* Points: src/crd/crd.h.in:70-90 (enum), :125-332 (struct)                   */
+/* ------------------------------------------------------------------------- */
+enum
+{
+    CHARM_CRD_CELL_GRID = -2,
+    CHARM_CRD_CELL_SCATTERED,
+    CHARM_CRD_POINT_SCATTERED = 1,
+    CHARM_CRD_POINT_GRID,
+    CHARM_CRD_POINT_GRID_GL,
+    CHARM_CRD_POINT_GRID_DH1,
+    CHARM_CRD_POINT_GRID_DH2
+};
+
+typedef struct
+{
+    int type;
+    size_t nlat;
+    size_t nlon;
+    size_t npoint;
+    double *lat;
+    double *lon;
+    double *r;
+    double *w;
+    _Bool owner;
+    _Bool distributed;
+} charm_point;
+
+/* crd.h.in:477-564 */
+CHARM_EXTERN charm_point * CHARM_CDECL charm_crd_point_malloc(int type,
+                                                              size_t nlat,
+                                                              size_t nlon);
+CHARM_EXTERN charm_point * CHARM_CDECL charm_crd_point_calloc(int type,
+                                                              size_t nlat,
+                                                              size_t nlon);
+CHARM_EXTERN charm_point * CHARM_CDECL charm_crd_point_init(int type,
+                                                            size_t nlat,
+                                                            size_t nlon,
+                                                            double *lat,
+                                                            double *lon,
+                                                            double *r);
+CHARM_EXTERN void CHARM_CDECL charm_crd_point_free(charm_point *pnt);
+/* crd.h.in:615-686: quadrature grids (nodes and weights computed on the
+ * GPU) */
+CHARM_EXTERN charm_point * CHARM_CDECL charm_crd_point_gl(unsigned long nmax,
+                                                          double r);
+CHARM_EXTERN charm_point * CHARM_CDECL charm_crd_point_dh1(unsigned long nmax,
+                                                           double r);
+CHARM_EXTERN charm_point * CHARM_CDECL charm_crd_point_dh2(unsigned long nmax,
+                                                           double r);
+/* crd.h.in:700-760: shapes of the quadrature grids */
+CHARM_EXTERN void CHARM_CDECL charm_crd_point_gl_shape(unsigned long nmax,
+                                                       size_t *nlat,
+                                                       size_t *nlon);
+CHARM_EXTERN void CHARM_CDECL charm_crd_point_dh1_shape(unsigned long nmax,
+                                                        size_t *nlat,
+                                                        size_t *nlon);
+CHARM_EXTERN void CHARM_CDECL charm_crd_point_dh2_shape(unsigned long nmax,
+                                                        size_t *nlat,
+                                                        size_t *nlon);
+
+/* ------------------------------------------------------------------------- */
+/* Spherical harmonic coefficients: src/shc/shc.h.in:139-381 (struct)         */
+/* ------------------------------------------------------------------------- */
+typedef struct
+{
+    unsigned long nmax;
+    double mu;
+    double r;
+    size_t nc;
+    size_t ns;
+    double **c;
+    double **s;
+    _Bool owner;
+    _Bool distributed;
+} charm_shc;
+
+/* shc.h.in:423-602 */
+CHARM_EXTERN charm_shc * CHARM_CDECL charm_shc_malloc(unsigned long nmax,
+                                                      double mu, double r);
+CHARM_EXTERN charm_shc * CHARM_CDECL charm_shc_calloc(unsigned long nmax,
+                                                      double mu, double r);
+CHARM_EXTERN charm_shc * CHARM_CDECL charm_shc_init(unsigned long nmax,
+                                                    double mu, double r,
+                                                    double *c, double *s);
+CHARM_EXTERN void CHARM_CDECL charm_shc_free(charm_shc *shcs);
+
+/* ------------------------------------------------------------------------- */
+/* Synthesis: src/shs/shs.h.in:168-173, :239-244, :344-349, :428-435          */
+/* ------------------------------------------------------------------------- */
+CHARM_EXTERN void CHARM_CDECL charm_shs_point(const charm_point *pnt,
+                                              const charm_shc *shcs,
+                                              unsigned long nmax,
+                                              double *f,
+                                              charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_shs_point_grad1(const charm_point *pnt,
+                                                    const charm_shc *shcs,
+                                                    unsigned long nmax,
+                                                    double **f,
+                                                    charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_shs_point_grad2(const charm_point *pnt,
+                                                    const charm_shc *shcs,
+                                                    unsigned long nmax,
+                                                    double **f,
+                                                    charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_shs_point_guru(const charm_point *pnt,
+                                                   const charm_shc *shcs,
+                                                   unsigned long nmax,
+                                                   unsigned dr,
+                                                   unsigned dlat,
+                                                   unsigned dlon,
+                                                   double *f,
+                                                   charm_err *err);
+
+/* ------------------------------------------------------------------------- */
+/* Analysis: src/sha/sha.h.in:164-169                                         */
+/* ------------------------------------------------------------------------- */
+CHARM_EXTERN void CHARM_CDECL charm_sha_point(const charm_point *pnt,
+                                              const double *f,
+                                              unsigned long nmax,
+                                              charm_shc *shcs,
+                                              charm_err *err);
+
+/* ------------------------------------------------------------------------- */
+/* Runtime globals: src/glob/glob.h.in:66-241 (values glob.c:16-23)            */
+/* ------------------------------------------------------------------------- */
+CHARM_EXTERN extern double charm_glob_threshold;
+CHARM_EXTERN extern double charm_glob_threshold2;
+CHARM_EXTERN extern unsigned long charm_glob_polar_optimization_a1;
+CHARM_EXTERN extern double charm_glob_polar_optimization_a2;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
