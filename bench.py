@@ -1,0 +1,433 @@
+"""Benchmark: FP64 spherical-harmonic synthesis + analysis round trip on a
+Gauss--Legendre grid (CHarm's charm_shs_point + charm_sha_point), nmax 2190,
+grid 2191 x 4382, Kaula-decay coefficients (seed 2000), r = R.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--nmax N]
+                    [--impl ours|reference]
+
+One step = one SHS + SHA round trip.  "value" is seconds per round trip with
+the coefficients and the grid resident in HBM (device-timed with CUDA
+events on the library's stream, L2 flushed between steps by a 256 MiB
+write); "e2e" is the same round trip through the C ABI with pinned host
+buffers, host<->device copies included.  With --gpus N > 1 (torchrun) every
+rank runs its own round trips (replicas, no collective on the data path);
+value = max-over-ranks time / (N * K).
+
+--impl reference times the CPU oracle (the restatement of CHarm's algorithm
+in oracle/, OpenMP on all host cores) on a bounded sample of latitude rows
+of the same workload, scaled to a full round trip.
+"""
+import argparse
+import ctypes as ct
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("SHS+SHA s at nmax 2190/10800: plain FP64 vs batched split-prec, "
+          "% FP64 peak")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--nmax", type=int, default=2190)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# Clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,"
+         "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    import charm_b200 as cb
+    from charm_b200._lib import _libcharm
+    from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula
+
+    L = _libcharm
+    L.charm_b200_shs_point_dev.argtypes = [
+        ct.c_void_p, ct.c_ulong, ct.c_double, ct.c_double, ct.c_void_p,
+        ct.c_void_p, ct.c_ulong, ct.c_int, ct.c_uint, ct.c_uint, ct.c_uint,
+        ct.c_void_p, ct.c_void_p]
+    L.charm_b200_sha_point_dev.argtypes = [
+        ct.c_void_p, ct.c_void_p, ct.c_ulong, ct.c_double, ct.c_double,
+        ct.c_ulong, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+    L.charm_b200_stream.restype = ct.c_void_p
+    L.charm_b200_timing.argtypes = [ct.c_int]
+    L.charm_b200_timing_read.argtypes = [
+        ct.POINTER(ct.c_double), ct.POINTER(ct.c_ulonglong), ct.c_int,
+        ct.POINTER(ct.c_ulonglong), ct.POINTER(ct.c_ulonglong)]
+    L.charm_b200_fp64_peak_tflops.restype = ct.c_double
+
+    N = args.nmax
+    c, s = kaula(N, 2000)
+    pnt = cb.PointGridGL(N, R_EARTH)
+    nlat, nlon = pnt.lat.size, pnt.lon.size
+    T = c.size
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_c = torch.from_numpy(c).to(dev)
+    d_s = torch.from_numpy(s).to(dev)
+    d_f = torch.empty(nlat * nlon, dtype=torch.float64, device=dev)
+    d_c2 = torch.empty(T, dtype=torch.float64, device=dev)
+    d_s2 = torch.empty(T, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    sptr = L.charm_b200_stream()
+    stream = torch.cuda.ExternalStream(sptr)
+    err = L.charm_err_init()
+
+    def check():
+        if not L.charm_err_isempty(err):
+            msg = ct.string_at(err.contents.msg).decode()
+            raise RuntimeError(msg)
+
+    def step_dev():
+        L.charm_b200_shs_point_dev(ct.cast(pnt._Point, ct.c_void_p), N, GM,
+                                   R_EARTH, d_c.data_ptr(), d_s.data_ptr(), N,
+                                   0, 0, 0, 0, d_f.data_ptr(),
+                                   ct.cast(err, ct.c_void_p))
+        check()
+        L.charm_b200_sha_point_dev(ct.cast(pnt._Point, ct.c_void_p),
+                                   d_f.data_ptr(), N, GM, R_EARTH, N,
+                                   d_c2.data_ptr(), d_s2.data_ptr(),
+                                   ct.cast(err, ct.c_void_p))
+        check()
+
+    # warm-up (plans, tables, buffers)
+    for _ in range(args.warmup):
+        step_dev()
+    torch.cuda.synchronize()
+    rt = coef_rel_rms(d_c2.cpu().numpy(), d_s2.cpu().numpy(), c, s)
+
+    peak = L.charm_b200_fp64_peak_tflops()
+
+    # ---- device-resident timed region --------------------------------
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    L.charm_b200_timing(1)
+    per_step = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)           # L2 flush, outside the step's events
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        step_dev()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        per_step.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    ms = (ct.c_double * 7)()
+    cnt = (ct.c_ulonglong * 7)()
+    kl = ct.c_ulonglong()
+    fe = ct.c_ulonglong()
+    L.charm_b200_timing_read(ms, cnt, 7, ct.byref(kl), ct.byref(fe))
+    L.charm_b200_timing(0)
+    clk = clocks.stop()
+    total_ms = float(sum(per_step))
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+
+    # ---- end to end through the C ABI with pinned host buffers -------
+    hc = torch.from_numpy(c).pin_memory()
+    hs = torch.from_numpy(s).pin_memory()
+    hf = torch.empty(nlat * nlon, dtype=torch.float64).pin_memory()
+    oc = torch.empty(T, dtype=torch.float64).pin_memory()
+    os_ = torch.empty(T, dtype=torch.float64).pin_memory()
+    P = ct.POINTER(ct.c_double)
+    shc_in = L.charm_shc_init(N, GM, R_EARTH, ct.cast(hc.data_ptr(), P),
+                              ct.cast(hs.data_ptr(), P))
+    shc_out = L.charm_shc_init(N, GM, R_EARTH, ct.cast(oc.data_ptr(), P),
+                               ct.cast(os_.data_ptr(), P))
+
+    def step_e2e():
+        L.charm_shs_point(pnt._Point, shc_in, N, ct.cast(hf.data_ptr(), P), err)
+        check()
+        L.charm_sha_point(pnt._Point, ct.cast(hf.data_ptr(), P), N, shc_out,
+                          err)
+        check()
+
+    for _ in range(max(1, args.warmup)):
+        step_e2e()
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    with torch.cuda.stream(stream):
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        step_e2e()
+    wall = time.perf_counter() - t0
+    with torch.cuda.stream(stream):
+        f1.record(stream)
+    f1.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    rt_e2e = coef_rel_rms(oc.numpy(), os_.numpy(), c, s)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel ------------------------------
+    P_pairs = (nlat + 1) // 2
+    units = T * P_pairs                 # (n, m, latitude pair) triples
+    flops_per_unit = 8.0                # 2 DMUL + 1 DFMA recurrence, 2 DFMA sums
+    shs_ms = ms[0] / max(cnt[0], 1)
+    sha_ms = ms[1] / max(cnt[1], 1)
+    dom = "shs_grid" if shs_ms >= sha_ms else "sha_grid"
+    dom_ms = max(shs_ms, sha_ms)
+    achieved = units * flops_per_unit / (dom_ms * 1e-3) / 1e12
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic_gl2190.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(dom)
+        except Exception:
+            traffic = None
+    step_s = total_ms / 1e3 / args.steps
+    value = total_ms / 1e3 / (args.steps * ws)
+    h2d = 16 * T + 8 * nlat * nlon
+    d2h = 8 * nlat * nlon + 16 * T
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_s * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (Kaula-decay coefficients, seed 2000)",
+        "config": {
+            "workload": "GL-grid SHS+SHA round trip, plain FP64",
+            "nmax": N, "grid": "%dx%d" % (nlat, nlon), "r": "R",
+            "GM": GM, "R": R_EARTH,
+            "l2": "flushed between steps (256 MiB write outside the timed "
+                  "events)",
+            "parallelism": "replicas" if ws > 1 else "single GPU",
+        },
+        "round_trip_rel_rms": rt,
+        "kernel_ms": {"shs_grid": shs_ms, "sha_grid": sha_ms,
+                      "fft_total_per_step": ms[3] / args.steps,
+                      "prep_total_per_step": ms[5] / args.steps},
+        "roofline": {
+            "bound": "fp64",
+            "kernel": dom,
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak if peak > 0 else None,
+            "peak_source": "measured live: FP64 FMA probe kernel "
+                           "(charm_b200_fp64_peak_tflops), this GPU",
+            "flops_per_unit": flops_per_unit,
+            "units_per_launch": units,
+            "traffic": traffic,
+        },
+        "e2e": {"value": e2e_ms / 1e3 / e2e_steps, "unit": "s",
+                "wall_s": wall / e2e_steps,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "round_trip_rel_rms": rt_e2e},
+        "gpu_launches": int(kl.value),
+        "fft_execs": int(fe.value),
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(N, c, s, sample_rows=None)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (reference arm and cpu_baseline leg)
+# ---------------------------------------------------------------------------
+def cpu_baseline(N, c, s, sample_rows=None):
+    """Times the CPU oracle on a sample of latitude pairs of the GL grid and
+    scales the Legendre part to the full grid; the FFTs run over all rows.
+    Returns the cpu_baseline object (seconds per round trip)."""
+    from oracle import orc
+    from charm_b200.workloads import GM, R_EARTH
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    p = orc.gl(N, R_EARTH)
+    shc = orc.Shc(N, GM, R_EARTH, c, s)
+    rows, mirrors, flags = orc.grid_rows(p)
+    npairs = len(rows)
+    if sample_rows is None:
+        # about 10-30 s of CPU work on 8 cores for nmax 2190
+        sample_rows = max(8, min(npairs, int(npairs * 8 / max(N / 360.0, 1) ** 2) + 8))
+    sel = np.linspace(0, npairs - 1, sample_rows).astype(int)
+    lat = p.lat[rows[sel]]
+    ones = np.ones(sel.size)
+    t0 = time.perf_counter()
+    a, b, a2, b2 = orc.lumped(shc, N, lat, ones, ones, flags[sel], "pot")
+    t_shs = time.perf_counter() - t0
+    nlon = p.lon.size
+    t0 = time.perf_counter()
+    fn = orc.lon_synthesis_fft(np.repeat(a[0][:1], p.lat.size, axis=0),
+                               np.repeat(b[0][:1], p.lat.size, axis=0), nlon,
+                               1.0)
+    t_fft1 = time.perf_counter() - t0
+    L = N + 1
+    amp = np.ascontiguousarray(a[0] + a2[0])
+    amm = np.ascontiguousarray(a[0] - a2[0])
+    bmp = np.ascontiguousarray(b[0] + b2[0])
+    bmm = np.ascontiguousarray(b[0] - b2[0])
+    cc = np.zeros(L * (L + 1) // 2)
+    ss = np.zeros_like(cc)
+    t0 = time.perf_counter()
+    orc.lib("d").orc_d_sha_contract(N, sel.size, orc._ptr(np.ascontiguousarray(lat)),
+                                    orc._ptr(amp), orc._ptr(amm), orc._ptr(bmp),
+                                    orc._ptr(bmm), orc._ptr(cc), orc._ptr(ss))
+    t_sha = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    np.fft.rfft(fn, axis=1)
+    t_fft2 = time.perf_counter() - t0
+    scale = npairs / sel.size
+    total = (t_shs + t_sha) * scale + t_fft1 + t_fft2
+    return {"value": total, "unit": "s", "cores": cores, "kind": "port",
+            "sample": "%d of %d latitude pairs of the nmax %d GL grid (Legendre "
+                      "sums scaled by %.1f; FFTs on all rows, numpy)" % (
+                          sel.size, npairs, N, scale),
+            "measured_s": t_shs + t_sha + t_fft1 + t_fft2}
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    from charm_b200.workloads import kaula
+    N = args.nmax
+    c, s = kaula(N, 2000)
+    times = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(N, c, s)
+        if i >= args.warmup:
+            times.append(cb["value"])
+    v = float(np.mean(times))
+    cb["value"] = v
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": v, "unit": "s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (Kaula-decay coefficients, seed 2000)",
+        "config": {"workload": "GL-grid SHS+SHA round trip, plain FP64",
+                   "nmax": N, "grid": "%dx%d" % (N + 1, 2 * (N + 1)), "r": "R"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

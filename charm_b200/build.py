@@ -25,8 +25,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-ccbin", HOST_CXX,
           "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "--expt-relaxed-constexpr"]
 
-SOURCES = ["shs_grid.cu", "sha_grid.cu", "sctr.cu", "crd.cu", "engine.cpp",
-           "capi.cpp"]
+SOURCES = ["shs_grid.cu", "sha_grid.cu", "sctr.cu", "crd.cu", "probe.cu",
+           "engine.cpp", "capi.cpp"]
 
 
 def nvcc():

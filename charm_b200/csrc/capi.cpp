@@ -594,3 +594,108 @@ void charm_sha_point(const charm_point *pnt, const double *f,
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Extensions (include/charm_b200.h): device-resident calls and measurement
+// hooks.  They have no counterpart in CHarm's API.
+// ---------------------------------------------------------------------------
+extern "C"
+{
+
+void charm_b200_shs_point_dev(const charm_point *pnt, unsigned long shc_nmax,
+                              double mu, double r, const double *d_c,
+                              const double *d_s, unsigned long nmax,
+                              int kgrad, unsigned dr, unsigned dlat,
+                              unsigned dlon, double *d_f, charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (kgrad < 0 || kgrad > 2 || (kgrad == 0 && dr + dlat + dlon > 2))
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "Unsupported derivative selection.");
+        return;
+    }
+    if (!check_type_shs(pnt, err))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    report(err, __func__,
+           cb::shs_point_dev(pnt, shc_nmax, mu, r, d_c, d_s, nmax, kgrad,
+                             kgrad ? kgrad : (int)dr,
+                             kgrad ? kgrad : (int)dlat,
+                             kgrad ? kgrad : (int)dlon, d_f));
+}
+
+void charm_b200_sha_point_dev(const charm_point *pnt, const double *d_f,
+                              unsigned long nmax, double mu, double r,
+                              unsigned long shc_nmax, double *d_c,
+                              double *d_s, charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (!is_quad_type(pnt->type))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic analysis of "
+                "point data values.");
+        return;
+    }
+    unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                 ? (unsigned long)pnt->nlat - 1
+                                 : ((unsigned long)pnt->nlat - 2) / 2;
+    if (nmax > nmax_grd)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The input data grid \"pnt\" was created for a maximum degree "
+                "that is not high enough to recover harmonics up to the "
+                "specified maximum degree of the analysis.");
+        return;
+    }
+    report(err, __func__,
+           cb::sha_point_dev(pnt, d_f, nmax, mu, r, shc_nmax, d_c, d_s));
+}
+
+void *charm_b200_stream(void)
+{
+    return cb::stream_handle();
+}
+
+void charm_b200_timing(int enable)
+{
+    cb::set_timing(enable != 0);
+}
+
+int charm_b200_timing_read(double *ms, unsigned long long *count, int n,
+                           unsigned long long *kernel_launches,
+                           unsigned long long *fft_execs)
+{
+    double tms[cb::TIMER_COUNT];
+    unsigned long long tn[cb::TIMER_COUNT];
+    cb::read_timing(tms, tn, kernel_launches, fft_execs);
+    for (int i = 0; i < n && i < cb::TIMER_COUNT; i++)
+    {
+        if (ms)
+            ms[i] = tms[i];
+        if (count)
+            count[i] = tn[i];
+    }
+    return cb::TIMER_COUNT;
+}
+
+double charm_b200_fp64_peak_tflops(void)
+{
+    double t = -1.0;
+    if (!cb::fp64_peak(&t).ok())
+        return -1.0;
+    return t;
+}
+
+} // extern "C"

@@ -58,14 +58,84 @@ struct Context
     std::map<std::string, DevBuf> bufs;
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
-    // recurrence tables of the last maximum degree
-    long long tab_nmax = -1;
+    long long tab_nmax = -1;     // recurrence tables of this maximum degree
     bool tab_has_en = false;
     std::map<std::tuple<int, int, long long>, cufftHandle> plans;
-    std::mutex mtx;
+    std::recursive_mutex mtx;
+    // optional per-kernel timing (CUDA events on the library stream)
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    double timer_ms[TIMER_COUNT] = {};
+    unsigned long long timer_n[TIMER_COUNT] = {};
+    unsigned long long launches = 0;   // kernels of this library
+    unsigned long long fft_execs = 0;  // cuFFT executions
 };
 
 Context g_ctx;
+
+cudaEvent_t ev_get(Context &c)
+{
+    if (!c.ev_pool.empty())
+    {
+        cudaEvent_t e = c.ev_pool.back();
+        c.ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch: counts it and, when timing is on, records a pair of
+// events that finish() turns into elapsed milliseconds.
+struct Scope
+{
+    Context &c;
+    int id;
+    bool lib;
+    cudaEvent_t a = nullptr;
+    Scope(Context &cc, int timer, bool library_kernel = true)
+        : c(cc), id(timer), lib(library_kernel)
+    {
+        if (c.timing)
+        {
+            a = ev_get(c);
+            cudaEventRecord(a, c.stream);
+        }
+    }
+    ~Scope()
+    {
+        if (lib)
+            c.launches++;
+        else
+            c.fft_execs++;
+        if (c.timing)
+        {
+            cudaEvent_t b = ev_get(c);
+            cudaEventRecord(b, c.stream);
+            c.pending.push_back({id, {a, b}});
+        }
+    }
+};
+
+void resolve_timers(Context &c)
+{
+    for (auto &pe : c.pending)
+    {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) ==
+            cudaSuccess)
+        {
+            c.timer_ms[pe.first] += ms;
+            c.timer_n[pe.first] += 1;
+        }
+        c.ev_pool.push_back(pe.second.first);
+        c.ev_pool.push_back(pe.second.second);
+    }
+    c.pending.clear();
+    cudaGetLastError();
+}
 
 #define CB_CUDA(call, st)                                                     \
     do                                                                        \
@@ -79,6 +149,14 @@ Context g_ctx;
                        cudaGetErrorString(e_);                                \
             return st;                                                        \
         }                                                                     \
+    } while (0)
+
+#define CB_TRY(expr)                                                          \
+    do                                                                        \
+    {                                                                         \
+        Status s_ = (expr);                                                   \
+        if (!s_.ok())                                                         \
+            return s_;                                                        \
     } while (0)
 
 Status init(Context &c)
@@ -193,44 +271,32 @@ Status tables(Context &c, long long nmax, bool need_en, double2 **ab,
 {
     Status st;
     long long T = (nmax + 1) * (nmax + 2) / 2;
-    st = dbuf(c, "tab_ab", (size_t)T, ab);
-    if (!st.ok())
-        return st;
+    CB_TRY(dbuf(c, "tab_ab", (size_t)T, ab));
     if (need_en)
-    {
-        st = dbuf(c, "tab_en", (size_t)T, en);
-        if (!st.ok())
-            return st;
-    }
-    st = dbuf(c, "tab_dm", (size_t)(nmax + 1), dm);
-    if (!st.ok())
-        return st;
+        CB_TRY(dbuf(c, "tab_en", (size_t)T, en));
+    CB_TRY(dbuf(c, "tab_dm", (size_t)(nmax + 1), dm));
     bool fresh = (c.tab_nmax != nmax);
     if (!fresh && (!need_en || c.tab_has_en))
         return st;
     std::vector<double> r, ri, dmh;
     host_r_ri_dm(nmax, r, ri, dmh);
     double *dr = nullptr, *dri = nullptr;
-    st = dbuf(c, "tab_r", r.size(), &dr);
-    if (!st.ok())
-        return st;
-    st = dbuf(c, "tab_ri", ri.size(), &dri);
-    if (!st.ok())
-        return st;
+    CB_TRY(dbuf(c, "tab_r", r.size(), &dr));
+    CB_TRY(dbuf(c, "tab_ri", ri.size(), &dri));
     CB_CUDA(cudaMemcpyAsync(dr, r.data(), r.size() * 8, cudaMemcpyHostToDevice,
                             c.stream), st);
     CB_CUDA(cudaMemcpyAsync(dri, ri.data(), ri.size() * 8,
                             cudaMemcpyHostToDevice, c.stream), st);
     CB_CUDA(cudaMemcpyAsync(*dm, dmh.data(), dmh.size() * 8,
                             cudaMemcpyHostToDevice, c.stream), st);
-    CB_CUDA(launch_tables(nmax, dr, dri, *ab, need_en ? *en : nullptr,
-                          c.stream), st);
+    {
+        Scope sc(c, TIMER_TABLES);
+        CB_CUDA(launch_tables(nmax, dr, dri, *ab, need_en ? *en : nullptr,
+                              c.stream), st);
+    }
     // the host vectors must outlive the copies
     CB_CUDA(cudaStreamSynchronize(c.stream), st);
-    if (fresh)
-        c.tab_has_en = need_en;
-    else
-        c.tab_has_en = c.tab_has_en || need_en;
+    c.tab_has_en = fresh ? need_en : (c.tab_has_en || need_en);
     c.tab_nmax = nmax;
     return st;
 }
@@ -256,12 +322,13 @@ Status plan(Context &c, cufftType type, int n, long long batch,
     cufftHandle h;
     int nn[1] = {n};
     int nfc = n / 2 + 1;
+    int nc[1] = {nfc};
     cufftResult r;
     if (type == CUFFT_Z2D)
-        r = cufftPlanMany(&h, 1, nn, nn, 1, nfc, nn, 1, n, CUFFT_Z2D,
+        r = cufftPlanMany(&h, 1, nn, nc, 1, nfc, nn, 1, n, CUFFT_Z2D,
                           (int)batch);
     else
-        r = cufftPlanMany(&h, 1, nn, nn, 1, n, nn, 1, nfc, CUFFT_D2Z,
+        r = cufftPlanMany(&h, 1, nn, nn, 1, n, nc, 1, nfc, CUFFT_D2Z,
                           (int)batch);
     if (r != CUFFT_SUCCESS)
     {
@@ -276,9 +343,9 @@ Status plan(Context &c, cufftType type, int n, long long batch,
     return st;
 }
 
-// Triangle pointer of a charm_shc if c[m] are laid out contiguously as in
-// src/shc/shc_init_chunk.c:126-145 (the case for every charm_shc built by
-// CHarm's constructors), else null.
+// Triangle pointer of a charm_shc whose columns c[m] lie contiguously as in
+// src/shc/shc_init_chunk.c:126-145 (every charm_shc built by CHarm's
+// constructors), else null.
 const double *contiguous_tri(double *const *cols, unsigned long nmax)
 {
     if (!cols || !cols[0])
@@ -294,7 +361,6 @@ const double *contiguous_tri(double *const *cols, unsigned long nmax)
     return base;
 }
 
-// Uploads a coefficient triangle of degree shc_nmax to the device.
 Status upload_tri(Context &c, double *const *cols, unsigned long shc_nmax,
                   double *dst)
 {
@@ -352,7 +418,7 @@ bool is_dh(int t)
     return t == CHARM_CRD_POINT_GRID_DH1 || t == CHARM_CRD_POINT_GRID_DH2;
 }
 
-// src/misc/misc_arr_chck_symm.c
+// src/misc/misc_arr_chck_symm.c with centre 0
 int arr_chck_symm(const double *a, size_t n, double eps)
 {
     size_t middle = n / 2;
@@ -364,7 +430,7 @@ int arr_chck_symm(const double *a, size_t n, double eps)
     return 0;
 }
 
-// Latitude pairs of a grid: evaluated rows, mirror rows (-1 when none),
+// Latitude pairs of a grid: evaluated rows and mirror rows (-1 when none),
 // following src/shs/shs_point_grd.c:113-197 and
 // src/crd/crd_grd_check_symm.c:21-72.
 struct Pairs
@@ -398,9 +464,7 @@ void grid_pairs(const charm_point *pnt, double thr2, bool allow_symm,
         if (!(pnt->type == CHARM_CRD_POINT_GRID_GL && (nmax_grd % 2)))
             equator = nlat / 2;
     }
-    size_t nlatdo = symm ? (pnt_nlat + 1 - (even ? 1 : 0)) / 2 : pnt_nlat;
-    if (!symm && dh)
-        nlatdo = nlat; // no phantom south pole when every row is evaluated
+    size_t nlatdo = symm ? (pnt_nlat + 1 - (even ? 1 : 0)) / 2 : nlat;
     P.row_n.clear();
     P.row_s.clear();
     for (size_t ipv = 0; ipv < nlatdo; ipv++)
@@ -409,14 +473,7 @@ void grid_pairs(const charm_point *pnt, double thr2, bool allow_symm,
         if (!symm)
             s = 0;
         else if (quad)
-        {
-            if (dh && ipv == 0)
-                s = 0;
-            else if (ipv < equator)
-                s = 1;
-            else
-                s = 0;
-        }
+            s = (dh && ipv == 0) ? 0 : (ipv < equator ? 1 : 0);
         else
             s = (!even && ipv == nlatdo - 1) ? 0 : 1;
         P.row_n.push_back((int)ipv);
@@ -442,6 +499,8 @@ Status finish(Context &c, unsigned *d_status)
     CB_CUDA(cudaMemcpyAsync(&h_status, d_status, sizeof(unsigned),
                             cudaMemcpyDeviceToHost, c.stream), st);
     CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    if (c.timing)
+        resolve_timers(c);
     if (h_status)
     {
         st.code = CHARM_EFUNCARG;
@@ -456,9 +515,7 @@ Status status_words(Context &c, unsigned **d_status,
 {
     Status st;
     void *p = nullptr;
-    st = buf(c, "status", 256, &p);
-    if (!st.ok())
-        return st;
+    CB_TRY(buf(c, "status", 256, &p));
     *d_status = static_cast<unsigned *>(p);
     *d_counter = reinterpret_cast<unsigned long long *>(
         static_cast<char *>(p) + 64);
@@ -476,7 +533,7 @@ double polar_threshold(unsigned long nmax)
 }
 
 // src/shs/shs_get_mur_dorder_npar.c:30-72
-void mur_dorder(const charm_shc *shcs, int kgrad, int dr, int dlat, int dlon,
+void mur_dorder(double mu, double R, int kgrad, int dr, int dlat, int dlon,
                 double *mur, int *dorder, int *npar)
 {
     if (kgrad == 1)
@@ -494,18 +551,51 @@ void mur_dorder(const charm_shc *shcs, int kgrad, int dr, int dlat, int dlon,
         *dorder = dr + dlat + dlon;
         *npar = 1;
     }
-    double rpow = shcs->r;
+    double rpow = R;
     for (int i = 1; i <= *dorder; i++)
-        rpow *= shcs->r;
-    *mur = shcs->mu / rpow;
+        rpow *= R;
+    *mur = mu / rpow;
+}
+
+// Coefficients entering a synthesis: host columns (CHarm's charm_shc) or a
+// device-resident triangle of degree nmax_shc.
+struct CoefIn
+{
+    unsigned long nmax;
+    double mu, r;
+    double *const *hc = nullptr, *const *hs = nullptr;
+    const double *dc = nullptr, *ds = nullptr;
+};
+
+Status coef_to_device(Context &c, const CoefIn &in, unsigned long nmax,
+                      double2 **dcs)
+{
+    Status st;
+    const long long Ts = (long long)(in.nmax + 1) * (in.nmax + 2) / 2;
+    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
+    CB_TRY(dbuf(c, "cs", (size_t)T, dcs));
+    const double *src_c = in.dc, *src_s = in.ds;
+    if (!src_c)
+    {
+        double *raw = nullptr;
+        CB_TRY(dbuf(c, "shc_in", (size_t)(2 * Ts), &raw));
+        CB_TRY(upload_tri(c, in.hc, in.nmax, raw));
+        CB_TRY(upload_tri(c, in.hs, in.nmax, raw + Ts));
+        src_c = raw;
+        src_s = raw + Ts;
+    }
+    Scope sc(c, TIMER_PREP);
+    CB_CUDA(launch_interleave((long long)nmax, (long long)in.nmax, src_c,
+                              src_s, *dcs, c.stream), st);
+    return st;
 }
 
 // ---------------------------------------------------------------------------
 // Grid synthesis
 // ---------------------------------------------------------------------------
-Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
+Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
                 unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
-                double **f)
+                double **f, double *d_f)
 {
     Status st;
     const double thr = charm_glob_threshold, thr2 = charm_glob_threshold2;
@@ -533,15 +623,16 @@ Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
             return st;
         }
     }
+    // src/shs/shs_grd_point_fft_check.c:30-55
     double dlon_step = nlon > 1 ? pnt->lon[1] - pnt->lon[0] : 0.0;
     bool use_fft = (nlon >= 1) && ((nlon - 1) / 2 >= nmax) &&
                    nearly_equal(pnt->lon[0], 0.0, thr) &&
                    nearly_equal(pnt->lon[nlon - 1] + dlon_step, 2.0 * PI, thr);
 
-    // radii: r == R everywhere selects the faster kernels
+    // r == R everywhere selects the faster kernels (shs_r_eq_rref.c)
     bool r_eq = true;
     for (size_t i = 0; i < nlat; i++)
-        if (!nearly_equal(pnt->r[i], shcs->r, thr))
+        if (!nearly_equal(pnt->r[i], in.r, thr))
         {
             r_eq = false;
             break;
@@ -563,14 +654,12 @@ Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
 
     double mur;
     int dorder, npar;
-    mur_dorder(shcs, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
+    mur_dorder(in.mu, in.r, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
 
-    // per-pair geometry staged through pinned memory (one upload)
+    // per-pair geometry, staged through pinned memory (one upload)
     size_t geo_bytes = (size_t)np * (3 * 8 + 2 * 4);
     void *hp = nullptr;
-    st = pinned(c, geo_bytes, &hp);
-    if (!st.ok())
-        return st;
+    CB_TRY(pinned(c, geo_bytes, &hp));
     double *ht = static_cast<double *>(hp);
     double *hu = ht + np;
     double *hrho = hu + np;
@@ -581,14 +670,12 @@ Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
         double la = pnt->lat[P.row_n[p]];
         ht[p] = std::sin(la);
         hu[p] = std::cos(la);
-        hrho[p] = r_eq ? 1.0 : shcs->r / pnt->r[P.row_n[p]];
+        hrho[p] = r_eq ? 1.0 : in.r / pnt->r[P.row_n[p]];
         hrn[p] = P.row_n[p];
         hrs[p] = P.row_s[p];
     }
     void *dgeo = nullptr;
-    st = buf(c, "geo", geo_bytes, &dgeo);
-    if (!st.ok())
-        return st;
+    CB_TRY(buf(c, "geo", geo_bytes, &dgeo));
     CB_CUDA(cudaMemcpyAsync(dgeo, hp, geo_bytes, cudaMemcpyHostToDevice,
                             c.stream), st);
     const double *dt = static_cast<const double *>(dgeo);
@@ -600,56 +687,31 @@ Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
     bool need_en = (kgrad > 0) || (dlat > 0);
     double2 *ab = nullptr, *en = nullptr;
     double *dm = nullptr;
-    st = tables(c, (long long)nmax, need_en, &ab, &en, &dm);
-    if (!st.ok())
-        return st;
-
-    // coefficients
-    const long long Ts = (long long)(shcs->nmax + 1) * (shcs->nmax + 2) / 2;
-    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
-    double *dcs_raw = nullptr;
+    CB_TRY(tables(c, (long long)nmax, need_en, &ab, &en, &dm));
     double2 *dcs = nullptr;
-    st = dbuf(c, "shc_in", (size_t)(2 * Ts), &dcs_raw);
-    if (!st.ok())
-        return st;
-    st = dbuf(c, "cs", (size_t)T, &dcs);
-    if (!st.ok())
-        return st;
-    st = upload_tri(c, shcs->c, shcs->nmax, dcs_raw);
-    if (!st.ok())
-        return st;
-    st = upload_tri(c, shcs->s, shcs->nmax, dcs_raw + Ts);
-    if (!st.ok())
-        return st;
-    CB_CUDA(launch_interleave((long long)nmax, (long long)shcs->nmax, dcs_raw,
-                              dcs_raw + Ts, dcs, c.stream), st);
+    CB_TRY(coef_to_device(c, in, nmax, &dcs));
 
     // sectorial seeds
     double *psx = nullptr;
     int *pse = nullptr;
-    st = dbuf(c, "psx", (size_t)(nmax + 1) * np, &psx);
-    if (!st.ok())
-        return st;
-    st = dbuf(c, "pse", (size_t)(nmax + 1) * np, &pse);
-    if (!st.ok())
-        return st;
-    CB_CUDA(launch_sectorial((long long)nmax, np, du, drho, r_eq ? 0 : 1,
-                             dorder, dm, psx, pse, c.stream), st);
+    CB_TRY(dbuf(c, "psx", (size_t)(nmax + 1) * np, &psx));
+    CB_TRY(dbuf(c, "pse", (size_t)(nmax + 1) * np, &pse));
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_sectorial((long long)nmax, np, du, drho, r_eq ? 0 : 1,
+                                 dorder, dm, psx, pse, c.stream), st);
+    }
 
     // lumped coefficients
     const int ldf = use_fft ? (int)(nlon / 2 + 1) : (int)(nmax + 1);
     double2 *lc = nullptr;
-    st = dbuf(c, "lumped", (size_t)npar * nlat * ldf, &lc);
-    if (!st.ok())
-        return st;
-    if (use_fft)
+    CB_TRY(dbuf(c, "lumped", (size_t)npar * nlat * ldf, &lc));
+    if (use_fft && (size_t)ldf > nmax + 1)
         CB_CUDA(cudaMemsetAsync(lc, 0, (size_t)npar * nlat * ldf * 16,
                                 c.stream), st);
     unsigned *d_status;
     unsigned long long *d_counter;
-    st = status_words(c, &d_status, &d_counter);
-    if (!st.ok())
-        return st;
+    CB_TRY(status_words(c, &d_status, &d_counter));
 
     const int K = choose_k(kgrad, dlat, np);
     const int ntiles = (np + 32 * K - 1) / (32 * K);
@@ -677,25 +739,25 @@ Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
     A.polar_thr = polar_threshold(nmax);
     A.counter = d_counter;
     A.status = d_status;
-    long long warps_needed = A.nitems;
-    int grid = (int)std::min<long long>((warps_needed + 3) / 4,
+    int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                         (long long)c.num_sms * 8);
-    CB_CUDA(launch_shs_grid(A, kgrad, dr, dlat, !r_eq, K, std::max(grid, 1),
-                            c.stream), st);
+    {
+        Scope sc(c, TIMER_SHS);
+        CB_CUDA(launch_shs_grid(A, kgrad, dr, dlat, !r_eq, K,
+                                std::max(grid, 1), c.stream), st);
+    }
 
-    // longitude sums
-    double *fg = nullptr;
-    st = dbuf(c, "fgrid", (size_t)npar * nlat * nlon, &fg);
-    if (!st.ok())
-        return st;
+    // longitude sums into the output grid(s)
+    double *fg = d_f;
+    if (!fg)
+        CB_TRY(dbuf(c, "fgrid", (size_t)npar * nlat * nlon, &fg));
     if (use_fft)
     {
         cufftHandle h;
-        st = plan(c, CUFFT_Z2D, (int)nlon, (long long)npar * nlat, &h);
-        if (!st.ok())
-            return st;
-        cufftResult r = cufftExecZ2D(h, reinterpret_cast<cufftDoubleComplex *>(lc),
-                                     fg);
+        CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)npar * nlat, &h));
+        Scope sc(c, TIMER_FFT, false);
+        cufftResult r = cufftExecZ2D(
+            h, reinterpret_cast<cufftDoubleComplex *>(lc), fg);
         if (r != CUFFT_SUCCESS)
         {
             st.code = CHARM_EFUNCARG;
@@ -706,68 +768,48 @@ Status shs_grid(Context &c, const charm_point *pnt, const charm_shc *shcs,
     else
     {
         double *dlon_arr = nullptr;
-        st = dbuf(c, "lon", nlon, &dlon_arr);
-        if (!st.ok())
-            return st;
+        CB_TRY(dbuf(c, "lon", nlon, &dlon_arr));
         CB_CUDA(cudaMemcpyAsync(dlon_arr, pnt->lon, nlon * 8,
                                 cudaMemcpyHostToDevice, c.stream), st);
+        Scope sc(c, TIMER_LON);
         CB_CUDA(launch_lon_direct(npar, (int)nlat, (int)nlon, (long long)nmax,
                                   lc, ldf, dlon_arr, fg, c.stream), st);
     }
-    for (int q = 0; q < npar; q++)
-        CB_CUDA(cudaMemcpyAsync(f[q], fg + (size_t)q * nlat * nlon,
-                                nlat * nlon * 8, cudaMemcpyDeviceToHost,
-                                c.stream), st);
+    if (!d_f)
+        for (int q = 0; q < npar; q++)
+            CB_CUDA(cudaMemcpyAsync(f[q], fg + (size_t)q * nlat * nlon,
+                                    nlat * nlon * 8, cudaMemcpyDeviceToHost,
+                                    c.stream), st);
     return finish(c, d_status);
 }
 
 // ---------------------------------------------------------------------------
 // Scattered synthesis
 // ---------------------------------------------------------------------------
-Status shs_sctr(Context &c, const charm_point *pnt, const charm_shc *shcs,
+Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
                 unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
-                double **f)
+                double **f, double *d_f)
 {
     Status st;
     const size_t npt = pnt->nlat;
     bool r_eq = true;
     for (size_t i = 0; i < npt; i++)
-        if (!nearly_equal(pnt->r[i], shcs->r, charm_glob_threshold))
+        if (!nearly_equal(pnt->r[i], in.r, charm_glob_threshold))
         {
             r_eq = false;
             break;
         }
     double mur;
     int dorder, npar;
-    mur_dorder(shcs, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
+    mur_dorder(in.mu, in.r, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
     bool need_en = (kgrad > 0) || (dlat > 0);
     double2 *ab = nullptr, *en = nullptr;
     double *dm = nullptr;
-    st = tables(c, (long long)nmax, need_en, &ab, &en, &dm);
-    if (!st.ok())
-        return st;
-    const long long Ts = (long long)(shcs->nmax + 1) * (shcs->nmax + 2) / 2;
-    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
-    double *dcs_raw = nullptr;
+    CB_TRY(tables(c, (long long)nmax, need_en, &ab, &en, &dm));
     double2 *dcs = nullptr;
-    st = dbuf(c, "shc_in", (size_t)(2 * Ts), &dcs_raw);
-    if (!st.ok())
-        return st;
-    st = dbuf(c, "cs", (size_t)T, &dcs);
-    if (!st.ok())
-        return st;
-    st = upload_tri(c, shcs->c, shcs->nmax, dcs_raw);
-    if (!st.ok())
-        return st;
-    st = upload_tri(c, shcs->s, shcs->nmax, dcs_raw + Ts);
-    if (!st.ok())
-        return st;
-    CB_CUDA(launch_interleave((long long)nmax, (long long)shcs->nmax, dcs_raw,
-                              dcs_raw + Ts, dcs, c.stream), st);
+    CB_TRY(coef_to_device(c, in, nmax, &dcs));
     double *dpts = nullptr;
-    st = dbuf(c, "sctr_pts", 3 * npt, &dpts);
-    if (!st.ok())
-        return st;
+    CB_TRY(dbuf(c, "sctr_pts", 3 * npt, &dpts));
     CB_CUDA(cudaMemcpyAsync(dpts, pnt->lat, npt * 8, cudaMemcpyHostToDevice,
                             c.stream), st);
     CB_CUDA(cudaMemcpyAsync(dpts + npt, pnt->lon, npt * 8,
@@ -775,15 +817,12 @@ Status shs_sctr(Context &c, const charm_point *pnt, const charm_shc *shcs,
     if (!r_eq)
         CB_CUDA(cudaMemcpyAsync(dpts + 2 * npt, pnt->r, npt * 8,
                                 cudaMemcpyHostToDevice, c.stream), st);
-    double *fo = nullptr;
-    st = dbuf(c, "sctr_f", (size_t)npar * npt, &fo);
-    if (!st.ok())
-        return st;
+    double *fo = d_f;
+    if (!fo)
+        CB_TRY(dbuf(c, "sctr_f", (size_t)npar * npt, &fo));
     unsigned *d_status;
     unsigned long long *d_counter;
-    st = status_words(c, &d_status, &d_counter);
-    if (!st.ok())
-        return st;
+    CB_TRY(status_words(c, &d_status, &d_counter));
     const int K = choose_k(kgrad, dlat, (long long)npt);
     SctrArgs A{};
     A.nmax = (long long)nmax;
@@ -796,7 +835,7 @@ Status shs_sctr(Context &c, const charm_point *pnt, const charm_shc *shcs,
     A.lat = dpts;
     A.lon = dpts + npt;
     A.r = dpts + 2 * npt;
-    A.R = shcs->r;
+    A.R = in.r;
     A.f = fo;
     A.mur = mur;
     A.dlon = dlon;
@@ -805,62 +844,44 @@ Status shs_sctr(Context &c, const charm_point *pnt, const charm_shc *shcs,
     A.status = d_status;
     int grid = (int)std::min<long long>((A.ntiles + 3) / 4,
                                         (long long)c.num_sms * 8);
-    CB_CUDA(launch_sctr(A, kgrad, dr, dlat, !r_eq, K, std::max(grid, 1),
-                        c.stream), st);
-    for (int q = 0; q < npar; q++)
-        CB_CUDA(cudaMemcpyAsync(f[q], fo + (size_t)q * npt, npt * 8,
-                                cudaMemcpyDeviceToHost, c.stream), st);
+    {
+        Scope sc(c, TIMER_SCTR);
+        CB_CUDA(launch_sctr(A, kgrad, dr, dlat, !r_eq, K, std::max(grid, 1),
+                            c.stream), st);
+    }
+    if (!d_f)
+        for (int q = 0; q < npar; q++)
+            CB_CUDA(cudaMemcpyAsync(f[q], fo + (size_t)q * npt, npt * 8,
+                                    cudaMemcpyDeviceToHost, c.stream), st);
     return finish(c, d_status);
 }
 
-} // namespace
-
 // ---------------------------------------------------------------------------
-// Public engine entry points
+// Grid analysis
 // ---------------------------------------------------------------------------
-Status shs_point(const charm_point *pnt, const charm_shc *shcs,
-                 unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
-                 double **f)
+Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
+                const double *d_fin, unsigned long nmax, double mu, double R,
+                unsigned long shc_nmax, double *const *hc, double *const *hs,
+                double *d_c, double *d_s)
 {
-    std::lock_guard<std::mutex> lock(g_ctx.mtx);
-    Status st = init(g_ctx);
-    if (!st.ok())
-        return st;
-    if (pnt->type == CHARM_CRD_POINT_SCATTERED)
-        return shs_sctr(g_ctx, pnt, shcs, nmax, kgrad, dr, dlat, dlon, f);
-    return shs_grid(g_ctx, pnt, shcs, nmax, kgrad, dr, dlat, dlon, f);
-}
-
-Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
-                 charm_shc *shcs)
-{
-    std::lock_guard<std::mutex> lock(g_ctx.mtx);
-    Context &c = g_ctx;
-    Status st = init(c);
-    if (!st.ok())
-        return st;
+    Status st;
     const size_t nlat = pnt->nlat, nlon = pnt->nlon;
     const double r0 = pnt->r[0];
     const unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
                                        ? nlat - 1
                                        : (nlat - 2) / 2;
     // quadrature constant, src/sha/sha_point.c:313-322
-    double cq = 0.0;
-    if (pnt->type == CHARM_CRD_POINT_GRID_GL ||
-        pnt->type == CHARM_CRD_POINT_GRID_DH1)
-        cq = PI / (double)(nmax_grd + 1);
-    else
-        cq = PI / (double)(2 * nmax_grd + 2);
-    cq *= 1.0 / (4.0 * PI) * (r0 / shcs->mu);
+    double cq = (pnt->type == CHARM_CRD_POINT_GRID_DH2)
+                    ? PI / (double)(2 * nmax_grd + 2)
+                    : PI / (double)(nmax_grd + 1);
+    cq *= 1.0 / (4.0 * PI) * (r0 / mu);
 
     Pairs P;
     grid_pairs(pnt, charm_glob_threshold2, true, P);
     const int np = (int)P.row_n.size();
     size_t geo_bytes = (size_t)np * (4 * 8 + 2 * 4);
     void *hp = nullptr;
-    st = pinned(c, geo_bytes, &hp);
-    if (!st.ok())
-        return st;
+    CB_TRY(pinned(c, geo_bytes, &hp));
     double *ht = static_cast<double *>(hp);
     double *hu = ht + np;
     double *hcn = hu + np;
@@ -878,9 +899,7 @@ Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
         hrs[p] = P.row_s[p];
     }
     void *dgeo = nullptr;
-    st = buf(c, "geo", geo_bytes, &dgeo);
-    if (!st.ok())
-        return st;
+    CB_TRY(buf(c, "geo", geo_bytes, &dgeo));
     CB_CUDA(cudaMemcpyAsync(dgeo, hp, geo_bytes, cudaMemcpyHostToDevice,
                             c.stream), st);
     const double *dt = static_cast<const double *>(dgeo);
@@ -892,50 +911,48 @@ Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
 
     double2 *ab = nullptr, *en = nullptr;
     double *dm = nullptr;
-    st = tables(c, (long long)nmax, false, &ab, &en, &dm);
-    if (!st.ok())
-        return st;
+    CB_TRY(tables(c, (long long)nmax, false, &ab, &en, &dm));
 
-    // grid upload and r2c along the parallels
-    double *fg = nullptr;
-    st = dbuf(c, "fgrid", nlat * nlon, &fg);
-    if (!st.ok())
-        return st;
-    CB_CUDA(cudaMemcpyAsync(fg, f, nlat * nlon * 8, cudaMemcpyHostToDevice,
-                            c.stream), st);
+    // grid on the device and r2c along the parallels
+    const double *fg = d_fin;
+    if (!fg)
+    {
+        double *tmp = nullptr;
+        CB_TRY(dbuf(c, "fgrid", nlat * nlon, &tmp));
+        CB_CUDA(cudaMemcpyAsync(tmp, f_host, nlat * nlon * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        fg = tmp;
+    }
     const int ldF = (int)(nlon / 2 + 1);
     double2 *F = nullptr;
-    st = dbuf(c, "lumped", nlat * (size_t)ldF, &F);
-    if (!st.ok())
-        return st;
-    cufftHandle h;
-    st = plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h);
-    if (!st.ok())
-        return st;
-    if (cufftExecD2Z(h, fg, reinterpret_cast<cufftDoubleComplex *>(F)) !=
-        CUFFT_SUCCESS)
+    CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
     {
-        st.code = CHARM_EFUNCARG;
-        st.msg = "cuFFT D2Z failed";
-        return st;
+        cufftHandle h;
+        CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
+        Scope sc(c, TIMER_FFT, false);
+        if (cufftExecD2Z(h, const_cast<double *>(fg),
+                         reinterpret_cast<cufftDoubleComplex *>(F)) !=
+            CUFFT_SUCCESS)
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "cuFFT D2Z failed";
+            return st;
+        }
     }
 
     double *psx = nullptr;
     int *pse = nullptr;
-    st = dbuf(c, "psx", (size_t)(nmax + 1) * np, &psx);
-    if (!st.ok())
-        return st;
-    st = dbuf(c, "pse", (size_t)(nmax + 1) * np, &pse);
-    if (!st.ok())
-        return st;
-    CB_CUDA(launch_sectorial((long long)nmax, np, du, nullptr, 0, 0, dm, psx,
-                             pse, c.stream), st);
+    CB_TRY(dbuf(c, "psx", (size_t)(nmax + 1) * np, &psx));
+    CB_TRY(dbuf(c, "pse", (size_t)(nmax + 1) * np, &pse));
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_sectorial((long long)nmax, np, du, nullptr, 0, 0, dm,
+                                 psx, pse, c.stream), st);
+    }
 
     unsigned *d_status;
     unsigned long long *d_counter;
-    st = status_words(c, &d_status, &d_counter);
-    if (!st.ok())
-        return st;
+    CB_TRY(status_words(c, &d_status, &d_counter));
     const int K = choose_k(0, 0, np);
     const int ntiles = (np + 32 * K - 1) / (32 * K);
     const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
@@ -945,9 +962,7 @@ Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
     int tpg = (int)((ntiles + G - 1) / G);
     G = (ntiles + tpg - 1) / tpg;
     double2 *part = nullptr;
-    st = dbuf(c, "sha_part", (size_t)G * T, &part);
-    if (!st.ok())
-        return st;
+    CB_TRY(dbuf(c, "sha_part", (size_t)G * T, &part));
     ShaGridArgs A{};
     A.nmax = (long long)nmax;
     A.npairs = np;
@@ -972,17 +987,20 @@ Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
     A.status = d_status;
     int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                         (long long)c.num_sms * 8);
-    CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
+    {
+        Scope sc(c, TIMER_SHA);
+        CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
+    }
 
-    // rescaling from r0 to shcs->r (src/sha/sha_point.c:1088-1108 with
-    // src/shc/shc_rescale.c)
-    const unsigned long sn = shcs->nmax;
+    // rescaling from r0 to the coefficients' radius
+    // (src/sha/sha_point.c:1088-1108 with src/shc/shc_rescale.c)
+    const unsigned long sn = shc_nmax;
     double *dres = nullptr;
     std::vector<double> res;
-    if (!nearly_equal(shcs->r, r0, charm_glob_threshold))
+    if (!nearly_equal(R, r0, charm_glob_threshold))
     {
-        double mu_ratio = shcs->mu / shcs->mu;
-        double r_ratio = r0 / shcs->r;
+        double mu_ratio = mu / mu;
+        double r_ratio = r0 / R;
         res.resize(sn + 1);
         double tmp2 = mu_ratio * r_ratio;
         res[0] = mu_ratio;
@@ -991,50 +1009,114 @@ Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
             res[n] = tmp2;
             tmp2 *= r_ratio;
         }
-        st = dbuf(c, "sha_rescale", sn + 1, &dres);
-        if (!st.ok())
-            return st;
+        CB_TRY(dbuf(c, "sha_rescale", sn + 1, &dres));
         CB_CUDA(cudaMemcpyAsync(dres, res.data(), (sn + 1) * 8,
                                 cudaMemcpyHostToDevice, c.stream), st);
     }
     const long long Ts = (long long)(sn + 1) * (sn + 2) / 2;
-    double *dout = nullptr;
-    st = dbuf(c, "shc_out", (size_t)(2 * Ts), &dout);
-    if (!st.ok())
-        return st;
-    CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T, part,
-                              dres, dout, dout + Ts, c.stream), st);
-    st = download_tri(c, dout, sn, shcs->c);
-    if (!st.ok())
-        return st;
-    st = download_tri(c, dout + Ts, sn, shcs->s);
-    if (!st.ok())
-        return st;
+    double *oc = d_c, *os = d_s;
+    if (!oc)
+    {
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "shc_out", (size_t)(2 * Ts), &dout));
+        oc = dout;
+        os = dout + Ts;
+    }
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T,
+                                  part, dres, oc, os, c.stream), st);
+    }
+    if (!d_c)
+    {
+        CB_TRY(download_tri(c, oc, sn, hc));
+        CB_TRY(download_tri(c, os, sn, hs));
+    }
+    // res must stay alive until the copy ran: finish() synchronises
     return finish(c, d_status);
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Public engine entry points
+// ---------------------------------------------------------------------------
+Status shs_point(const charm_point *pnt, const charm_shc *shcs,
+                 unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
+                 double **f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    CoefIn in;
+    in.nmax = shcs->nmax;
+    in.mu = shcs->mu;
+    in.r = shcs->r;
+    in.hc = shcs->c;
+    in.hs = shcs->s;
+    if (pnt->type == CHARM_CRD_POINT_SCATTERED)
+        return shs_sctr(g_ctx, pnt, in, nmax, kgrad, dr, dlat, dlon, f,
+                        nullptr);
+    return shs_grid(g_ctx, pnt, in, nmax, kgrad, dr, dlat, dlon, f, nullptr);
+}
+
+Status shs_point_dev(const charm_point *pnt, unsigned long shc_nmax,
+                     double mu, double r, const double *d_c,
+                     const double *d_s, unsigned long nmax, int kgrad, int dr,
+                     int dlat, int dlon, double *d_f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    CoefIn in;
+    in.nmax = shc_nmax;
+    in.mu = mu;
+    in.r = r;
+    in.dc = d_c;
+    in.ds = d_s;
+    if (pnt->type == CHARM_CRD_POINT_SCATTERED)
+        return shs_sctr(g_ctx, pnt, in, nmax, kgrad, dr, dlat, dlon, nullptr,
+                        d_f);
+    return shs_grid(g_ctx, pnt, in, nmax, kgrad, dr, dlat, dlon, nullptr, d_f);
+}
+
+Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
+                 charm_shc *shcs)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_grid(g_ctx, pnt, f, nullptr, nmax, shcs->mu, shcs->r,
+                    shcs->nmax, shcs->c, shcs->s, nullptr, nullptr);
+}
+
+Status sha_point_dev(const charm_point *pnt, const double *d_f,
+                     unsigned long nmax, double mu, double r,
+                     unsigned long shc_nmax, double *d_c, double *d_s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
+                    nullptr, d_c, d_s);
 }
 
 Status quad_nodes(int type, unsigned long nmax, double *lat, double *w)
 {
-    std::lock_guard<std::mutex> lock(g_ctx.mtx);
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
     Context &c = g_ctx;
-    Status st = init(c);
-    if (!st.ok())
-        return st;
+    CB_TRY(init(c));
+    Status st;
     size_t nlat = type == CHARM_CRD_POINT_GRID_GL ? nmax + 1 : 2 * (nmax + 1);
     double *d = nullptr;
-    st = dbuf(c, "crd", 2 * nlat, &d);
-    if (!st.ok())
-        return st;
+    CB_TRY(dbuf(c, "crd", 2 * nlat, &d));
     CB_CUDA(cudaMemsetAsync(d, 0, 2 * nlat * 8, c.stream), st);
     unsigned *d_status;
     unsigned long long *d_counter;
-    st = status_words(c, &d_status, &d_counter);
-    if (!st.ok())
-        return st;
-    if (type == CHARM_CRD_POINT_GRID_GL)
-        CB_CUDA(launch_gl_nodes(nmax, d, d + nlat, d_status, c.stream), st);
-    else
-        CB_CUDA(launch_dh_nodes(nmax, d, d + nlat, c.stream), st);
+    CB_TRY(status_words(c, &d_status, &d_counter));
+    {
+        Scope sc(c, TIMER_PREP);
+        if (type == CHARM_CRD_POINT_GRID_GL)
+            CB_CUDA(launch_gl_nodes(nmax, d, d + nlat, d_status, c.stream), st);
+        else
+            CB_CUDA(launch_dh_nodes(nmax, d, d + nlat, c.stream), st);
+    }
     CB_CUDA(cudaMemcpyAsync(lat, d, nlat * 8, cudaMemcpyDeviceToHost, c.stream),
             st);
     CB_CUDA(cudaMemcpyAsync(w, d + nlat, nlat * 8, cudaMemcpyDeviceToHost,
@@ -1047,9 +1129,72 @@ Status quad_nodes(int type, unsigned long nmax, double *lat, double *w)
     return st;
 }
 
+Status fp64_peak(double *tflops)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    Context &c = g_ctx;
+    CB_TRY(init(c));
+    Status st;
+    double *sink = nullptr;
+    CB_TRY(dbuf(c, "probe", 1024, &sink));
+    const int threads = 256, blocks = c.num_sms * 8;
+    const long long iters = 1 << 16;
+    cudaEvent_t a = ev_get(c), b = ev_get(c);
+    CB_CUDA(launch_fp64_probe(iters / 8, blocks, threads, sink, c.stream), st);
+    CB_CUDA(cudaEventRecord(a, c.stream), st);
+    CB_CUDA(launch_fp64_probe(iters, blocks, threads, sink, c.stream), st);
+    CB_CUDA(cudaEventRecord(b, c.stream), st);
+    CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    float ms = 0.f;
+    CB_CUDA(cudaEventElapsedTime(&ms, a, b), st);
+    c.ev_pool.push_back(a);
+    c.ev_pool.push_back(b);
+    double flops = 2.0 * 8.0 * (double)iters * threads * (double)blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return st;
+}
+
+void *stream_handle()
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    if (!init(g_ctx).ok())
+        return nullptr;
+    return (void *)g_ctx.stream;
+}
+
+void set_timing(bool on)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    g_ctx.timing = on;
+    for (int i = 0; i < TIMER_COUNT; i++)
+    {
+        g_ctx.timer_ms[i] = 0.0;
+        g_ctx.timer_n[i] = 0;
+    }
+    g_ctx.launches = 0;
+    g_ctx.fft_execs = 0;
+}
+
+void read_timing(double *ms, unsigned long long *n, unsigned long long *kern,
+                 unsigned long long *ffts)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    for (int i = 0; i < TIMER_COUNT; i++)
+    {
+        if (ms)
+            ms[i] = g_ctx.timer_ms[i];
+        if (n)
+            n[i] = g_ctx.timer_n[i];
+    }
+    if (kern)
+        *kern = g_ctx.launches;
+    if (ffts)
+        *ffts = g_ctx.fft_execs;
+}
+
 void shutdown()
 {
-    std::lock_guard<std::mutex> lock(g_ctx.mtx);
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
     Context &c = g_ctx;
     if (!c.ready)
         return;

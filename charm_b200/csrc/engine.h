@@ -11,6 +11,19 @@
 namespace cb
 {
 
+// Per-kernel timers (indices of charm_b200_timing_read).
+enum
+{
+    TIMER_SHS = 0,   // grid synthesis Legendre kernel
+    TIMER_SHA = 1,   // grid analysis Legendre kernel
+    TIMER_SCTR = 2,  // scattered synthesis kernel
+    TIMER_FFT = 3,   // cuFFT along the parallels
+    TIMER_LON = 4,   // direct longitude sums (non-FFT grids)
+    TIMER_PREP = 5,  // seeds, interleave, reductions, nodes
+    TIMER_TABLES = 6,
+    TIMER_COUNT = 7
+};
+
 // Result of an engine call: CHARM_SUCCESS or a CHarm error code with a
 // message.
 struct Status
@@ -27,14 +40,38 @@ Status shs_point(const charm_point *pnt, const charm_shc *shcs,
                  unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
                  double **f);
 
+// Same with the coefficient triangles (degree shc_nmax) and the output
+// ([npar][npoint]) in device memory.
+Status shs_point_dev(const charm_point *pnt, unsigned long shc_nmax,
+                     double mu, double r, const double *d_c,
+                     const double *d_s, unsigned long nmax, int kgrad, int dr,
+                     int dlat, int dlon, double *d_f);
+
 // Analysis on GL/DH grids; overwrites shcs->c, shcs->s.
 Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
                  charm_shc *shcs);
 
+// Same with the grid values and the output triangles (degree shc_nmax) in
+// device memory.
+Status sha_point_dev(const charm_point *pnt, const double *d_f,
+                     unsigned long nmax, double mu, double r,
+                     unsigned long shc_nmax, double *d_c, double *d_s);
+
 // Quadrature grid nodes and weights on the GPU (north to south).
 Status quad_nodes(int type, unsigned long nmax, double *lat, double *w);
 
-// Releases all device memory and plans (called at process exit).
+// Measured FP64 FMA throughput of this device in TFLOP/s.
+Status fp64_peak(double *tflops);
+
+// The library's CUDA stream (cudaStream_t), or null without a device.
+void *stream_handle();
+
+// Per-kernel event timing and launch counting.
+void set_timing(bool on);
+void read_timing(double *ms, unsigned long long *n, unsigned long long *kern,
+                 unsigned long long *ffts);
+
+// Releases all device memory and plans.
 void shutdown();
 
 } // namespace cb

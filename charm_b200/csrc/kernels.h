@@ -109,6 +109,8 @@ cudaError_t launch_gl_nodes(unsigned long nmax, double *lat, double *w,
                             unsigned *status, cudaStream_t st);
 cudaError_t launch_dh_nodes(unsigned long nmax, double *lat, double *w,
                             cudaStream_t st);
+cudaError_t launch_fp64_probe(long long iters, int blocks, int threads,
+                              double *sink, cudaStream_t st);
 cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
                         bool rr, int K, int grid, cudaStream_t st);
 

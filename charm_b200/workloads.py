@@ -50,3 +50,14 @@ def rel_rms(x, ref):
     den = np.sqrt(np.mean(ref ** 2))
     return float(np.sqrt(np.mean((x - ref) ** 2)) / den) if den > 0 else \
         float(np.sqrt(np.mean((x - ref) ** 2)))
+
+
+def coef_rel_rms(c, s, ref_c, ref_s):
+    """Relative RMS difference of a whole coefficient set (C and S together):
+    sqrt(sum dC^2 + dS^2) / sqrt(sum C^2 + S^2).  Normalising S on its own
+    would measure the double-precision noise floor of the smallest
+    coefficients instead of the agreement of the transforms."""
+    d = np.concatenate([np.ravel(c) - np.ravel(ref_c),
+                        np.ravel(s) - np.ravel(ref_s)])
+    r = np.concatenate([np.ravel(ref_c), np.ravel(ref_s)])
+    return float(np.sqrt(np.sum(d * d) / np.sum(r * r)))

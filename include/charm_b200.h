@@ -206,6 +206,49 @@ CHARM_EXTERN extern double charm_glob_threshold2;
 CHARM_EXTERN extern unsigned long charm_glob_polar_optimization_a1;
 CHARM_EXTERN extern double charm_glob_polar_optimization_a2;
 
+/* ------------------------------------------------------------------------- */
+/* Extensions of this library (no counterpart in CHarm's API).               */
+/* ------------------------------------------------------------------------- */
+/* Synthesis with the coefficient triangles and the output in device memory:
+ * d_c, d_s hold order-major triangles of degree shc_nmax (CHarm's layout of
+ * charm_shc.c[0]), d_f receives [npar][npoint] values (npar = 1, 3 or 6 as
+ * for charm_shs_point, charm_shs_point_grad1/2; grad outputs in CHarm's
+ * computation order l, r, p and ll, lr, lp, rr, rp, pp).  kgrad 0 with
+ * (dr, dlat, dlon) selects a single quantity as charm_shs_point_guru.  pnt
+ * stays in host memory.  Errors as charm_shs_point. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_dev(
+    const charm_point *pnt, unsigned long shc_nmax, double mu, double r,
+    const double *d_c, const double *d_s, unsigned long nmax, int kgrad,
+    unsigned dr, unsigned dlat, unsigned dlon, double *d_f, charm_err *err);
+
+/* Analysis with the grid values (d_f, nlat x nlon) and the output triangles
+ * (degree shc_nmax, zero above nmax) in device memory; the coefficients
+ * refer to (mu, r) as charm_sha_point's shcs would. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev(
+    const charm_point *pnt, const double *d_f, unsigned long nmax, double mu,
+    double r, unsigned long shc_nmax, double *d_c, double *d_s,
+    charm_err *err);
+
+/* The CUDA stream the library runs on (a cudaStream_t), or NULL when no
+ * usable device is present. */
+CHARM_EXTERN void *CHARM_CDECL charm_b200_stream(void);
+
+/* Per-kernel event timing: enable (resets the counters) or disable. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_timing(int enable);
+
+/* Reads the accumulated timers: ms[i], count[i] for i < n (0 grid synthesis
+ * kernel, 1 grid analysis kernel, 2 scattered synthesis kernel, 3 cuFFT, 4
+ * direct longitude sums, 5 preparation kernels, 6 tables) and the number of
+ * this library's kernel launches and of cuFFT executions since enabled.
+ * Returns the number of timers available. */
+CHARM_EXTERN int CHARM_CDECL charm_b200_timing_read(
+    double *ms, unsigned long long *count, int n,
+    unsigned long long *kernel_launches, unsigned long long *fft_execs);
+
+/* Measured FP64 fused-multiply-add throughput of the current device,
+ * TFLOP/s (an FMA counted as two flops); negative on error. */
+CHARM_EXTERN double CHARM_CDECL charm_b200_fp64_peak_tflops(void);
+
 #ifdef __cplusplus
 }
 #endif
