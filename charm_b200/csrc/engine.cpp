@@ -266,37 +266,64 @@ void host_r_ri_dm(long long nmax, std::vector<double> &r,
         dm[n] = r[2 * n + 3] * ri[2 * n + 2];
 }
 
-Status tables(Context &c, long long nmax, bool need_en, double2 **ab,
-              double2 **en, double **dm)
+// Recurrence tables of the rescaled recurrence (leg.cuh, tables.cu), built
+// once per maximum degree and kept on the device.
+struct Tabs
+{
+    double2 *tb = nullptr;
+    double *tc = nullptr;
+    double *tmul = nullptr;
+    int ldmul = 0;
+    double *sg = nullptr;
+    double *dm = nullptr;
+};
+
+Status tables(Context &c, long long nmax, Tabs *tab)
 {
     Status st;
     long long T = (nmax + 1) * (nmax + 2) / 2;
-    CB_TRY(dbuf(c, "tab_ab", (size_t)T, ab));
-    if (need_en)
-        CB_TRY(dbuf(c, "tab_en", (size_t)T, en));
-    CB_TRY(dbuf(c, "tab_dm", (size_t)(nmax + 1), dm));
-    bool fresh = (c.tab_nmax != nmax);
-    if (!fresh && (!need_en || c.tab_has_en))
+    tab->ldmul = (int)((nmax + 1 + 63) / 64);
+    CB_TRY(dbuf(c, "tab_b", (size_t)T, &tab->tb));
+    CB_TRY(dbuf(c, "tab_c", (size_t)T, &tab->tc));
+    CB_TRY(dbuf(c, "tab_mul", (size_t)(nmax + 1) * tab->ldmul, &tab->tmul));
+    CB_TRY(dbuf(c, "tab_sg", (size_t)(2 * (nmax + 1)), &tab->sg));
+    CB_TRY(dbuf(c, "tab_dm", (size_t)(nmax + 1), &tab->dm));
+    if (c.tab_nmax == nmax)
         return st;
     std::vector<double> r, ri, dmh;
     host_r_ri_dm(nmax, r, ri, dmh);
-    double *dr = nullptr, *dri = nullptr;
+    // S_m = P_mm(u) / u^m = sqrt(3) prod_{k=1}^{m-1} d_k
+    // (src/leg/leg_func_prepare.c), in extended precision
+    std::vector<double> smm(nmax + 1);
+    long double s = 1.0L;
+    smm[0] = 1.0;
+    for (long long m = 1; m <= nmax; m++)
+    {
+        if (m == 1)
+            s = sqrtl(3.0L);
+        else
+            s *= sqrtl((long double)(2 * m + 1) / (long double)(2 * m));
+        smm[m] = (double)s;
+    }
+    double *dr = nullptr, *dri = nullptr, *dsm = nullptr;
     CB_TRY(dbuf(c, "tab_r", r.size(), &dr));
     CB_TRY(dbuf(c, "tab_ri", ri.size(), &dri));
+    CB_TRY(dbuf(c, "tab_smm", smm.size(), &dsm));
     CB_CUDA(cudaMemcpyAsync(dr, r.data(), r.size() * 8, cudaMemcpyHostToDevice,
                             c.stream), st);
     CB_CUDA(cudaMemcpyAsync(dri, ri.data(), ri.size() * 8,
                             cudaMemcpyHostToDevice, c.stream), st);
-    CB_CUDA(cudaMemcpyAsync(*dm, dmh.data(), dmh.size() * 8,
+    CB_CUDA(cudaMemcpyAsync(dsm, smm.data(), smm.size() * 8,
+                            cudaMemcpyHostToDevice, c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(tab->dm, dmh.data(), dmh.size() * 8,
                             cudaMemcpyHostToDevice, c.stream), st);
     {
         Scope sc(c, TIMER_TABLES);
-        CB_CUDA(launch_tables(nmax, dr, dri, *ab, need_en ? *en : nullptr,
-                              c.stream), st);
+        CB_CUDA(launch_tables(nmax, dr, dri, dsm, tab->tb, tab->tc, tab->tmul,
+                              tab->ldmul, tab->sg, c.stream), st);
     }
     // the host vectors must outlive the copies
     CB_CUDA(cudaStreamSynchronize(c.stream), st);
-    c.tab_has_en = fresh ? need_en : (c.tab_has_en || need_en);
     c.tab_nmax = nmax;
     return st;
 }
@@ -568,7 +595,7 @@ struct CoefIn
 };
 
 Status coef_to_device(Context &c, const CoefIn &in, unsigned long nmax,
-                      double2 **dcs)
+                      const Tabs &tab, double2 **dcs)
 {
     Status st;
     const long long Ts = (long long)(in.nmax + 1) * (in.nmax + 2) / 2;
@@ -585,8 +612,8 @@ Status coef_to_device(Context &c, const CoefIn &in, unsigned long nmax,
         src_s = raw + Ts;
     }
     Scope sc(c, TIMER_PREP);
-    CB_CUDA(launch_interleave((long long)nmax, (long long)in.nmax, src_c,
-                              src_s, *dcs, c.stream), st);
+    CB_CUDA(launch_scale_cs((long long)nmax, (long long)in.nmax, src_c, src_s,
+                            tab.tc, *dcs, c.stream), st);
     return st;
 }
 
@@ -684,23 +711,10 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     const int *drn = reinterpret_cast<const int *>(drho + np);
     const int *drs = drn + np;
 
-    bool need_en = (kgrad > 0) || (dlat > 0);
-    double2 *ab = nullptr, *en = nullptr;
-    double *dm = nullptr;
-    CB_TRY(tables(c, (long long)nmax, need_en, &ab, &en, &dm));
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
     double2 *dcs = nullptr;
-    CB_TRY(coef_to_device(c, in, nmax, &dcs));
-
-    // sectorial seeds
-    double *psx = nullptr;
-    int *pse = nullptr;
-    CB_TRY(dbuf(c, "psx", (size_t)(nmax + 1) * np, &psx));
-    CB_TRY(dbuf(c, "pse", (size_t)(nmax + 1) * np, &pse));
-    {
-        Scope sc(c, TIMER_PREP);
-        CB_CUDA(launch_sectorial((long long)nmax, np, du, drho, r_eq ? 0 : 1,
-                                 dorder, dm, psx, pse, c.stream), st);
-    }
+    CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
 
     // lumped coefficients
     const int ldf = use_fft ? (int)(nlon / 2 + 1) : (int)(nmax + 1);
@@ -720,11 +734,11 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     A.npairs = np;
     A.ntiles = ntiles;
     A.nitems = (long long)(nmax + 1) * ntiles;
-    A.ab = ab;
+    A.tb = tab.tb;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
     A.cs = dcs;
-    A.en = en;
-    A.psx = psx;
-    A.pse = pse;
     A.t = dt;
     A.u = du;
     A.rho = drho;
@@ -802,12 +816,10 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
     double mur;
     int dorder, npar;
     mur_dorder(in.mu, in.r, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
-    bool need_en = (kgrad > 0) || (dlat > 0);
-    double2 *ab = nullptr, *en = nullptr;
-    double *dm = nullptr;
-    CB_TRY(tables(c, (long long)nmax, need_en, &ab, &en, &dm));
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
     double2 *dcs = nullptr;
-    CB_TRY(coef_to_device(c, in, nmax, &dcs));
+    CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
     double *dpts = nullptr;
     CB_TRY(dbuf(c, "sctr_pts", 3 * npt, &dpts));
     CB_CUDA(cudaMemcpyAsync(dpts, pnt->lat, npt * 8, cudaMemcpyHostToDevice,
@@ -828,10 +840,12 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
     A.nmax = (long long)nmax;
     A.npoint = (long long)npt;
     A.ntiles = ((long long)npt + 32 * K - 1) / (32 * K);
-    A.ab = ab;
+    A.tb = tab.tb;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
     A.cs = dcs;
-    A.en = en;
-    A.dm = dm;
+    A.dm = tab.dm;
     A.lat = dpts;
     A.lon = dpts + npt;
     A.r = dpts + 2 * npt;
@@ -909,9 +923,8 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     const int *drn = reinterpret_cast<const int *>(dcsw + np);
     const int *drs = drn + np;
 
-    double2 *ab = nullptr, *en = nullptr;
-    double *dm = nullptr;
-    CB_TRY(tables(c, (long long)nmax, false, &ab, &en, &dm));
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
 
     // grid on the device and r2c along the parallels
     const double *fg = d_fin;
@@ -940,16 +953,6 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         }
     }
 
-    double *psx = nullptr;
-    int *pse = nullptr;
-    CB_TRY(dbuf(c, "psx", (size_t)(nmax + 1) * np, &psx));
-    CB_TRY(dbuf(c, "pse", (size_t)(nmax + 1) * np, &pse));
-    {
-        Scope sc(c, TIMER_PREP);
-        CB_CUDA(launch_sectorial((long long)nmax, np, du, nullptr, 0, 0, dm,
-                                 psx, pse, c.stream), st);
-    }
-
     unsigned *d_status;
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
@@ -970,9 +973,10 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     A.ngroups = (int)G;
     A.tiles_per_group = tpg;
     A.nitems = (long long)(nmax + 1) * G;
-    A.ab = ab;
-    A.psx = psx;
-    A.pse = pse;
+    A.tb = tab.tb;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
     A.t = dt;
     A.u = du;
     A.row_n = drn;
@@ -1025,7 +1029,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     {
         Scope sc(c, TIMER_PREP);
         CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T,
-                                  part, dres, oc, os, c.stream), st);
+                                  part, tab.tc, dres, oc, os, c.stream), st);
     }
     if (!d_c)
     {

@@ -8,18 +8,19 @@ namespace cb
 {
 
 // Grid synthesis: lumped coefficients out[q][row][m] of every output
-// component q, row and order m (see shs_grid.cu).
+// component q, row and order m (shs_grid.cu).  tb, tmul, sg are the
+// recurrence tables of leg.cuh / tables.cu.
 struct ShsGridArgs
 {
     long long nmax;
     int npairs;            // evaluated latitudes (north rows of the pairs)
     int ntiles;            // latitude tiles per order
     long long nitems;      // (nmax + 1) * ntiles
-    const double2 *ab;     // (a_nm, b_nm), order-major triangle
-    const double2 *cs;     // (C_nm, S_nm)
-    const double2 *en;     // (e_nm, n), derivatives only
-    const double *psx;     // sectorial seeds [m][pair] mantissa
-    const int *pse;        // sectorial seeds [m][pair] binary exponent
+    const double2 *tb;     // (beta_n, e_n / a_n) per (n, m), order-major
+    const double *tmul;    // chunk entry multipliers [m][chunk]
+    int ldmul;
+    const double *sg;      // per m: (S_m 2^g_0, g_0)
+    const double2 *cs;     // (ct C_nm, ct S_nm)
     const double *t;       // sin(lat) per pair
     const double *u;       // cos(lat) per pair
     const double *rho;     // R / r per pair (r != R only)
@@ -45,9 +46,10 @@ struct ShaGridArgs
     int ngroups;           // tile groups per order (partial sums)
     int tiles_per_group;
     long long nitems;      // (nmax + 1) * ngroups
-    const double2 *ab;
-    const double *psx;
-    const int *pse;
+    const double2 *tb;
+    const double *tmul;
+    int ldmul;
+    const double *sg;
     const double *t;
     const double *u;
     const int *row_n;
@@ -56,7 +58,7 @@ struct ShaGridArgs
     const double *cw_s;    // same for the mirror row (0 when none)
     const double2 *F;      // r2c output [nlat][ldF]
     int ldF;
-    double2 *part;         // [ngroups][T] (C, S) partial sums
+    double2 *part;         // [ngroups][T] (C, S) partial sums in R~ units
     double polar_thr;
     unsigned long long *counter;
     unsigned *status;
@@ -68,10 +70,12 @@ struct SctrArgs
     long long nmax;
     long long npoint;
     long long ntiles;
-    const double2 *ab;
+    const double2 *tb;
+    const double *tmul;
+    int ldmul;
+    const double *sg;
+    const double *dm;      // sectorial factors d_m (leg_func_dm.c)
     const double2 *cs;
-    const double2 *en;
-    const double *dm;
     const double *lat;
     const double *lon;
     const double *r;       // radius per point (read when r != R)
@@ -85,14 +89,12 @@ struct SctrArgs
 };
 
 cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
-                          double2 *ab, double2 *en, cudaStream_t st);
-cudaError_t launch_interleave(long long nmax, long long shc_nmax,
-                              const double *c, const double *s, double2 *cs,
-                              cudaStream_t st);
-cudaError_t launch_sectorial(long long nmax, int np, const double *u,
-                             const double *rho, int use_rho, int dorder,
-                             const double *dm, double *psx, int *pse,
-                             cudaStream_t st);
+                          const double *smm, double2 *tb, double *tc,
+                          double *tmul, int ldmul, double *sg,
+                          cudaStream_t st);
+cudaError_t launch_scale_cs(long long nmax, long long shc_nmax,
+                            const double *c, const double *s,
+                            const double *tc, double2 *cs, cudaStream_t st);
 cudaError_t launch_shs_grid(const ShsGridArgs &A, int kgrad, int dr,
                             int dlat, bool rr, int K, int grid,
                             cudaStream_t st);
@@ -103,8 +105,8 @@ cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
                             cudaStream_t st);
 cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                               long long T, const double2 *part,
-                              const double *rescale, double *c, double *s,
-                              cudaStream_t st);
+                              const double *tc, const double *rescale,
+                              double *c, double *s, cudaStream_t st);
 cudaError_t launch_gl_nodes(unsigned long nmax, double *lat, double *w,
                             unsigned *status, cudaStream_t st);
 cudaError_t launch_dh_nodes(unsigned long nmax, double *lat, double *w,

@@ -3,11 +3,11 @@
 // Work item = tile of 32*K points; one warp per item.  The warp walks all
 // orders m = 0..nmax: the sectorial seed follows CHarm's sequence
 // (src/leg/leg_func_prepare.c) in registers, the degree loop streams the
-// whole coefficient triangle (a_nm, b_nm), (C_nm, S_nm) and, for
-// derivatives, (e_nm, n) through a two-stage shared-memory ring filled by
-// 1-D bulk copies, and each order's lumped coefficients are folded into
-// f += a_m cos(m lon) + b_m sin(m lon) (shs_point_sctr.c:599-641).  Every
-// point is written exactly once, so no reduction is needed.
+// whole recurrence table and scaled coefficient triangle through a
+// two-stage shared-memory ring filled by 1-D bulk copies and runs the
+// rescaled recurrence of leg.cuh, and each order's lumped coefficients are
+// folded into f += a_m cos(m lon) + b_m sin(m lon)
+// (shs_point_sctr.c:599-641).  Every point is written exactly once.
 #include <cstdint>
 
 #include "common.cuh"
@@ -24,12 +24,12 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
     using Q = Qty<KIND, DL, DR>;
     constexpr int NQ = Q::NQ;
     constexpr int ND = Q::NEEDD;
-    constexpr int NSLOT = ND > 0 ? 3 : 2;
+    constexpr bool NEEDN = (ND > 0) || (KIND == 0 && DR > 0) || (KIND > 0);
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = threadIdx.x >> 5;
-    const size_t stage_bytes = (size_t)NSLOT * LEG_CHUNK * sizeof(double2);
+    const size_t stage_bytes = 2 * LEG_CHUNK * sizeof(double2);
     unsigned char *wbase =
         smem_raw + (size_t)warp * (2 * stage_bytes + 2 * sizeof(uint64_t));
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + 2 * stage_bytes);
@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
     const double BIG = 0x1p960, BIGI = 0x1p-960;
     const double BIGS = 0x1p480, BIGSI = 0x1p-480;
     const double ROOT3 = 1.73205080756887729353;
+    const int dorder = KIND == 0 ? (DR + DL + A.dlon) : KIND;
     bool failed = false;
 
     for (;;)
@@ -84,20 +85,19 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
             u2r[k] = ur * ur;
             xs[k] = 1.0;
             ixs[k] = 0;
-            rp[k] = 1.0;
+            // (R/r)^(1 + dorder) for m = 0 (src/shs/shs_rpows.c)
+            double r0 = 1.0;
+            for (int i = 0; i < 1 + dorder; i++)
+                r0 *= rh;
+            rp[k] = r0;
 #pragma unroll
             for (int q = 0; q < NQ; q++)
                 fa[q][k] = 0.0;
         }
-        // (R/r)^(1 + dorder) for m = 0 (src/shs/shs_rpows.c)
-        const int dorder = KIND == 0 ? (DR + DL + A.dlon) : KIND;
-#pragma unroll
-        for (int k = 0; k < K; k++)
-            for (int i = 0; i < 1 + dorder; i++)
-                rp[k] *= rho1[k];
 
         // chunk stream over the whole triangle, column by column
-        int im = 0, ij = 0;               // next chunk to issue
+        long long im = 0;
+        int ij = 0;                      // next chunk to issue
         auto ncol_of = [&](long long m) { return N - m + 1; };
         auto nch_of = [&](long long m) {
             return (int)((ncol_of(m) + LEG_CHUNK - 1) / LEG_CHUNK);
@@ -112,11 +112,9 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                 if (cnt > LEG_CHUNK)
                     cnt = LEG_CHUNK;
                 unsigned bytes = (unsigned)(cnt * sizeof(double2));
-                mbar_arrive_expect_tx(&bar[s], bytes * NSLOT);
-                bulk_g2s(stg[s], A.ab + off, bytes, &bar[s]);
+                mbar_arrive_expect_tx(&bar[s], 2 * bytes);
+                bulk_g2s(stg[s], A.tb + off, bytes, &bar[s]);
                 bulk_g2s(stg[s] + LEG_CHUNK, A.cs + off, bytes, &bar[s]);
-                if (ND > 0)
-                    bulk_g2s(stg[s] + 2 * LEG_CHUNK, A.en + off, bytes, &bar[s]);
             }
             if (++ij >= nch_of(im))
             {
@@ -130,7 +128,9 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
 
         for (long long m = 0; m <= N && !failed; m++)
         {
-            // sectorial seed of order m (leg_func_prepare.c:18-69)
+            // sectorial seed of order m (leg_func_prepare.c:18-69) times the
+            // chunk-0 power of two of the rescaled recurrence
+            const int g0 = (int)A.sg[2 * m + 1];
             double x[K], y[K];
             int E[K];
             bool skip = A.polar_thr >= 0.0;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                 if (m >= 1)
                     rp[k] *= rho1[k];
                 x[k] = (m == 0) ? rp[k] : (RR ? xs[k] * rp[k] : xs[k]);
-                E[k] = (m == 0) ? 0 : 960 * ixs[k];
+                E[k] = ((m == 0) ? 0 : 960 * ixs[k]) + g0;
                 y[k] = 0.0;
                 leg_seed_normalise(x[k], E[k]);
                 if (pk[k] < A.npoint &&
@@ -181,7 +181,6 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
             const double m2 = md * md;
             const long long ncol = ncol_of(m);
             const int nch = nch_of(m);
-            int since_fix = 0;
             for (int j = 0; j < nch; j++)
             {
                 const int s = consumed & 1;
@@ -191,19 +190,29 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                     break;
                 }
                 phase[s] ^= 1u;
+                if (j > 0)
+                {
+                    const double mul = A.tmul[(size_t)m * A.ldmul + j];
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                    {
+                        x[k] *= mul;
+                        y[k] *= mul;
+                    }
+                }
                 long long cntl = ncol - (long long)j * LEG_CHUNK;
                 const int cnt = cntl > LEG_CHUNK ? LEG_CHUNK : (int)cntl;
-                const double2 *sab = stg[s];
+                const double2 *stb = stg[s];
                 const double2 *scs = stg[s] + LEG_CHUNK;
-                const double2 *sen = stg[s] + 2 * LEG_CHUNK;
+                const long long nbase = m + (long long)j * LEG_CHUNK;
                 if (!skip)
                 {
                     int i = 0;
                     if (j == 0)
                     {
                         // n = m
-                        double2 c = scs[0];
-                        double np1 = md + 1.0;
+                        const double2 c = scs[0];
+                        const double np1 = md + 1.0;
 #pragma unroll
                         for (int k = 0; k < K; k++)
                         {
@@ -221,25 +230,24 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                                 acc.v[q][1][0][k] = fma(v, c.y, acc.v[q][1][0][k]);
                             }
                         }
-                        // n = m + 1
+                        // n = m + 1 (beta = 0)
                         if (cnt > 1)
                         {
-                            double a = sab[1].x;
-                            double2 c1 = scs[1];
-                            double e = ND > 0 ? sen[1].x : 0.0;
-                            double nd = md + 1.0, np2 = nd + 1.0;
+                            const double et = stb[1].y;
+                            const double2 c1 = scs[1];
+                            const double nd = md + 1.0, np2 = nd + 1.0;
 #pragma unroll
                             for (int k = 0; k < K; k++)
                             {
                                 double xo = x[k];
-                                double z = (a * tq[k]) * xo;
+                                double z = tq[k] * xo;
                                 y[k] = xo;
                                 x[k] = z;
                                 double dp = 0.0, ddp = 0.0;
                                 if (ND >= 1)
                                     dp = (m == 0)
-                                             ? (ROOT3 * uk[k]) * (RR ? rho1[k] * xo : xo)
-                                             : fma(e * urr[k], xo, -((nd * tu[k]) * z));
+                                             ? (uk[k] * rho1[k]) * xo
+                                             : fma(et * urr[k], xo, -((nd * tu[k]) * z));
                                 if (ND >= 2)
                                     ddp = (m == 0) ? -z
                                                    : fma(tu[k], dp,
@@ -254,53 +262,51 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                             }
                         }
                         i = 2;
-                        since_fix = 2;
                     }
+#pragma unroll 4
                     for (; i < cnt; i++)
                     {
-                        double2 ab = sab[i];
-                        double2 c = scs[i];
-                        double2 en = ND > 0 ? sen[i] : make_double2(0.0, 0.0);
-                        double nd = ND > 0 ? en.y
-                                           : (double)(m + (long long)j * LEG_CHUNK + i);
-                        double np1 = nd + 1.0;
+                        const double2 tbv = stb[i];
+                        const double2 c = scs[i];
+                        const double nd = NEEDN ? (double)(nbase + i) : 0.0;
+                        const double np1 = nd + 1.0;
 #pragma unroll
                         for (int k = 0; k < K; k++)
                         {
-                            double xo = x[k];
-                            double by = RR ? ab.y * (rho2[k] * y[k]) : ab.y * y[k];
-                            double z = fma(ab.x * tq[k], xo, -by);
+                            const double xo = x[k];
+                            const double by = RR ? tbv.x * (rho2[k] * y[k])
+                                                 : tbv.x * y[k];
+                            const double z = fma(tq[k], xo, -by);
                             y[k] = xo;
                             x[k] = z;
                             double dp = 0.0, ddp = 0.0;
                             if (ND >= 1)
-                                dp = fma(en.x * urr[k], xo, -((nd * tu[k]) * z));
+                                dp = fma(tbv.y * urr[k], xo, -((nd * tu[k]) * z));
                             if (ND >= 2)
                                 ddp = fma(tu[k], dp,
                                           fma(m2, u2r[k], -(nd * np1)) * z);
 #pragma unroll
                             for (int q = 0; q < NQ; q++)
                             {
-                                double v = (KIND == 0 && DL == 0 && DR == 0)
-                                               ? z
-                                               : Q::val(q, z, dp, ddp, np1);
+                                const double v = (KIND == 0 && DL == 0 && DR == 0)
+                                                     ? z
+                                                     : Q::val(q, z, dp, ddp, np1);
                                 acc.v[q][0][0][k] = fma(v, c.x, acc.v[q][0][0][k]);
                                 acc.v[q][1][0][k] = fma(v, c.y, acc.v[q][1][0][k]);
                             }
                         }
-                        if (any_scaled && ++since_fix >= LEG_FIX_EVERY)
-                        {
-                            since_fix = 0;
-                            bool still = false;
+                    }
+                    if (any_scaled)
+                    {
+                        bool still = false;
 #pragma unroll
-                            for (int k = 0; k < K; k++)
-                            {
-                                if (leg_fixup(x[k], y[k], E[k]))
-                                    acc.zero_k(k);
-                                still |= (E[k] != 0);
-                            }
-                            any_scaled = __any_sync(0xffffffffu, still);
+                        for (int k = 0; k < K; k++)
+                        {
+                            if (leg_fixup(x[k], y[k], E[k]))
+                                acc.zero_k(k);
+                            still |= (E[k] != 0);
                         }
+                        any_scaled = __any_sync(0xffffffffu, still);
                     }
                 }
                 __syncwarp();
@@ -348,11 +354,9 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
 template <int KIND, int DL, int DR, int K, bool RR>
 static cudaError_t launch_s1(const SctrArgs &A, int grid, cudaStream_t st)
 {
-    constexpr int ND = Qty<KIND, DL, DR>::NEEDD;
-    constexpr int NSLOT = ND > 0 ? 3 : 2;
     const int warps = 4;
     size_t smem = (size_t)warps *
-                  (2 * NSLOT * LEG_CHUNK * sizeof(double2) + 2 * sizeof(uint64_t));
+                  (2 * 2 * LEG_CHUNK * sizeof(double2) + 2 * sizeof(uint64_t));
     k_sctr<KIND, DL, DR, K, RR><<<grid, warps * 32, smem, st>>>(A);
     return cudaGetLastError();
 }

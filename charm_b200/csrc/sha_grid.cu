@@ -3,13 +3,13 @@
 // the grid rows.
 //
 // Work item = (order m, group g of latitude tiles); one warp per item.  For
-// each tile of 32*K latitude pairs the warp runs the recurrence over n and
-// forms, per degree, the lane partial sum over its K pairs of
-// P_nm(t) * {a, b}^(n+m parity).  Every 32 degrees the warp transpose-reduce
-// leaves lane l with the warp total of degree n0 + l, which is added to the
-// group's partial column (plain read-modify-write: the warp owns it).  A
-// second kernel sums the groups in a fixed order, so results are
-// deterministic.
+// each tile of 32*K latitude pairs the warp runs the rescaled recurrence of
+// leg.cuh over n and forms, per degree, the lane partial sum over its K
+// pairs of R~_n(t) * {a, b}^(n+m parity).  Every 32 degrees the warp
+// transpose-reduce leaves lane l with the warp total of degree n0 + l,
+// which is added to the group's partial column (plain read-modify-write:
+// the warp owns it).  k_sha_reduce (tables.cu) sums the groups in a fixed
+// order and applies ct_n, so results are deterministic.
 #include <cstdint>
 
 #include "common.cuh"
@@ -96,6 +96,7 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
         int tile1 = tile0 + A.tiles_per_group;
         if (tile1 > A.ntiles)
             tile1 = A.ntiles;
+        const double sigma = A.sg[2 * m];
         bool stored = false;
 
         for (int tile = tile0; tile < tile1 && !failed; tile++)
@@ -111,12 +112,16 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                 bool valid = p < np;
                 t[k] = valid ? A.t[p] : 0.0;
                 double u = valid ? A.u[p] : 1.0;
-                x[k] = valid ? A.psx[(size_t)m * np + p] : 0.0;
-                E[k] = valid ? A.pse[(size_t)m * np + p] : 0;
                 y[k] = 0.0;
+                if (valid)
+                    leg_seed(sigma, u, 1.0, false, m, 0, x[k], E[k]);
+                else
+                {
+                    x[k] = 0.0;
+                    E[k] = 0;
+                }
                 if (valid && !((double)m - (double)N * u > A.polar_thr))
                     skip = false;
-                leg_seed_normalise(x[k], E[k]);
                 // scaled latitudes contribute nothing until they switch
                 pa[k] = (E[k] == 0) ? load_pair_A(A, p, m)
                                     : PairA{0.0, 0.0, 0.0, 0.0};
@@ -137,7 +142,7 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                         cnt = LEG_CHUNK;
                     unsigned bytes = (unsigned)(cnt * sizeof(double2));
                     mbar_arrive_expect_tx(&bar[s], bytes);
-                    bulk_g2s(stg[s], A.ab + c0 + (long long)j * LEG_CHUNK,
+                    bulk_g2s(stg[s], A.tb + c0 + (long long)j * LEG_CHUNK,
                              bytes, &bar[s]);
                 }
             };
@@ -154,16 +159,26 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                     break;
                 }
                 phase[s] ^= 1u;
+                if (j > 0)
+                {
+                    const double mul = A.tmul[(size_t)m * A.ldmul + j];
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                    {
+                        x[k] *= mul;
+                        y[k] *= mul;
+                    }
+                }
                 long long cntl = ncol - (long long)j * LEG_CHUNK;
                 const int cnt = cntl > LEG_CHUNK ? LEG_CHUNK : (int)cntl;
-                double2 *sab = stg[s];
-                // degrees beyond nmax read zero coefficients
+                double2 *stb = stg[s];
+                // degrees beyond nmax read beta = 0 and contribute 0
                 if (cnt < LEG_CHUNK)
                 {
                     if ((int)lane >= cnt)
-                        sab[lane] = make_double2(0.0, 0.0);
+                        stb[lane] = make_double2(0.0, 0.0);
                     if ((int)lane + 32 >= cnt)
-                        sab[lane + 32] = make_double2(0.0, 0.0);
+                        stb[lane + 32] = make_double2(0.0, 0.0);
                     __syncwarp();
                 }
 #pragma unroll 1
@@ -172,7 +187,7 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                     const long long n0 = m + (long long)j * LEG_CHUNK + 32 * half;
                     if (n0 > N)
                         break;
-                    const double2 *blk = sab + 32 * half;
+                    const double2 *blk = stb + 32 * half;
                     const bool first = (j == 0 && half == 0);
                     double pc[5], ps[5];
                     double outc = 0.0, outs = 0.0;
@@ -191,11 +206,11 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                         }
                         else
                         {
-                            double2 ab = blk[jj];
+                            const double beta = blk[jj].x;
 #pragma unroll
                             for (int k = 0; k < K; k++)
                             {
-                                double z = fma(ab.x * t[k], x[k], -(ab.y * y[k]));
+                                double z = fma(t[k], x[k], -(beta * y[k]));
                                 y[k] = x[k];
                                 x[k] = z;
                                 if ((jj & 1) == 0)
@@ -235,21 +250,6 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                                 }
                             }
                         }
-                        if ((jj & 15) == 15 && any_scaled)
-                        {
-                            bool still = false;
-#pragma unroll
-                            for (int k = 0; k < K; k++)
-                            {
-                                if (leg_fixup(x[k], y[k], E[k]))
-                                {
-                                    int p = tile * (32 * K) + k * 32 + (int)lane;
-                                    pa[k] = load_pair_A(A, p, m);
-                                }
-                                still |= (E[k] != 0);
-                            }
-                            any_scaled = __any_sync(0xffffffffu, still);
-                        }
                     }
                     const long long n = n0 + lane;
                     if (n <= N)
@@ -263,6 +263,21 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                         else
                             *dst = make_double2(outc, outs);
                     }
+                }
+                if (any_scaled)
+                {
+                    bool still = false;
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                    {
+                        if (leg_fixup(x[k], y[k], E[k]))
+                        {
+                            int p = tile * (32 * K) + k * 32 + (int)lane;
+                            pa[k] = load_pair_A(A, p, m);
+                        }
+                        still |= (E[k] != 0);
+                    }
+                    any_scaled = __any_sync(0xffffffffu, still);
                 }
                 __syncwarp();
                 if (j + 2 < nchunks)
@@ -283,41 +298,6 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
     }
 }
 
-// Sums the group partials and writes C, S in the caller's layout (degree
-// shc_nmax triangle), zero above nmax, with the degree-wise rescaling of
-// src/shc/shc_rescale.c applied (rescale[n], or none when null).
-__global__ void k_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
-                             long long T, const double2 *__restrict__ part,
-                             const double *__restrict__ rescale, double *c,
-                             double *s)
-{
-    long long m = blockIdx.x;
-    if (m > shc_nmax)
-        return;
-    long long d0 = tri_col0(shc_nmax, m);
-    long long c0 = tri_col0(nmax, m);
-    for (long long n = m + threadIdx.x; n <= shc_nmax; n += blockDim.x)
-    {
-        double vc = 0.0, vs = 0.0;
-        if (m <= nmax && n <= nmax)
-        {
-            for (int g = 0; g < ngroups; g++)
-            {
-                double2 v = part[(size_t)g * T + c0 + n - m];
-                vc += v.x;
-                vs += v.y;
-            }
-            if (rescale)
-            {
-                vc *= rescale[n];
-                vs *= rescale[n];
-            }
-        }
-        c[d0 + n - m] = vc;
-        s[d0 + n - m] = vs;
-    }
-}
-
 cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
                             cudaStream_t st)
 {
@@ -330,16 +310,6 @@ cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
         k_sha_grid<2><<<grid, warps * 32, smem, st>>>(A);
     else
         k_sha_grid<1><<<grid, warps * 32, smem, st>>>(A);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
-                              long long T, const double2 *part,
-                              const double *rescale, double *c, double *s,
-                              cudaStream_t st)
-{
-    k_sha_reduce<<<(int)(shc_nmax + 1), 128, 0, st>>>(nmax, shc_nmax, ngroups,
-                                                       T, part, rescale, c, s);
     return cudaGetLastError();
 }
 

@@ -62,10 +62,16 @@ def test_dh_above_sphere_vs_oracle(cb, grid):
     f = cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s), N)
     fo = orc.shs_point(orc.dh(N, r, kind), ora_shc(N, c, s), N)[0]
     assert rel_rms(f, fo) <= TOL
-    out = cb.sha_point(p, f, N, GM, R_EARTH)
-    ref = orc.sha_point(orc.dh(N, r, kind), f, N, GM, R_EARTH)
+    # the transforms compared on the analysis sphere (no rescaling)
+    out = cb.sha_point(p, f, N, GM, r)
+    ref = orc.sha_point(orc.dh(N, r, kind), f, N, GM, r)
     assert coef_rel_rms(out.c, out.s, ref.c, ref.s) <= TOL
-    assert coef_rel_rms(out.c, out.s, c, s) <= 1e-12
+    # round trip referred back to R: CHarm's rescaling by (r/R)^n
+    # (src/shc/shc_rescale.c) amplifies the double-precision noise of the
+    # field by up to (r/R)^N ~ 2e3 at degree 200, hence the looser bound
+    back = cb.sha_point(p, f, N, GM, R_EARTH)
+    amp = (r / R_EARTH) ** N
+    assert coef_rel_rms(back.c, back.s, c, s) <= 1e-14 * amp
 
 
 @pytest.mark.parametrize("kind", ["grad1", "grad2"] + [k for k in gd.GURU])
