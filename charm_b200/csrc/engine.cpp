@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -59,8 +60,9 @@ struct Context
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
     long long tab_nmax = -1;     // recurrence tables of this maximum degree
-    bool tab_has_en = false;
     std::map<std::tuple<int, int, long long>, cufftHandle> plans;
+    std::map<long long, RfftArgs> rffts;   // row transforms by row length
+    std::map<long long, void *> rfft_mem;  // their tables
     std::recursive_mutex mtx;
     // optional per-kernel timing (CUDA events on the library stream)
     bool timing = false;
@@ -370,6 +372,128 @@ Status plan(Context &c, cufftType type, int n, long long batch,
     return st;
 }
 
+// Shared-memory transform of grid rows of length L (rfft.cu), or nullptr
+// when it does not apply: L odd, or a transform length M beyond 9216
+// (the shared memory of one CTA), or CHARM_B200_ROW_FFT=library.
+Status row_fft(Context &c, long long L, const RfftArgs **out)
+{
+    Status st;
+    *out = nullptr;
+    const char *e = std::getenv("CHARM_B200_ROW_FFT");
+    if (e && std::strcmp(e, "library") == 0)
+        return st;
+    auto it = c.rffts.find(L);
+    if (it != c.rffts.end())
+    {
+        *out = it->second.M > 0 ? &it->second : nullptr;
+        return st;
+    }
+    RfftArgs A{};
+    A.M = 0;
+    const long long H = L / 2;
+    auto smooth = [](long long n, int *a, int *b) {
+        *a = *b = 0;
+        while (n > 1 && n % 2 == 0)
+        {
+            n /= 2;
+            (*a)++;
+        }
+        while (n > 1 && n % 3 == 0)
+        {
+            n /= 3;
+            (*b)++;
+        }
+        return n == 1;
+    };
+    int a = 0, b = 0;
+    if (L % 2 == 0 && H >= 8)
+    {
+        if (smooth(H, &a, &b) && a >= 3 && H <= 9216)
+        {
+            A.M = (int)H;
+            A.direct = 1;
+        }
+        else
+        {
+            long long best = 0;
+            for (long long p2 = 8; p2 <= 9216; p2 *= 2)
+                for (long long m = p2; m <= 9216; m *= 3)
+                    if (m >= 2 * H - 1 && (best == 0 || m < best))
+                        best = m;
+            if (best > 0)
+            {
+                A.M = (int)best;
+                A.direct = 0;
+                smooth(best, &a, &b);
+            }
+        }
+    }
+    // 16 values per thread where M allows (M / 16 threads, two CTAs per
+    // SM up to M = 4608), else 8
+    if (A.M > 0)
+    {
+        if (A.M % 16 == 0)
+            A.V = 16;
+        else if (A.M % 8 == 0 && A.M <= 8192)
+            A.V = 8;
+        else
+            A.M = 0;
+    }
+    if (A.M == 0)
+    {
+        c.rffts[L] = A;
+        return st;
+    }
+    A.H = (int)H;
+    // radix 8 passes, then 4, then 2 (powers of two), then 3
+    int p8 = a / 3, p4 = 0, p2 = 0;
+    if (a % 3 == 2)
+        p4 = 1;
+    else if (a % 3 == 1)
+    {
+        if (p8 > 0)
+        {
+            p8--;
+            p4 = 2;
+        }
+        else
+            p2 = 1;
+    }
+    A.npass = make_int4(p8, p4, p2, b);
+    const size_t nM = (size_t)A.M, nH = (size_t)H;
+    const size_t n_tab = nM + (A.direct ? 0 : nH + nM) + nH + 1;
+    void *mem = nullptr;
+    CB_CUDA(cudaMalloc(&mem, n_tab * sizeof(double2)), st);
+    double2 *tw = static_cast<double2 *>(mem);
+    double2 *w = A.direct ? nullptr : tw + nM;
+    double2 *bh = A.direct ? nullptr : w + nH;
+    double2 *ht = A.direct ? tw + nM : bh + nM;
+    A.tw = tw;
+    A.w = w;
+    A.bh = bh;
+    A.ht = ht;
+    // the largest transform of either width, so that no later plan needs
+    // a different limit
+    cudaError_t ce = rfft_set_smem(rfft_smem_bytes(9216));
+    if (ce == cudaSuccess)
+        ce = launch_rfft_tables(A, tw, w, ht, bh, c.stream);
+    if (ce == cudaSuccess)
+        ce = cudaStreamSynchronize(c.stream);
+    if (ce != cudaSuccess)
+    {
+        cudaFree(mem);
+        st.code = CHARM_EFUNCARG;
+        st.msg = std::string("row transform set-up failed: ") +
+                 cudaGetErrorString(ce);
+        return st;
+    }
+    c.launches += A.direct ? 1 : 2;
+    c.rffts[L] = A;
+    c.rfft_mem[L] = mem;
+    *out = &c.rffts[L];
+    return st;
+}
+
 // Triangle pointer of a charm_shc whose columns c[m] lie contiguously as in
 // src/shc/shc_init_chunk.c:126-145 (every charm_shc built by CHarm's
 // constructors), else null.
@@ -517,6 +641,26 @@ int choose_k(int kgrad, int dlat, long long nunits)
     if (nunits >= 1024)
         return 4;
     return nunits >= 64 ? 2 : 1;
+}
+
+// Latitude pairs per lane of the analysis kernel.  Wider tiles amortise
+// the per-degree beta load and the transpose-reduce over more latitudes but
+// lower the resident warps (sha_grid.cu); CHARM_B200_SHA_K (1, 2, 4, 6 or
+// 8) overrides the choice for tuning.
+int choose_k_sha(long long npairs)
+{
+    static const int forced = [] {
+        const char *e = std::getenv("CHARM_B200_SHA_K");
+        int k = e ? std::atoi(e) : 0;
+        return (k == 1 || k == 2 || k == 4 || k == 6 || k == 8) ? k : 0;
+    }();
+    if (forced)
+        return forced;
+    if (npairs < 64)
+        return 1;
+    if (npairs < 1024)
+        return 2;
+    return 4;
 }
 
 Status finish(Context &c, unsigned *d_status)
@@ -720,7 +864,15 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     const int ldf = use_fft ? (int)(nlon / 2 + 1) : (int)(nmax + 1);
     double2 *lc = nullptr;
     CB_TRY(dbuf(c, "lumped", (size_t)npar * nlat * ldf, &lc));
-    if (use_fft && (size_t)ldf > nmax + 1)
+    double *fg = d_f;
+    if (!fg)
+        CB_TRY(dbuf(c, "fgrid", (size_t)npar * nlat * nlon, &fg));
+    const RfftArgs *rf = nullptr;
+    if (use_fft && reinterpret_cast<uintptr_t>(fg) % 16 == 0)
+        CB_TRY(row_fft(c, (long long)nlon, &rf));
+    // the library transform reads the whole half spectrum; the row
+    // transform reads orders <= nmax only
+    if (use_fft && !rf && (size_t)ldf > nmax + 1)
         CB_CUDA(cudaMemsetAsync(lc, 0, (size_t)npar * nlat * ldf * 16,
                                 c.stream), st);
     unsigned *d_status;
@@ -762,10 +914,19 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     }
 
     // longitude sums into the output grid(s)
-    double *fg = d_f;
-    if (!fg)
-        CB_TRY(dbuf(c, "fgrid", (size_t)npar * nlat * nlon, &fg));
-    if (use_fft)
+    if (rf)
+    {
+        RfftArgs R = *rf;
+        R.nrows = (long long)npar * nlat;
+        R.x = fg;
+        R.ldx = (long long)nlon;
+        R.X = lc;
+        R.ldX = ldf;
+        R.kmax = (int)nmax;
+        Scope sc(c, TIMER_FFT);
+        CB_CUDA(launch_rfft(R, true, c.stream), st);
+    }
+    else if (use_fft)
     {
         cufftHandle h;
         CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)npar * nlat, &h));
@@ -939,6 +1100,22 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     const int ldF = (int)(nlon / 2 + 1);
     double2 *F = nullptr;
     CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
+    const RfftArgs *rf = nullptr;
+    if (reinterpret_cast<uintptr_t>(fg) % 16 == 0)
+        CB_TRY(row_fft(c, (long long)nlon, &rf));
+    if (rf)
+    {
+        RfftArgs R = *rf;
+        R.nrows = (long long)nlat;
+        R.x = const_cast<double *>(fg);
+        R.ldx = (long long)nlon;
+        R.X = F;
+        R.ldX = ldF;
+        R.kmax = (int)nmax;
+        Scope sc(c, TIMER_FFT);
+        CB_CUDA(launch_rfft(R, false, c.stream), st);
+    }
+    else
     {
         cufftHandle h;
         CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
@@ -956,7 +1133,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     unsigned *d_status;
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
-    const int K = choose_k(0, 0, np);
+    const int K = choose_k_sha(np);
     const int ntiles = (np + 32 * K - 1) / (32 * K);
     const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
     long long slots = (long long)c.num_sms * 8 * 4;
@@ -1206,6 +1383,10 @@ void shutdown()
     for (auto &kv : c.plans)
         cufftDestroy(kv.second);
     c.plans.clear();
+    for (auto &kv : c.rfft_mem)
+        cudaFree(kv.second);
+    c.rfft_mem.clear();
+    c.rffts.clear();
     for (auto &kv : c.bufs)
         if (kv.second.p)
             cudaFree(kv.second.p);

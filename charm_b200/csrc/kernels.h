@@ -88,6 +88,27 @@ struct SctrArgs
     unsigned *status;
 };
 
+// Real <-> half-spectrum transforms of grid rows of even length L = 2H in
+// shared memory (rfft.cu).
+struct RfftArgs
+{
+    long long nrows;
+    int H;                 // half length
+    int M;                 // FFT length: H (direct) or >= 2H - 1 (Bluestein)
+    int V;                 // values per thread (8 or 16); M / V threads
+    int direct;            // 1: H = 2^a 3^b, no chirp convolution
+    int4 npass;            // passes of FFT_M of radix 8, 4, 2, 3 (in order)
+    const double2 *tw;     // exp(-2 pi i k / M), k < M
+    const double2 *w;      // chirp exp(-i pi n^2 / H), n < H (Bluestein)
+    const double2 *bh;     // FFT_M of the wrapped conjugate chirp, / M
+    const double2 *ht;     // exp(-i pi k / H), k <= H
+    double *x;             // real rows, leading dimension ldx (even)
+    long long ldx;
+    double2 *X;            // half spectra, leading dimension ldX
+    long long ldX;
+    int kmax;              // spectrum entries read (inverse) / written (forward)
+};
+
 cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
                           const double *smm, double2 *tb, double *tc,
                           double *tmul, int ldmul, double *sg,
@@ -115,5 +136,10 @@ cudaError_t launch_fp64_probe(long long iters, int blocks, int threads,
                               double *sink, cudaStream_t st);
 cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
                         bool rr, int K, int grid, cudaStream_t st);
+cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
+                               double2 *ht, double2 *bh, cudaStream_t st);
+size_t rfft_smem_bytes(int M);
+cudaError_t rfft_set_smem(size_t smem);
+cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st);
 
 } // namespace cb

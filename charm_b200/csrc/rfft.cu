@@ -1,0 +1,486 @@
+// Longitude transforms of whole grid rows in shared memory.
+//
+// CHarm hands every grid row to FFTW: a c2r transform of the lumped
+// coefficients in synthesis (src/shs/shs_grd_fft.c) and an r2c transform of
+// the row in analysis (src/sha/sha_point.c, FFTW_FORWARD of the real row).
+// Grid rows of the quadrature grids have an even length L = 2H whose half
+// length H is often not smooth (GL: H = nmax + 1, e.g. 2191 = 7 * 313), so a
+// library FFT falls back to slow multi-pass algorithms.  Here one CTA owns a
+// row and does everything in shared memory:
+//
+//   * real <-> complex of half length: z_j = x_2j + i x_2j+1 and
+//       X_k = (Z_k + conj Z_H-k)/2 - (i/2) e^(-i pi k/H) (Z_k - conj Z_H-k);
+//   * the complex length-H DFT either directly (H = 2^a 3^b) or by
+//     Bluestein's chirp-z algorithm (Bluestein 1970): with
+//     w_n = exp(-i pi n^2 / H),  DFT(z)_k = w_k sum_j (z_j w_j) conj(w_k-j),
+//     a circular convolution of length M >= 2H - 1, M = 2^a 3^b, evaluated
+//     as FFT_M, a pointwise product with the precomputed FFT_M of the chirp,
+//     and a second FFT_M (conjugated in and out, which inverts it);
+//   * FFT_M by in-place Stockham autosort passes of radix 8, 4, 2 and 3:
+//     every thread holds V values across the barrier that separates the
+//     loads of a pass from its stores, so one buffer of M values suffices.
+//     The first pass reads its inputs straight from global memory (with the
+//     chirp applied), and the last pass of the first FFT applies the
+//     pointwise product as it stores.  Element i lives at i + i/8 in shared
+//     memory, which spreads the strided stores of the first pass over all
+//     banks.
+//
+// Both directions are unnormalised, as FFTW's and CHarm's: the synthesis
+// output is sum_k X_k e^(+2 pi i k n / L) over the Hermitian spectrum, and
+// the analysis output is X_k = sum_n x_n e^(-2 pi i k n / L), k <= kmax.
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace cb
+{
+
+namespace
+{
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+__device__ __forceinline__ double2 conj2(double2 a)
+{
+    return make_double2(a.x, -a.y);
+}
+
+__device__ __forceinline__ double2 add2(double2 a, double2 b)
+{
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+
+__device__ __forceinline__ double2 sub2(double2 a, double2 b)
+{
+    return make_double2(a.x - b.x, a.y - b.y);
+}
+
+// -i a
+__device__ __forceinline__ double2 mul_mi(double2 a)
+{
+    return make_double2(a.y, -a.x);
+}
+
+// shared-memory position of element i
+__device__ __forceinline__ int pidx(int i)
+{
+    return i + (i >> 3);
+}
+
+constexpr double RSQRT2 = 0.70710678118654752440;
+constexpr double SQRT3_2 = 0.86602540378443864676;
+
+// In-register forward DFTs, X_k = sum_r v_r exp(-2 pi i r k / R).
+__device__ __forceinline__ void dft2(double2 *v)
+{
+    double2 a = v[0], b = v[1];
+    v[0] = add2(a, b);
+    v[1] = sub2(a, b);
+}
+
+__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2,
+                                     double2 &a3)
+{
+    double2 t0 = add2(a0, a2), t1 = sub2(a0, a2);
+    double2 t2 = add2(a1, a3), t3 = mul_mi(sub2(a1, a3));
+    a0 = add2(t0, t2);
+    a2 = sub2(t0, t2);
+    a1 = add2(t1, t3);
+    a3 = sub2(t1, t3);
+}
+
+__device__ __forceinline__ void dft8(double2 *v)
+{
+    // even / odd halves, then one radix-2 step with W8^k
+    double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4(e0, e1, e2, e3);
+    dft4(o0, o1, o2, o3);
+    double2 w1 = make_double2((o1.x + o1.y) * RSQRT2, (o1.y - o1.x) * RSQRT2);
+    double2 w2 = mul_mi(o2);
+    double2 w3 = make_double2((o3.y - o3.x) * RSQRT2, -(o3.x + o3.y) * RSQRT2);
+    v[0] = add2(e0, o0);
+    v[4] = sub2(e0, o0);
+    v[1] = add2(e1, w1);
+    v[5] = sub2(e1, w1);
+    v[2] = add2(e2, w2);
+    v[6] = sub2(e2, w2);
+    v[3] = add2(e3, w3);
+    v[7] = sub2(e3, w3);
+}
+
+__device__ __forceinline__ void dft3(double2 *v)
+{
+    double2 t = add2(v[1], v[2]);
+    double2 d = sub2(v[1], v[2]);
+    double2 h = make_double2(fma(-0.5, t.x, v[0].x), fma(-0.5, t.y, v[0].y));
+    double2 q = mul_mi(make_double2(SQRT3_2 * d.x, SQRT3_2 * d.y));
+    v[0] = add2(v[0], t);
+    v[1] = add2(h, q);
+    v[2] = sub2(h, q);
+}
+
+template <int R>
+__device__ __forceinline__ void dft(double2 *v)
+{
+    if constexpr (R == 2)
+        dft2(v);
+    else if constexpr (R == 3)
+        dft3(v);
+    else if constexpr (R == 4)
+        dft4(v[0], v[1], v[2], v[3]);
+    else
+        dft8(v);
+}
+
+// Input of the first pass: element i of the sequence to transform.
+struct SrcSmem
+{
+    const double2 *s;
+    __device__ __forceinline__ double2 operator()(int i) const
+    {
+        return s[pidx(i)];
+    }
+};
+
+// One Stockham pass of radix R over s[0..M): butterfly j reads element
+// j + r M/R (twiddled by exp(-2 pi i (j mod Ns) r / (Ns R))) and writes its
+// R outputs to elements (j - j mod Ns) R + j mod Ns + r Ns.  The first pass
+// (Ns = 1, no twiddles) reads through `src`; a non-null `bh` multiplies the
+// stored outputs by bh and conjugates them.
+template <int R, int V, class Src>
+__device__ __forceinline__ void stockham_pass(double2 *s,
+                                              const double2 *__restrict__ tw,
+                                              int M, int Ns, int tid, int T,
+                                              bool first, const Src &src,
+                                              const double2 *__restrict__ bh)
+{
+    constexpr int BPT = (V + R - 1) / R;
+    const int nb = M / R;
+    const int step = M / (Ns * R);
+    double2 v[BPT][R];
+    if (first)
+    {
+#pragma unroll
+        for (int c = 0; c < BPT; c++)
+        {
+            const int j = tid + c * T;
+            if (j < nb)
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    v[c][r] = src(j + r * nb);
+                dft<R>(v[c]);
+            }
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int c = 0; c < BPT; c++)
+        {
+            const int j = tid + c * T;
+            if (j < nb)
+            {
+                const int k = j % Ns;
+                v[c][0] = s[pidx(j)];
+#pragma unroll
+                for (int r = 1; r < R; r++)
+                    v[c][r] = cmul(s[pidx(j + r * nb)],
+                                   __ldg(&tw[k * r * step]));
+                dft<R>(v[c]);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < BPT; c++)
+    {
+        const int j = tid + c * T;
+        if (j < nb)
+        {
+            const int k = j % Ns;
+            const int d = (j - k) * R + k;
+            if (bh)
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    s[pidx(d + r * Ns)] =
+                        conj2(cmul(v[c][r], __ldg(&bh[d + r * Ns])));
+            }
+            else
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    s[pidx(d + r * Ns)] = v[c][r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Forward FFT of length M = 8^n8 4^n4 2^n2 3^n3 (passes in that order) of
+// the sequence src(0..M), result in s (natural order).  One loop per radix
+// keeps every pass's registers separate.
+template <int V, class Src>
+__device__ __forceinline__ void fft_m(double2 *s,
+                                      const double2 *__restrict__ tw, int M,
+                                      int4 np, int tid, int T, const Src &src,
+                                      const double2 *__restrict__ bh_last)
+{
+    const int last = np.x + np.y + np.z + np.w - 1;
+    int Ns = 1, p = 0;
+    for (int i = 0; i < np.x; i++, p++, Ns *= 8)
+        stockham_pass<8, V>(s, tw, M, Ns, tid, T, p == 0, src,
+                            p == last ? bh_last : nullptr);
+    for (int i = 0; i < np.y; i++, p++, Ns *= 4)
+        stockham_pass<4, V>(s, tw, M, Ns, tid, T, p == 0, src,
+                            p == last ? bh_last : nullptr);
+    for (int i = 0; i < np.z; i++, p++, Ns *= 2)
+        stockham_pass<2, V>(s, tw, M, Ns, tid, T, p == 0, src,
+                            p == last ? bh_last : nullptr);
+    for (int i = 0; i < np.w; i++, p++, Ns *= 3)
+        stockham_pass<3, V>(s, tw, M, Ns, tid, T, p == 0, src,
+                            p == last ? bh_last : nullptr);
+}
+
+// Complex DFT of length H of the sequence z(0..H), zero-padded to M when
+// Bluestein is used; `pre` returns z_j already multiplied by the chirp
+// (Bluestein) and 0 for j >= H.  On return the DFT value k is dft_h_out(k).
+template <int V, class Pre>
+__device__ __forceinline__ void dft_h(double2 *s, const RfftArgs &A, int tid,
+                                      int T, const Pre &pre)
+{
+    if (A.direct)
+    {
+        fft_m<V>(s, A.tw, A.M, A.npass, tid, T, pre, nullptr);
+        return;
+    }
+    fft_m<V>(s, A.tw, A.M, A.npass, tid, T, pre, A.bh);
+    fft_m<V>(s, A.tw, A.M, A.npass, tid, T, SrcSmem{s}, nullptr);
+}
+
+// value k (< H) of the length-H DFT after dft_h
+__device__ __forceinline__ double2 dft_h_out(const double2 *s,
+                                             const RfftArgs &A, int k)
+{
+    if (A.direct)
+        return s[pidx(k)];
+    return cmul(__ldg(&A.w[k]), conj2(s[pidx(k)]));
+}
+
+// Analysis input: z_j = x_2j + i x_2j+1 times the chirp.
+struct SrcRow
+{
+    const double2 *x2;
+    const double2 *w;
+    int H;
+    __device__ __forceinline__ double2 operator()(int i) const
+    {
+        if (i >= H)
+            return make_double2(0.0, 0.0);
+        double2 z = x2[i];
+        return w ? cmul(z, __ldg(&w[i])) : z;
+    }
+};
+
+// Synthesis input: conj Z_k times the chirp, with
+// Z_k = (X_k + conj X_H-k) + i e^(i pi k/H) (X_k - conj X_H-k) and X_k = 0
+// above kmax (the inverse DFT is conj(DFT(conj Z))).
+struct SrcSpectrum
+{
+    const double2 *X;
+    const double2 *w;
+    const double2 *ht;
+    int H, kmax;
+    __device__ __forceinline__ double2 operator()(int k) const
+    {
+        if (k >= H)
+            return make_double2(0.0, 0.0);
+        const int kh = H - k;
+        double2 xk = k <= kmax ? X[k] : make_double2(0.0, 0.0);
+        double2 xh = kh <= kmax ? conj2(X[kh]) : make_double2(0.0, 0.0);
+        double2 e = cmul(conj2(__ldg(&ht[k])), sub2(xk, xh));
+        double2 zc = make_double2(xk.x + xh.x - e.y, -(xk.y + xh.y + e.x));
+        return w ? cmul(zc, __ldg(&w[k])) : zc;
+    }
+};
+
+// Bluestein kernel b_n = conj w_|n| on the circle of length M
+struct SrcKernel
+{
+    const double2 *w;
+    int H, M;
+    __device__ __forceinline__ double2 operator()(int n) const
+    {
+        if (n < H)
+            return conj2(w[n]);
+        if (n > M - H)
+            return conj2(w[M - n]);
+        return make_double2(0.0, 0.0);
+    }
+};
+
+} // namespace
+
+// Register caps NR: M / 8 <= 1024 threads of 64 registers for V = 8;
+// M / 16 <= 576 threads of 96 registers for V = 16 (five warps on one
+// scheduler's 16384 registers; two CTAs of 288 threads per SM up to
+// M = 4608).
+#define RFFT_BOUNDS(NR) __maxnreg__(NR)
+
+// Analysis direction: real rows x[row][0..L) -> X[row][0..kmax]; one CTA
+// per row (a loop over rows would let the compiler hoist every pass's
+// twiddles out of it and run out of registers).
+template <int V, int NR>
+__global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
+{
+    extern __shared__ __align__(16) double2 s[];
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int H = A.H;
+    const long long row = blockIdx.x;
+    SrcRow src{reinterpret_cast<const double2 *>(A.x + row * A.ldx),
+               A.direct ? nullptr : A.w, H};
+    dft_h<V>(s, A, tid, T, src);
+    double2 *X = A.X + row * A.ldX;
+    for (int k = tid; k <= A.kmax; k += T)
+    {
+        const int ka = (k == H) ? 0 : k;
+        const int kb = (k == 0) ? 0 : H - k;
+        double2 zk = dft_h_out(s, A, ka);
+        double2 zh = conj2(dft_h_out(s, A, kb));
+        double2 e = cmul(__ldg(&A.ht[k]), sub2(zk, zh));
+        double2 sm = add2(zk, zh);
+        X[k] = make_double2(0.5 * (sm.x + e.y), 0.5 * (sm.y - e.x));
+    }
+}
+
+// Synthesis direction: X[row][0..kmax] (zero above) -> real rows x[row].
+template <int V, int NR>
+__global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
+{
+    extern __shared__ __align__(16) double2 s[];
+    const int tid = threadIdx.x, T = blockDim.x;
+    const long long row = blockIdx.x;
+    SrcSpectrum src{A.X + row * A.ldX, A.direct ? nullptr : A.w, A.ht, A.H,
+                    A.kmax};
+    dft_h<V>(s, A, tid, T, src);
+    double2 *x2 = reinterpret_cast<double2 *>(A.x + row * A.ldx);
+    for (int j = tid; j < A.H; j += T)
+        x2[j] = conj2(dft_h_out(s, A, j));
+}
+
+// Tables of one transform length: twiddles exp(-2 pi i k / M), chirp
+// w_n = exp(-i pi n^2 / H) (n^2 reduced mod 2H in integers), and
+// ht_k = exp(-i pi k / H), k <= H.
+__global__ void k_rfft_tables(int H, int M, double2 *tw, double2 *w,
+                              double2 *ht)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double sn, cs;
+    if (i < M)
+    {
+        sincospi(2.0 * (double)i / (double)M, &sn, &cs);
+        tw[i] = make_double2(cs, -sn);
+    }
+    if (w && i < H)
+    {
+        long long q = ((long long)i * i) % (2LL * H);
+        sincospi((double)q / (double)H, &sn, &cs);
+        w[i] = make_double2(cs, -sn);
+    }
+    if (i <= H)
+    {
+        sincospi((double)i / (double)H, &sn, &cs);
+        ht[i] = make_double2(cs, -sn);
+    }
+}
+
+// FFT_M of the Bluestein kernel, times 1/M.
+template <int V, int NR>
+__global__ void RFFT_BOUNDS(NR) k_rfft_kernel_spectrum(RfftArgs A, double2 *bh)
+{
+    extern __shared__ __align__(16) double2 s[];
+    const int tid = threadIdx.x, T = blockDim.x;
+    fft_m<V>(s, A.tw, A.M, A.npass, tid, T, SrcKernel{A.w, A.H, A.M},
+             nullptr);
+    const double inv = 1.0 / (double)A.M;
+    for (int k = tid; k < A.M; k += T)
+    {
+        double2 v = s[pidx(k)];
+        bh[k] = make_double2(v.x * inv, v.y * inv);
+    }
+}
+
+size_t rfft_smem_bytes(int M)
+{
+    return (size_t)(M + M / 8) * sizeof(double2);
+}
+
+cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
+                               double2 *ht, double2 *bh, cudaStream_t st)
+{
+    const int n = (A.M > A.H + 1 ? A.M : A.H + 1);
+    k_rfft_tables<<<(n + 255) / 256, 256, 0, st>>>(A.H, A.M, tw, w, ht);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || A.direct)
+        return e;
+    A.tw = tw;
+    A.w = w;
+    A.ht = ht;
+    const size_t smem = rfft_smem_bytes(A.M);
+    const int T = A.M / A.V;
+    if (A.V == 8)
+        k_rfft_kernel_spectrum<8, 64><<<1, T, smem, st>>>(A, bh);
+    else
+        k_rfft_kernel_spectrum<16, 96><<<1, T, smem, st>>>(A, bh);
+    return cudaGetLastError();
+}
+
+cudaError_t rfft_set_smem(size_t smem)
+{
+    const void *fns[] = {(const void *)k_rfft_fwd<8, 64>,
+                         (const void *)k_rfft_inv<8, 64>,
+                         (const void *)k_rfft_kernel_spectrum<8, 64>,
+                         (const void *)k_rfft_fwd<16, 96>,
+                         (const void *)k_rfft_inv<16, 96>,
+                         (const void *)k_rfft_kernel_spectrum<16, 96>};
+    for (const void *f : fns)
+    {
+        cudaError_t e = cudaFuncSetAttribute(
+            f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
+{
+    const unsigned grid = (unsigned)A.nrows;
+    if (grid == 0)
+        return cudaSuccess;
+    const size_t smem = rfft_smem_bytes(A.M);
+    const int T = A.M / A.V;
+    if (A.V == 8)
+    {
+        if (inverse)
+            k_rfft_inv<8, 64><<<grid, T, smem, st>>>(A);
+        else
+            k_rfft_fwd<8, 64><<<grid, T, smem, st>>>(A);
+    }
+    else
+    {
+        if (inverse)
+            k_rfft_inv<16, 96><<<grid, T, smem, st>>>(A);
+        else
+            k_rfft_fwd<16, 96><<<grid, T, smem, st>>>(A);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace cb

@@ -22,6 +22,10 @@ namespace cb
 namespace
 {
 
+// per warp: two beta stages, two mbarriers (16 B), 32 x 32 partial sums
+constexpr size_t SHA_WARP_SMEM =
+    2 * LEG_CHUNK * sizeof(double2) + 16 + 32 * 32 * sizeof(double2);
+
 struct PairA
 {
     double ae, ao, be, bo;
@@ -54,16 +58,20 @@ __device__ __forceinline__ PairA load_pair_A(const ShaGridArgs &A, int p,
 
 } // namespace
 
+// resident blocks per SM at which each tile width stays free of spills
+// (measured with -Xptxas -v: K=8 246, K=6 215, K=4 166, K=2 128 registers)
+constexpr int sha_min_blocks(int K) { return K >= 6 ? 2 : (K >= 4 ? 3 : 4); }
+
 template <int K>
-__global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
+__global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = threadIdx.x >> 5;
     const size_t stage_bytes = LEG_CHUNK * sizeof(double2);
-    unsigned char *wbase =
-        smem_raw + (size_t)warp * (2 * stage_bytes + 2 * sizeof(uint64_t));
+    unsigned char *wbase = smem_raw + (size_t)warp * SHA_WARP_SMEM;
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + 2 * stage_bytes);
+    double2 *red = reinterpret_cast<double2 *>(wbase + 2 * stage_bytes + 16);
     double2 *stg[2] = {reinterpret_cast<double2 *>(wbase),
                        reinterpret_cast<double2 *>(wbase + stage_bytes)};
     if (lane == 0)
@@ -189,9 +197,10 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                         break;
                     const double2 *blk = stb + 32 * half;
                     const bool first = (j == 0 && half == 0);
-                    double pc[5], ps[5];
-                    double outc = 0.0, outs = 0.0;
-#pragma unroll
+                    // lane partial sums of the 32 degrees, stored swizzled
+                    // (row jj, column lane ^ jj) so that the transposed
+                    // read-back below is free of bank conflicts
+#pragma unroll 8
                     for (int jj = 0; jj < 32; jj++)
                     {
                         double vc = 0.0, vs = 0.0;
@@ -225,32 +234,24 @@ __global__ void __launch_bounds__(128) k_sha_grid(ShaGridArgs A)
                                 }
                             }
                         }
-                        // streaming transpose-reduce (static levels)
-                        double wc = vc, ws = vs;
-                        bool done = false;
-#pragma unroll
-                        for (int L = 0; L < 5; L++)
-                        {
-                            if (done)
-                                break;
-                            if (((jj >> L) & 1) == 0)
-                            {
-                                pc[L] = wc;
-                                ps[L] = ws;
-                                done = true;
-                            }
-                            else
-                            {
-                                wc = tr_combine(pc[L], wc, 1 << L, lane);
-                                ws = tr_combine(ps[L], ws, 1 << L, lane);
-                                if (L == 4)
-                                {
-                                    outc = wc;
-                                    outs = ws;
-                                }
-                            }
-                        }
+                        red[jj * 32 + (int)(lane ^ (unsigned)jj)] =
+                            make_double2(vc, vs);
                     }
+                    __syncwarp();
+                    // lane l: warp total of degree n0 + l, fixed order
+                    double oc0 = 0.0, os0 = 0.0, oc1 = 0.0, os1 = 0.0;
+#pragma unroll 8
+                    for (int q = 0; q < 32; q += 2)
+                    {
+                        double2 a = red[lane * 32 + (lane ^ (unsigned)q)];
+                        double2 b = red[lane * 32 + (lane ^ (unsigned)(q + 1))];
+                        oc0 += a.x;
+                        os0 += a.y;
+                        oc1 += b.x;
+                        os1 += b.y;
+                    }
+                    __syncwarp();
+                    const double outc = oc0 + oc1, outs = os0 + os1;
                     const long long n = n0 + lane;
                     if (n <= N)
                     {
@@ -302,9 +303,32 @@ cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
                             cudaStream_t st)
 {
     const int warps = 4;
-    size_t smem = (size_t)warps *
-                  (2 * LEG_CHUNK * sizeof(double2) + 2 * sizeof(uint64_t));
-    if (K == 4)
+    const size_t smem = (size_t)warps * SHA_WARP_SMEM;
+    static bool attr_set = false;
+    if (!attr_set)
+    {
+        cudaFuncSetAttribute(k_sha_grid<8>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(k_sha_grid<6>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(k_sha_grid<4>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(k_sha_grid<2>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(k_sha_grid<1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        attr_set = true;
+    }
+    if (K == 8)
+        k_sha_grid<8><<<grid, warps * 32, smem, st>>>(A);
+    else if (K == 6)
+        k_sha_grid<6><<<grid, warps * 32, smem, st>>>(A);
+    else if (K == 4)
         k_sha_grid<4><<<grid, warps * 32, smem, st>>>(A);
     else if (K == 2)
         k_sha_grid<2><<<grid, warps * 32, smem, st>>>(A);
