@@ -268,6 +268,22 @@ void host_r_ri_dm(long long nmax, std::vector<double> &r,
         dm[n] = r[2 * n + 3] * ri[2 * n + 2];
 }
 
+// S_m = P_mm(u) / u^m = sqrt(3) prod_{k=1}^{m-1} d_k
+// (src/leg/leg_func_prepare.c), in extended precision, m = 0..nmax.
+void host_smm(long long nmax, double *smm)
+{
+    long double s = 1.0L;
+    smm[0] = 1.0;
+    for (long long m = 1; m <= nmax; m++)
+    {
+        if (m == 1)
+            s = sqrtl(3.0L);
+        else
+            s *= sqrtl((long double)(2 * m + 1) / (long double)(2 * m));
+        smm[m] = (double)s;
+    }
+}
+
 // Recurrence tables of the rescaled recurrence (leg.cuh, tables.cu), built
 // once per maximum degree and kept on the device.
 struct Tabs
@@ -294,19 +310,8 @@ Status tables(Context &c, long long nmax, Tabs *tab)
         return st;
     std::vector<double> r, ri, dmh;
     host_r_ri_dm(nmax, r, ri, dmh);
-    // S_m = P_mm(u) / u^m = sqrt(3) prod_{k=1}^{m-1} d_k
-    // (src/leg/leg_func_prepare.c), in extended precision
     std::vector<double> smm(nmax + 1);
-    long double s = 1.0L;
-    smm[0] = 1.0;
-    for (long long m = 1; m <= nmax; m++)
-    {
-        if (m == 1)
-            s = sqrtl(3.0L);
-        else
-            s *= sqrtl((long double)(2 * m + 1) / (long double)(2 * m));
-        smm[m] = (double)s;
-    }
+    host_smm(nmax, smm.data());
     double *dr = nullptr, *dri = nullptr, *dsm = nullptr;
     CB_TRY(dbuf(c, "tab_r", r.size(), &dr));
     CB_TRY(dbuf(c, "tab_ri", ri.size(), &dri));
@@ -372,22 +377,11 @@ Status plan(Context &c, cufftType type, int n, long long batch,
     return st;
 }
 
-// Shared-memory transform of grid rows of length L (rfft.cu), or nullptr
-// when it does not apply: L odd, or a transform length M beyond 9216
-// (the shared memory of one CTA), or CHARM_B200_ROW_FFT=library.
-Status row_fft(Context &c, long long L, const RfftArgs **out)
+// Shape of the shared-memory transform of rows of length L (rfft.cu):
+// H, M, V, direct and the passes of FFT_M, or false when it does not apply
+// (L odd, H < 8, or M beyond 9216, the shared memory of one CTA).
+bool rfft_shape(long long L, RfftArgs *out)
 {
-    Status st;
-    *out = nullptr;
-    const char *e = std::getenv("CHARM_B200_ROW_FFT");
-    if (e && std::strcmp(e, "library") == 0)
-        return st;
-    auto it = c.rffts.find(L);
-    if (it != c.rffts.end())
-    {
-        *out = it->second.M > 0 ? &it->second : nullptr;
-        return st;
-    }
     RfftArgs A{};
     A.M = 0;
     const long long H = L / 2;
@@ -441,8 +435,8 @@ Status row_fft(Context &c, long long L, const RfftArgs **out)
     }
     if (A.M == 0)
     {
-        c.rffts[L] = A;
-        return st;
+        *out = A;
+        return false;
     }
     A.H = (int)H;
     // radix 8 passes, then 4, then 2 (powers of two), then 3
@@ -460,6 +454,33 @@ Status row_fft(Context &c, long long L, const RfftArgs **out)
             p2 = 1;
     }
     A.npass = make_int4(p8, p4, p2, b);
+    *out = A;
+    return true;
+}
+
+// Shared-memory transform of grid rows of length L (rfft.cu), or nullptr
+// when it does not apply: L odd, or a transform length M beyond 9216
+// (the shared memory of one CTA), or CHARM_B200_ROW_FFT=library.
+Status row_fft(Context &c, long long L, const RfftArgs **out)
+{
+    Status st;
+    *out = nullptr;
+    const char *e = std::getenv("CHARM_B200_ROW_FFT");
+    if (e && std::strcmp(e, "library") == 0)
+        return st;
+    auto it = c.rffts.find(L);
+    if (it != c.rffts.end())
+    {
+        *out = it->second.M > 0 ? &it->second : nullptr;
+        return st;
+    }
+    RfftArgs A{};
+    if (!rfft_shape(L, &A))
+    {
+        c.rffts[L] = A;
+        return st;
+    }
+    const long long H = A.H;
     const size_t nM = (size_t)A.M, nH = (size_t)H;
     const size_t n_tab = nM + (A.direct ? 0 : nH + nM) + nH + 1;
     void *mem = nullptr;
@@ -1217,6 +1238,319 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     return finish(c, d_status);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free analysis (charm_b200_sha_point_dev_static)
+// ---------------------------------------------------------------------------
+// The same kernels as sha_grid with the row transform of rfft.cu, every
+// temporary carved from the fixed device scratch of sha_static.cu and every
+// host-side staging array fixed in size, so that a call allocates neither
+// device, pinned nor heap memory.  Its callers cannot allocate during the
+// call (device memory owned by another allocator, or a loop that must not
+// synchronise the device as cudaMalloc / cudaFree do).
+
+constexpr long long STATIC_MAX_ROWS = 8192;  // grid latitudes served
+
+struct StaticHost
+{
+    double r[2 * STATIC_NMAX + 4], ri[2 * STATIC_NMAX + 4];
+    double smm[STATIC_NMAX + 1];
+    double rescale[STATIC_NMAX + 1];
+    double geo_d[4 * STATIC_MAX_ROWS];  // t, u, cw_n, cw_s per pair
+    int geo_i[2 * STATIC_MAX_ROWS];     // row_n, row_s per pair
+};
+StaticHost g_static_host;
+
+// per device: the scratch address (cudaGetSymbolAddress, once) and what
+// the scratch currently holds
+struct StaticDev
+{
+    unsigned char *base = nullptr;
+    long long tab_nmax = -1;
+    long long fft_L = -1, fft_nmax = -1;
+};
+constexpr int STATIC_MAX_DEVICES = 64;
+StaticDev g_static_dev[STATIC_MAX_DEVICES];
+
+struct Carve
+{
+    size_t off = 0;
+    size_t take(size_t bytes)
+    {
+        size_t o = off;
+        off = (off + bytes + 255) & ~(size_t)255;
+        return o;
+    }
+};
+
+Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
+                                 const double *d_f, unsigned long nmax,
+                                 double mu, double R, unsigned long shc_nmax,
+                                 double *d_c, double *d_s)
+{
+    Status st;
+    if (c.device < 0 || c.device >= STATIC_MAX_DEVICES)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200_sha_point_dev_static serves device ordinals "
+                 "below 64 only.";
+        return st;
+    }
+    StaticDev &sd = g_static_dev[c.device];
+    if (!sd.base)
+    {
+        void *p = nullptr;
+        cudaError_t e = static_scratch_address(&p);
+        if (e != cudaSuccess || !p)
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = std::string("cudaGetSymbolAddress of the static scratch "
+                                 "failed: ") +
+                     cudaGetErrorString(e);
+            return st;
+        }
+        sd.base = static_cast<unsigned char *>(p);
+        CB_CUDA(rfft_set_smem(rfft_smem_bytes(9216)), st);
+    }
+    const long long N = (long long)nmax;
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    if (N > STATIC_NMAX)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200_sha_point_dev_static: nmax " +
+                 std::to_string(N) + " exceeds the static scratch limit of " +
+                 std::to_string(STATIC_NMAX) + ".";
+        return st;
+    }
+    if ((long long)nlat > STATIC_MAX_ROWS)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200_sha_point_dev_static: the grid has " +
+                 std::to_string(nlat) + " latitudes; the limit is " +
+                 std::to_string(STATIC_MAX_ROWS) + ".";
+        return st;
+    }
+    RfftArgs RF{};
+    if (!rfft_shape((long long)nlon, &RF))
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200_sha_point_dev_static: no shared-memory row "
+                 "transform for rows of " +
+                 std::to_string(nlon) + " longitudes.";
+        return st;
+    }
+    if (reinterpret_cast<uintptr_t>(d_f) % 16 != 0)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200_sha_point_dev_static: the grid values must "
+                 "start on a 16-byte boundary.";
+        return st;
+    }
+
+    // latitude pairs of a quadrature grid (the rules of grid_pairs for
+    // GL / DH grids, src/shs/shs_point_grd.c:113-197)
+    const bool dh = is_dh(pnt->type);
+    const size_t pnt_nlat = dh ? nlat + 1 : nlat;
+    const bool even = (pnt_nlat % 2) == 0;
+    const bool symm = pnt_nlat != 1;
+    const unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                       ? nlat - 1
+                                       : (nlat - 2) / 2;
+    size_t equator = (size_t)-1;
+    if (!(pnt->type == CHARM_CRD_POINT_GRID_GL && (nmax_grd % 2)))
+        equator = nlat / 2;
+    const int np =
+        (int)(symm ? (pnt_nlat + 1 - (even ? 1 : 0)) / 2 : nlat);
+    double cq = (pnt->type == CHARM_CRD_POINT_GRID_DH2)
+                    ? PI / (double)(2 * nmax_grd + 2)
+                    : PI / (double)(nmax_grd + 1);
+    const double r0 = pnt->r[0];
+    cq *= 1.0 / (4.0 * PI) * (r0 / mu);
+    StaticHost &hs = g_static_host;
+    for (int p = 0; p < np; p++)
+    {
+        int s = !symm ? 0 : ((dh && p == 0) ? 0 : ((size_t)p < equator));
+        int rs = s ? (int)(pnt_nlat - p - 1) : -1;
+        double la = pnt->lat[p];
+        hs.geo_d[p] = std::sin(la);
+        hs.geo_d[np + p] = std::cos(la);
+        hs.geo_d[2 * np + p] = cq * pnt->w[p];
+        hs.geo_d[3 * np + p] = rs >= 0 ? cq * pnt->w[rs] : 0.0;
+        hs.geo_i[p] = p;
+        hs.geo_i[np + p] = rs;
+    }
+
+    // scratch layout: words, recurrence tables and transform tables first
+    // (their offsets depend on nmax only, so they stay valid while nmax and
+    // the row length repeat), then the per-call arrays
+    const long long T = (N + 1) * (N + 2) / 2;
+    const int ldmul = (int)((N + 1 + 63) / 64);
+    const int K = choose_k_sha(np);
+    const int ntiles = (np + 32 * K - 1) / (32 * K);
+    Carve cv;
+    const size_t o_words = cv.take(256);
+    const size_t o_tb = cv.take((size_t)T * 16);
+    const size_t o_tc = cv.take((size_t)T * 8);
+    const size_t o_tmul = cv.take((size_t)(N + 1) * ldmul * 8);
+    const size_t o_sg = cv.take((size_t)(2 * (N + 1)) * 8);
+    const size_t o_r = cv.take((size_t)(2 * N + 4) * 8);
+    const size_t o_ri = cv.take((size_t)(2 * N + 4) * 8);
+    const size_t o_smm = cv.take((size_t)(N + 1) * 8);
+    const size_t o_tw = cv.take((size_t)RF.M * 16);
+    const size_t o_w = RF.direct ? 0 : cv.take((size_t)RF.H * 16);
+    const size_t o_bh = RF.direct ? 0 : cv.take((size_t)RF.M * 16);
+    const size_t o_ht = cv.take((size_t)(RF.H + 1) * 16);
+    const size_t o_geod = cv.take((size_t)np * 32);
+    const size_t o_geoi = cv.take((size_t)np * 8);
+    const size_t o_res = cv.take((size_t)(N + 1) * 8);
+    const size_t o_F = cv.take(nlat * (size_t)(N + 1) * 16);
+    const size_t part_from = cv.off;
+    // the groups of sha_grid, fewer when the partial sums would not fit
+    long long slots = (long long)c.num_sms * 8 * 4;
+    long long G = std::max<long long>(1, (2 * slots + N) / (N + 1));
+    G = std::min<long long>(G, ntiles);
+    int tpg = (int)((ntiles + G - 1) / G);
+    G = (ntiles + tpg - 1) / tpg;
+    while (part_from + (size_t)G * T * 16 > STATIC_SCRATCH_BYTES && G > 1)
+    {
+        tpg++;
+        G = (ntiles + tpg - 1) / tpg;
+    }
+    const size_t need = part_from + (size_t)G * T * 16;
+    if (need > STATIC_SCRATCH_BYTES)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200_sha_point_dev_static: this grid and nmax need " +
+                 std::to_string(need) + " bytes of static scratch; it has " +
+                 std::to_string(STATIC_SCRATCH_BYTES) + ".";
+        return st;
+    }
+    unsigned char *b = sd.base;
+    unsigned *d_status = reinterpret_cast<unsigned *>(b + o_words);
+    unsigned long long *d_counter =
+        reinterpret_cast<unsigned long long *>(b + o_words + 64);
+    double2 *tb = reinterpret_cast<double2 *>(b + o_tb);
+    double *tc = reinterpret_cast<double *>(b + o_tc);
+    double *tmul = reinterpret_cast<double *>(b + o_tmul);
+    double *sg = reinterpret_cast<double *>(b + o_sg);
+
+    // recurrence tables (kept while nmax repeats)
+    if (sd.tab_nmax != N)
+    {
+        for (long long k = 0; k <= 2 * N + 3; k++)
+        {
+            double w = std::sqrt((double)k);
+            hs.r[k] = w;
+            hs.ri[k] = k ? 1.0 / w : 0.0;
+        }
+        host_smm(N, hs.smm);
+        double *dr = reinterpret_cast<double *>(b + o_r);
+        double *dri = reinterpret_cast<double *>(b + o_ri);
+        double *dsm = reinterpret_cast<double *>(b + o_smm);
+        CB_CUDA(cudaMemcpyAsync(dr, hs.r, (size_t)(2 * N + 4) * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_CUDA(cudaMemcpyAsync(dri, hs.ri, (size_t)(2 * N + 4) * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_CUDA(cudaMemcpyAsync(dsm, hs.smm, (size_t)(N + 1) * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_CUDA(launch_tables(N, dr, dri, dsm, tb, tc, tmul, ldmul, sg,
+                              c.stream), st);
+        c.launches++;
+        sd.tab_nmax = N;
+        sd.fft_L = -1;
+    }
+    // transform tables (kept while the row length and nmax repeat)
+    RF.tw = reinterpret_cast<double2 *>(b + o_tw);
+    RF.w = RF.direct ? nullptr : reinterpret_cast<double2 *>(b + o_w);
+    RF.bh = RF.direct ? nullptr : reinterpret_cast<double2 *>(b + o_bh);
+    RF.ht = reinterpret_cast<double2 *>(b + o_ht);
+    if (sd.fft_L != (long long)nlon || sd.fft_nmax != N)
+    {
+        RfftArgs tmp = RF;
+        CB_CUDA(launch_rfft_tables(tmp, const_cast<double2 *>(RF.tw),
+                                   const_cast<double2 *>(RF.w),
+                                   const_cast<double2 *>(RF.ht),
+                                   const_cast<double2 *>(RF.bh), c.stream),
+                st);
+        c.launches += RF.direct ? 1 : 2;
+        sd.fft_L = (long long)nlon;
+        sd.fft_nmax = N;
+    }
+
+    // geometry and rescaling factors (pageable copies from fixed arrays)
+    double *dgd = reinterpret_cast<double *>(b + o_geod);
+    int *dgi = reinterpret_cast<int *>(b + o_geoi);
+    if (np > 0)
+    {
+        // the four double arrays are contiguous per quantity in geo_d
+        CB_CUDA(cudaMemcpyAsync(dgd, hs.geo_d, (size_t)np * 32,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_CUDA(cudaMemcpyAsync(dgi, hs.geo_i, (size_t)np * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+    }
+    double *dres = nullptr;
+    if (!nearly_equal(R, r0, charm_glob_threshold))
+    {
+        // src/sha/sha_point.c:1088-1108 with src/shc/shc_rescale.c; only
+        // degrees <= nmax carry nonzero coefficients
+        double r_ratio = r0 / R, tmp2 = (mu / mu) * r_ratio;
+        hs.rescale[0] = mu / mu;
+        for (long long n = 1; n <= N; n++)
+        {
+            hs.rescale[n] = tmp2;
+            tmp2 *= r_ratio;
+        }
+        dres = reinterpret_cast<double *>(b + o_res);
+        CB_CUDA(cudaMemcpyAsync(dres, hs.rescale, (size_t)(N + 1) * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+    }
+
+    // r2c of the rows into the scratch, orders 0..nmax
+    double2 *F = reinterpret_cast<double2 *>(b + o_F);
+    RF.nrows = (long long)nlat;
+    RF.x = const_cast<double *>(d_f);
+    RF.ldx = (long long)nlon;
+    RF.X = F;
+    RF.ldX = N + 1;
+    RF.kmax = (int)N;
+    CB_CUDA(launch_rfft(RF, false, c.stream), st);
+    c.launches++;
+
+    // Legendre contraction with the partial sums in the scratch
+    CB_CUDA(cudaMemsetAsync(b + o_words, 0, 256, c.stream), st);
+    double2 *part = reinterpret_cast<double2 *>(b + part_from);
+    ShaGridArgs A{};
+    A.nmax = N;
+    A.npairs = np;
+    A.ntiles = ntiles;
+    A.ngroups = (int)G;
+    A.tiles_per_group = tpg;
+    A.nitems = (N + 1) * G;
+    A.tb = tb;
+    A.tmul = tmul;
+    A.ldmul = ldmul;
+    A.sg = sg;
+    A.t = dgd;
+    A.u = dgd + np;
+    A.cw_n = dgd + 2 * np;
+    A.cw_s = dgd + 3 * np;
+    A.row_n = dgi;
+    A.row_s = dgi + np;
+    A.F = F;
+    A.ldF = (int)(N + 1);
+    A.part = part;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                        (long long)c.num_sms * 8);
+    CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
+    c.launches++;
+    CB_CUDA(launch_sha_reduce(N, (long long)shc_nmax, (int)G, T, part, tc,
+                              dres, d_c, d_s, c.stream), st);
+    c.launches++;
+    return finish(c, d_status);
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -1276,6 +1610,16 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
                     nullptr, d_c, d_s);
+}
+
+Status sha_point_dev_static(const charm_point *pnt, const double *d_f,
+                            unsigned long nmax, double mu, double r,
+                            unsigned long shc_nmax, double *d_c, double *d_s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_point_dev_static_impl(g_ctx, pnt, d_f, nmax, mu, r, shc_nmax,
+                                     d_c, d_s);
 }
 
 Status quad_nodes(int type, unsigned long nmax, double *lat, double *w)

@@ -57,6 +57,15 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
                      unsigned long nmax, double mu, double r,
                      unsigned long shc_nmax, double *d_c, double *d_s);
 
+// sha_point_dev without any allocation: every temporary lives in a fixed
+// static device scratch (sha_static.cu); nmax <= 511, grids of at most 8192
+// latitudes and rows the shared-memory transform handles.  Calls are
+// serialised and synchronous; the first call on a device does the set-up
+// (scratch address, tables).
+Status sha_point_dev_static(const charm_point *pnt, const double *d_f,
+                            unsigned long nmax, double mu, double r,
+                            unsigned long shc_nmax, double *d_c, double *d_s);
+
 // Quadrature grid nodes and weights on the GPU (north to south).
 Status quad_nodes(int type, unsigned long nmax, double *lat, double *w);
 

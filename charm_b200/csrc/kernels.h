@@ -109,6 +109,13 @@ struct RfftArgs
     int kmax;              // spectrum entries read (inverse) / written (forward)
 };
 
+// Size of the fixed device scratch of the allocation-free analysis
+// (sha_static.cu) and the largest degree it serves.
+constexpr size_t STATIC_SCRATCH_BYTES = 32u << 20;
+constexpr long long STATIC_NMAX = 511;
+// device address of that scratch on the current device
+cudaError_t static_scratch_address(void **ptr);
+
 cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
                           const double *smm, double2 *tb, double *tc,
                           double *tmul, int ldmul, double *sg,

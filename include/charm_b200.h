@@ -229,6 +229,35 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev(
     double r, unsigned long shc_nmax, double *d_c, double *d_s,
     charm_err *err);
 
+/* Largest degree and size of the fixed device scratch of
+ * charm_b200_sha_point_dev_static. */
+#define CHARM_B200_STATIC_NMAX 511
+#define CHARM_B200_STATIC_SCRATCH_BYTES 33554432
+
+/* charm_b200_sha_point_dev that allocates nothing: no cudaMalloc, cudaFree,
+ * pinned or heap memory and no allocating library routine (no cuFFT plan).
+ * No counterpart in CHarm; it serves callers that cannot allocate during
+ * the call -- device memory owned by another allocator (a framework's
+ * caching pool), or a loop that must not synchronise the device as
+ * cudaMalloc / cudaFree do.  Every temporary lives in one file-scope static
+ * device array of CHARM_B200_STATIC_SCRATCH_BYTES (32 MiB) whose address is
+ * taken once per device with cudaGetSymbolAddress.  Limits: GL / DH grids,
+ * nmax <= CHARM_B200_STATIC_NMAX, at most 8192 latitudes, an even number
+ * of longitudes whose shared-memory transform exists (half length >= 8,
+ * transform length <= 9216), d_f on a 16-byte boundary, and the scratch
+ * large enough for the grid and nmax; anything else is rejected with
+ * CHARM_EFUNCARG and a message naming the limit.  The library serialises
+ * these calls on its stream and returns after the stream is idle; kernels
+ * of calls that overlap on the GPU (another process's context aside) would
+ * race on the scratch.  The first call on a device performs the set-up
+ * (symbol address, kernel attributes, recurrence and transform tables) and
+ * should precede any stream capture.  Only the scratch's status and
+ * work-counter words must start at zero; each call clears them. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev_static(
+    const charm_point *pnt, const double *d_f, unsigned long nmax, double mu,
+    double r, unsigned long shc_nmax, double *d_c, double *d_s,
+    charm_err *err);
+
 /* The CUDA stream the library runs on (a cudaStream_t), or NULL when no
  * usable device is present. */
 CHARM_EXTERN void *CHARM_CDECL charm_b200_stream(void);
