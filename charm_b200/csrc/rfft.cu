@@ -137,6 +137,23 @@ __device__ __forceinline__ void dft(double2 *v)
         dft8(v);
 }
 
+// w[r] = w[1]^r for r = 2..R-1 by at most three levels of products
+template <int R>
+__device__ __forceinline__ void twiddle_powers(double2 *w)
+{
+    if constexpr (R >= 3)
+        w[2] = cmul(w[1], w[1]);
+    if constexpr (R >= 4)
+        w[3] = cmul(w[2], w[1]);
+    if constexpr (R == 8)
+    {
+        w[4] = cmul(w[2], w[2]);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    }
+}
+
 // Input of the first pass: element i of the sequence to transform.
 struct SrcSmem
 {
@@ -187,11 +204,14 @@ __device__ __forceinline__ void stockham_pass(double2 *s,
             if (j < nb)
             {
                 const int k = j % Ns;
+                // one table twiddle per butterfly, its powers by products
+                double2 wp[R];
+                wp[1] = __ldg(&tw[k * step]);
+                twiddle_powers<R>(wp);
                 v[c][0] = s[pidx(j)];
 #pragma unroll
                 for (int r = 1; r < R; r++)
-                    v[c][r] = cmul(s[pidx(j + r * nb)],
-                                   __ldg(&tw[k * r * step]));
+                    v[c][r] = cmul(s[pidx(j + r * nb)], wp[r]);
                 dft<R>(v[c]);
             }
         }

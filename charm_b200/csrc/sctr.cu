@@ -33,8 +33,12 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
     unsigned char *wbase =
         smem_raw + (size_t)warp * (2 * stage_bytes + 2 * sizeof(uint64_t));
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + 2 * stage_bytes);
-    double2 *stg[2] = {reinterpret_cast<double2 *>(wbase),
-                       reinterpret_cast<double2 *>(wbase + stage_bytes)};
+    // stage s starts at wbase + s * stage_bytes; the mbarrier phases of
+    // the two stages are bits 0 and 1 of `phases` (scalars, so that nothing
+    // is indexed at run time and spilled to local memory)
+    auto stg = [&](int s) {
+        return reinterpret_cast<double2 *>(wbase + (size_t)s * stage_bytes);
+    };
     if (lane == 0)
     {
         mbar_init(&bar[0], 1);
@@ -42,7 +46,7 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
         fence_mbar_init();
     }
     __syncwarp();
-    unsigned phase[2] = {0u, 0u};
+    unsigned phases = 0u;
     const long long N = A.nmax;
     const double BIG = 0x1p960, BIGI = 0x1p-960;
     const double BIGS = 0x1p480, BIGSI = 0x1p-480;
@@ -113,8 +117,8 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                     cnt = LEG_CHUNK;
                 unsigned bytes = (unsigned)(cnt * sizeof(double2));
                 mbar_arrive_expect_tx(&bar[s], 2 * bytes);
-                bulk_g2s(stg[s], A.tb + off, bytes, &bar[s]);
-                bulk_g2s(stg[s] + LEG_CHUNK, A.cs + off, bytes, &bar[s]);
+                bulk_g2s(stg(s), A.tb + off, bytes, &bar[s]);
+                bulk_g2s(stg(s) + LEG_CHUNK, A.cs + off, bytes, &bar[s]);
             }
             if (++ij >= nch_of(im))
             {
@@ -184,12 +188,12 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
             for (int j = 0; j < nch; j++)
             {
                 const int s = consumed & 1;
-                if (!mbar_wait_bounded(&bar[s], phase[s], A.status))
+                if (!mbar_wait_bounded(&bar[s], (phases >> s) & 1u, A.status))
                 {
                     failed = true;
                     break;
                 }
-                phase[s] ^= 1u;
+                phases ^= 1u << s;
                 if (j > 0)
                 {
                     const double mul = A.tmul[(size_t)m * A.ldmul + j];
@@ -202,8 +206,8 @@ __global__ void __launch_bounds__(128) k_sctr(SctrArgs A)
                 }
                 long long cntl = ncol - (long long)j * LEG_CHUNK;
                 const int cnt = cntl > LEG_CHUNK ? LEG_CHUNK : (int)cntl;
-                const double2 *stb = stg[s];
-                const double2 *scs = stg[s] + LEG_CHUNK;
+                const double2 *stb = stg(s);
+                const double2 *scs = stg(s) + LEG_CHUNK;
                 const long long nbase = m + (long long)j * LEG_CHUNK;
                 if (!skip)
                 {

@@ -72,8 +72,12 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
     unsigned char *wbase = smem_raw + (size_t)warp * SHA_WARP_SMEM;
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + 2 * stage_bytes);
     double2 *red = reinterpret_cast<double2 *>(wbase + 2 * stage_bytes + 16);
-    double2 *stg[2] = {reinterpret_cast<double2 *>(wbase),
-                       reinterpret_cast<double2 *>(wbase + stage_bytes)};
+    // stage s starts at wbase + s * stage_bytes; the mbarrier phases of
+    // the two stages are bits 0 and 1 of `phases` (scalars, so that nothing
+    // is indexed at run time and spilled to local memory)
+    auto stg = [&](int s) {
+        return reinterpret_cast<double2 *>(wbase + (size_t)s * stage_bytes);
+    };
     if (lane == 0)
     {
         mbar_init(&bar[0], 1);
@@ -81,7 +85,7 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
         fence_mbar_init();
     }
     __syncwarp();
-    unsigned phase[2] = {0u, 0u};
+    unsigned phases = 0u;
     const long long N = A.nmax;
     const int np = A.npairs;
     bool failed = false;
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                         cnt = LEG_CHUNK;
                     unsigned bytes = (unsigned)(cnt * sizeof(double2));
                     mbar_arrive_expect_tx(&bar[s], bytes);
-                    bulk_g2s(stg[s], A.tb + c0 + (long long)j * LEG_CHUNK,
+                    bulk_g2s(stg(s), A.tb + c0 + (long long)j * LEG_CHUNK,
                              bytes, &bar[s]);
                 }
             };
@@ -161,12 +165,12 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
             for (int j = 0; j < nchunks; j++)
             {
                 const int s = j & 1;
-                if (!mbar_wait_bounded(&bar[s], phase[s], A.status))
+                if (!mbar_wait_bounded(&bar[s], (phases >> s) & 1u, A.status))
                 {
                     failed = true;
                     break;
                 }
-                phase[s] ^= 1u;
+                phases ^= 1u << s;
                 if (j > 0)
                 {
                     const double mul = A.tmul[(size_t)m * A.ldmul + j];
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                 }
                 long long cntl = ncol - (long long)j * LEG_CHUNK;
                 const int cnt = cntl > LEG_CHUNK ? LEG_CHUNK : (int)cntl;
-                double2 *stb = stg[s];
+                double2 *stb = stg(s);
                 // degrees beyond nmax read beta = 0 and contribute 0
                 if (cnt < LEG_CHUNK)
                 {
@@ -197,6 +201,12 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                         break;
                     const double2 *blk = stb + 32 * half;
                     const bool first = (j == 0 && half == 0);
+                    // the group's running sum of degree n0 + lane, loaded
+                    // now so that its latency hides behind the block
+                    const long long n = n0 + lane;
+                    double2 prev = make_double2(0.0, 0.0);
+                    if (stored && n <= N)
+                        prev = col[n - m];
                     // lane partial sums of the 32 degrees, stored swizzled
                     // (row jj, column lane ^ jj) so that the transposed
                     // read-back below is free of bank conflicts
@@ -252,18 +262,10 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                     }
                     __syncwarp();
                     const double outc = oc0 + oc1, outs = os0 + os1;
-                    const long long n = n0 + lane;
                     if (n <= N)
-                    {
-                        double2 *dst = col + (n - m);
-                        if (stored)
-                        {
-                            double2 o = *dst;
-                            *dst = make_double2(o.x + outc, o.y + outs);
-                        }
-                        else
-                            *dst = make_double2(outc, outs);
-                    }
+                        col[n - m] = stored ? make_double2(prev.x + outc,
+                                                           prev.y + outs)
+                                            : make_double2(outc, outs);
                 }
                 if (any_scaled)
                 {

@@ -40,8 +40,12 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
     unsigned char *wbase =
         smem_raw + (size_t)warp * (2 * stage_bytes + 2 * sizeof(uint64_t));
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + 2 * stage_bytes);
-    double2 *stg[2] = {reinterpret_cast<double2 *>(wbase),
-                       reinterpret_cast<double2 *>(wbase + stage_bytes)};
+    // stage s starts at wbase + s * stage_bytes; the mbarrier phases of
+    // the two stages are bits 0 and 1 of `phases` (scalars, so that nothing
+    // is indexed at run time and spilled to local memory)
+    auto stg = [&](int s) {
+        return reinterpret_cast<double2 *>(wbase + (size_t)s * stage_bytes);
+    };
     if (lane == 0)
     {
         mbar_init(&bar[0], 1);
@@ -49,7 +53,7 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
         fence_mbar_init();
     }
     __syncwarp();
-    unsigned phase[2] = {0u, 0u};
+    unsigned phases = 0u;
     const long long N = A.nmax;
     const int np = A.npairs;
     const int dorder = dorder_c >= 0 ? dorder_c : (DR + DL + A.dlon);
@@ -119,8 +123,8 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
                         cnt = LEG_CHUNK;
                     unsigned bytes = (unsigned)(cnt * sizeof(double2));
                     mbar_arrive_expect_tx(&bar[s], 2 * bytes);
-                    bulk_g2s(stg[s], A.tb + off, bytes, &bar[s]);
-                    bulk_g2s(stg[s] + LEG_CHUNK, A.cs + off, bytes, &bar[s]);
+                    bulk_g2s(stg(s), A.tb + off, bytes, &bar[s]);
+                    bulk_g2s(stg(s) + LEG_CHUNK, A.cs + off, bytes, &bar[s]);
                 }
             };
             issue(0, 0);
@@ -135,13 +139,13 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
             const double md = (double)m;
             const double m2 = md * md;
 
-            if (!mbar_wait_bounded(&bar[0], phase[0], A.status))
+            if (!mbar_wait_bounded(&bar[0], (phases >> 0) & 1u, A.status))
                 break;
-            phase[0] ^= 1u;
+            phases ^= 1u << 0;
 
             // ---- n = m (sectorial, even) --------------------------------
             {
-                const double2 c = stg[0][LEG_CHUNK];
+                const double2 c = stg(0)[LEG_CHUNK];
                 const double np1 = md + 1.0;
 #pragma unroll
                 for (int k = 0; k < K; k++)
@@ -164,8 +168,8 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
             // ---- n = m + 1 (odd; beta = 0, R_m+1 = t R_m) ---------------
             if (ncol > 1)
             {
-                const double et = stg[0][1].y;
-                const double2 c = stg[0][LEG_CHUNK + 1];
+                const double et = stg(0)[1].y;
+                const double2 c = stg(0)[LEG_CHUNK + 1];
                 const double nd = md + 1.0, np1 = nd + 1.0;
 #pragma unroll
                 for (int k = 0; k < K; k++)
@@ -199,12 +203,12 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
                 const int s = j & 1;
                 if (j > 0)
                 {
-                    if (!mbar_wait_bounded(&bar[s], phase[s], A.status))
+                    if (!mbar_wait_bounded(&bar[s], (phases >> s) & 1u, A.status))
                     {
                         ok = false;
                         break;
                     }
-                    phase[s] ^= 1u;
+                    phases ^= 1u << s;
                     const double mul = A.tmul[(size_t)m * A.ldmul + j];
 #pragma unroll
                     for (int k = 0; k < K; k++)
@@ -215,8 +219,8 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
                 }
                 long long cntl = ncol - (long long)j * LEG_CHUNK;
                 const int cnt = cntl > LEG_CHUNK ? LEG_CHUNK : (int)cntl;
-                const double2 *stb = stg[s];
-                const double2 *scs = stg[s] + LEG_CHUNK;
+                const double2 *stb = stg(s);
+                const double2 *scs = stg(s) + LEG_CHUNK;
                 const long long nbase = m + (long long)j * LEG_CHUNK;
 
                 auto step = [&](auto parc, int i) {
