@@ -22,9 +22,9 @@ namespace cb
 namespace
 {
 
-// per warp: two beta stages, two mbarriers (16 B), 32 x 32 partial sums
+// per warp: two beta stages, two mbarriers (16 B), 32 x 33 partial sums
 constexpr size_t SHA_WARP_SMEM =
-    2 * LEG_CHUNK * sizeof(double2) + 16 + 32 * 32 * sizeof(double2);
+    2 * LEG_CHUNK * sizeof(double2) + 16 + 32 * 33 * sizeof(double2);
 
 struct PairA
 {
@@ -124,7 +124,6 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                 bool valid = p < np;
                 t[k] = valid ? A.t[p] : 0.0;
                 double u = valid ? A.u[p] : 1.0;
-                y[k] = 0.0;
                 if (valid)
                     leg_seed(sigma, u, 1.0, false, m, 0, x[k], E[k]);
                 else
@@ -132,6 +131,12 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                     x[k] = 0.0;
                     E[k] = 0;
                 }
+                // state (R~_n-1, R~_n-2) = (0, seed): the first step, with
+                // beta = -1 at n = m (set in the staged table below),
+                // yields the seed itself, so every degree takes the same
+                // recurrence step
+                y[k] = x[k];
+                x[k] = 0.0;
                 if (valid && !((double)m - (double)N * u > A.polar_thr))
                     skip = false;
                 // scaled latitudes contribute nothing until they switch
@@ -193,6 +198,12 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                         stb[lane + 32] = make_double2(0.0, 0.0);
                     __syncwarp();
                 }
+                if (j == 0)
+                {
+                    if (lane == 0)
+                        stb[0].x = -1.0;
+                    __syncwarp();
+                }
 #pragma unroll 1
                 for (int half = 0; half < 2; half++)
                 {
@@ -200,61 +211,50 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                     if (n0 > N)
                         break;
                     const double2 *blk = stb + 32 * half;
-                    const bool first = (j == 0 && half == 0);
                     // the group's running sum of degree n0 + lane, loaded
                     // now so that its latency hides behind the block
                     const long long n = n0 + lane;
                     double2 prev = make_double2(0.0, 0.0);
                     if (stored && n <= N)
                         prev = col[n - m];
-                    // lane partial sums of the 32 degrees, stored swizzled
-                    // (row jj, column lane ^ jj) so that the transposed
-                    // read-back below is free of bank conflicts
+                    // lane partial sums of the 32 degrees: row jj, column
+                    // lane of a 32 x 33 array (one pad column keeps both
+                    // the row-wise stores and the column-wise read-back
+                    // free of bank conflicts, with constant offsets)
+                    double2 *redl = red + lane;
 #pragma unroll 8
                     for (int jj = 0; jj < 32; jj++)
                     {
                         double vc = 0.0, vs = 0.0;
-                        if (first && jj == 0)
-                        {
+                        const double beta = blk[jj].x;
 #pragma unroll
-                            for (int k = 0; k < K; k++)
+                        for (int k = 0; k < K; k++)
+                        {
+                            double z = fma(t[k], x[k], -(beta * y[k]));
+                            y[k] = x[k];
+                            x[k] = z;
+                            if ((jj & 1) == 0)
                             {
-                                vc = fma(x[k], pa[k].ae, vc);
-                                vs = fma(x[k], pa[k].be, vs);
+                                vc = fma(z, pa[k].ae, vc);
+                                vs = fma(z, pa[k].be, vs);
+                            }
+                            else
+                            {
+                                vc = fma(z, pa[k].ao, vc);
+                                vs = fma(z, pa[k].bo, vs);
                             }
                         }
-                        else
-                        {
-                            const double beta = blk[jj].x;
-#pragma unroll
-                            for (int k = 0; k < K; k++)
-                            {
-                                double z = fma(t[k], x[k], -(beta * y[k]));
-                                y[k] = x[k];
-                                x[k] = z;
-                                if ((jj & 1) == 0)
-                                {
-                                    vc = fma(z, pa[k].ae, vc);
-                                    vs = fma(z, pa[k].be, vs);
-                                }
-                                else
-                                {
-                                    vc = fma(z, pa[k].ao, vc);
-                                    vs = fma(z, pa[k].bo, vs);
-                                }
-                            }
-                        }
-                        red[jj * 32 + (int)(lane ^ (unsigned)jj)] =
-                            make_double2(vc, vs);
+                        redl[jj * 33] = make_double2(vc, vs);
                     }
                     __syncwarp();
                     // lane l: warp total of degree n0 + l, fixed order
+                    const double2 *row = red + lane * 33;
                     double oc0 = 0.0, os0 = 0.0, oc1 = 0.0, os1 = 0.0;
-#pragma unroll 8
+#pragma unroll
                     for (int q = 0; q < 32; q += 2)
                     {
-                        double2 a = red[lane * 32 + (lane ^ (unsigned)q)];
-                        double2 b = red[lane * 32 + (lane ^ (unsigned)(q + 1))];
+                        double2 a = row[q];
+                        double2 b = row[q + 1];
                         oc0 += a.x;
                         os0 += a.y;
                         oc1 += b.x;
