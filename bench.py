@@ -48,10 +48,8 @@ def parse():
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from charm_b200.replicas import dist_env as env
+    return env()
 
 
 # ---------------------------------------------------------------------------
@@ -124,6 +122,7 @@ def run_ours(args):
         torch.cuda.set_device(0)
     import charm_b200 as cb
     from charm_b200._lib import _libcharm
+    from charm_b200.replicas import job_seconds_per_transform, max_over_ranks
     from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula
 
     L = _libcharm
@@ -209,11 +208,8 @@ def run_ours(args):
     L.charm_b200_timing_read(ms, cnt, 7, ct.byref(kl), ct.byref(fe))
     L.charm_b200_timing(0)
     clk = clocks.stop()
-    total_ms = float(sum(per_step))
+    total_ms = max_over_ranks(float(sum(per_step)), dev)
     if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
 
     # ---- end to end through the C ABI with pinned host buffers -------
@@ -252,11 +248,7 @@ def run_ours(args):
     with torch.cuda.stream(stream):
         f1.record(stream)
     f1.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), dev)
     rt_e2e = coef_rel_rms(oc.numpy(), os_.numpy(), c, s)
 
     if rank != 0:
@@ -291,7 +283,7 @@ def run_ours(args):
     dom = max(kern, key=lambda n: kern[n]["ms"])
     traffic = profiled_traffic(dom, N)
     step_s = total_ms / 1e3 / args.steps
-    value = total_ms / 1e3 / (args.steps * ws)
+    value = job_seconds_per_transform(total_ms / 1e3, args.steps, ws)
     h2d = 16 * T + 8 * nlat * nlon
     d2h = 8 * nlat * nlon + 16 * T
     line = {
@@ -334,7 +326,8 @@ def run_ours(args):
             "traffic": traffic,
             "kernels": kern,
         },
-        "e2e": {"value": e2e_ms / 1e3 / e2e_steps, "unit": "s",
+        "e2e": {"value": job_seconds_per_transform(e2e_ms / 1e3, e2e_steps, ws),
+                "unit": "s",
                 "wall_s": wall / e2e_steps,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "round_trip_rel_rms": rt_e2e},
