@@ -222,10 +222,30 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                     // the row-wise stores and the column-wise read-back
                     // free of bank conflicts, with constant offsets)
                     double2 *redl = red + lane;
-#pragma unroll 8
+                    // accumulation of degree jj - 1 follows the recurrence
+                    // step of degree jj (its value is then in y), so that
+                    // each step's sums overlap the next step's products
+                    auto accumulate = [&](const double *v, int row) {
+                        double vc = 0.0, vs = 0.0;
+#pragma unroll
+                        for (int k = 0; k < K; k++)
+                        {
+                            if ((row & 1) == 0)
+                            {
+                                vc = fma(v[k], pa[k].ae, vc);
+                                vs = fma(v[k], pa[k].be, vs);
+                            }
+                            else
+                            {
+                                vc = fma(v[k], pa[k].ao, vc);
+                                vs = fma(v[k], pa[k].bo, vs);
+                            }
+                        }
+                        redl[row * 33] = make_double2(vc, vs);
+                    };
+#pragma unroll
                     for (int jj = 0; jj < 32; jj++)
                     {
-                        double vc = 0.0, vs = 0.0;
                         const double beta = blk[jj].x;
 #pragma unroll
                         for (int k = 0; k < K; k++)
@@ -233,19 +253,11 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                             double z = fma(t[k], x[k], -(beta * y[k]));
                             y[k] = x[k];
                             x[k] = z;
-                            if ((jj & 1) == 0)
-                            {
-                                vc = fma(z, pa[k].ae, vc);
-                                vs = fma(z, pa[k].be, vs);
-                            }
-                            else
-                            {
-                                vc = fma(z, pa[k].ao, vc);
-                                vs = fma(z, pa[k].bo, vs);
-                            }
                         }
-                        redl[jj * 33] = make_double2(vc, vs);
+                        if (jj > 0)
+                            accumulate(y, jj - 1);
                     }
+                    accumulate(x, 31);
                     __syncwarp();
                     // lane l: warp total of degree n0 + l, fixed order
                     const double2 *row = red + lane * 33;
