@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--nmax", type=int, default=2190)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-n10800", action="store_true",
+                    help="skip the nmax 10800 round trip")
     return ap.parse_args()
 
 
@@ -251,6 +253,9 @@ def run_ours(args):
     e2e_ms = max_over_ranks(f0.elapsed_time(f1), dev)
     rt_e2e = coef_rel_rms(oc.numpy(), os_.numpy(), c, s)
 
+    hi = None if args.no_n10800 else ultra_high_degree(L, err, dev, stream,
+                                                        flush, peak)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -335,6 +340,8 @@ def run_ours(args):
         "fft_execs": int(fe.value),
         "clocks": clk,
     }
+    if hi is not None:
+        line["nmax10800"] = hi
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, c, s, sample_rows=None)
     print(json.dumps(line), flush=True)
@@ -345,6 +352,77 @@ def run_ours(args):
 # ---------------------------------------------------------------------------
 # CPU oracle (reference arm and cpu_baseline leg)
 # ---------------------------------------------------------------------------
+def ultra_high_degree(L, err, dev, stream, flush, peak, steps=2):
+    """The nmax 10800 GL round trip (10801 x 21602 grid, Kaula decay
+    1e-5 n^-2, seed 3000), device resident: one untimed round trip, then
+    `steps` timed ones (CUDA events on the library stream, L2 flushed
+    between them).  Returns its summary for the JSON line."""
+    import torch
+    import charm_b200 as cb
+    from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula
+    N = 10800
+    c, s = kaula(N, 3000, sqrt_scaling=False)
+    pnt = cb.PointGridGL(N, R_EARTH)
+    nlat, nlon = pnt.lat.size, pnt.lon.size
+    d_c = torch.from_numpy(c).to(dev)
+    d_s = torch.from_numpy(s).to(dev)
+    d_f = torch.empty(nlat * nlon, dtype=torch.float64, device=dev)
+    o_c = torch.empty_like(d_c)
+    o_s = torch.empty_like(d_s)
+
+    def check():
+        if not L.charm_err_isempty(err):
+            raise RuntimeError(ct.string_at(err.contents.msg).decode())
+
+    def step():
+        L.charm_b200_shs_point_dev(ct.cast(pnt._Point, ct.c_void_p), N, GM,
+                                   R_EARTH, d_c.data_ptr(), d_s.data_ptr(), N,
+                                   0, 0, 0, 0, d_f.data_ptr(),
+                                   ct.cast(err, ct.c_void_p))
+        check()
+        L.charm_b200_sha_point_dev(ct.cast(pnt._Point, ct.c_void_p),
+                                   d_f.data_ptr(), N, GM, R_EARTH, N,
+                                   o_c.data_ptr(), o_s.data_ptr(),
+                                   ct.cast(err, ct.c_void_p))
+        check()
+
+    step()
+    torch.cuda.synchronize()
+    rt = coef_rel_rms(o_c.cpu().numpy(), o_s.cpu().numpy(), c, s)
+    L.charm_b200_timing(1)
+    total = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        step()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    ms = (ct.c_double * 7)()
+    cnt = (ct.c_ulonglong * 7)()
+    L.charm_b200_timing_read(ms, cnt, 7, None, None)
+    L.charm_b200_timing(0)
+    T = c.size
+    units = T * ((nlat + 1) // 2)
+    shs = ms[0] / max(cnt[0], 1)
+    sha = ms[1] / max(cnt[1], 1)
+    leg_tflops = units * 20.0 / ((shs + sha) * 1e-3) / 1e12
+    del d_c, d_s, d_f, o_c, o_s
+    torch.cuda.empty_cache()
+    return {"workload": "GL-grid SHS+SHA round trip, plain FP64, nmax 10800, "
+                        "grid %dx%d, Kaula 1e-5 n^-2 (seed 3000)" % (nlat, nlon),
+            "ms_per_round_trip": total / steps, "steps": steps,
+            "round_trip_rel_rms": rt,
+            "kernel_ms": {"shs_grid": shs, "sha_grid": sha,
+                          "fft_total_per_step": ms[3] / steps},
+            "legendre_tflops": leg_tflops,
+            "legendre_frac_of_fp64_peak": leg_tflops / peak if peak > 0 else None}
+
+
 def profiled_traffic(kernel, N):
     """DRAM bytes (read + write) per launch of `kernel` at this nmax from
     the committed ncu summary profiles/<kernel>_gl<N>.md (its line
