@@ -57,7 +57,7 @@ def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             "charm_b200: %s is missing; build it with "
-            "`python -m charm_b200.build` (needs nvcc with sm_100a)" % LIB_PATH)
+            "`python charm_b200/build.py` (needs nvcc with sm_100a)" % LIB_PATH)
     lib = ct.CDLL(LIB_PATH)
     P, D, UL, SZ = ct.POINTER, _ct_flt, _ct_ulong, _ct_size_t
     sig = {

@@ -1,7 +1,7 @@
 """Builds charm_b200/libcharm.so: the sm_100a CUDA kernels and the C++ host
 runtime behind the C ABI of include/charm_b200.h.
 
-    python -m charm_b200.build            # or python charm_b200/build.py
+    python charm_b200/build.py
 
 Objects go to charm_b200/_build/; the shared library is written in-tree so
 that it ships together with the sources.
