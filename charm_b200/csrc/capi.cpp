@@ -8,6 +8,8 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <cuda_runtime.h>
+
 #include "../../include/charm_b200.h"
 #include "engine.h"
 
@@ -661,6 +663,71 @@ void charm_b200_sha_point_dev(const charm_point *pnt, const double *d_f,
     }
     report(err, __func__,
            cb::sha_point_dev(pnt, d_f, nmax, mu, r, shc_nmax, d_c, d_s));
+}
+
+// Adjoint of the scattered synthesis: no CHarm counterpart; the checks are
+// those of charm_shs_point plus the point type.
+static bool check_adjoint(const charm_point *pnt, unsigned long nmax,
+                          unsigned long shc_nmax, charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than the maximum harmonic degree "
+                "of the coefficients.");
+        return false;
+    }
+    if (pnt->type != CHARM_CRD_POINT_SCATTERED)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The adjoint of the synthesis requires scattered points "
+                "(\"pnt->type\" must be CHARM_CRD_POINT_SCATTERED).");
+        return false;
+    }
+    return true;
+}
+
+void charm_b200_shs_point_sctr_adjoint(const charm_point *pnt,
+                                       const double *g, unsigned long nmax,
+                                       charm_shc *shcs, charm_err *err)
+{
+    if (!check_adjoint(pnt, nmax, shcs->nmax, err))
+        return;
+    if (pnt->npoint == 0)
+    {
+        // no points: every derivative is zero
+        for (unsigned long m = 0; m <= shcs->nmax; m++)
+            for (unsigned long n = m; n <= shcs->nmax; n++)
+            {
+                shcs->c[m][n - m] = 0.0;
+                shcs->s[m][n - m] = 0.0;
+            }
+        return;
+    }
+    report(err, __func__, cb::shs_point_sctr_adjoint(pnt, g, nmax, shcs));
+}
+
+void charm_b200_shs_point_sctr_adjoint_dev(const charm_point *pnt,
+                                           const double *d_g,
+                                           unsigned long nmax, double mu,
+                                           double r, unsigned long shc_nmax,
+                                           double *d_c, double *d_s,
+                                           charm_err *err)
+{
+    if (!check_adjoint(pnt, nmax, shc_nmax, err))
+        return;
+    if (pnt->npoint == 0)
+    {
+        const size_t T = (size_t)(shc_nmax + 1) * (shc_nmax + 2) / 2;
+        cudaStream_t st = (cudaStream_t)cb::stream_handle();
+        cudaMemsetAsync(d_c, 0, T * sizeof(double), st);
+        cudaMemsetAsync(d_s, 0, T * sizeof(double), st);
+        cudaStreamSynchronize(st);
+        return;
+    }
+    report(err, __func__,
+           cb::shs_point_sctr_adjoint_dev(pnt, d_g, nmax, mu, r, shc_nmax,
+                                          d_c, d_s));
 }
 
 void charm_b200_sha_point_dev_static(const charm_point *pnt,

@@ -1053,6 +1053,107 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
 }
 
 // ---------------------------------------------------------------------------
+// Adjoint of the scattered synthesis with respect to the coefficients
+// ---------------------------------------------------------------------------
+// C_nm = (GM/R) sum_i g_i (R/r_i)^(n+1) P_nm(sin lat_i) cos(m lon_i), S_nm
+// with sin: the transpose of shs_sctr's potential (dorder 0), computed by
+// the analysis kernel with points as amplitude source.
+Status sctr_adjoint(Context &c, const charm_point *pnt, const double *g_host,
+                    const double *d_g, unsigned long nmax, double mu,
+                    double R, unsigned long shc_nmax, double *const *hc,
+                    double *const *hs, double *d_c, double *d_s)
+{
+    Status st;
+    const size_t npt = pnt->nlat;
+    bool r_eq = true;
+    for (size_t i = 0; i < npt; i++)
+        if (!nearly_equal(pnt->r[i], R, charm_glob_threshold))
+        {
+            r_eq = false;
+            break;
+        }
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
+    double *dpts = nullptr;
+    CB_TRY(dbuf(c, "sctr_pts", 3 * npt + (d_g ? 0 : npt), &dpts));
+    CB_CUDA(cudaMemcpyAsync(dpts, pnt->lat, npt * 8, cudaMemcpyHostToDevice,
+                            c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(dpts + npt, pnt->lon, npt * 8,
+                            cudaMemcpyHostToDevice, c.stream), st);
+    if (!r_eq)
+        CB_CUDA(cudaMemcpyAsync(dpts + 2 * npt, pnt->r, npt * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+    const double *gw = d_g;
+    if (!gw)
+    {
+        CB_CUDA(cudaMemcpyAsync(dpts + 3 * npt, g_host, npt * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        gw = dpts + 3 * npt;
+    }
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+    const int K = choose_k_sha((long long)npt);
+    const long long ntiles = ((long long)npt + 32 * K - 1) / (32 * K);
+    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
+    long long slots = (long long)c.num_sms * 8 * 4;
+    long long G = std::max<long long>(1, (2 * slots + nmax) / (nmax + 1));
+    G = std::min<long long>(G, ntiles);
+    long long tpg = (ntiles + G - 1) / G;
+    G = (ntiles + tpg - 1) / tpg;
+    double2 *part = nullptr;
+    CB_TRY(dbuf(c, "sha_part", (size_t)G * T, &part));
+    ShaGridArgs A{};
+    A.nmax = (long long)nmax;
+    A.npairs = (int)npt;
+    A.ntiles = (int)ntiles;
+    A.ngroups = (int)G;
+    A.tiles_per_group = (int)tpg;
+    A.nitems = (long long)(nmax + 1) * G;
+    A.tb = tab.tb;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
+    A.part = part;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    A.lat = dpts;
+    A.lon = dpts + npt;
+    A.r = dpts + 2 * npt;
+    A.g = gw;
+    A.R = R;
+    int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                        (long long)c.num_sms * 8);
+    {
+        Scope sc(c, TIMER_SCTR);
+        CB_CUDA(launch_sha_points(A, r_eq ? 1 : 2, K, std::max(grid, 1),
+                                  c.stream), st);
+    }
+    const long long Ts = (long long)(shc_nmax + 1) * (shc_nmax + 2) / 2;
+    double *oc = d_c, *os = d_s;
+    if (!oc)
+    {
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "shc_out", (size_t)(2 * Ts), &dout));
+        oc = dout;
+        os = dout + Ts;
+    }
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_sha_reduce((long long)nmax, (long long)shc_nmax,
+                                  (int)G, T, part, tab.tc, nullptr, mu / R,
+                                  oc, os, c.stream), st);
+    }
+    if (!d_c)
+    {
+        CB_TRY(download_tri(c, oc, shc_nmax, hc));
+        CB_TRY(download_tri(c, os, shc_nmax, hs));
+    }
+    return finish(c, d_status);
+}
+
+// ---------------------------------------------------------------------------
 // Grid analysis
 // ---------------------------------------------------------------------------
 Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
@@ -1227,7 +1328,8 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     {
         Scope sc(c, TIMER_PREP);
         CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T,
-                                  part, tab.tc, dres, oc, os, c.stream), st);
+                                  part, tab.tc, dres, 1.0, oc, os, c.stream),
+                st);
     }
     if (!d_c)
     {
@@ -1546,7 +1648,7 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
     CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
     c.launches++;
     CB_CUDA(launch_sha_reduce(N, (long long)shc_nmax, (int)G, T, part, tc,
-                              dres, d_c, d_s, c.stream), st);
+                              dres, 1.0, d_c, d_s, c.stream), st);
     c.launches++;
     return finish(c, d_status);
 }
@@ -1610,6 +1712,26 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
                     nullptr, d_c, d_s);
+}
+
+Status shs_point_sctr_adjoint(const charm_point *pnt, const double *g,
+                              unsigned long nmax, charm_shc *shcs)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sctr_adjoint(g_ctx, pnt, g, nullptr, nmax, shcs->mu, shcs->r,
+                        shcs->nmax, shcs->c, shcs->s, nullptr, nullptr);
+}
+
+Status shs_point_sctr_adjoint_dev(const charm_point *pnt, const double *d_g,
+                                  unsigned long nmax, double mu, double r,
+                                  unsigned long shc_nmax, double *d_c,
+                                  double *d_s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sctr_adjoint(g_ctx, pnt, nullptr, d_g, nmax, mu, r, shc_nmax,
+                        nullptr, nullptr, d_c, d_s);
 }
 
 Status sha_point_dev_static(const charm_point *pnt, const double *d_f,

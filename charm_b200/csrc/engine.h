@@ -57,6 +57,19 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
                      unsigned long nmax, double mu, double r,
                      unsigned long shc_nmax, double *d_c, double *d_s);
 
+// Adjoint of the scattered-point potential synthesis with respect to the
+// coefficients: shcs->c, shcs->s (degree shcs->nmax, zero above nmax)
+// receive sum_i g_i d f_i / d C_nm and d f_i / d S_nm for the model
+// (shcs->mu, shcs->r).
+Status shs_point_sctr_adjoint(const charm_point *pnt, const double *g,
+                              unsigned long nmax, charm_shc *shcs);
+
+// Same with the weights and the output triangles in device memory.
+Status shs_point_sctr_adjoint_dev(const charm_point *pnt, const double *d_g,
+                                  unsigned long nmax, double mu, double r,
+                                  unsigned long shc_nmax, double *d_c,
+                                  double *d_s);
+
 // sha_point_dev without any allocation: every temporary lives in a fixed
 // static device scratch (sha_static.cu); nmax <= 511, grids of at most 8192
 // latitudes and rows the shared-memory transform handles.  Calls are

@@ -62,6 +62,13 @@ struct ShaGridArgs
     double polar_thr;
     unsigned long long *counter;
     unsigned *status;
+    // scattered points instead of grid pairs (adjoint of the scattered
+    // synthesis): npairs counts points, and these replace t, u, F, cw_*
+    const double *lat;
+    const double *lon;
+    const double *r;       // radius per point (read when r != R)
+    const double *g;       // weight of each point's value
+    double R;              // reference radius of the coefficients
 };
 
 // Scattered-point synthesis (sctr.cu).
@@ -131,10 +138,15 @@ cudaError_t launch_lon_direct(int npar, int nlat, int nlon, long long nmax,
                               double *f, cudaStream_t st);
 cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
                             cudaStream_t st);
+// src: 0 grid pairs, 1 scattered points on the sphere r = R, 2 scattered
+// points with their own radii
+cudaError_t launch_sha_points(const ShaGridArgs &A, int src, int K, int grid,
+                              cudaStream_t st);
 cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                               long long T, const double2 *part,
                               const double *tc, const double *rescale,
-                              double *c, double *s, cudaStream_t st);
+                              double scale, double *c, double *s,
+                              cudaStream_t st);
 cudaError_t launch_gl_nodes(unsigned long nmax, double *lat, double *w,
                             unsigned *status, cudaStream_t st);
 cudaError_t launch_dh_nodes(unsigned long nmax, double *lat, double *w,

@@ -10,11 +10,19 @@
 // which is added to the group's partial column (plain read-modify-write:
 // the warp owns it).  k_sha_reduce (tables.cu) sums the groups in a fixed
 // order and applies ct_n, so results are deterministic.
+//
+// The same kernel computes the adjoint of the scattered-point synthesis
+// (src/shs/shs_point_sctr.c:86-728) with respect to the coefficients: the
+// "pairs" are then single points (no mirror, so both parities share one
+// amplitude g_i (cos m lon_i, sin m lon_i)), and points off the sphere r = R
+// fold (R/r)^(n+1) into the recurrence as the synthesis does.
+
 #include <cstdint>
 
 #include "common.cuh"
 #include "kernels.h"
 #include "leg.cuh"
+#include "synth.cuh"
 
 namespace cb
 {
@@ -62,9 +70,34 @@ __device__ __forceinline__ PairA load_pair_A(const ShaGridArgs &A, int p,
 // (measured with -Xptxas -v: K=8 246, K=6 215, K=4 166, K=2 128 registers)
 constexpr int sha_min_blocks(int K) { return K >= 6 ? 2 : (K >= 4 ? 3 : 4); }
 
-template <int K>
+// amplitude source of k_sha_grid
+enum
+{
+    SHA_SRC_GRID = 0,     // latitude pairs of a grid, r2c rows
+    SHA_SRC_POINTS = 1,   // scattered points on the sphere r = R
+    SHA_SRC_POINTS_R = 2  // scattered points with their own radii
+};
+
+// amplitudes of point p for order m: g_p (cos m lon_p, sin m lon_p)
+__device__ __forceinline__ PairA load_point_A(const ShaGridArgs &A, int p,
+                                              long long m)
+{
+    PairA r{0.0, 0.0, 0.0, 0.0};
+    if (p >= A.npairs)
+        return r;
+    double sm, cm;
+    sincos_mlon((double)m, A.lon[p], &sm, &cm);
+    const double g = A.g[p];
+    r.ae = r.ao = g * cm;
+    r.be = r.bo = g * sm;
+    return r;
+}
+
+template <int K, int SRC>
 __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs A)
 {
+    constexpr bool PTS = SRC != SHA_SRC_GRID;
+    constexpr bool RR = SRC == SHA_SRC_POINTS_R;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = threadIdx.x >> 5;
@@ -113,7 +146,7 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
 
         for (int tile = tile0; tile < tile1 && !failed; tile++)
         {
-            double t[K], x[K], y[K];
+            double t[K], x[K], y[K], rho2[K];
             int E[K];
             PairA pa[K];
             bool skip = A.polar_thr >= 0.0;
@@ -122,10 +155,26 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
             {
                 int p = tile * (32 * K) + k * 32 + (int)lane;
                 bool valid = p < np;
-                t[k] = valid ? A.t[p] : 0.0;
-                double u = valid ? A.u[p] : 1.0;
+                double u = 1.0, rh = 1.0;
+                if (PTS)
+                {
+                    double tt = 0.0;
+                    if (valid)
+                        sincos(A.lat[p], &tt, &u);
+                    if (RR && valid)
+                        rh = A.R / A.r[p];
+                    // (R/r)^(n+1) folded into the recurrence: t rho and
+                    // beta rho^2, seed times rho^(m+1)
+                    t[k] = RR ? tt * rh : tt;
+                }
+                else
+                {
+                    t[k] = valid ? A.t[p] : 0.0;
+                    u = valid ? A.u[p] : 1.0;
+                }
+                rho2[k] = rh * rh;
                 if (valid)
-                    leg_seed(sigma, u, 1.0, false, m, 0, x[k], E[k]);
+                    leg_seed(sigma, u, rh, RR, m, 0, x[k], E[k]);
                 else
                 {
                     x[k] = 0.0;
@@ -140,8 +189,8 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                 if (valid && !((double)m - (double)N * u > A.polar_thr))
                     skip = false;
                 // scaled latitudes contribute nothing until they switch
-                pa[k] = (E[k] == 0) ? load_pair_A(A, p, m)
-                                    : PairA{0.0, 0.0, 0.0, 0.0};
+                pa[k] = (E[k] != 0) ? PairA{0.0, 0.0, 0.0, 0.0}
+                        : (PTS ? load_point_A(A, p, m) : load_pair_A(A, p, m));
             }
             if (__all_sync(0xffffffffu, skip))
                 continue;
@@ -225,6 +274,7 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                     // accumulation of degree jj - 1 follows the recurrence
                     // step of degree jj (its value is then in y), so that
                     // each step's sums overlap the next step's products
+                    // (points off the sphere accumulate each degree at once)
                     auto accumulate = [&](const double *v, int row) {
                         double vc = 0.0, vs = 0.0;
 #pragma unroll
@@ -250,14 +300,19 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
 #pragma unroll
                         for (int k = 0; k < K; k++)
                         {
+                            // off the sphere y holds rho^2 R~_n-2, so that
+                            // the seed injection (beta = -1) stays exact
                             double z = fma(t[k], x[k], -(beta * y[k]));
-                            y[k] = x[k];
+                            y[k] = RR ? rho2[k] * x[k] : x[k];
                             x[k] = z;
                         }
-                        if (jj > 0)
+                        if (RR)
+                            accumulate(x, jj);
+                        else if (jj > 0)
                             accumulate(y, jj - 1);
                     }
-                    accumulate(x, 31);
+                    if (!RR)
+                        accumulate(x, 31);
                     __syncwarp();
                     // lane l: warp total of degree n0 + l, fixed order
                     const double2 *row = red + lane * 33;
@@ -288,7 +343,8 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                         if (leg_fixup(x[k], y[k], E[k]))
                         {
                             int p = tile * (32 * K) + k * 32 + (int)lane;
-                            pa[k] = load_pair_A(A, p, m);
+                            pa[k] = PTS ? load_point_A(A, p, m)
+                                        : load_pair_A(A, p, m);
                         }
                         still |= (E[k] != 0);
                     }
@@ -313,42 +369,57 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
     }
 }
 
-cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
-                            cudaStream_t st)
+template <int SRC>
+static cudaError_t launch_src(const ShaGridArgs &A, int K, int grid,
+                              cudaStream_t st)
 {
     const int warps = 4;
     const size_t smem = (size_t)warps * SHA_WARP_SMEM;
+    // the dynamic shared memory exceeds the 48 KB default; set once
     static bool attr_set = false;
     if (!attr_set)
     {
-        cudaFuncSetAttribute(k_sha_grid<8>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        cudaFuncSetAttribute(k_sha_grid<6>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        cudaFuncSetAttribute(k_sha_grid<4>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        cudaFuncSetAttribute(k_sha_grid<2>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        cudaFuncSetAttribute(k_sha_grid<1>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+        const void *fns[] = {(const void *)k_sha_grid<8, SRC>,
+                             (const void *)k_sha_grid<6, SRC>,
+                             (const void *)k_sha_grid<4, SRC>,
+                             (const void *)k_sha_grid<2, SRC>,
+                             (const void *)k_sha_grid<1, SRC>};
+        for (const void *f : fns)
+        {
+            cudaError_t e = cudaFuncSetAttribute(
+                f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess)
+                return e;
+        }
         attr_set = true;
     }
     if (K == 8)
-        k_sha_grid<8><<<grid, warps * 32, smem, st>>>(A);
+        k_sha_grid<8, SRC><<<grid, warps * 32, smem, st>>>(A);
     else if (K == 6)
-        k_sha_grid<6><<<grid, warps * 32, smem, st>>>(A);
+        k_sha_grid<6, SRC><<<grid, warps * 32, smem, st>>>(A);
     else if (K == 4)
-        k_sha_grid<4><<<grid, warps * 32, smem, st>>>(A);
+        k_sha_grid<4, SRC><<<grid, warps * 32, smem, st>>>(A);
     else if (K == 2)
-        k_sha_grid<2><<<grid, warps * 32, smem, st>>>(A);
+        k_sha_grid<2, SRC><<<grid, warps * 32, smem, st>>>(A);
     else
-        k_sha_grid<1><<<grid, warps * 32, smem, st>>>(A);
+        k_sha_grid<1, SRC><<<grid, warps * 32, smem, st>>>(A);
     return cudaGetLastError();
+}
+
+cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
+                            cudaStream_t st)
+{
+    return launch_src<SHA_SRC_GRID>(A, K, grid, st);
+}
+
+cudaError_t launch_sha_points(const ShaGridArgs &A, int src, int K, int grid,
+                              cudaStream_t st)
+{
+    if (src == SHA_SRC_POINTS_R)
+        return launch_src<SHA_SRC_POINTS_R>(A, K, grid, st);
+    if (src == SHA_SRC_POINTS)
+        return launch_src<SHA_SRC_POINTS>(A, K, grid, st);
+    return launch_src<SHA_SRC_GRID>(A, K, grid, st);
 }
 
 } // namespace cb

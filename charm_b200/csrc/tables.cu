@@ -142,14 +142,15 @@ __global__ void k_scale_cs(long long nmax, long long shc_nmax,
     }
 }
 
-// Sums the group partials of the analysis, applies ct_n and the degree-wise
-// rescaling of src/shc/shc_rescale.c (rescale[n], or none when null), and
-// writes C, S in the caller's layout (degree shc_nmax, zero above nmax).
+// Sums the group partials of the analysis, applies ct_n, a constant factor
+// and the degree-wise rescaling of src/shc/shc_rescale.c (rescale[n], or
+// none when null), and writes C, S in the caller's layout (degree shc_nmax,
+// zero above nmax).
 __global__ void k_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                              long long T, const double2 *__restrict__ part,
                              const double *__restrict__ tc,
-                             const double *__restrict__ rescale, double *c,
-                             double *s)
+                             const double *__restrict__ rescale, double scale,
+                             double *c, double *s)
 {
     long long m = blockIdx.x;
     if (m > shc_nmax)
@@ -167,7 +168,7 @@ __global__ void k_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                 vc += v.x;
                 vs += v.y;
             }
-            double k = tc[c0 + n - m];
+            double k = tc[c0 + n - m] * scale;
             vc *= k;
             vs *= k;
             if (rescale)
@@ -204,10 +205,11 @@ cudaError_t launch_scale_cs(long long nmax, long long shc_nmax,
 cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                               long long T, const double2 *part,
                               const double *tc, const double *rescale,
-                              double *c, double *s, cudaStream_t st)
+                              double scale, double *c, double *s,
+                              cudaStream_t st)
 {
     k_sha_reduce<<<(int)(shc_nmax + 1), 128, 0, st>>>(
-        nmax, shc_nmax, ngroups, T, part, tc, rescale, c, s);
+        nmax, shc_nmax, ngroups, T, part, tc, rescale, scale, c, s);
     return cudaGetLastError();
 }
 

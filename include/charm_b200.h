@@ -229,6 +229,27 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev(
     double r, unsigned long shc_nmax, double *d_c, double *d_s,
     charm_err *err);
 
+/* Adjoint of charm_shs_point on scattered points with respect to the
+ * coefficients (no counterpart in CHarm, which has no transpose routine;
+ * the forward it transposes is src/shs/shs_point_sctr.c:86-728): for the
+ * model (shcs->mu, shcs->r) and weights g[npoint] it overwrites shcs->c and
+ * shcs->s with
+ *     C_nm = (mu / r) sum_i g_i (r / r_i)^(n+1) P_nm(sin lat_i) cos(m lon_i)
+ * (sin for S_nm), degrees above nmax zero, i.e. the gradient of
+ * sum_i g_i f_i with f = charm_shs_point(pnt, shcs, nmax).  pnt must hold
+ * scattered points (CHARM_CRD_POINT_SCATTERED). */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_sctr_adjoint(
+    const charm_point *pnt, const double *g, unsigned long nmax,
+    charm_shc *shcs, charm_err *err);
+
+/* Same with the weights d_g[npoint] and the output triangles d_c, d_s
+ * (degree shc_nmax, order-major) in device memory; mu, r describe the
+ * model as shcs->mu, shcs->r would. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_sctr_adjoint_dev(
+    const charm_point *pnt, const double *d_g, unsigned long nmax, double mu,
+    double r, unsigned long shc_nmax, double *d_c, double *d_s,
+    charm_err *err);
+
 /* Largest degree and size of the fixed device scratch of
  * charm_b200_sha_point_dev_static. */
 #define CHARM_B200_STATIC_NMAX 511
