@@ -78,16 +78,17 @@ enum
     SHA_SRC_POINTS_R = 2  // scattered points with their own radii
 };
 
-// amplitudes of point p for order m: g_p (cos m lon_p, sin m lon_p)
+// amplitudes of point p for order m: g_p (cos m lon_p, sin m lon_p), times
+// `scale`
 __device__ __forceinline__ PairA load_point_A(const ShaGridArgs &A, int p,
-                                              long long m)
+                                              long long m, double scale)
 {
     PairA r{0.0, 0.0, 0.0, 0.0};
     if (p >= A.npairs)
         return r;
     double sm, cm;
     sincos_mlon((double)m, A.lon[p], &sm, &cm);
-    const double g = A.g[p];
+    const double g = A.g[p] * scale;
     r.ae = r.ao = g * cm;
     r.be = r.bo = g * sm;
     return r;
@@ -189,8 +190,11 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                 if (valid && !((double)m - (double)N * u > A.polar_thr))
                     skip = false;
                 // scaled latitudes contribute nothing until they switch
+                // off the sphere the sums read rho^2 R~ (see below), so
+                // the amplitudes carry 1 / rho^2
                 pa[k] = (E[k] != 0) ? PairA{0.0, 0.0, 0.0, 0.0}
-                        : (PTS ? load_point_A(A, p, m) : load_pair_A(A, p, m));
+                        : (PTS ? load_point_A(A, p, m, RR ? 1.0 / rho2[k] : 1.0)
+                               : load_pair_A(A, p, m));
             }
             if (__all_sync(0xffffffffu, skip))
                 continue;
@@ -274,7 +278,6 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                     // accumulation of degree jj - 1 follows the recurrence
                     // step of degree jj (its value is then in y), so that
                     // each step's sums overlap the next step's products
-                    // (points off the sphere accumulate each degree at once)
                     auto accumulate = [&](const double *v, int row) {
                         double vc = 0.0, vs = 0.0;
 #pragma unroll
@@ -306,12 +309,18 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                             y[k] = RR ? rho2[k] * x[k] : x[k];
                             x[k] = z;
                         }
-                        if (RR)
-                            accumulate(x, jj);
-                        else if (jj > 0)
+                        if (jj > 0)
                             accumulate(y, jj - 1);
                     }
-                    if (!RR)
+                    if (RR)
+                    {
+                        double xr[K];
+#pragma unroll
+                        for (int k = 0; k < K; k++)
+                            xr[k] = rho2[k] * x[k];
+                        accumulate(xr, 31);
+                    }
+                    else
                         accumulate(x, 31);
                     __syncwarp();
                     // lane l: warp total of degree n0 + l, fixed order
@@ -343,7 +352,8 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
                         if (leg_fixup(x[k], y[k], E[k]))
                         {
                             int p = tile * (32 * K) + k * 32 + (int)lane;
-                            pa[k] = PTS ? load_point_A(A, p, m)
+                            pa[k] = PTS ? load_point_A(A, p, m,
+                                                       RR ? 1.0 / rho2[k] : 1.0)
                                         : load_pair_A(A, p, m);
                         }
                         still |= (E[k] != 0);
