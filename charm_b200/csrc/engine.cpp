@@ -402,7 +402,9 @@ bool rfft_shape(long long L, RfftArgs *out)
     int a = 0, b = 0;
     if (L % 2 == 0 && H >= 8)
     {
-        if (smooth(H, &a, &b) && a >= 3 && H <= 9216)
+        // transform lengths are 2^a 3^b with a >= 6: the passes then start
+        // with two of radix 8 and every stride is a multiple of 8 (rfft.cu)
+        if (smooth(H, &a, &b) && a >= 6 && H <= 9216)
         {
             A.M = (int)H;
             A.direct = 1;
@@ -410,7 +412,7 @@ bool rfft_shape(long long L, RfftArgs *out)
         else
         {
             long long best = 0;
-            for (long long p2 = 8; p2 <= 9216; p2 *= 2)
+            for (long long p2 = 64; p2 <= 9216; p2 *= 2)
                 for (long long m = p2; m <= 9216; m *= 3)
                     if (m >= 2 * H - 1 && (best == 0 || m < best))
                         best = m;
@@ -422,17 +424,9 @@ bool rfft_shape(long long L, RfftArgs *out)
             }
         }
     }
-    // 16 values per thread where M allows (M / 16 threads, two CTAs per
-    // SM up to M = 4608), else 8
-    if (A.M > 0)
-    {
-        if (A.M % 16 == 0)
-            A.V = 16;
-        else if (A.M % 8 == 0 && A.M <= 8192)
-            A.V = 8;
-        else
-            A.M = 0;
-    }
+    // 16 values per thread: M / 16 threads, two CTAs per SM up to
+    // M = 4608
+    A.V = 16;
     if (A.M == 0)
     {
         *out = A;

@@ -102,7 +102,7 @@ struct RfftArgs
     long long nrows;
     int H;                 // half length
     int M;                 // FFT length: H (direct) or >= 2H - 1 (Bluestein)
-    int V;                 // values per thread (8 or 16); M / V threads
+    int V;                 // values per thread (16); M / V threads
     int direct;            // 1: H = 2^a 3^b, no chirp convolution
     int4 npass;            // passes of FFT_M of radix 8, 4, 2, 3 (in order)
     const double2 *tw;     // exp(-2 pi i k / M), k < M

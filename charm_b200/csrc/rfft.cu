@@ -164,11 +164,22 @@ struct SrcSmem
     }
 };
 
+// j div Ns and j mod Ns (one division by the run-time stride)
+__device__ __forceinline__ void divmod_ns(int j, int Ns, int &q, int &k)
+{
+    k = j % Ns;
+    q = (j - k) / Ns;
+}
+
 // One Stockham pass of radix R over s[0..M): butterfly j reads element
 // j + r M/R (twiddled by exp(-2 pi i (j mod Ns) r / (Ns R))) and writes its
 // R outputs to elements (j - j mod Ns) R + j mod Ns + r Ns.  The first pass
 // (Ns = 1, no twiddles) reads through `src`; a non-null `bh` multiplies the
-// stored outputs by bh and conjugates them.
+// stored outputs by bh and conjugates them.  Plans have 64 | M and start
+// with two radix-8 passes, so M/R and every Ns > 1 are multiples of 8: the
+// padded positions of a butterfly's elements are then a base plus a
+// constant stride (r (M/R + M/8R) for loads, r (Ns + Ns/8) for stores, and
+// r for the first pass's stores, whose bases are multiples of 8).
 template <int R, int V, class Src>
 __device__ __forceinline__ void stockham_pass(double2 *s,
                                               const double2 *__restrict__ tw,
@@ -179,6 +190,8 @@ __device__ __forceinline__ void stockham_pass(double2 *s,
     constexpr int BPT = (V + R - 1) / R;
     const int nb = M / R;
     const int step = M / (Ns * R);
+    const int ld_stride = nb + (nb >> 3);
+    const int st_stride = (Ns == 1) ? 1 : Ns + (Ns >> 3);
     double2 v[BPT][R];
     if (first)
     {
@@ -203,15 +216,17 @@ __device__ __forceinline__ void stockham_pass(double2 *s,
             const int j = tid + c * T;
             if (j < nb)
             {
-                const int k = j % Ns;
+                int q, k;
+                divmod_ns(j, Ns, q, k);
                 // one table twiddle per butterfly, its powers by products
                 double2 wp[R];
                 wp[1] = __ldg(&tw[k * step]);
                 twiddle_powers<R>(wp);
-                v[c][0] = s[pidx(j)];
+                const int b = pidx(j);
+                v[c][0] = s[b];
 #pragma unroll
                 for (int r = 1; r < R; r++)
-                    v[c][r] = cmul(s[pidx(j + r * nb)], wp[r]);
+                    v[c][r] = cmul(s[b + r * ld_stride], wp[r]);
                 dft<R>(v[c]);
             }
         }
@@ -223,20 +238,22 @@ __device__ __forceinline__ void stockham_pass(double2 *s,
         const int j = tid + c * T;
         if (j < nb)
         {
-            const int k = j % Ns;
-            const int d = (j - k) * R + k;
+            int q, k;
+            divmod_ns(j, Ns, q, k);
+            const int d = q * Ns * R + k;
+            const int b = pidx(d);
             if (bh)
             {
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    s[pidx(d + r * Ns)] =
+                    s[b + r * st_stride] =
                         conj2(cmul(v[c][r], __ldg(&bh[d + r * Ns])));
             }
             else
             {
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    s[pidx(d + r * Ns)] = v[c][r];
+                    s[b + r * st_stride] = v[c][r];
             }
         }
     }
@@ -347,10 +364,9 @@ struct SrcKernel
 
 } // namespace
 
-// Register caps NR: M / 8 <= 1024 threads of 64 registers for V = 8;
-// M / 16 <= 576 threads of 96 registers for V = 16 (five warps on one
-// scheduler's 16384 registers; two CTAs of 288 threads per SM up to
-// M = 4608).
+// Register cap NR: M / 16 <= 576 threads of 96 registers with V = 16 values
+// per thread (five warps on one scheduler's 16384 registers; two CTAs of
+// 288 threads per SM up to M = 4608).
 #define RFFT_BOUNDS(NR) __maxnreg__(NR)
 
 // Analysis direction: real rows x[row][0..L) -> X[row][0..kmax]; one CTA
@@ -453,20 +469,13 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
     A.w = w;
     A.ht = ht;
     const size_t smem = rfft_smem_bytes(A.M);
-    const int T = A.M / A.V;
-    if (A.V == 8)
-        k_rfft_kernel_spectrum<8, 64><<<1, T, smem, st>>>(A, bh);
-    else
-        k_rfft_kernel_spectrum<16, 96><<<1, T, smem, st>>>(A, bh);
+    k_rfft_kernel_spectrum<16, 96><<<1, A.M / 16, smem, st>>>(A, bh);
     return cudaGetLastError();
 }
 
 cudaError_t rfft_set_smem(size_t smem)
 {
-    const void *fns[] = {(const void *)k_rfft_fwd<8, 64>,
-                         (const void *)k_rfft_inv<8, 64>,
-                         (const void *)k_rfft_kernel_spectrum<8, 64>,
-                         (const void *)k_rfft_fwd<16, 96>,
+    const void *fns[] = {(const void *)k_rfft_fwd<16, 96>,
                          (const void *)k_rfft_inv<16, 96>,
                          (const void *)k_rfft_kernel_spectrum<16, 96>};
     for (const void *f : fns)
@@ -485,21 +494,11 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
     if (grid == 0)
         return cudaSuccess;
     const size_t smem = rfft_smem_bytes(A.M);
-    const int T = A.M / A.V;
-    if (A.V == 8)
-    {
-        if (inverse)
-            k_rfft_inv<8, 64><<<grid, T, smem, st>>>(A);
-        else
-            k_rfft_fwd<8, 64><<<grid, T, smem, st>>>(A);
-    }
+    const int T = A.M / 16;
+    if (inverse)
+        k_rfft_inv<16, 96><<<grid, T, smem, st>>>(A);
     else
-    {
-        if (inverse)
-            k_rfft_inv<16, 96><<<grid, T, smem, st>>>(A);
-        else
-            k_rfft_fwd<16, 96><<<grid, T, smem, st>>>(A);
-    }
+        k_rfft_fwd<16, 96><<<grid, T, smem, st>>>(A);
     return cudaGetLastError();
 }
 

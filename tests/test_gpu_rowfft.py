@@ -4,9 +4,8 @@ lumped coefficients / grids, through the public synthesis and analysis.
 CHARM_B200_ROW_FFT=library routes the longitude transforms through cuFFT
 instead; both compute the same unnormalised DFTs, so the outputs agree to a
 few units of rounding.  The grids cover every transform plan: direct
-mixed radix (H = 2^a 3^b), Bluestein with 8 values per thread, Bluestein
-with 16 values per thread (M = 9216), and lengths where the row transform
-does not apply (H < 8)."""
+mixed radix (H = 2^a 3^b, a >= 6), Bluestein for every other length up to
+M = 9216, and lengths where the row transform does not apply (H < 8)."""
 import os
 
 import numpy as np
@@ -39,10 +38,11 @@ def both(fn):
 
 
 @pytest.mark.parametrize("grid,N", [
-    ("GL", 7),      # H = 8, direct, one pass of radix 8
-    ("GL", 287),    # H = 288 = 2^5 3^2, direct
+    ("GL", 7),      # H = 8, Bluestein M = 64
+    ("GL", 191),    # H = 192 = 2^6 3, direct
+    ("GL", 287),    # H = 288 = 2^5 3^2, Bluestein M = 576
     ("GL", 360),    # H = 361 = 19^2, Bluestein M = 768
-    ("DH1", 100),   # H = 101, Bluestein M = 216
+    ("DH1", 100),   # H = 101, Bluestein M = 256
     ("DH2", 2190),  # H = 4382, Bluestein M = 9216, 16 values per thread
     ("GL", 2190),   # H = 2191, Bluestein M = 4608
     ("GL", 2),      # H = 3, library transform
