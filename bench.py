@@ -259,6 +259,8 @@ def run_ours(args):
     e2e_ms = max_over_ranks(f0.elapsed_time(f1), dev)
     rt_e2e = coef_rel_rms(oc.numpy(), os_.numpy(), c, s)
 
+    f32 = single_precision(L, err, pnt, N, c, s, d_f, stream, flush,
+                           args.steps)
     hi = None if args.no_n10800 else ultra_high_degree(L, err, dev, stream,
                                                         flush, peak)
 
@@ -346,6 +348,7 @@ def run_ours(args):
         "fft_execs": int(fe.value),
         "clocks": clk,
     }
+    line["f32"] = f32
     if hi is not None:
         line["nmax10800"] = hi
     if not args.no_cpu_baseline:
@@ -358,6 +361,72 @@ def run_ours(args):
 # ---------------------------------------------------------------------------
 # CPU oracle (reference arm and cpu_baseline leg)
 # ---------------------------------------------------------------------------
+def single_precision(L, err, pnt, N, c, s, d_f64, stream, flush, steps):
+    """The same round trip in the single-precision mode (FP32 Legendre
+    recurrence and sums, FP64 row transforms, float inputs and outputs),
+    device resident; its field is compared with the FP64 path's d_f64."""
+    import torch
+    from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, rel_rms
+    P = ct.c_void_p
+    L.charm_b200_shs_point_dev_f32.argtypes = [
+        P, ct.c_ulong, ct.c_double, ct.c_double, P, P, ct.c_ulong, P, P]
+    L.charm_b200_sha_point_dev_f32.argtypes = [
+        P, P, ct.c_ulong, ct.c_double, ct.c_double, ct.c_ulong, P, P, P]
+    dev = d_f64.device
+    d_c = torch.from_numpy(c.astype(np.float32)).to(dev)
+    d_s = torch.from_numpy(s.astype(np.float32)).to(dev)
+    d_f = torch.empty(d_f64.numel(), dtype=torch.float32, device=dev)
+    o_c = torch.empty_like(d_c)
+    o_s = torch.empty_like(d_s)
+
+    def check():
+        if not L.charm_err_isempty(err):
+            raise RuntimeError(ct.string_at(err.contents.msg).decode())
+
+    def step():
+        L.charm_b200_shs_point_dev_f32(ct.cast(pnt._Point, P), N, GM, R_EARTH,
+                                       d_c.data_ptr(), d_s.data_ptr(), N,
+                                       d_f.data_ptr(), ct.cast(err, P))
+        check()
+        L.charm_b200_sha_point_dev_f32(ct.cast(pnt._Point, P), d_f.data_ptr(),
+                                       N, GM, R_EARTH, N, o_c.data_ptr(),
+                                       o_s.data_ptr(), ct.cast(err, P))
+        check()
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e_field = rel_rms(d_f.cpu().numpy().astype(np.float64),
+                      d_f64.cpu().numpy())
+    e_rt = coef_rel_rms(o_c.cpu().numpy().astype(np.float64),
+                        o_s.cpu().numpy().astype(np.float64), c, s)
+    L.charm_b200_timing(1)
+    total = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        step()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    ms = (ct.c_double * 7)()
+    cnt = (ct.c_ulonglong * 7)()
+    L.charm_b200_timing_read(ms, cnt, 7, None, None)
+    L.charm_b200_timing(0)
+    return {"workload": "GL-grid SHS+SHA round trip, single-precision mode, "
+                        "nmax %d" % N,
+            "ms_per_round_trip": total / steps, "steps": steps,
+            "kernel_ms": {"shs_grid_f32": ms[0] / max(cnt[0], 1),
+                          "sha_grid_f32": ms[1] / max(cnt[1], 1),
+                          "fft_total_per_step": ms[3] / steps},
+            "field_rel_rms_vs_fp64": e_field,
+            "round_trip_rel_rms": e_rt}
+
+
 def ultra_high_degree(L, err, dev, stream, flush, peak, steps=2):
     """The nmax 10800 GL round trip (10801 x 21602 grid, Kaula decay
     1e-5 n^-2, seed 3000), device resident: one untimed round trip, then

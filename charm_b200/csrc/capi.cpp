@@ -665,6 +665,66 @@ void charm_b200_sha_point_dev(const charm_point *pnt, const double *d_f,
            cb::sha_point_dev(pnt, d_f, nmax, mu, r, shc_nmax, d_c, d_s));
 }
 
+// Single-precision mode: no CHarm counterpart at this ABI level (CHarm's
+// float build is a separate library, charmf_*); the checks mirror the
+// double-precision device entry points.
+void charm_b200_shs_point_dev_f32(const charm_point *pnt,
+                                  unsigned long shc_nmax, double mu, double r,
+                                  const float *d_c, const float *d_s,
+                                  unsigned long nmax, float *d_f,
+                                  charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (pnt->type == CHARM_CRD_POINT_SCATTERED)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The single-precision mode synthesises on grids only.");
+        return;
+    }
+    if (pnt->npoint == 0)
+        return;
+    report(err, __func__,
+           cb::shs_point_dev_f32(pnt, shc_nmax, mu, r, d_c, d_s, nmax, d_f));
+}
+
+void charm_b200_sha_point_dev_f32(const charm_point *pnt, const float *d_f,
+                                  unsigned long nmax, double mu, double r,
+                                  unsigned long shc_nmax, float *d_c,
+                                  float *d_s, charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (!is_quad_type(pnt->type))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic analysis of "
+                "point data values.");
+        return;
+    }
+    unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                 ? (unsigned long)pnt->nlat - 1
+                                 : ((unsigned long)pnt->nlat - 2) / 2;
+    if (nmax > nmax_grd)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The input data grid \"pnt\" was created for a maximum degree "
+                "that is not high enough to recover harmonics up to the "
+                "specified maximum degree of the analysis.");
+        return;
+    }
+    report(err, __func__,
+           cb::sha_point_dev_f32(pnt, d_f, nmax, mu, r, shc_nmax, d_c, d_s));
+}
+
 // Adjoint of the scattered synthesis: no CHarm counterpart; the checks are
 // those of charm_shs_point plus the point type.
 static bool check_adjoint(const charm_point *pnt, unsigned long nmax,

@@ -60,6 +60,7 @@ struct Context
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
     long long tab_nmax = -1;     // recurrence tables of this maximum degree
+    long long tab32_nmax = -1;   // single-precision tables of this degree
     std::map<std::tuple<int, int, long long>, cufftHandle> plans;
     std::map<long long, RfftArgs> rffts;   // row transforms by row length
     std::map<long long, void *> rfft_mem;  // their tables
@@ -1047,6 +1048,314 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
 }
 
 // ---------------------------------------------------------------------------
+// Single-precision mode (f32.cu): potential on FFT grids, r = R
+// ---------------------------------------------------------------------------
+// Tables (a_nm, b_nm) in float and S_m in double, built once per nmax.
+Status tables_f32(Context &c, long long nmax, float4 **ab, double **smm)
+{
+    Status st;
+    const long long T = (nmax + 1) * (nmax + 2) / 2;
+    CB_TRY(dbuf(c, "tab32_ab", (size_t)T, ab));
+    CB_TRY(dbuf(c, "tab32_smm", (size_t)(nmax + 1), smm));
+    if (c.tab32_nmax == nmax)
+        return st;
+    std::vector<double> r, ri, dmh, hs(nmax + 1);
+    host_r_ri_dm(nmax, r, ri, dmh);
+    host_smm(nmax, hs.data());
+    double *dr = nullptr, *dri = nullptr;
+    CB_TRY(dbuf(c, "tab32_r", r.size(), &dr));
+    CB_TRY(dbuf(c, "tab32_ri", ri.size(), &dri));
+    CB_CUDA(cudaMemcpyAsync(dr, r.data(), r.size() * 8,
+                            cudaMemcpyHostToDevice, c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(dri, ri.data(), ri.size() * 8,
+                            cudaMemcpyHostToDevice, c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(*smm, hs.data(), hs.size() * 8,
+                            cudaMemcpyHostToDevice, c.stream), st);
+    {
+        Scope sc(c, TIMER_TABLES);
+        CB_CUDA(launch_tables_f32(nmax, dr, dri, *ab, c.stream), st);
+    }
+    // the host vectors must outlive the copies
+    CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    c.tab32_nmax = nmax;
+    return st;
+}
+
+// Checks shared by both directions: equally spaced longitudes starting at
+// 0 with a shared-memory row transform, orders up to nmax resolvable, and
+// every row on the sphere r = R.
+Status f32_grid_checks(Context &c, const charm_point *pnt, unsigned long nmax,
+                       double R, const RfftArgs **rf)
+{
+    Status st;
+    if (nmax > 2200)
+    {
+        // the scaled-seed renormalisation every 16 degrees keeps the float
+        // recurrence in range up to this degree
+        st.code = CHARM_EFUNCARG;
+        st.msg = "The single-precision mode serves nmax <= 2200.";
+        return st;
+    }
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    const double thr = charm_glob_threshold;
+    double step = nlon > 1 ? pnt->lon[1] - pnt->lon[0] : 0.0;
+    bool fft = nlon >= 2 && (nlon - 1) / 2 >= nmax &&
+               nearly_equal(pnt->lon[0], 0.0, thr) &&
+               nearly_equal(pnt->lon[nlon - 1] + step, 2.0 * PI, thr);
+    for (size_t j = 1; fft && j < nlon; j++)
+        if (!nearly_equal(step, pnt->lon[j] - pnt->lon[j - 1],
+                          charm_glob_threshold2))
+            fft = false;
+    *rf = nullptr;
+    if (fft)
+        CB_TRY(row_fft(c, (long long)nlon, rf));
+    if (!*rf)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "The single-precision mode needs a grid whose longitudes "
+                 "0, 2 pi / nlon, ... admit the shared-memory row transform "
+                 "(even nlon, nlon / 2 + 1 > nmax).";
+        return st;
+    }
+    for (size_t i = 0; i < nlat; i++)
+        if (!nearly_equal(pnt->r[i], R, thr))
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "The single-precision mode needs every grid row on the "
+                     "sphere of the coefficients' radius (r = R).";
+            return st;
+        }
+    return st;
+}
+
+Status shs_grid_f32(Context &c, const charm_point *pnt, unsigned long shc_nmax,
+                    double mu, double R, const float *d_c, const float *d_s,
+                    unsigned long nmax, float *d_f)
+{
+    Status st;
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    const RfftArgs *rf = nullptr;
+    CB_TRY(f32_grid_checks(c, pnt, nmax, R, &rf));
+    if (reinterpret_cast<uintptr_t>(d_f) % 8 != 0)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "The grid values must start on an 8-byte boundary.";
+        return st;
+    }
+    Pairs P;
+    grid_pairs(pnt, charm_glob_threshold2, true, P);
+    const int np = (int)P.row_n.size();
+    size_t geo_bytes = (size_t)np * (2 * 8 + 2 * 4);
+    void *hp = nullptr;
+    CB_TRY(pinned(c, geo_bytes, &hp));
+    double *ht = static_cast<double *>(hp);
+    double *hu = ht + np;
+    int *hrn = reinterpret_cast<int *>(hu + np);
+    int *hrs = hrn + np;
+    for (int p = 0; p < np; p++)
+    {
+        double la = pnt->lat[P.row_n[p]];
+        ht[p] = std::sin(la);
+        hu[p] = std::cos(la);
+        hrn[p] = P.row_n[p];
+        hrs[p] = P.row_s[p];
+    }
+    void *dgeo = nullptr;
+    CB_TRY(buf(c, "geo", geo_bytes, &dgeo));
+    CB_CUDA(cudaMemcpyAsync(dgeo, hp, geo_bytes, cudaMemcpyHostToDevice,
+                            c.stream), st);
+    float4 *ab = nullptr;
+    double *smm = nullptr;
+    CB_TRY(tables_f32(c, (long long)nmax, &ab, &smm));
+    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
+    float4 *abcs = nullptr;
+    CB_TRY(dbuf(c, "abcs32", (size_t)(2 * T), &abcs));
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_pack_cs_f32((long long)nmax, (long long)shc_nmax, d_c,
+                                   d_s, ab, abcs, c.stream), st);
+    }
+    const int ldf = (int)(nlon / 2 + 1);
+    double2 *lc = nullptr;
+    CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldf, &lc));
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+    const int K = np >= 4096 ? 8 : (np >= 128 ? 4 : 2);
+    ShsF32Args A{};
+    A.nmax = (long long)nmax;
+    A.npairs = np;
+    A.ntiles = (np + 32 * K - 1) / (32 * K);
+    A.nitems = (long long)(nmax + 1) * A.ntiles;
+    A.abcs = abcs;
+    A.smm = smm;
+    A.t = static_cast<const double *>(dgeo);
+    A.u = A.t + np;
+    A.row_n = reinterpret_cast<const int *>(A.u + np);
+    A.row_s = A.row_n + np;
+    A.nlat = (int)nlat;
+    A.ldf = ldf;
+    A.out = lc;
+    A.mur = mu / R;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                        (long long)c.num_sms * 8);
+    {
+        Scope sc(c, TIMER_SHS);
+        CB_CUDA(launch_shs_grid_f32(A, K, std::max(grid, 1), c.stream), st);
+    }
+    RfftArgs R2 = *rf;
+    R2.nrows = (long long)nlat;
+    R2.x = reinterpret_cast<double *>(d_f);
+    R2.ldx = (long long)nlon;
+    R2.X = lc;
+    R2.ldX = ldf;
+    R2.kmax = (int)nmax;
+    R2.f32_rows = 1;
+    {
+        Scope sc(c, TIMER_FFT);
+        CB_CUDA(launch_rfft(R2, true, c.stream), st);
+    }
+    return finish(c, d_status);
+}
+
+Status sha_grid_f32(Context &c, const charm_point *pnt, const float *d_f,
+                    unsigned long nmax, double mu, double R,
+                    unsigned long shc_nmax, float *d_c, float *d_s)
+{
+    Status st;
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    const double r0 = pnt->r[0];
+    const RfftArgs *rf = nullptr;
+    CB_TRY(f32_grid_checks(c, pnt, nmax, r0, &rf));
+    if (reinterpret_cast<uintptr_t>(d_f) % 8 != 0)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "The grid values must start on an 8-byte boundary.";
+        return st;
+    }
+    const unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                       ? nlat - 1
+                                       : (nlat - 2) / 2;
+    // quadrature constant, src/sha/sha_point.c:313-322
+    double cq = (pnt->type == CHARM_CRD_POINT_GRID_DH2)
+                    ? PI / (double)(2 * nmax_grd + 2)
+                    : PI / (double)(nmax_grd + 1);
+    cq *= 1.0 / (4.0 * PI) * (r0 / mu);
+    Pairs P;
+    grid_pairs(pnt, charm_glob_threshold2, true, P);
+    const int np = (int)P.row_n.size();
+    size_t geo_bytes = (size_t)np * (4 * 8 + 2 * 4);
+    void *hp = nullptr;
+    CB_TRY(pinned(c, geo_bytes, &hp));
+    double *ht = static_cast<double *>(hp);
+    double *hu = ht + np;
+    double *hcn = hu + np;
+    double *hcs = hcn + np;
+    int *hrn = reinterpret_cast<int *>(hcs + np);
+    int *hrs = hrn + np;
+    for (int p = 0; p < np; p++)
+    {
+        double la = pnt->lat[P.row_n[p]];
+        ht[p] = std::sin(la);
+        hu[p] = std::cos(la);
+        hcn[p] = cq * pnt->w[P.row_n[p]];
+        hcs[p] = P.row_s[p] >= 0 ? cq * pnt->w[P.row_s[p]] : 0.0;
+        hrn[p] = P.row_n[p];
+        hrs[p] = P.row_s[p];
+    }
+    void *dgeo = nullptr;
+    CB_TRY(buf(c, "geo", geo_bytes, &dgeo));
+    CB_CUDA(cudaMemcpyAsync(dgeo, hp, geo_bytes, cudaMemcpyHostToDevice,
+                            c.stream), st);
+    float4 *ab = nullptr;
+    double *smm = nullptr;
+    CB_TRY(tables_f32(c, (long long)nmax, &ab, &smm));
+    const int ldF = (int)(nlon / 2 + 1);
+    double2 *F = nullptr;
+    CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
+    RfftArgs R2 = *rf;
+    R2.nrows = (long long)nlat;
+    R2.x = const_cast<double *>(reinterpret_cast<const double *>(d_f));
+    R2.ldx = (long long)nlon;
+    R2.X = F;
+    R2.ldX = ldF;
+    R2.kmax = (int)nmax;
+    R2.f32_rows = 1;
+    {
+        Scope sc(c, TIMER_FFT);
+        CB_CUDA(launch_rfft(R2, false, c.stream), st);
+    }
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+    const int K = np >= 4096 ? 8 : (np >= 128 ? 4 : 2);
+    const int ntiles = (np + 32 * K - 1) / (32 * K);
+    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
+    long long slots = (long long)c.num_sms * 8 * 4;
+    long long G = std::max<long long>(1, (2 * slots + nmax) / (nmax + 1));
+    G = std::min<long long>(G, ntiles);
+    int tpg = (int)((ntiles + G - 1) / G);
+    G = (ntiles + tpg - 1) / tpg;
+    float2 *part = nullptr;
+    CB_TRY(dbuf(c, "sha_part32", (size_t)G * T, &part));
+    ShaF32Args A{};
+    A.nmax = (long long)nmax;
+    A.npairs = np;
+    A.ntiles = ntiles;
+    A.ngroups = (int)G;
+    A.tiles_per_group = tpg;
+    A.nitems = (long long)(nmax + 1) * G;
+    A.ab = ab;
+    A.smm = smm;
+    A.t = static_cast<const double *>(dgeo);
+    A.u = A.t + np;
+    A.cw_n = A.u + np;
+    A.cw_s = A.cw_n + np;
+    A.row_n = reinterpret_cast<const int *>(A.cw_s + np);
+    A.row_s = A.row_n + np;
+    A.F = F;
+    A.ldF = ldF;
+    A.part = part;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                        (long long)c.num_sms * 8);
+    {
+        Scope sc(c, TIMER_SHA);
+        CB_CUDA(launch_sha_grid_f32(A, K, std::max(grid, 1), c.stream), st);
+    }
+    // rescaling from r0 to the coefficients' radius (as sha_grid)
+    double *dres = nullptr;
+    std::vector<double> res;
+    if (!nearly_equal(R, r0, charm_glob_threshold))
+    {
+        double r_ratio = r0 / R;
+        res.resize(nmax + 1);
+        double tmp2 = r_ratio;
+        res[0] = 1.0;
+        for (unsigned long n = 1; n <= nmax; n++)
+        {
+            res[n] = tmp2;
+            tmp2 *= r_ratio;
+        }
+        CB_TRY(dbuf(c, "sha_rescale", nmax + 1, &dres));
+        CB_CUDA(cudaMemcpyAsync(dres, res.data(), (nmax + 1) * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+    }
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_sha_reduce_f32((long long)nmax, (long long)shc_nmax,
+                                      (int)G, T, part, dres, d_c, d_s,
+                                      c.stream), st);
+    }
+    return finish(c, d_status);
+}
+
+// ---------------------------------------------------------------------------
 // Adjoint of the scattered synthesis with respect to the coefficients
 // ---------------------------------------------------------------------------
 // C_nm = (GM/R) sum_i g_i (R/r_i)^(n+1) P_nm(sin lat_i) cos(m lon_i), S_nm
@@ -1706,6 +2015,24 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
                     nullptr, d_c, d_s);
+}
+
+Status shs_point_dev_f32(const charm_point *pnt, unsigned long shc_nmax,
+                         double mu, double r, const float *d_c,
+                         const float *d_s, unsigned long nmax, float *d_f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return shs_grid_f32(g_ctx, pnt, shc_nmax, mu, r, d_c, d_s, nmax, d_f);
+}
+
+Status sha_point_dev_f32(const charm_point *pnt, const float *d_f,
+                         unsigned long nmax, double mu, double r,
+                         unsigned long shc_nmax, float *d_c, float *d_s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_grid_f32(g_ctx, pnt, d_f, nmax, mu, r, shc_nmax, d_c, d_s);
 }
 
 Status shs_point_sctr_adjoint(const charm_point *pnt, const double *g,

@@ -57,6 +57,16 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
                      unsigned long nmax, double mu, double r,
                      unsigned long shc_nmax, double *d_c, double *d_s);
 
+// Single-precision potential synthesis / analysis on grids whose rows admit
+// the shared-memory row transform, every row at r = R; float coefficient
+// triangles (degree shc_nmax) and float grid [nlat][nlon] in device memory.
+Status shs_point_dev_f32(const charm_point *pnt, unsigned long shc_nmax,
+                         double mu, double r, const float *d_c,
+                         const float *d_s, unsigned long nmax, float *d_f);
+Status sha_point_dev_f32(const charm_point *pnt, const float *d_f,
+                         unsigned long nmax, double mu, double r,
+                         unsigned long shc_nmax, float *d_c, float *d_s);
+
 // Adjoint of the scattered-point potential synthesis with respect to the
 // coefficients: shcs->c, shcs->s (degree shcs->nmax, zero above nmax)
 // receive sum_i g_i d f_i / d C_nm and d f_i / d S_nm for the model

@@ -95,6 +95,53 @@ struct SctrArgs
     unsigned *status;
 };
 
+// Single-precision grid synthesis and analysis (f32.cu): potential only,
+// r = R.  Same work split as the FP64 kernels.
+struct ShsF32Args
+{
+    long long nmax;
+    int npairs;
+    int ntiles;
+    long long nitems;
+    const float4 *abcs;    // (a, a, -b, -b), (C, C, S, S) per (n, m)
+    const double *smm;     // S_m = P_mm / u^m
+    const double *t;
+    const double *u;
+    const int *row_n;
+    const int *row_s;
+    int nlat;
+    int ldf;
+    double2 *out;          // lumped coefficients [nlat][ldf], FFTW packing
+    double mur;
+    double polar_thr;
+    unsigned long long *counter;
+    unsigned *status;
+};
+
+struct ShaF32Args
+{
+    long long nmax;
+    int npairs;
+    int ntiles;
+    int ngroups;
+    int tiles_per_group;
+    long long nitems;
+    const float4 *ab;      // (a_nm, a_nm, -b_nm, -b_nm) per (n, m)
+    const double *smm;
+    const double *t;
+    const double *u;
+    const int *row_n;
+    const int *row_s;
+    const double *cw_n;
+    const double *cw_s;
+    const double2 *F;
+    int ldF;
+    float2 *part;          // [ngroups][T] partial sums
+    double polar_thr;
+    unsigned long long *counter;
+    unsigned *status;
+};
+
 // Real <-> half-spectrum transforms of grid rows of even length L = 2H in
 // shared memory (rfft.cu).
 struct RfftArgs
@@ -114,6 +161,7 @@ struct RfftArgs
     double2 *X;            // half spectra, leading dimension ldX
     long long ldX;
     int kmax;              // spectrum entries read (inverse) / written (forward)
+    int f32_rows;          // 1: x points to float rows (converted on the fly)
 };
 
 // Size of the fixed device scratch of the allocation-free analysis
@@ -160,5 +208,19 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
 size_t rfft_smem_bytes(int M);
 cudaError_t rfft_set_smem(size_t smem);
 cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st);
+cudaError_t launch_tables_f32(long long nmax, const double *r,
+                              const double *ri, float4 *ab, cudaStream_t st);
+cudaError_t launch_pack_cs_f32(long long nmax, long long shc_nmax,
+                               const float *c, const float *s,
+                               const float4 *ab, float4 *abcs,
+                               cudaStream_t st);
+cudaError_t launch_shs_grid_f32(const ShsF32Args &A, int K, int grid,
+                                cudaStream_t st);
+cudaError_t launch_sha_grid_f32(const ShaF32Args &A, int K, int grid,
+                                cudaStream_t st);
+cudaError_t launch_sha_reduce_f32(long long nmax, long long shc_nmax,
+                                  int ngroups, long long T,
+                                  const float2 *part, const double *rescale,
+                                  float *c, float *s, cudaStream_t st);
 
 } // namespace cb

@@ -325,6 +325,22 @@ struct SrcRow
     }
 };
 
+// Analysis input from float rows (the single-precision mode)
+struct SrcRowF
+{
+    const float2 *x2;
+    const double2 *w;
+    int H;
+    __device__ __forceinline__ double2 operator()(int i) const
+    {
+        if (i >= H)
+            return make_double2(0.0, 0.0);
+        const float2 f = x2[i];
+        double2 z = make_double2((double)f.x, (double)f.y);
+        return w ? cmul(z, __ldg(&w[i])) : z;
+    }
+};
+
 // Synthesis input: conj Z_k times the chirp, with
 // Z_k = (X_k + conj X_H-k) + i e^(i pi k/H) (X_k - conj X_H-k) and X_k = 0
 // above kmax (the inverse DFT is conj(DFT(conj Z))).
@@ -372,16 +388,26 @@ struct SrcKernel
 // Analysis direction: real rows x[row][0..L) -> X[row][0..kmax]; one CTA
 // per row (a loop over rows would let the compiler hoist every pass's
 // twiddles out of it and run out of registers).
-template <int V, int NR>
+template <int V, int NR, bool F32>
 __global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
 {
     extern __shared__ __align__(16) double2 s[];
     const int tid = threadIdx.x, T = blockDim.x;
     const int H = A.H;
     const long long row = blockIdx.x;
-    SrcRow src{reinterpret_cast<const double2 *>(A.x + row * A.ldx),
-               A.direct ? nullptr : A.w, H};
-    dft_h<V>(s, A, tid, T, src);
+    if constexpr (F32)
+    {
+        const float *xf = reinterpret_cast<const float *>(A.x);
+        SrcRowF src{reinterpret_cast<const float2 *>(xf + row * A.ldx),
+                    A.direct ? nullptr : A.w, H};
+        dft_h<V>(s, A, tid, T, src);
+    }
+    else
+    {
+        SrcRow src{reinterpret_cast<const double2 *>(A.x + row * A.ldx),
+                   A.direct ? nullptr : A.w, H};
+        dft_h<V>(s, A, tid, T, src);
+    }
     double2 *X = A.X + row * A.ldX;
     for (int k = tid; k <= A.kmax; k += T)
     {
@@ -396,7 +422,7 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
 }
 
 // Synthesis direction: X[row][0..kmax] (zero above) -> real rows x[row].
-template <int V, int NR>
+template <int V, int NR, bool F32>
 __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
 {
     extern __shared__ __align__(16) double2 s[];
@@ -405,9 +431,22 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
     SrcSpectrum src{A.X + row * A.ldX, A.direct ? nullptr : A.w, A.ht, A.H,
                     A.kmax};
     dft_h<V>(s, A, tid, T, src);
-    double2 *x2 = reinterpret_cast<double2 *>(A.x + row * A.ldx);
-    for (int j = tid; j < A.H; j += T)
-        x2[j] = conj2(dft_h_out(s, A, j));
+    if constexpr (F32)
+    {
+        float *xf = reinterpret_cast<float *>(A.x);
+        float2 *x2 = reinterpret_cast<float2 *>(xf + row * A.ldx);
+        for (int j = tid; j < A.H; j += T)
+        {
+            const double2 z = conj2(dft_h_out(s, A, j));
+            x2[j] = make_float2((float)z.x, (float)z.y);
+        }
+    }
+    else
+    {
+        double2 *x2 = reinterpret_cast<double2 *>(A.x + row * A.ldx);
+        for (int j = tid; j < A.H; j += T)
+            x2[j] = conj2(dft_h_out(s, A, j));
+    }
 }
 
 // Tables of one transform length: twiddles exp(-2 pi i k / M), chirp
@@ -475,8 +514,10 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
 
 cudaError_t rfft_set_smem(size_t smem)
 {
-    const void *fns[] = {(const void *)k_rfft_fwd<16, 96>,
-                         (const void *)k_rfft_inv<16, 96>,
+    const void *fns[] = {(const void *)k_rfft_fwd<16, 96, false>,
+                         (const void *)k_rfft_inv<16, 96, false>,
+                         (const void *)k_rfft_fwd<16, 96, true>,
+                         (const void *)k_rfft_inv<16, 96, true>,
                          (const void *)k_rfft_kernel_spectrum<16, 96>};
     for (const void *f : fns)
     {
@@ -495,10 +536,17 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         return cudaSuccess;
     const size_t smem = rfft_smem_bytes(A.M);
     const int T = A.M / 16;
-    if (inverse)
-        k_rfft_inv<16, 96><<<grid, T, smem, st>>>(A);
+    if (A.f32_rows)
+    {
+        if (inverse)
+            k_rfft_inv<16, 96, true><<<grid, T, smem, st>>>(A);
+        else
+            k_rfft_fwd<16, 96, true><<<grid, T, smem, st>>>(A);
+    }
+    else if (inverse)
+        k_rfft_inv<16, 96, false><<<grid, T, smem, st>>>(A);
     else
-        k_rfft_fwd<16, 96><<<grid, T, smem, st>>>(A);
+        k_rfft_fwd<16, 96, false><<<grid, T, smem, st>>>(A);
     return cudaGetLastError();
 }
 

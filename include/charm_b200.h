@@ -229,6 +229,23 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev(
     double r, unsigned long shc_nmax, double *d_c, double *d_s,
     charm_err *err);
 
+/* Single-precision mode of the device-resident potential synthesis and
+ * analysis: the Legendre recurrence and sums in FP32 (as CHarm's float
+ * build, charmf_shs_point / charmf_sha_point, does them), the longitude
+ * transforms in FP64; float coefficient triangles (degree shc_nmax,
+ * order-major) and a float grid [nlat][nlon] in device memory.  Grids whose
+ * longitudes are 0, 2 pi / nlon, ... with even nlon (the quadrature grids
+ * and such user grids), every row at the coefficients' radius r;
+ * anything else is rejected with CHARM_EFUNCARG. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_dev_f32(
+    const charm_point *pnt, unsigned long shc_nmax, double mu, double r,
+    const float *d_c, const float *d_s, unsigned long nmax, float *d_f,
+    charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev_f32(
+    const charm_point *pnt, const float *d_f, unsigned long nmax, double mu,
+    double r, unsigned long shc_nmax, float *d_c, float *d_s,
+    charm_err *err);
+
 /* Adjoint of charm_shs_point on scattered points with respect to the
  * coefficients (no counterpart in CHarm, which has no transpose routine;
  * the forward it transposes is src/shs/shs_point_sctr.c:86-728): for the
