@@ -1048,6 +1048,263 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
 }
 
 // ---------------------------------------------------------------------------
+// Batched synthesis: many coefficient sets on one grid
+// ---------------------------------------------------------------------------
+// All sets share the grid, its geometry, the recurrence tables of the
+// largest degree and one persistent launch per derivative kind; each work
+// item (set, order, latitude tile) stops at its set's own nmax.  kgrad 0:
+// potential, 1: grad1, 2: grad2, 3: all ten quantities (potential, grad1
+// x y z, grad2 xx xy xz yy yz zz, in CHarm's output order) per set.
+Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
+                 const unsigned long *nmax_v, const unsigned long *shc_nmax_v,
+                 const double *mu_v, double R, const double *const *d_c,
+                 const double *const *d_s, int kgrad, double *const *d_f)
+{
+    Status st;
+    const double thr = charm_glob_threshold, thr2 = charm_glob_threshold2;
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    unsigned long N = 0;
+    for (size_t j = 0; j < nsets; j++)
+        N = std::max(N, nmax_v[j]);
+    if (pnt->type == CHARM_CRD_POINT_GRID && nlon > 1)
+    {
+        double step = pnt->lon[1] - pnt->lon[0];
+        for (size_t j = 1; j < nlon; j++)
+            if (!(step > 0.0) ||
+                !nearly_equal(step, pnt->lon[j] - pnt->lon[j - 1], thr2))
+            {
+                st.code = CHARM_EFUNCARG;
+                st.msg = "\"pnt->lon\" is not a linearly increasing array "
+                         "within the \"threshold2\".";
+                return st;
+            }
+    }
+    double dlon_step = nlon > 1 ? pnt->lon[1] - pnt->lon[0] : 0.0;
+    const bool use_fft = (nlon >= 1) && ((nlon - 1) / 2 >= N) &&
+                         nearly_equal(pnt->lon[0], 0.0, thr) &&
+                         nearly_equal(pnt->lon[nlon - 1] + dlon_step, 2.0 * PI,
+                                      thr);
+    if (!use_fft)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "The batched synthesis needs a grid with FFT longitudes "
+                 "(0, 2 pi / nlon, ..., nlon > 2 nmax).";
+        return st;
+    }
+    bool r_eq = true;
+    for (size_t i = 0; i < nlat; i++)
+        if (!nearly_equal(pnt->r[i], R, thr))
+        {
+            r_eq = false;
+            break;
+        }
+    Pairs P;
+    grid_pairs(pnt, thr2, true, P);
+    if (!r_eq)
+        for (size_t p = 0; p < P.row_n.size(); p++)
+            if (P.row_s[p] >= 0 && P.row_s[p] < (int)nlat &&
+                pnt->r[P.row_s[p]] != pnt->r[P.row_n[p]])
+            {
+                grid_pairs(pnt, thr2, false, P);
+                break;
+            }
+    const int np = (int)P.row_n.size();
+    size_t geo_bytes = (size_t)np * (3 * 8 + 2 * 4);
+    void *hp = nullptr;
+    CB_TRY(pinned(c, geo_bytes, &hp));
+    double *ht = static_cast<double *>(hp);
+    double *hu = ht + np;
+    double *hrho = hu + np;
+    int *hrn = reinterpret_cast<int *>(hrho + np);
+    int *hrs = hrn + np;
+    for (int p = 0; p < np; p++)
+    {
+        double la = pnt->lat[P.row_n[p]];
+        ht[p] = std::sin(la);
+        hu[p] = std::cos(la);
+        hrho[p] = r_eq ? 1.0 : R / pnt->r[P.row_n[p]];
+        hrn[p] = P.row_n[p];
+        hrs[p] = P.row_s[p];
+    }
+    void *dgeo = nullptr;
+    CB_TRY(buf(c, "geo", geo_bytes, &dgeo));
+    CB_CUDA(cudaMemcpyAsync(dgeo, hp, geo_bytes, cudaMemcpyHostToDevice,
+                            c.stream), st);
+    const double *dt = static_cast<const double *>(dgeo);
+
+    Tabs tab;
+    CB_TRY(tables(c, (long long)N, &tab));
+    const long long T = (long long)(N + 1) * (N + 2) / 2;
+    double2 *cs_all = nullptr;
+    CB_TRY(dbuf(c, "batch_cs", (size_t)nsets * T, &cs_all));
+    for (size_t j = 0; j < nsets; j++)
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_scale_cs_set((long long)N, (long long)nmax_v[j],
+                                    (long long)shc_nmax_v[j], d_c[j], d_s[j],
+                                    tab.tc, cs_all + (size_t)j * T, c.stream),
+                st);
+    }
+    const RfftArgs *rf = nullptr;
+    CB_TRY(row_fft(c, (long long)nlon, &rf));
+    const int ldf = (int)(nlon / 2 + 1);
+    const size_t grid_sz = nlat * nlon;
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+
+    // derivative kinds of this call and where their components go in the
+    // caller's per-set output (CHarm's order after its pointer reordering,
+    // src/shs/shs_point_gradn.c:133-165)
+    struct Kind
+    {
+        int kgrad, npar, base;
+        int slot[6];
+    };
+    std::vector<Kind> kinds;
+    const Kind K0{0, 1, 0, {0}};
+    const Kind K1{1, 3, 0, {1, 2, 0}};
+    const Kind K2{2, 6, 0, {3, 4, 1, 5, 2, 0}};
+    if (kgrad == 0 || kgrad == 3)
+        kinds.push_back(K0);
+    if (kgrad == 1 || kgrad == 3)
+    {
+        kinds.push_back(K1);
+        kinds.back().base = kgrad == 3 ? 1 : 0;
+    }
+    if (kgrad == 2 || kgrad == 3)
+    {
+        kinds.push_back(K2);
+        kinds.back().base = kgrad == 3 ? 4 : 0;
+    }
+    const int ncomp = kgrad == 3 ? 10 : kinds[0].npar;
+    for (const Kind &kd : kinds)
+    {
+        const int kg = kd.kgrad, npar = kd.npar;
+        const int dd = kg;   // grad kinds: dr = dlat = dlon = kgrad
+        // sets per launch, bounded by the lumped-coefficient buffer (8 GB)
+        const size_t per_set = (size_t)npar * nlat * ldf * sizeof(double2);
+        size_t bsz = std::max<size_t>(1, ((size_t)8 << 30) / per_set);
+        bsz = std::min(bsz, nsets);
+        double2 *lc = nullptr;
+        CB_TRY(dbuf(c, "batch_lumped", bsz * per_set / sizeof(double2), &lc));
+        BatchSet *dsets = nullptr;
+        CB_TRY(dbuf(c, "batch_sets", bsz, &dsets));
+        std::vector<BatchSet> hsets(bsz);
+        const int K = choose_k(kg, dd, np);
+        const int ntiles = (np + 32 * K - 1) / (32 * K);
+        for (size_t j0 = 0; j0 < nsets; j0 += bsz)
+        {
+            const size_t nb = std::min(bsz, nsets - j0);
+            long long items = 0;
+            for (size_t b = 0; b < nb; b++)
+            {
+                const size_t j = j0 + b;
+                double mur;
+                int dorder, npar_j;
+                mur_dorder(mu_v[j], R, kg, dd, dd, dd, &mur, &dorder,
+                           &npar_j);
+                hsets[b].nmax = (long long)nmax_v[j];
+                hsets[b].item0 = items;
+                hsets[b].cs = cs_all + j * T;
+                hsets[b].out = lc + b * (per_set / sizeof(double2));
+                hsets[b].mur = mur;
+                hsets[b].polar_thr = polar_threshold(nmax_v[j]);
+                items += (long long)(nmax_v[j] + 1) * ntiles;
+            }
+            CB_CUDA(cudaMemcpyAsync(dsets, hsets.data(),
+                                    nb * sizeof(BatchSet),
+                                    cudaMemcpyHostToDevice, c.stream), st);
+            if (!rf)
+                CB_CUDA(cudaMemsetAsync(lc, 0, nb * per_set, c.stream), st);
+            CB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long),
+                                    c.stream), st);
+            ShsGridArgs A{};
+            A.nmax = (long long)N;
+            A.npairs = np;
+            A.ntiles = ntiles;
+            A.nitems = items;
+            A.tb = tab.tb;
+            A.tmul = tab.tmul;
+            A.ldmul = tab.ldmul;
+            A.sg = tab.sg;
+            A.t = dt;
+            A.u = dt + np;
+            A.rho = dt + 2 * np;
+            A.row_n = reinterpret_cast<const int *>(dt + 3 * np);
+            A.row_s = A.row_n + np;
+            A.nlat = (int)nlat;
+            A.ldf = ldf;
+            A.fft_pack = 1;
+            A.dlon = dd;
+            A.counter = d_counter;
+            A.status = d_status;
+            A.sets = dsets;
+            A.nsets = (int)nb;
+            int grid = (int)std::min<long long>((items + 3) / 4,
+                                                (long long)c.num_sms * 8);
+            {
+                Scope sc(c, TIMER_SHS);
+                CB_CUDA(launch_shs_grid(A, kg, dd, dd, !r_eq, K,
+                                        std::max(grid, 1), c.stream), st);
+            }
+            // longitude transforms, component by component into the
+            // caller's output slots
+            for (size_t b = 0; b < nb; b++)
+                for (int q = 0; q < npar; q++)
+                {
+                    double *dst = d_f[j0 + b] +
+                                  (size_t)(kd.base + kd.slot[q]) * grid_sz;
+                    double2 *src = lc + b * (per_set / sizeof(double2)) +
+                                   (size_t)q * nlat * ldf;
+                    if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
+                    {
+                        RfftArgs R2 = *rf;
+                        R2.nrows = (long long)nlat;
+                        R2.x = dst;
+                        R2.ldx = (long long)nlon;
+                        R2.X = src;
+                        R2.ldX = ldf;
+                        R2.kmax = (int)N;
+                        Scope sc(c, TIMER_FFT);
+                        CB_CUDA(launch_rfft(R2, true, c.stream), st);
+                    }
+                    else
+                    {
+                        if (rf)
+                        {
+                            // the row transform reads orders <= nmax only;
+                            // the library one needs the rest zero
+                            st.code = CHARM_EFUNCARG;
+                            st.msg = "batched synthesis outputs must start "
+                                     "on a 16-byte boundary";
+                            return st;
+                        }
+                        cufftHandle h;
+                        CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)nlat,
+                                    &h));
+                        Scope sc(c, TIMER_FFT, false);
+                        if (cufftExecZ2D(h,
+                                         reinterpret_cast<cufftDoubleComplex *>(
+                                             src),
+                                         dst) != CUFFT_SUCCESS)
+                        {
+                            st.code = CHARM_EFUNCARG;
+                            st.msg = "cuFFT Z2D failed";
+                            return st;
+                        }
+                    }
+                }
+            // the set descriptors and the lumped buffer are reused by the
+            // next sub-batch: wait for this one
+            CB_CUDA(cudaStreamSynchronize(c.stream), st);
+        }
+    }
+    (void)ncomp;
+    return finish(c, d_status);
+}
+
+// ---------------------------------------------------------------------------
 // Single-precision mode (f32.cu): potential on FFT grids, r = R
 // ---------------------------------------------------------------------------
 // Tables (a_nm, b_nm) in float and S_m in double, built once per nmax.
@@ -2015,6 +2272,19 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
                     nullptr, d_c, d_s);
+}
+
+Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
+                           const unsigned long *nmax,
+                           const unsigned long *shc_nmax, const double *mu,
+                           double r, const double *const *d_c,
+                           const double *const *d_s, int kgrad,
+                           double *const *d_f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return shs_batch(g_ctx, pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
+                     kgrad, d_f);
 }
 
 Status shs_point_dev_f32(const charm_point *pnt, unsigned long shc_nmax,

@@ -57,6 +57,18 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
                      unsigned long nmax, double mu, double r,
                      unsigned long shc_nmax, double *d_c, double *d_s);
 
+// Batched synthesis of nsets coefficient sets (degree shc_nmax[j], maximum
+// degree nmax[j], scaling mu[j], common reference radius r; device
+// triangles d_c[j], d_s[j]) on one grid with FFT longitudes; kgrad 0, 1, 2
+// or 3 (potential, grad1 and grad2: ten quantities); d_f[j] receives
+// ncomp x nlat x nlon doubles in CHarm's component order.
+Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
+                           const unsigned long *nmax,
+                           const unsigned long *shc_nmax, const double *mu,
+                           double r, const double *const *d_c,
+                           const double *const *d_s, int kgrad,
+                           double *const *d_f);
+
 // Single-precision potential synthesis / analysis on grids whose rows admit
 // the shared-memory row transform, every row at r = R; float coefficient
 // triangles (degree shc_nmax) and float grid [nlat][nlon] in device memory.

@@ -7,6 +7,19 @@
 namespace cb
 {
 
+// One coefficient set of a batched synthesis: its degree, its first work
+// item, its scaled coefficients (in the layout of the shared tables' degree)
+// and its lumped-coefficient output.
+struct BatchSet
+{
+    long long nmax;
+    long long item0;
+    const double2 *cs;
+    double2 *out;
+    double mur;
+    double polar_thr;
+};
+
 // Grid synthesis: lumped coefficients out[q][row][m] of every output
 // component q, row and order m (shs_grid.cu).  tb, tmul, sg are the
 // recurrence tables of leg.cuh / tables.cu.
@@ -35,6 +48,11 @@ struct ShsGridArgs
     double polar_thr;      // polar optimisation threshold, < 0 when off
     unsigned long long *counter;
     unsigned *status;
+    // batched sets (nsets > 0): each item belongs to the set j with
+    // sets[j].item0 <= item < sets[j + 1].item0, whose nmax (<= the tables'
+    // nmax), cs, out, mur and polar_thr replace the fields above
+    const BatchSet *sets;
+    int nsets;
 };
 
 // Grid analysis: C_nm, S_nm partial sums per latitude group (sha_grid.cu).
@@ -178,6 +196,11 @@ cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
 cudaError_t launch_scale_cs(long long nmax, long long shc_nmax,
                             const double *c, const double *s,
                             const double *tc, double2 *cs, cudaStream_t st);
+// same into the layout of degree ntab >= nmax (zero above nmax)
+cudaError_t launch_scale_cs_set(long long ntab, long long nmax,
+                                long long shc_nmax, const double *c,
+                                const double *s, const double *tc,
+                                double2 *cs, cudaStream_t st);
 cudaError_t launch_shs_grid(const ShsGridArgs &A, int kgrad, int dr,
                             int dlat, bool rr, int K, int grid,
                             cudaStream_t st);

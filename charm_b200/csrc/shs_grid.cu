@@ -66,8 +66,34 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= (unsigned long long)A.nitems)
             break;
-        const long long m = (long long)(item / (unsigned long long)A.ntiles);
-        const int tile = (int)(item % (unsigned long long)A.ntiles);
+        // batched sets: find the set of this item (items of set j start at
+        // sets[j].item0), its degree, coefficients and output
+        long long Nset = N;
+        const double2 *csp = A.cs;
+        double2 *outp = A.out;
+        double mur = A.mur, polar_thr = A.polar_thr;
+        unsigned long long local = item;
+        if (A.nsets > 0)
+        {
+            int lo = 0, hi = A.nsets - 1;
+            while (lo < hi)
+            {
+                int mid = (lo + hi + 1) >> 1;
+                if ((unsigned long long)A.sets[mid].item0 <= item)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const BatchSet &bs = A.sets[lo];
+            Nset = bs.nmax;
+            csp = bs.cs;
+            outp = bs.out;
+            mur = bs.mur;
+            polar_thr = bs.polar_thr;
+            local = item - (unsigned long long)bs.item0;
+        }
+        const long long m = (long long)(local / (unsigned long long)A.ntiles);
+        const int tile = (int)(local % (unsigned long long)A.ntiles);
         const double sigma = A.sg[2 * m];
 
         // ---- geometry and seeds of this lane's latitude pairs ----------
@@ -75,7 +101,7 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
         double tq[K], tu[K], urr[K], u2r[K], uk[K], rho1[K], rho2[K];
         double x[K], y[K];
         int E[K];
-        bool polar_skip = A.polar_thr >= 0.0;
+        bool polar_skip = polar_thr >= 0.0;
 #pragma unroll
         for (int k = 0; k < K; k++)
         {
@@ -101,7 +127,7 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
                 x[k] = 0.0;
                 E[k] = 0;
             }
-            if (valid && !((double)m - (double)N * u > A.polar_thr))
+            if (valid && !((double)m - (double)Nset * u > polar_thr))
                 polar_skip = false;
         }
         polar_skip = __all_sync(0xffffffffu, polar_skip);
@@ -111,8 +137,10 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
 
         if (!polar_skip)
         {
+            // table offsets of the degree-N triangle; a set of lower degree
+            // (coefficients in the same layout) stops at its own nmax
             const long long c0 = tri_col0(N, m);
-            const long long ncol = N - m + 1;
+            const long long ncol = Nset - m + 1;
             const int nchunks = (int)((ncol + LEG_CHUNK - 1) / LEG_CHUNK);
             auto issue = [&](int j, int s) {
                 if (lane == 0)
@@ -124,7 +152,7 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
                     unsigned bytes = (unsigned)(cnt * sizeof(double2));
                     mbar_arrive_expect_tx(&bar[s], 2 * bytes);
                     bulk_g2s(stg(s), A.tb + off, bytes, &bar[s]);
-                    bulk_g2s(stg(s) + LEG_CHUNK, A.cs + off, bytes, &bar[s]);
+                    bulk_g2s(stg(s) + LEG_CHUNK, csp + off, bytes, &bar[s]);
                 }
             };
             issue(0, 0);
@@ -344,8 +372,8 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
                 for (int q = 0; q < NQ; q++)
                 {
                     size_t o = ((size_t)q * A.nlat + row) * (size_t)A.ldf + m;
-                    A.out[o] = make_double2(cpack * A.mur * a[q],
-                                            sgnb * (cpack * A.mur * b[q]));
+                    outp[o] = make_double2(cpack * mur * a[q],
+                                           sgnb * (cpack * mur * b[q]));
                 }
             }
         }

@@ -142,6 +142,32 @@ __global__ void k_scale_cs(long long nmax, long long shc_nmax,
     }
 }
 
+// k_scale_cs for one set of a batch: the degree-nmax set in the layout of
+// the degree-ntab tables, zero above nmax.
+__global__ void k_scale_cs_set(long long ntab, long long nmax,
+                               long long shc_nmax,
+                               const double *__restrict__ c,
+                               const double *__restrict__ s,
+                               const double *__restrict__ tc, double2 *cs)
+{
+    long long m = blockIdx.x;
+    if (m > ntab)
+        return;
+    long long c0 = tri_col0(ntab, m);
+    long long s0 = tri_col0(shc_nmax, m);
+    for (long long n = m + threadIdx.x; n <= ntab; n += blockDim.x)
+    {
+        double2 v = make_double2(0.0, 0.0);
+        if (n <= nmax)
+        {
+            double k = tc[c0 + n - m];
+            v = make_double2(k * c[s0 + n - m],
+                             m == 0 ? 0.0 : k * s[s0 + n - m]);
+        }
+        cs[c0 + n - m] = v;
+    }
+}
+
 // Sums the group partials of the analysis, applies ct_n, a constant factor
 // and the degree-wise rescaling of src/shc/shc_rescale.c (rescale[n], or
 // none when null), and writes C, S in the caller's layout (degree shc_nmax,
@@ -191,6 +217,17 @@ cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
     int blocks = (int)((nmax + 1 + threads - 1) / threads);
     k_tables<<<blocks, threads, 0, st>>>(nmax, r, ri, smm, tb, tc, tmul,
                                           ldmul, sg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_cs_set(long long ntab, long long nmax,
+                                long long shc_nmax, const double *c,
+                                const double *s, const double *tc,
+                                double2 *cs, cudaStream_t st)
+{
+    // orders above nmax are never read: only columns m <= nmax are written
+    k_scale_cs_set<<<(int)(nmax + 1), 128, 0, st>>>(ntab, nmax, shc_nmax, c,
+                                                     s, tc, cs);
     return cudaGetLastError();
 }
 

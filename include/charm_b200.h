@@ -229,6 +229,22 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev(
     double r, unsigned long shc_nmax, double *d_c, double *d_s,
     charm_err *err);
 
+/* Batched synthesis of nsets coefficient sets on one grid (no counterpart
+ * in CHarm, which synthesises one set per charm_shs_point call): set j has
+ * device triangles d_c[j], d_s[j] of degree shc_nmax[j] (order-major),
+ * maximum degree nmax[j] and scaling mu[j]; all share the reference radius
+ * r.  kgrad 0: the potential; 1: grad1 (x, y, z); 2: grad2 (xx, xy, xz, yy,
+ * yz, zz); 3: all ten quantities in that order.  d_f[j] (device) receives
+ * ncomp x nlat x nlon doubles, components in that order (CHarm's order after
+ * its pointer reordering, src/shs/shs_point_gradn.c:133-165).  The grid
+ * needs FFT longitudes (0, 2 pi / nlon, ..., nlon > 2 max nmax); every work
+ * item (set, order, latitude tile) of a derivative kind runs in one launch. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_dev(
+    const charm_point *pnt, size_t nsets, const unsigned long *nmax,
+    const unsigned long *shc_nmax, const double *mu, double r,
+    const double *const *d_c, const double *const *d_s, int kgrad,
+    double *const *d_f, charm_err *err);
+
 /* Single-precision mode of the device-resident potential synthesis and
  * analysis: the Legendre recurrence and sums in FP32 (as CHarm's float
  * build, charmf_shs_point / charmf_sha_point, does them), the longitude
