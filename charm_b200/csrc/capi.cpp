@@ -707,6 +707,48 @@ void charm_b200_shs_point_batch_dev(const charm_point *pnt, size_t nsets,
                                    d_s, kgrad, d_f));
 }
 
+// Split-precision batched synthesis: the same call with the degree sums on
+// the tensor cores.  kgrad 0 (the potential).
+void charm_b200_shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
+                                       const unsigned long *nmax,
+                                       const unsigned long *shc_nmax,
+                                       const double *mu, double r,
+                                       const double *const *d_c,
+                                       const double *const *d_s, int kgrad,
+                                       double *const *d_f, charm_err *err)
+{
+    if (kgrad != 0)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The split-precision batched synthesis computes the "
+                "potential (\"kgrad = 0\").");
+        return;
+    }
+    if (!(pnt->type == CHARM_CRD_POINT_GRID ||
+          is_quad_type(pnt->type)))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The batched synthesis works on grids (\"pnt->type\").");
+        return;
+    }
+    for (size_t j = 0; j < nsets; j++)
+        if (nmax[j] > shc_nmax[j])
+        {
+            char msg[CHARM_ERR_MAX_MSG];
+            snprintf(msg, sizeof msg,
+                     "Set %zu: \"nmax = %lu\" cannot be larger than the "
+                     "degree of its coefficients \"%lu\".",
+                     j, nmax[j], shc_nmax[j]);
+            SET_ERR(err, CHARM_EFUNCARG, msg);
+            return;
+        }
+    if (nsets == 0 || pnt->npoint == 0)
+        return;
+    report(err, __func__,
+           cb::shs_point_batch_i8_dev(pnt, nsets, nmax, shc_nmax, mu, r, d_c,
+                                      d_s, d_f));
+}
+
 // Single-precision mode: no CHarm counterpart at this ABI level (CHarm's
 // float build is a separate library, charmf_*); the checks mirror the
 // double-precision device entry points.

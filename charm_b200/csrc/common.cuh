@@ -7,15 +7,11 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "kernels.h"
+
 namespace cb
 {
 
-// Error bits written by kernels into the per-call device status word.
-enum : unsigned
-{
-    DEV_ERR_WAIT_TIMEOUT = 1u,   // an mbarrier wait exceeded its limit
-    DEV_ERR_BAD_ARGS = 2u        // a kernel received inconsistent sizes
-};
 
 // Index of C_nm in an order-major triangle of maximum degree nmax:
 // column m starts at m (2 nmax + 3 - m) / 2 (CHarm's layout,

@@ -61,6 +61,7 @@ struct Context
     size_t pinned_bytes = 0;
     long long tab_nmax = -1;     // recurrence tables of this maximum degree
     long long tab32_nmax = -1;   // single-precision tables of this degree
+    long long tcp_nmax = -1;     // padded ct_n rows of the tensor-core path
     std::map<std::tuple<int, int, long long>, cufftHandle> plans;
     std::map<long long, RfftArgs> rffts;   // row transforms by row length
     std::map<long long, void *> rfft_mem;  // their tables
@@ -693,6 +694,10 @@ Status finish(Context &c, unsigned *d_status)
         st.code = CHARM_EFUNCARG;
         st.msg = "A GPU kernel reported an internal error (status " +
                  std::to_string(h_status) + ").";
+        if (h_status == DEV_ERR_TC_RANGE)
+            st.msg = "The split-precision synthesis met a Legendre value "
+                     "outside its fixed-point range (status " +
+                     std::to_string(h_status) + ").";
     }
     return st;
 }
@@ -1047,25 +1052,23 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
     return finish(c, d_status);
 }
 
-// ---------------------------------------------------------------------------
-// Batched synthesis: many coefficient sets on one grid
-// ---------------------------------------------------------------------------
-// All sets share the grid, its geometry, the recurrence tables of the
-// largest degree and one persistent launch per derivative kind; each work
-// item (set, order, latitude tile) stops at its set's own nmax.  kgrad 0:
-// potential, 1: grad1, 2: grad2, 3: all ten quantities (potential, grad1
-// x y z, grad2 xx xy xz yy yz zz, in CHarm's output order) per set.
-Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
-                 const unsigned long *nmax_v, const unsigned long *shc_nmax_v,
-                 const double *mu_v, double R, const double *const *d_c,
-                 const double *const *d_s, int kgrad, double *const *d_f)
+// Grid checks, latitude pairs and their geometry on the device for the
+// batched syntheses: FFT longitudes are required; r may vary by latitude
+// (pairs only where the mirror row has the same radius).
+struct BatchGeo
+{
+    Pairs P;
+    int np = 0;
+    bool r_eq = true;
+    const double *dt = nullptr;   // t[np], u[np], rho[np], row_n, row_s
+};
+
+Status batch_geometry(Context &c, const charm_point *pnt, unsigned long N,
+                      double R, BatchGeo *G)
 {
     Status st;
     const double thr = charm_glob_threshold, thr2 = charm_glob_threshold2;
     const size_t nlat = pnt->nlat, nlon = pnt->nlon;
-    unsigned long N = 0;
-    for (size_t j = 0; j < nsets; j++)
-        N = std::max(N, nmax_v[j]);
     if (pnt->type == CHARM_CRD_POINT_GRID && nlon > 1)
     {
         double step = pnt->lon[1] - pnt->lon[0];
@@ -1098,7 +1101,7 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
             r_eq = false;
             break;
         }
-    Pairs P;
+    Pairs &P = G->P;
     grid_pairs(pnt, thr2, true, P);
     if (!r_eq)
         for (size_t p = 0; p < P.row_n.size(); p++)
@@ -1131,6 +1134,41 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
     CB_CUDA(cudaMemcpyAsync(dgeo, hp, geo_bytes, cudaMemcpyHostToDevice,
                             c.stream), st);
     const double *dt = static_cast<const double *>(dgeo);
+
+    G->np = np;
+    G->r_eq = r_eq;
+    G->dt = dt;
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// Batched synthesis: many coefficient sets on one grid
+// ---------------------------------------------------------------------------
+// All sets share the grid, its geometry, the recurrence tables of the
+// largest degree and one persistent launch per derivative kind; each work
+// item (set, order, latitude tile) stops at its set's own nmax.  kgrad 0:
+// potential, 1: grad1, 2: grad2, 3: all ten quantities (potential, grad1
+// x y z, grad2 xx xy xz yy yz zz, in CHarm's output order) per set.
+Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
+                 const unsigned long *nmax_v, const unsigned long *shc_nmax_v,
+                 const double *mu_v, double R, const double *const *d_c,
+                 const double *const *d_s, int kgrad, double *const *d_f)
+{
+    Status st;
+    const double thr = charm_glob_threshold, thr2 = charm_glob_threshold2;
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    unsigned long N = 0;
+    for (size_t j = 0; j < nsets; j++)
+        N = std::max(N, nmax_v[j]);
+    BatchGeo G;
+    CB_TRY(batch_geometry(c, pnt, N, R, &G));
+    const Pairs &P = G.P;
+    const int np = G.np;
+    const bool r_eq = G.r_eq;
+    const double *dt = G.dt;
+    (void)thr;
+    (void)thr2;
+    (void)P;
 
     Tabs tab;
     CB_TRY(tables(c, (long long)N, &tab));
@@ -1265,7 +1303,10 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                         R2.ldx = (long long)nlon;
                         R2.X = src;
                         R2.ldX = ldf;
-                        R2.kmax = (int)N;
+                        // orders above this set's degree are not written
+                        // by the kernel (the buffer is reused): the row
+                        // transform takes them as zero
+                        R2.kmax = (int)nmax_v[j0 + b];
                         Scope sc(c, TIMER_FFT);
                         CB_CUDA(launch_rfft(R2, true, c.stream), st);
                     }
@@ -1301,6 +1342,182 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
         }
     }
     (void)ncomp;
+    return finish(c, d_status);
+}
+
+// ---------------------------------------------------------------------------
+// Batched synthesis with the degree sums on the tensor cores (shs_tc.cu)
+// ---------------------------------------------------------------------------
+// The potential of up to SHS_TC_SETS sets per launch: their coefficients
+// are cut into INT8 digit tiles once per call, one persistent launch forms
+// the lumped coefficients of all sets for every (order, 128-pair tile) and
+// the row transforms follow per set.  Same grids and outputs as
+// shs_batch's kgrad 0.
+Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
+                    const unsigned long *nmax_v,
+                    const unsigned long *shc_nmax_v, const double *mu_v,
+                    double R, const double *const *d_c,
+                    const double *const *d_s, double *const *d_f)
+{
+    Status st;
+    const size_t nlat = pnt->nlat, nlon = pnt->nlon;
+    unsigned long N = 0;
+    for (size_t j = 0; j < nsets; j++)
+        N = std::max(N, nmax_v[j]);
+    if (polar_threshold(N) >= 0.0)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "The split-precision batched synthesis does not apply the "
+                 "polar optimisation; switch it off.";
+        return st;
+    }
+    BatchGeo G;
+    CB_TRY(batch_geometry(c, pnt, N, R, &G));
+    const int np = G.np;
+    const double *dt = G.dt;
+
+    Tabs tab;
+    CB_TRY(tables(c, (long long)N, &tab));
+    const int ld = tab.ldmul * 64;
+    double *btp = nullptr;
+    CB_TRY(dbuf(c, "tc_btab", (size_t)(N + 1) * ld * 2, &btp));
+    double *ctp = btp + (size_t)(N + 1) * ld;
+    if (c.tcp_nmax != (long long)N)
+    {
+        Scope sc(c, TIMER_TABLES);
+        CB_CUDA(launch_tc_ctab((long long)N, ld, tab.tb, tab.tc, btp, ctp,
+                               c.stream), st);
+        c.tcp_nmax = (long long)N;
+    }
+    // chunks of 64 degrees per order, and where each order's tiles start
+    std::vector<long long> h0(N + 2);
+    h0[0] = 0;
+    for (unsigned long m = 0; m <= N; m++)
+        h0[m + 1] = h0[m] + (long long)((N - m + 64) / 64);
+    const long long nchunks = h0[N + 1];
+    long long *d_chunk0 = nullptr;
+    CB_TRY(dbuf(c, "tc_chunk0", h0.size(), &d_chunk0));
+    CB_CUDA(cudaMemcpyAsync(d_chunk0, h0.data(), h0.size() * sizeof(long long),
+                            cudaMemcpyHostToDevice, c.stream), st);
+    int *d_ecol = nullptr;
+    CB_TRY(dbuf(c, "tc_ecol", (size_t)(N + 1) * 32, &d_ecol));
+    void *bdig = nullptr;
+    CB_TRY(buf(c, "tc_bdig", (size_t)nchunks * shs_tc_chunk_bytes(), &bdig));
+
+    const RfftArgs *rf = nullptr;
+    CB_TRY(row_fft(c, (long long)nlon, &rf));
+    const int ldf = (int)(nlon / 2 + 1);
+    const size_t per_set = nlat * (size_t)ldf;
+    const size_t bsz = std::min<size_t>(nsets, SHS_TC_SETS);
+    double2 *lc = nullptr;
+    CB_TRY(dbuf(c, "batch_lumped", bsz * per_set, &lc));
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+    const int ntiles = (np + 127) / 128;
+
+    for (size_t j0 = 0; j0 < nsets; j0 += SHS_TC_SETS)
+    {
+        const int nb = (int)std::min<size_t>(SHS_TC_SETS, nsets - j0);
+        ShsTcPrep P{};
+        P.nmax = (long long)N;
+        P.nsets = nb;
+        for (int b = 0; b < nb; b++)
+        {
+            P.set_nmax[b] = (long long)nmax_v[j0 + b];
+            P.shc_nmax[b] = (long long)shc_nmax_v[j0 + b];
+            P.c[b] = d_c[j0 + b];
+            P.s[b] = d_s[j0 + b];
+        }
+        P.chunk0 = d_chunk0;
+        P.ecol = d_ecol;
+        P.bdig = static_cast<unsigned char *>(bdig);
+        P.status = d_status;
+        {
+            Scope sc(c, TIMER_PREP);
+            CB_CUDA(launch_tc_prep(P, c.stream), st);
+        }
+        if (!rf)
+            CB_CUDA(cudaMemsetAsync(lc, 0, nb * per_set * sizeof(double2),
+                                    c.stream), st);
+        CB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long),
+                                c.stream), st);
+        ShsTcArgs A{};
+        A.nmax = (long long)N;
+        A.npairs = np;
+        A.ntiles = ntiles;
+        A.nitems = (long long)(N + 1) * ntiles;
+        A.tb = tab.tb;
+        A.tmul = tab.tmul;
+        A.ldmul = tab.ldmul;
+        A.sg = tab.sg;
+        A.btp = btp;
+        A.ctp = ctp;
+        A.bdig = static_cast<const unsigned char *>(bdig);
+        A.chunk0 = d_chunk0;
+        A.ecol = d_ecol;
+        A.t = dt;
+        A.u = dt + np;
+        A.rho = dt + 2 * np;
+        A.row_n = reinterpret_cast<const int *>(dt + 3 * np);
+        A.row_s = A.row_n + np;
+        A.nlat = (int)nlat;
+        A.ldf = ldf;
+        A.nsets = nb;
+        for (int b = 0; b < nb; b++)
+        {
+            A.out[b] = lc + (size_t)b * per_set;
+            A.mur[b] = mu_v[j0 + b] / R;
+        }
+        A.counter = d_counter;
+        A.status = d_status;
+        const int grid = (int)std::min<long long>(A.nitems,
+                                                  (long long)c.num_sms);
+        {
+            Scope sc(c, TIMER_SHS);
+            CB_CUDA(launch_shs_tc(A, !G.r_eq, std::max(grid, 1), c.stream),
+                    st);
+        }
+        for (int b = 0; b < nb; b++)
+        {
+            double *dst = d_f[j0 + b];
+            double2 *src = lc + (size_t)b * per_set;
+            if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
+            {
+                RfftArgs R2 = *rf;
+                R2.nrows = (long long)nlat;
+                R2.x = dst;
+                R2.ldx = (long long)nlon;
+                R2.X = src;
+                R2.ldX = ldf;
+                R2.kmax = (int)nmax_v[j0 + b];
+                Scope sc(c, TIMER_FFT);
+                CB_CUDA(launch_rfft(R2, true, c.stream), st);
+            }
+            else
+            {
+                if (rf)
+                {
+                    st.code = CHARM_EFUNCARG;
+                    st.msg = "batched synthesis outputs must start on a "
+                             "16-byte boundary";
+                    return st;
+                }
+                cufftHandle h;
+                CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)nlat, &h));
+                Scope sc(c, TIMER_FFT, false);
+                if (cufftExecZ2D(h, reinterpret_cast<cufftDoubleComplex *>(src),
+                                 dst) != CUFFT_SUCCESS)
+                {
+                    st.code = CHARM_EFUNCARG;
+                    st.msg = "cuFFT Z2D failed";
+                    return st;
+                }
+            }
+        }
+        // the digit tiles and the lumped buffer are reused by the next group
+        CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    }
     return finish(c, d_status);
 }
 
@@ -2285,6 +2502,18 @@ Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
     CB_TRY(init(g_ctx));
     return shs_batch(g_ctx, pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
                      kgrad, d_f);
+}
+
+Status shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
+                              const unsigned long *nmax,
+                              const unsigned long *shc_nmax, const double *mu,
+                              double r, const double *const *d_c,
+                              const double *const *d_s, double *const *d_f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return shs_batch_tc(g_ctx, pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
+                        d_f);
 }
 
 Status shs_point_dev_f32(const charm_point *pnt, unsigned long shc_nmax,

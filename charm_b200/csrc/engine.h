@@ -68,6 +68,13 @@ Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
                            double r, const double *const *d_c,
                            const double *const *d_s, int kgrad,
                            double *const *d_f);
+// The potential of the batch with the degree sums on the tensor cores
+// (INT8 digit products, FP64 recombination).
+Status shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
+                              const unsigned long *nmax,
+                              const unsigned long *shc_nmax, const double *mu,
+                              double r, const double *const *d_c,
+                              const double *const *d_s, double *const *d_f);
 
 // Single-precision potential synthesis / analysis on grids whose rows admit
 // the shared-memory row transform, every row at r = R; float coefficient

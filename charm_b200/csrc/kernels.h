@@ -7,6 +7,16 @@
 namespace cb
 {
 
+// Error bits written by kernels into the per-call device status word.
+enum : unsigned
+{
+    DEV_ERR_WAIT_TIMEOUT = 1u,   // an mbarrier wait exceeded its limit
+    DEV_ERR_BAD_ARGS = 2u,       // a kernel received inconsistent sizes
+    DEV_ERR_TC_RANGE = 4u        // a value outside the fixed-point grid of
+                                 // the tensor-core synthesis
+};
+
+
 // One coefficient set of a batched synthesis: its degree, its first work
 // item, its scaled coefficients (in the layout of the shared tables' degree)
 // and its lumped-coefficient output.
@@ -231,6 +241,61 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
 size_t rfft_smem_bytes(int M);
 cudaError_t rfft_set_smem(size_t smem);
 cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st);
+
+// Batched grid synthesis with the degree sums on the tensor cores
+// (shs_tc.cu): up to SHS_TC_SETS coefficient sets per launch.
+constexpr int SHS_TC_SETS = 16;
+
+// Coefficient digit tiles of a batch: per order m and 64-degree chunk,
+// [parity][digit][32 columns x 32 bytes] (columns 2 s, 2 s + 1 = C, S of
+// set s), and the column exponents ecol[m][32].
+struct ShsTcPrep
+{
+    long long nmax;                       // table degree (largest set)
+    int nsets;
+    long long set_nmax[SHS_TC_SETS];
+    long long shc_nmax[SHS_TC_SETS];      // layout of each set's triangle
+    const double *c[SHS_TC_SETS];
+    const double *s[SHS_TC_SETS];
+    const long long *chunk0;              // first chunk of each order
+    int *ecol;
+    unsigned char *bdig;
+    unsigned *status;
+};
+
+struct ShsTcArgs
+{
+    long long nmax;
+    int npairs;
+    int ntiles;                           // tiles of 128 latitude pairs
+    long long nitems;                     // (nmax + 1) * ntiles
+    const double2 *tb;                    // recurrence tables (leg.cuh)
+    const double *tmul;
+    int ldmul;
+    const double *sg;
+    const double *btp;                    // beta_n rows of ldmul * 64
+    const double *ctp;                    // ct_n rows of ldmul * 64
+    const unsigned char *bdig;
+    const long long *chunk0;
+    const int *ecol;
+    const double *t, *u, *rho;
+    const int *row_n, *row_s;
+    int nlat, ldf;
+    int nsets;
+    double2 *out[SHS_TC_SETS];            // lumped coefficients [nlat][ldf]
+    double mur[SHS_TC_SETS];              // GM / R per set
+    unsigned long long *counter;
+    unsigned *status;
+};
+
+size_t shs_tc_smem_bytes();
+size_t shs_tc_chunk_bytes();
+cudaError_t launch_tc_ctab(long long nmax, int ld, const double2 *tb,
+                           const double *tc, double *btp, double *ctp,
+                           cudaStream_t st);
+cudaError_t launch_tc_prep(const ShsTcPrep &P, cudaStream_t st);
+cudaError_t launch_shs_tc(const ShsTcArgs &A, bool rr, int grid,
+                          cudaStream_t st);
 cudaError_t launch_tables_f32(long long nmax, const double *r,
                               const double *ri, float4 *ab, cudaStream_t st);
 cudaError_t launch_pack_cs_f32(long long nmax, long long shc_nmax,

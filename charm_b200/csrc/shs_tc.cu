@@ -1,0 +1,754 @@
+// Batched grid synthesis with the degree sums on the tensor cores
+// (split precision: exact INT8 digit products, recombined in FP64).
+//
+// For one order m and a tile of 128 latitude pairs the lumped coefficients
+// of all sets of a batch are a product of two matrices,
+//     a_s(lat) = sum_n  A[lat][n] B[n][s],
+//     A[lat][n] = P_nm(t_lat) (R/r)^(n+1)   (the Legendre block),
+//     B[n][s]   = C_nm or S_nm of set s    (32 columns: 16 sets x C, S),
+// with the even and odd (n - m) degrees summed separately for the north /
+// south symmetry (CHarm's shs_point_kernel, src/shs/shs_point_kernel.c:
+// 745-2010, forms the same sums one lane at a time).
+//
+// Precision.  Both operands become integers on fixed-point grids:
+//     A_int = round(A 2^(51 - eA)),  2^eA a bound of |A| on that latitude,
+//     B_int = round(B 2^(54 - eB)),  2^eB > max_n |B| of that column,
+// each written in base 256 with seven digits: A_int in two's complement
+// (digits 0..5 unsigned, the top digit signed), taken straight from the
+// mantissa of A 2^(51 - eA) + 1.5 2^52 (one FP64 add, no conversion
+// instruction); B_int with balanced digits in [-128, 127] (the bytes of
+// B_int + sum_i 128 256^i, minus 128), so that every dropped product has
+// zero mean.  The digit products a_i b_j are exact in the INT32
+// accumulators of tcgen05.mma kind::i8; products of level s = i + j are
+// summed in one accumulator and weighted by 256^s in FP64 afterwards.
+// Levels below 5 are dropped: they hold about 2^-53 of a typical term.
+// 34 digit pairs per degree tile and parity; 8 levels x 2 parities x 32
+// columns = all 512 TMEM columns of the SM.
+//
+// The bound 2^eA of a latitude and order is min(sqrt(2N + 1),
+// 6 (m + 1)^(1/4) / sqrt(cos lat)) (times (R/r)^(N+1) below the sphere):
+// |P_nm| <= sqrt(2n + 1) holds for the geodetic normalisation, and
+// sqrt(cos lat) |P_nm| stays below 4.2 (m + 1)^(1/4) for all n, m <= 2190
+// (evaluated on 190 latitudes; the maxima sit at the turning points).  A
+// value outside the grid sets DEV_ERR_TC_RANGE and the call fails.
+//
+// Pipeline per CTA (4 warps, one latitude pair per thread = one TMEM lane):
+// the coefficient digit tiles and the recurrence tables of a 64-degree
+// chunk arrive by one bulk copy (three stages); the threads run the
+// rescaled recurrence of leg.cuh in FP64, cut each value into digits and
+// store them as the K-major operand tiles (two stages); one thread issues
+// the 56 MMAs of the chunk and commits them to an mbarrier, so the tensor
+// cores work on chunk j while the threads prepare chunk j + 1.
+#include <cstdint>
+#include <type_traits>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "leg.cuh"
+
+namespace cb
+{
+
+namespace
+{
+
+constexpr int TC_M = 128;          // latitude pairs per item = TMEM lanes
+constexpr int TC_COLS = 32;        // accumulator columns
+constexpr int TC_D = 7;            // digits per operand
+constexpr int TC_LMIN = 5;         // lowest product level kept
+constexpr int TC_NLEV = 2 * TC_D - 1 - TC_LMIN;        // 8
+constexpr int TC_ATILE = TC_M * 32;                    // bytes
+constexpr int TC_BTILE = TC_COLS * 32;                 // bytes
+constexpr int TC_ASTAGE = 2 * TC_D * TC_ATILE;         // 57344
+constexpr int TC_BSTAGE = 2 * TC_D * TC_BTILE;         // 14336
+constexpr int TC_CH = 64;                              // degrees per chunk
+constexpr unsigned TC_TMEM_COLS = 512;
+// offset of the balanced digits of the coefficients: sum_{i<7} 128 256^i
+constexpr unsigned long long TC_BIAS = 0x0080808080808080ull;
+// x + 1.5 2^52 holds round(x) in its low mantissa bits for |x| < 2^51:
+// bits = 0x4338000000000000 + round(x) (two's complement)
+constexpr double TC_MAGIC = 6755399441055744.0;
+
+// byte offset of (row r, byte k) in a [rows x 32 B] K-major operand tile
+// without swizzle: 8-row x 16-byte core matrices, the two K halves of a
+// row group 128 B apart (leading byte offset), row groups 256 B apart
+// (stride byte offset)
+__host__ __device__ __forceinline__ int tc_tile_off(int r, int k)
+{
+    return (r >> 3) * 256 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+
+// shared-memory matrix descriptor of such a tile (sm_100 layout: start
+// address, LBO and SBO in 16-byte units, version 1, no swizzle)
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) |
+           ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
+           ((uint64_t)1 << 46);
+}
+
+// instruction descriptors: D int32, B signed 8-bit, A unsigned (digits
+// 0..5 of the Legendre values) or signed (their top digit), both K-major,
+// M = 128, N = TC_COLS
+// (N in bits 17..22, in units of 8)
+constexpr uint32_t TC_IDESC_U = (2u << 4) | (0u << 7) | (1u << 10) |
+                                ((uint32_t)(TC_M >> 4) << 24);
+constexpr uint32_t TC_IDESC_S = TC_IDESC_U | (1u << 7);
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b,
+                                       uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                 ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::"
+                 "cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before()
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after()
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 8 consecutive accumulator columns of this warp's 32 lanes
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, int (&v)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]),
+                   "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void tc_wait_ld()
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// zeros into 32 consecutive accumulator columns of this warp's 32 lanes
+__device__ __forceinline__ void tc_st_zero32(uint32_t taddr)
+{
+    const unsigned z = 0u;
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+                 "{%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+                 "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+                 "%1, %1, %1, %1};" ::"r"(taddr), "r"(z)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_wait_st()
+{
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// exact int32 -> double on the FP64 pipe: the bits 0x43300000:(v ^ 2^31)
+// are 2^52 + 2^31 + v
+__device__ __forceinline__ double i2d_exact(int v)
+{
+    return __hiloint2double(0x43300000, v ^ (int)0x80000000) -
+           4503601774854144.0;
+}
+
+// 2^e for |e| < 1000 (exact)
+__device__ __forceinline__ double pow2i(int e)
+{
+    return __hiloint2double((e + 1023) << 20, 0);
+}
+
+// Bytes d of four 64-bit words v0..v3 (as lo / hi halves) gathered into
+// one word per digit: w[d] = {v0.b_d, v1.b_d, v2.b_d, v3.b_d}.
+__device__ __forceinline__ void tc_transpose4(const unsigned (&lo)[4],
+                                              const unsigned (&hi)[4],
+                                              unsigned (&w)[TC_D])
+{
+    unsigned a = __byte_perm(lo[0], lo[1], 0x5140);
+    unsigned b = __byte_perm(lo[0], lo[1], 0x7362);
+    unsigned c = __byte_perm(lo[2], lo[3], 0x5140);
+    unsigned d = __byte_perm(lo[2], lo[3], 0x7362);
+    w[0] = __byte_perm(a, c, 0x5410);
+    w[1] = __byte_perm(a, c, 0x7632);
+    w[2] = __byte_perm(b, d, 0x5410);
+    w[3] = __byte_perm(b, d, 0x7632);
+    unsigned e = __byte_perm(hi[0], hi[1], 0x5140);
+    unsigned f = __byte_perm(hi[0], hi[1], 0x7362);
+    unsigned g = __byte_perm(hi[2], hi[3], 0x5140);
+    unsigned h = __byte_perm(hi[2], hi[3], 0x7362);
+    w[4] = __byte_perm(e, g, 0x5410);
+    w[5] = __byte_perm(e, g, 0x7632);
+    w[6] = __byte_perm(f, h, 0x5410);
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Preparation of the coefficient operand
+// ---------------------------------------------------------------------------
+// Column exponents: ecol[m][c] with 2^ecol > max_n |B[n][c]| (0 for an
+// all-zero column).  One block per order m, one warp per set.
+__global__ void k_tc_colexp(ShsTcPrep P)
+{
+    const long long m = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (m > P.nmax || warp >= 16)
+        return;
+    double mc = 0.0, ms = 0.0;
+    if (warp < P.nsets && m <= P.set_nmax[warp])
+    {
+        const long long s0 = tri_col0(P.shc_nmax[warp], m);
+        const double *c = P.c[warp] + s0 - m;
+        const double *s = P.s[warp] + s0 - m;
+        for (long long n = m + lane; n <= P.set_nmax[warp]; n += 32)
+        {
+            mc = fmax(mc, fabs(c[n]));
+            if (m > 0)
+                ms = fmax(ms, fabs(s[n]));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        mc = fmax(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+        ms = fmax(ms, __shfl_xor_sync(0xffffffffu, ms, o));
+    }
+    if (lane == 0)
+    {
+        // columns below 2^-900 are scaled as if of that size (their digits
+        // vanish); the range keeps every power of two of the kernels normal
+        const int ec = mc > 0.0 ? max(expo_of(mc) + 1, -900) : 0;
+        const int es = ms > 0.0 ? max(expo_of(ms) + 1, -900) : 0;
+        P.ecol[m * TC_COLS + 2 * warp] = ec;
+        P.ecol[m * TC_COLS + 2 * warp + 1] = es;
+        if (!isfinite(mc) || !isfinite(ms))
+            atomicOr(P.status, DEV_ERR_BAD_ARGS);
+    }
+}
+
+// Digit tiles of every (order, chunk): [parity][digit][32 columns x 32 B].
+// One block per order, thread = (parity, column, 16-degree half).
+__global__ void __launch_bounds__(128) k_tc_bdigits(ShsTcPrep P)
+{
+    const long long m = blockIdx.x;
+    if (m > P.nmax)
+        return;
+    const int t = threadIdx.x;
+    const int p = t >> 6, col = (t >> 1) & 31, h = t & 1;
+    const int set = col >> 1;
+    const bool is_s = col & 1;
+    const bool active = set < P.nsets && m <= P.set_nmax[set] &&
+                        !(is_s && m == 0);
+    const double *src = nullptr;
+    long long nset = -1;
+    if (active)
+    {
+        const long long s0 = tri_col0(P.shc_nmax[set], m);
+        src = (is_s ? P.s[set] : P.c[set]) + s0 - m;
+        nset = P.set_nmax[set];
+    }
+    const double sc = pow2i(54 - P.ecol[m * TC_COLS + col]);
+    const long long nch = (P.nmax - m + TC_CH) / TC_CH;
+    unsigned char *base = P.bdig + (size_t)P.chunk0[m] * TC_BSTAGE;
+    for (long long j = 0; j < nch; j++)
+    {
+        unsigned w[TC_D][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            unsigned lo[4], hi[4];
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+            {
+                const int k = 16 * h + 4 * q + b;
+                const long long n = m + j * TC_CH + 2 * k + p;
+                double v = (n <= nset) ? src[n] * sc : 0.0;
+                unsigned long long y =
+                    (unsigned long long)__double2ll_rn(v) + TC_BIAS;
+                lo[b] = (unsigned)y;
+                hi[b] = (unsigned)(y >> 32);
+            }
+            unsigned wd[TC_D];
+            tc_transpose4(lo, hi, wd);
+#pragma unroll
+            for (int d = 0; d < TC_D; d++)
+                w[d][q] = wd[d] ^ 0x80808080u;
+        }
+        unsigned char *ch = base + (size_t)j * TC_BSTAGE;
+#pragma unroll
+        for (int d = 0; d < TC_D; d++)
+        {
+            uint4 *dst = reinterpret_cast<uint4 *>(
+                ch + (p * TC_D + d) * TC_BTILE + tc_tile_off(col, 16 * h));
+            *dst = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+        }
+    }
+}
+
+// beta_n and ct_n of every order in rows of ldmul * 64 entries, zero
+// beyond the order's last degree: each chunk's slice is one 16-byte aligned
+// bulk copy, and the padding makes the tail of the last chunk contribute
+// nothing without a test per degree.
+__global__ void k_tc_ctab(long long nmax, int ld, const double2 *__restrict__ tb,
+                          const double *__restrict__ tc, double *btp,
+                          double *ctp)
+{
+    const long long m = blockIdx.x;
+    if (m > nmax)
+        return;
+    const long long c0 = tri_col0(nmax, m);
+    const long long ncol = nmax - m + 1;
+    for (long long i = threadIdx.x; i < ld; i += blockDim.x)
+    {
+        btp[m * ld + i] = i < ncol ? tb[c0 + i].x : 0.0;
+        ctp[m * ld + i] = i < ncol ? tc[c0 + i] : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The contraction kernel
+// ---------------------------------------------------------------------------
+template <bool RR>
+__global__ void __launch_bounds__(128, 1) k_shs_tc(ShsTcArgs A)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *sA = smem_raw;                         // 2 stages
+    unsigned char *sB = sA + 2 * TC_ASTAGE;               // 3 stages
+    double *sBt = reinterpret_cast<double *>(sB + 3 * TC_BSTAGE);
+    double *sCt = sBt + 3 * TC_CH;
+    double *sZero = sCt + 3 * TC_CH;                      // ct of no latitude
+    uint64_t *bar_b = reinterpret_cast<uint64_t *>(sZero + TC_CH);
+    uint64_t *bar_m = bar_b + 3;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar_m + 2);
+    int *sEcol = reinterpret_cast<int *>(tslot + 4);
+    unsigned long long *sItem =
+        reinterpret_cast<unsigned long long *>(sEcol + TC_COLS);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32"
+                     " [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile(
+            "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::
+                : "memory");
+    }
+    if (tid < TC_CH)
+        sZero[tid] = 0.0;
+    if (tid == 0)
+    {
+        for (int i = 0; i < 3; i++)
+            mbar_init(&bar_b[i], 1);
+        for (int i = 0; i < 2; i++)
+            mbar_init(&bar_m[i], 1);
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const long long N = A.nmax;
+    const int np = A.npairs;
+    unsigned long long g = 0;   // chunks issued by this CTA (stage counter)
+    bool ok = true;
+    unsigned range_err = 0u;
+
+    for (;;)
+    {
+        if (tid == 0)
+            *sItem = atomicAdd(A.counter, 1ull);
+        __syncthreads();
+        const unsigned long long item = *sItem;
+        if (item >= (unsigned long long)A.nitems)
+            break;
+        const long long m = (long long)(item / (unsigned long long)A.ntiles);
+        const int tile = (int)(item % (unsigned long long)A.ntiles);
+        if (tid < TC_COLS)
+            sEcol[tid] = A.ecol[m * TC_COLS + tid];
+
+        // ---- this thread's latitude pair: geometry, seed, row scale ----
+        const int p = tile * TC_M + tid;
+        const bool valid = p < np;
+        const double t = valid ? A.t[p] : 0.0;
+        const double u = valid ? A.u[p] : 1.0;
+        const double rh = (RR && valid) ? A.rho[p] : 1.0;
+        const double tq = RR ? t * rh : t;
+        const double rho2 = rh * rh;
+        double x = 0.0, y = 0.0;
+        int E = 0;
+        if (valid)
+            leg_seed(A.sg[2 * m], u, rh, RR, m, 0, x, E);
+        // bound of |P_nm (R/r)^(n+1)| on this latitude and order
+        double bnd = sqrt(2.0 * (double)N + 1.0);
+        if (u > 0.0)
+            bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
+        if (RR && rh > 1.0)
+            bnd *= pow(rh, (double)(N + 1));
+        const int eA = expo_of(bnd) + 1;
+        // the recurrence runs on values times 2^(51 - eA) once they are in
+        // range (linear, so the scaling carries through every step)
+        const double rs = pow2i(51 - eA);
+        if (E == 0)
+            x *= rs;
+        bool any_scaled = __syncthreads_or(E != 0);
+
+        // the MMAs of an item only accumulate: clear this warp's lanes of
+        // all accumulators (the previous item's MMAs and loads are done)
+        {
+            const uint32_t lb = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+            for (int cc = 0; cc < (int)TC_TMEM_COLS; cc += 32)
+                tc_st_zero32(lb + (uint32_t)cc);
+            tc_wait_st();
+        }
+
+        const long long ncol = N - m + 1;
+        const int nch = (int)((ncol + TC_CH - 1) / TC_CH);
+        const long long trow = m * (long long)A.ldmul * TC_CH;
+        const unsigned char *brow =
+            A.bdig + (size_t)A.chunk0[m] * TC_BSTAGE;
+        auto issue = [&](int j, unsigned long long gg) {
+            const int s = (int)(gg % 3);
+            mbar_arrive_expect_tx(&bar_b[s], TC_BSTAGE +
+                                                 2 * TC_CH * sizeof(double));
+            bulk_g2s(sB + s * TC_BSTAGE, brow + (size_t)j * TC_BSTAGE,
+                     TC_BSTAGE, &bar_b[s]);
+            bulk_g2s(sBt + s * TC_CH, A.btp + trow + (long long)j * TC_CH,
+                     TC_CH * sizeof(double), &bar_b[s]);
+            bulk_g2s(sCt + s * TC_CH, A.ctp + trow + (long long)j * TC_CH,
+                     TC_CH * sizeof(double), &bar_b[s]);
+        };
+
+        for (int j = 0; j < nch; j++, g++)
+        {
+            const int sa = (int)(g & 1), sb = (int)(g % 3);
+            // the MMAs of chunk g - 2 have read A stage sa and B stage
+            // (g + 1) % 3.  A wait that gives up only marks this thread;
+            // the decision to stop is taken together at the barrier below.
+            bool wok = g < 2 || mbar_wait_bounded(&bar_m[sa],
+                                                  (unsigned)(((g - 2) >> 1) & 1),
+                                                  A.status);
+            if (tid == 0 && wok)
+            {
+                if (j == 0)
+                    issue(0, g);
+                if (j + 1 < nch)
+                    issue(j + 1, g + 1);
+            }
+            wok = wok && mbar_wait_bounded(&bar_b[sb], (unsigned)((g / 3) & 1),
+                                           A.status);
+            if (j > 0)
+            {
+                const double mul = A.tmul[m * A.ldmul + j];
+                x *= mul;
+                y *= mul;
+            }
+            unsigned char *at = sA + sa * TC_ASTAGE;
+            // lanes below the double range (or past the grid) take ct = 0
+            const double2 *bt2 =
+                reinterpret_cast<const double2 *>(sBt + sb * TC_CH);
+            const double2 *ct2 = reinterpret_cast<const double2 *>(
+                (valid && E == 0) ? sCt + sb * TC_CH : sZero);
+            unsigned ov = 0u;
+            // one chunk of 64 degrees: recurrence, fixed point, digits;
+            // FIRST: chunk 0, whose degree m is the seed itself
+            auto prep = [&](auto first_c) {
+                constexpr bool FIRST = decltype(first_c)::value;
+#pragma unroll 1
+                for (int hh = 0; hh < 2; hh++)
+                {
+                    unsigned wE[TC_D][4], wO[TC_D][4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        unsigned loE[4], hiE[4], loO[4], hiO[4];
+                        double2 bp[4], cp[4];
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                        {
+                            bp[k] = bt2[16 * hh + 4 * q + k];
+                            cp[k] = ct2[16 * hh + 4 * q + k];
+                        }
+#pragma unroll
+                        for (int b = 0; b < 8; b++)
+                        {
+                            const double beta =
+                                (b & 1) ? bp[b >> 1].y : bp[b >> 1].x;
+                            const double ctn =
+                                (b & 1) ? cp[b >> 1].y : cp[b >> 1].x;
+                            if (!(FIRST && q == 0 && b == 0 && hh == 0))
+                            {
+                                const double by = RR ? beta * (rho2 * y)
+                                                     : beta * y;
+                                const double z = fma(tq, x, -by);
+                                y = x;
+                                x = z;
+                            }
+                            // round(v) in two's complement from the mantissa
+                            // of v + 1.5 2^52; the exponent field checks
+                            // |v| < 2^51
+                            const double tv = fma(x, ctn, TC_MAGIC);
+                            const unsigned lo = (unsigned)__double2loint(tv);
+                            const unsigned hw = (unsigned)__double2hiint(tv);
+                            ov |= hw ^ 0x43300000u;
+                            const unsigned hi = hw - 0x43380000u;
+                            if (b & 1)
+                            {
+                                loO[b >> 1] = lo;
+                                hiO[b >> 1] = hi;
+                            }
+                            else
+                            {
+                                loE[b >> 1] = lo;
+                                hiE[b >> 1] = hi;
+                            }
+                        }
+                        unsigned wd[TC_D];
+                        tc_transpose4(loE, hiE, wd);
+#pragma unroll
+                        for (int d = 0; d < TC_D; d++)
+                            wE[d][q] = wd[d];
+                        tc_transpose4(loO, hiO, wd);
+#pragma unroll
+                        for (int d = 0; d < TC_D; d++)
+                            wO[d][q] = wd[d];
+                    }
+                    const int off = tc_tile_off(tid, 16 * hh);
+#pragma unroll
+                    for (int d = 0; d < TC_D; d++)
+                    {
+                        *reinterpret_cast<uint4 *>(at + d * TC_ATILE + off) =
+                            make_uint4(wE[d][0], wE[d][1], wE[d][2], wE[d][3]);
+                        *reinterpret_cast<uint4 *>(at + (TC_D + d) * TC_ATILE +
+                                                   off) =
+                            make_uint4(wO[d][0], wO[d][1], wO[d][2], wO[d][3]);
+                    }
+                }
+            };
+            if (wok)
+            {
+                if (j == 0)
+                    prep(std::integral_constant<bool, true>{});
+                else
+                    prep(std::integral_constant<bool, false>{});
+            }
+            range_err |= ov >> 20;
+            if (any_scaled)
+            {
+                if (valid && leg_fixup(x, y, E))
+                {
+                    x *= rs;
+                    y *= rs;
+                }
+                any_scaled = __syncthreads_or(E != 0);
+            }
+            // operand tiles complete: hand them to the tensor cores
+            fence_proxy_async_smem();
+            tc_fence_before();
+            const bool all_ok = __syncthreads_and(wok) != 0;
+            tc_fence_after();
+            if (!all_ok)
+            {
+                ok = false;
+                break;
+            }
+            if (tid == 0)
+            {
+                // per parity and Legendre digit ia: one MMA against the
+                // stack of coefficient digits jb >= j0 (contiguous tiles,
+                // N = 32 (7 - j0) rows) whose 32-column blocks land in the
+                // accumulators of levels ia + jb - TC_LMIN
+                const uint64_t da0 = tc_sdesc(smem_u32(at));
+                const uint64_t db0 = tc_sdesc(smem_u32(sB + sb * TC_BSTAGE));
+#pragma unroll
+                for (int par = 0; par < 2; par++)
+#pragma unroll
+                    for (int ia = 0; ia < TC_D; ia++)
+                    {
+                        const int j0 = ia < TC_LMIN ? TC_LMIN - ia : 0;
+                        const int n = TC_COLS * (TC_D - j0);
+                        const uint64_t da =
+                            da0 + (uint64_t)(((par * TC_D + ia) * TC_ATILE) >>
+                                             4);
+                        const uint64_t db =
+                            db0 + (uint64_t)(((par * TC_D + j0) * TC_BTILE) >>
+                                             4);
+                        const uint32_t d =
+                            tmem + (uint32_t)((par * TC_NLEV + ia + j0 -
+                                               TC_LMIN) * TC_COLS);
+                        const uint32_t idesc =
+                            (ia == TC_D - 1 ? TC_IDESC_S : TC_IDESC_U) |
+                            ((uint32_t)(n >> 3) << 17);
+                        tc_mma(d, da, db, idesc, 1u);
+                    }
+                tc_commit(&bar_m[sa]);
+            }
+        }
+        if (!ok)
+            break;
+
+        // ---- epilogue: recombine the levels, north / south, write ----
+        const bool eok = mbar_wait_bounded(&bar_m[(g - 1) & 1],
+                                           (unsigned)(((g - 1) >> 1) & 1),
+                                           A.status);
+        if (!__syncthreads_and(eok))
+        {
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        const double cpack = m == 0 ? 1.0 : 0.5;
+        const double rsi = pow2i(eA - 105);
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        int rown = -1, rows = -1;
+        if (valid)
+        {
+            rown = A.row_n[p];
+            rows = A.row_s[p];
+        }
+#pragma unroll 1
+        for (int cb = 0; cb < TC_COLS / 8; cb++)
+        {
+            double tot[2][8];
+#pragma unroll
+            for (int par = 0; par < 2; par++)
+            {
+                int v[TC_NLEV][8];
+#pragma unroll
+                for (int L = 0; L < TC_NLEV; L++)
+                    tc_ld8(lane_base +
+                               (uint32_t)((par * TC_NLEV + L) * TC_COLS +
+                                          cb * 8),
+                           v[L]);
+                tc_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 8; c++)
+                {
+                    double s = 0.0;
+#pragma unroll
+                    for (int L = TC_NLEV - 1; L >= 0; L--)
+                        s = fma(i2d_exact(v[L][c]), pow2i(8 * (L + TC_LMIN)),
+                                s);
+                    tot[par][c] = s;
+                }
+            }
+            if (valid)
+            {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                {
+                    const int set = cb * 4 + k;
+                    if (set >= A.nsets)
+                        break;
+                    const double fc = pow2i(sEcol[2 * set]) * rsi;
+                    const double fs = pow2i(sEcol[2 * set + 1]) * rsi;
+                    const double w = cpack * A.mur[set];
+                    const double ac = (tot[0][2 * k] + tot[1][2 * k]) * fc;
+                    const double as = (tot[0][2 * k + 1] + tot[1][2 * k + 1]) *
+                                      fs;
+                    double2 *o = A.out[set];
+                    if (rown >= 0 && rown < A.nlat)
+                        o[(size_t)rown * A.ldf + m] =
+                            make_double2(w * ac, -(w * as));
+                    if (rows >= 0 && rows < A.nlat)
+                    {
+                        const double bc =
+                            (tot[0][2 * k] - tot[1][2 * k]) * fc;
+                        const double bs =
+                            (tot[0][2 * k + 1] - tot[1][2 * k + 1]) * fs;
+                        o[(size_t)rows * A.ldf + m] =
+                            make_double2(w * bc, -(w * bs));
+                    }
+                }
+            }
+        }
+        // the next item's MMAs overwrite the accumulators
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (range_err)
+        atomicOr(A.status, DEV_ERR_TC_RANGE);
+    // all MMAs of this CTA have completed (epilogue wait) unless a wait
+    // gave up; in that case wait once more for the last commit, bounded
+    if (!ok && g > 0)
+        mbar_wait_bounded(&bar_m[(g - 1) & 1], (unsigned)(((g - 1) >> 1) & 1),
+                          A.status);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+size_t shs_tc_smem_bytes()
+{
+    return 2 * TC_ASTAGE + 3 * TC_BSTAGE + 7 * TC_CH * sizeof(double) +
+           5 * sizeof(uint64_t) + 4 * sizeof(uint32_t) +
+           TC_COLS * sizeof(int) + sizeof(unsigned long long) + 64;
+}
+
+size_t shs_tc_chunk_bytes()
+{
+    return TC_BSTAGE;
+}
+
+cudaError_t launch_tc_ctab(long long nmax, int ld, const double2 *tb,
+                           const double *tc, double *btp, double *ctp,
+                           cudaStream_t st)
+{
+    k_tc_ctab<<<(unsigned)(nmax + 1), 128, 0, st>>>(nmax, ld, tb, tc, btp,
+                                                    ctp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_prep(const ShsTcPrep &P, cudaStream_t st)
+{
+    k_tc_colexp<<<(unsigned)(P.nmax + 1), 512, 0, st>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    k_tc_bdigits<<<(unsigned)(P.nmax + 1), 128, 0, st>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shs_tc(const ShsTcArgs &A, bool rr, int grid,
+                          cudaStream_t st)
+{
+    const size_t smem = shs_tc_smem_bytes();
+    cudaError_t e;
+    if (rr)
+    {
+        e = cudaFuncSetAttribute(k_shs_tc<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess)
+            return e;
+        k_shs_tc<true><<<grid, 128, smem, st>>>(A);
+    }
+    else
+    {
+        e = cudaFuncSetAttribute(k_shs_tc<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess)
+            return e;
+        k_shs_tc<false><<<grid, 128, smem, st>>>(A);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace cb

@@ -245,6 +245,19 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_dev(
     const double *const *d_c, const double *const *d_s, int kgrad,
     double *const *d_f, charm_err *err);
 
+/* charm_b200_shs_point_batch_dev with the degree sums of every (order,
+ * 128-latitude tile) on the tensor cores for up to 16 sets at once (no
+ * counterpart in CHarm): the Legendre values and the coefficients become
+ * 54-bit fixed-point integers, cut into seven 8-bit digits whose products
+ * are summed exactly in INT32 (tcgen05 kind::i8) and recombined in FP64.
+ * Agrees with the FP64 path to a relative RMS of about 1e-15 per set.
+ * kgrad must be 0 (the potential); the polar optimisation must be off. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_i8_dev(
+    const charm_point *pnt, size_t nsets, const unsigned long *nmax,
+    const unsigned long *shc_nmax, const double *mu, double r,
+    const double *const *d_c, const double *const *d_s, int kgrad,
+    double *const *d_f, charm_err *err);
+
 /* Single-precision mode of the device-resident potential synthesis and
  * analysis: the Legendre recurrence and sums in FP32 (as CHarm's float
  * build, charmf_shs_point / charmf_sha_point, does them), the longitude

@@ -89,6 +89,22 @@ def test_batch_all_ten_on_dh2_above_the_sphere(env):
             assert rel_rms(g[4 + q], g2[q]) <= 1e-12, (N, q)
 
 
+def test_batch_reused_buffers_low_degree_sets(env):
+    """A second call of the same shape, now with sets of lower degree, must
+    not see the orders the first call left in the lumped-coefficient
+    buffer."""
+    torch, cb, L = env
+    p = cb.PointGridDH2(240, R_EARTH)
+    batch(env, p, make_sets(300, [240, 240, 240]), R_EARTH, 1)
+    sets = make_sets(310, [240, 35, 120])
+    got = batch(env, p, sets, R_EARTH, 1)
+    for (N, c, s, mu), g in zip(sets, got):
+        shc = cb.Shc(N, mu, R_EARTH, c, s)
+        g1 = cb.shs_point_grad1(p, shc, N)
+        for q in range(3):
+            assert rel_rms(g[q], g1[q]) <= 1e-12, (N, q)
+
+
 def test_batch_potential_on_gl(env):
     torch, cb, L = env
     nmaxes = [360, 90, 359, 2, 200]
