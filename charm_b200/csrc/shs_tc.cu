@@ -32,13 +32,14 @@
 // (evaluated on 190 latitudes; the maxima sit at the turning points).  A
 // value outside the grid sets DEV_ERR_TC_RANGE and the call fails.
 //
-// Pipeline per CTA (4 warps, one latitude pair per thread = one TMEM lane):
-// the coefficient digit tiles and the recurrence tables of a 64-degree
-// chunk arrive by one bulk copy (three stages); the threads run the
-// rescaled recurrence of leg.cuh in FP64, cut each value into digits and
-// store them as the K-major operand tiles (two stages); one thread issues
-// the 56 MMAs of the chunk and commits them to an mbarrier, so the tensor
-// cores work on chunk j while the threads prepare chunk j + 1.
+// Pipeline per CTA (one latitude pair per TMEM lane): the coefficient digit
+// tiles and the recurrence tables of a 64-degree chunk arrive by bulk
+// copies, two chunks ahead (four stages, streamed across work items); 256
+// threads run the rescaled recurrence of leg.cuh in FP64, cut the values
+// into digits and store them as the K-major operand tiles (two stages); a
+// producer warp issues the 14 MMAs of the chunk and commits them to an
+// mbarrier, so the tensor cores work on chunk j while the threads prepare
+// chunk j + 1.
 #include <cstdint>
 #include <type_traits>
 
@@ -62,6 +63,8 @@ constexpr int TC_BTILE = TC_COLS * 32;                 // bytes
 constexpr int TC_ASTAGE = 2 * TC_D * TC_ATILE;         // 57344
 constexpr int TC_BSTAGE = 2 * TC_D * TC_BTILE;         // 14336
 constexpr int TC_CH = 64;                              // degrees per chunk
+constexpr int TC_NB = 4;           // coefficient / table stages
+constexpr int TC_AHEAD = TC_NB - 2;   // chunks loaded ahead of the MMAs' next
 constexpr unsigned TC_TMEM_COLS = 512;
 // offset of the balanced digits of the coefficients: sum_{i<7} 128 256^i
 constexpr unsigned long long TC_BIAS = 0x0080808080808080ull;
@@ -136,14 +139,13 @@ __device__ __forceinline__ void tc_wait_ld()
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// zeros into 32 consecutive accumulator columns of this warp's 32 lanes
-__device__ __forceinline__ void tc_st_zero32(uint32_t taddr)
+// zeros into 16 consecutive accumulator columns of this warp's 32 lanes
+__device__ __forceinline__ void tc_st_zero16(uint32_t taddr)
 {
     const unsigned z = 0u;
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
                  "{%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
-                 "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
-                 "%1, %1, %1, %1};" ::"r"(taddr), "r"(z)
+                 "%1, %1};" ::"r"(taddr), "r"(z)
                  : "memory");
 }
 
@@ -296,7 +298,8 @@ __global__ void __launch_bounds__(128) k_tc_bdigits(ShsTcPrep P)
 // beta_n and ct_n of every order in rows of ldmul * 64 entries, zero
 // beyond the order's last degree: each chunk's slice is one 16-byte aligned
 // bulk copy, and the padding makes the tail of the last chunk contribute
-// nothing without a test per degree.
+// nothing without a test per degree.  ct is stored by parity within each
+// chunk (the 32 even-(n - m) degrees, then the 32 odd ones).
 __global__ void k_tc_ctab(long long nmax, int ld, const double2 *__restrict__ tb,
                           const double *__restrict__ tc, double *btp,
                           double *ctp)
@@ -309,30 +312,78 @@ __global__ void k_tc_ctab(long long nmax, int ld, const double2 *__restrict__ tb
     for (long long i = threadIdx.x; i < ld; i += blockDim.x)
     {
         btp[m * ld + i] = i < ncol ? tb[c0 + i].x : 0.0;
-        ctp[m * ld + i] = i < ncol ? tc[c0 + i] : 0.0;
+        // ct in [chunk][parity][32] order: degree offset 64 j + 2 k + p
+        const long long r = i & 63;
+        const long long src = (i - r) + 2 * (r & 31) + (r >> 5);
+        ctp[m * ld + i] = src < ncol ? tc[c0 + src] : 0.0;
     }
 }
 
 // ---------------------------------------------------------------------------
 // The contraction kernel
 // ---------------------------------------------------------------------------
+// Warp roles (13 warps):
+//   0..3  preparation: one latitude pair per thread (TMEM lane 32 w + l);
+//         per chunk the recurrence on 64 degrees, fixed point, digits into
+//         A stage g % 2, then an arrival on bar_a;
+//   4     producer (lane 0): bulk loads TC_AHEAD + 1 chunks ahead of the
+//         MMAs, the 14 MMAs of each chunk once bar_a completes, a commit per
+//         chunk (bar_m: its stages are free again) and per work item
+//         (bar_acc: the accumulators hold the item's sums);
+//   5..12 epilogue: after bar_acc, read the accumulators (warp w: lanes of
+//         quarter w % 4, half of the columns), recombine, write, clear them
+//         and arrive on bar_free, which the producer waits for before the
+//         next item's first MMA.
+// The preparation of the next item runs while the tensor cores finish an
+// item and the epilogue drains it.  Every wait is bounded; a wait that gives
+// up raises the CTA's abort flag, which every loop reads, so all roles
+// reach the final barrier.
+constexpr int TC_PREP = 128;
+constexpr int TC_THREADS = 13 * 32;
+constexpr int TC_RING = 8;          // work items in flight (ring of ids)
+
+// barrier among the preparation threads (id 1) with an OR of a predicate
+__device__ __forceinline__ bool tc_prep_or(bool v)
+{
+    unsigned r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+                 "barrier.red.or.pred q, 1, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r)
+                 : "r"((unsigned)v)
+                 : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\t"
+                 "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
 template <bool RR>
-__global__ void __launch_bounds__(128, 1) k_shs_tc(ShsTcArgs A)
+__global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *sA = smem_raw;                         // 2 stages
-    unsigned char *sB = sA + 2 * TC_ASTAGE;               // 3 stages
-    double *sBt = reinterpret_cast<double *>(sB + 3 * TC_BSTAGE);
-    double *sCt = sBt + 3 * TC_CH;
-    double *sZero = sCt + 3 * TC_CH;                      // ct of no latitude
+    unsigned char *sB = sA + 2 * TC_ASTAGE;               // TC_NB stages
+    double *sBt = reinterpret_cast<double *>(sB + TC_NB * TC_BSTAGE);
+    double *sCt = sBt + TC_NB * TC_CH;
+    double *sZero = sCt + TC_NB * TC_CH;                  // ct of no latitude
     uint64_t *bar_b = reinterpret_cast<uint64_t *>(sZero + TC_CH);
-    uint64_t *bar_m = bar_b + 3;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar_m + 2);
-    int *sEcol = reinterpret_cast<int *>(tslot + 4);
-    unsigned long long *sItem =
-        reinterpret_cast<unsigned long long *>(sEcol + TC_COLS);
+    uint64_t *bar_m = bar_b + TC_NB;                      // 2
+    uint64_t *bar_a = bar_m + 2;                          // 2
+    uint64_t *bar_acc = bar_a + 2;
+    uint64_t *bar_free = bar_acc + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar_free + 1);
+    volatile int *sAbort = reinterpret_cast<volatile int *>(tslot + 1);
+    // work items in order of issue, written by the producer when its load
+    // cursor reaches them (several chunks before anyone reads them)
+    volatile unsigned long long *sQ =
+        reinterpret_cast<volatile unsigned long long *>(tslot + 4);
 
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32"
@@ -347,342 +398,466 @@ __global__ void __launch_bounds__(128, 1) k_shs_tc(ShsTcArgs A)
         sZero[tid] = 0.0;
     if (tid == 0)
     {
-        for (int i = 0; i < 3; i++)
+        for (int i = 0; i < TC_NB; i++)
             mbar_init(&bar_b[i], 1);
         for (int i = 0; i < 2; i++)
+        {
             mbar_init(&bar_m[i], 1);
+            mbar_init(&bar_a[i], TC_PREP);
+        }
+        mbar_init(bar_acc, 1);
+        mbar_init(bar_free, 8 * 32);
         fence_mbar_init();
+        *sAbort = 0;
+    }
+    const long long N = A.nmax;
+    const int np = A.npairs;
+
+    // ---- load cursor (producer lane 0) ----
+    unsigned long long lk = 0;
+    long long lm = 0, lj = 0, lnch = 0;
+    bool lend = false;
+    auto fetch_item = [&]() {
+        const unsigned long long it = atomicAdd(A.counter, 1ull);
+        sQ[lk % TC_RING] = it;
+        if (it >= (unsigned long long)A.nitems)
+        {
+            lend = true;
+            return;
+        }
+        lm = (long long)(it / (unsigned long long)A.ntiles);
+        lj = 0;
+        lnch = (N - lm + TC_CH) / TC_CH;
+    };
+    // loads chunk gg; the id of the next item is published before the
+    // arrival on this chunk's barrier (release), so a thread that has
+    // waited for the last chunk of an item also sees the next item's id
+    auto issue_next = [&](unsigned long long gg) {
+        if (lend)
+            return;
+        const long long cm = lm, cj = lj;
+        if (++lj == lnch)
+        {
+            ++lk;
+            fetch_item();
+        }
+        const int s = (int)(gg % TC_NB);
+        const long long trow = cm * (long long)A.ldmul * TC_CH + cj * TC_CH;
+        mbar_arrive_expect_tx(&bar_b[s],
+                              TC_BSTAGE + 2 * TC_CH * sizeof(double));
+        bulk_g2s(sB + s * TC_BSTAGE,
+                 A.bdig + ((size_t)A.chunk0[cm] + (size_t)cj) * TC_BSTAGE,
+                 TC_BSTAGE, &bar_b[s]);
+        bulk_g2s(sBt + s * TC_CH, A.btp + trow, TC_CH * sizeof(double),
+                 &bar_b[s]);
+        bulk_g2s(sCt + s * TC_CH, A.ctp + trow, TC_CH * sizeof(double),
+                 &bar_b[s]);
+    };
+    if (warp == 4 && lane == 0)
+    {
+        fetch_item();
+        for (int a = 0; a <= TC_AHEAD; a++)
+            issue_next((unsigned long long)a);
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
-    const long long N = A.nmax;
-    const int np = A.npairs;
-    unsigned long long g = 0;   // chunks issued by this CTA (stage counter)
-    bool ok = true;
-    unsigned range_err = 0u;
 
-    for (;;)
+    if (warp < 4)
     {
-        if (tid == 0)
-            *sItem = atomicAdd(A.counter, 1ull);
-        __syncthreads();
-        const unsigned long long item = *sItem;
-        if (item >= (unsigned long long)A.nitems)
-            break;
-        const long long m = (long long)(item / (unsigned long long)A.ntiles);
-        const int tile = (int)(item % (unsigned long long)A.ntiles);
-        if (tid < TC_COLS)
-            sEcol[tid] = A.ecol[m * TC_COLS + tid];
-
-        // ---- this thread's latitude pair: geometry, seed, row scale ----
-        const int p = tile * TC_M + tid;
-        const bool valid = p < np;
-        const double t = valid ? A.t[p] : 0.0;
-        const double u = valid ? A.u[p] : 1.0;
-        const double rh = (RR && valid) ? A.rho[p] : 1.0;
-        const double tq = RR ? t * rh : t;
-        const double rho2 = rh * rh;
-        double x = 0.0, y = 0.0;
-        int E = 0;
-        if (valid)
-            leg_seed(A.sg[2 * m], u, rh, RR, m, 0, x, E);
-        // bound of |P_nm (R/r)^(n+1)| on this latitude and order
-        double bnd = sqrt(2.0 * (double)N + 1.0);
-        if (u > 0.0)
-            bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
-        if (RR && rh > 1.0)
-            bnd *= pow(rh, (double)(N + 1));
-        const int eA = expo_of(bnd) + 1;
-        // the recurrence runs on values times 2^(51 - eA) once they are in
-        // range (linear, so the scaling carries through every step)
-        const double rs = pow2i(51 - eA);
-        if (E == 0)
-            x *= rs;
-        bool any_scaled = __syncthreads_or(E != 0);
-
-        // the MMAs of an item only accumulate: clear this warp's lanes of
-        // all accumulators (the previous item's MMAs and loads are done)
+        // ================= preparation =================
+        const int row = tid;
+        unsigned long long g = 0;
+        unsigned range_err = 0u;
+        for (unsigned long long k = 0;; k++)
         {
-            const uint32_t lb = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-            for (int cc = 0; cc < (int)TC_TMEM_COLS; cc += 32)
-                tc_st_zero32(lb + (uint32_t)cc);
-            tc_wait_st();
-        }
-
-        const long long ncol = N - m + 1;
-        const int nch = (int)((ncol + TC_CH - 1) / TC_CH);
-        const long long trow = m * (long long)A.ldmul * TC_CH;
-        const unsigned char *brow =
-            A.bdig + (size_t)A.chunk0[m] * TC_BSTAGE;
-        auto issue = [&](int j, unsigned long long gg) {
-            const int s = (int)(gg % 3);
-            mbar_arrive_expect_tx(&bar_b[s], TC_BSTAGE +
-                                                 2 * TC_CH * sizeof(double));
-            bulk_g2s(sB + s * TC_BSTAGE, brow + (size_t)j * TC_BSTAGE,
-                     TC_BSTAGE, &bar_b[s]);
-            bulk_g2s(sBt + s * TC_CH, A.btp + trow + (long long)j * TC_CH,
-                     TC_CH * sizeof(double), &bar_b[s]);
-            bulk_g2s(sCt + s * TC_CH, A.ctp + trow + (long long)j * TC_CH,
-                     TC_CH * sizeof(double), &bar_b[s]);
-        };
-
-        for (int j = 0; j < nch; j++, g++)
-        {
-            const int sa = (int)(g & 1), sb = (int)(g % 3);
-            // the MMAs of chunk g - 2 have read A stage sa and B stage
-            // (g + 1) % 3.  A wait that gives up only marks this thread;
-            // the decision to stop is taken together at the barrier below.
-            bool wok = g < 2 || mbar_wait_bounded(&bar_m[sa],
-                                                  (unsigned)(((g - 2) >> 1) & 1),
-                                                  A.status);
-            if (tid == 0 && wok)
+            // the same id for all 128 threads (written before the barrier
+            // arrival they all waited for); aborts are decided together at
+            // the end of an item
+            const unsigned long long item = sQ[k % TC_RING];
+            if (item >= (unsigned long long)A.nitems)
+                break;
+            const long long m =
+                (long long)(item / (unsigned long long)A.ntiles);
+            const int tile = (int)(item % (unsigned long long)A.ntiles);
+            const int p = tile * TC_M + row;
+            const bool valid = p < np;
+            const double t = valid ? A.t[p] : 0.0;
+            const double u = valid ? A.u[p] : 1.0;
+            const double rh = (RR && valid) ? A.rho[p] : 1.0;
+            const double tq = RR ? t * rh : t;
+            const double rho2 = rh * rh;
+            double x = 0.0, y = 0.0;
+            int E = 0;
+            if (valid)
+                leg_seed(A.sg[2 * m], u, rh, RR, m, 0, x, E);
+            double bnd = sqrt(2.0 * (double)N + 1.0);
+            if (u > 0.0)
+                bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
+            if (RR && rh > 1.0)
+                bnd *= pow(rh, (double)(N + 1));
+            const int eA = expo_of(bnd) + 1;
+            const double rs = pow2i(51 - eA);
+            if (E == 0)
+                x *= rs;
+            bool any_scaled = tc_prep_or(E != 0);
+            const long long ncol = N - m + 1;
+            const int nch = (int)((ncol + TC_CH - 1) / TC_CH);
+            double mul_next = 1.0;
+            bool bad = false;
+            for (int j = 0; j < nch; j++, g++)
             {
-                if (j == 0)
-                    issue(0, g);
+                const int sa = (int)(g & 1), sb = (int)(g % TC_NB);
+                // after a wait gave up, the rest of the item only keeps
+                // the barrier sequence of the preparation threads
+                bool wok = !bad &&
+                           (g < 2 ||
+                            mbar_wait_bounded(&bar_m[sa],
+                                              (unsigned)(((g - 2) >> 1) & 1),
+                                              A.status));
+                wok = wok && mbar_wait_bounded(&bar_b[sb],
+                                               (unsigned)((g / TC_NB) & 1),
+                                               A.status);
+                if (j > 0)
+                {
+                    x *= mul_next;
+                    y *= mul_next;
+                }
                 if (j + 1 < nch)
-                    issue(j + 1, g + 1);
-            }
-            wok = wok && mbar_wait_bounded(&bar_b[sb], (unsigned)((g / 3) & 1),
-                                           A.status);
-            if (j > 0)
-            {
-                const double mul = A.tmul[m * A.ldmul + j];
-                x *= mul;
-                y *= mul;
-            }
-            unsigned char *at = sA + sa * TC_ASTAGE;
-            // lanes below the double range (or past the grid) take ct = 0
-            const double2 *bt2 =
-                reinterpret_cast<const double2 *>(sBt + sb * TC_CH);
-            const double2 *ct2 = reinterpret_cast<const double2 *>(
-                (valid && E == 0) ? sCt + sb * TC_CH : sZero);
-            unsigned ov = 0u;
-            // one chunk of 64 degrees: recurrence, fixed point, digits;
-            // FIRST: chunk 0, whose degree m is the seed itself
-            auto prep = [&](auto first_c) {
-                constexpr bool FIRST = decltype(first_c)::value;
+                    mul_next = A.tmul[m * A.ldmul + j + 1];
+                unsigned char *at = sA + sa * TC_ASTAGE;
+                const double2 *bt2 =
+                    reinterpret_cast<const double2 *>(sBt + sb * TC_CH);
+                // lanes below the double range (or past the grid): ct = 0
+                const double2 *ct2 = reinterpret_cast<const double2 *>(
+                    (valid && E == 0) ? sCt + sb * TC_CH : sZero);
+                unsigned ov = 0u;
+                auto prep = [&](auto first_c) {
+                    constexpr bool FIRST = decltype(first_c)::value;
 #pragma unroll 1
-                for (int hh = 0; hh < 2; hh++)
+                    for (int hh = 0; hh < 2; hh++)
+                    {
+                        unsigned wE[TC_D][4], wO[TC_D][4];
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                        {
+                            unsigned loE[4], hiE[4], loO[4], hiO[4];
+                            double2 bp[4], cpE[2], cpO[2];
+#pragma unroll
+                            for (int kk = 0; kk < 4; kk++)
+                                bp[kk] = bt2[16 * hh + 4 * q + kk];
+                            cpE[0] = ct2[8 * hh + 2 * q];
+                            cpE[1] = ct2[8 * hh + 2 * q + 1];
+                            cpO[0] = ct2[16 + 8 * hh + 2 * q];
+                            cpO[1] = ct2[16 + 8 * hh + 2 * q + 1];
+#pragma unroll
+                            for (int b = 0; b < 8; b++)
+                            {
+                                const double beta =
+                                    (b & 1) ? bp[b >> 1].y : bp[b >> 1].x;
+                                if (!(FIRST && q == 0 && b == 0 && hh == 0))
+                                {
+                                    const double by = RR ? beta * (rho2 * y)
+                                                         : beta * y;
+                                    const double z = fma(tq, x, -by);
+                                    y = x;
+                                    x = z;
+                                }
+                                const int kv = b >> 1;
+                                const double2 c2 =
+                                    (b & 1) ? cpO[kv >> 1] : cpE[kv >> 1];
+                                const double ctn = (kv & 1) ? c2.y : c2.x;
+                                // round(x ct) in two's complement from the
+                                // mantissa of x ct + 1.5 2^52; the exponent
+                                // field checks |x ct| < 2^51
+                                const double tv = fma(x, ctn, TC_MAGIC);
+                                const unsigned hw =
+                                    (unsigned)__double2hiint(tv);
+                                const unsigned lo =
+                                    (unsigned)__double2loint(tv);
+                                ov |= hw ^ 0x43300000u;
+                                const unsigned hi = hw - 0x43380000u;
+                                if (b & 1)
+                                {
+                                    loO[kv] = lo;
+                                    hiO[kv] = hi;
+                                }
+                                else
+                                {
+                                    loE[kv] = lo;
+                                    hiE[kv] = hi;
+                                }
+                            }
+                            unsigned wd[TC_D];
+                            tc_transpose4(loE, hiE, wd);
+#pragma unroll
+                            for (int d = 0; d < TC_D; d++)
+                                wE[d][q] = wd[d];
+                            tc_transpose4(loO, hiO, wd);
+#pragma unroll
+                            for (int d = 0; d < TC_D; d++)
+                                wO[d][q] = wd[d];
+                        }
+                        const int off = tc_tile_off(row, 16 * hh);
+#pragma unroll
+                        for (int d = 0; d < TC_D; d++)
+                        {
+                            *reinterpret_cast<uint4 *>(at + d * TC_ATILE +
+                                                       off) =
+                                make_uint4(wE[d][0], wE[d][1], wE[d][2],
+                                           wE[d][3]);
+                            *reinterpret_cast<uint4 *>(
+                                at + (TC_D + d) * TC_ATILE + off) =
+                                make_uint4(wO[d][0], wO[d][1], wO[d][2],
+                                           wO[d][3]);
+                        }
+                    }
+                };
+                if (wok && !bad)
                 {
-                    unsigned wE[TC_D][4], wO[TC_D][4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++)
-                    {
-                        unsigned loE[4], hiE[4], loO[4], hiO[4];
-                        double2 bp[4], cp[4];
-#pragma unroll
-                        for (int k = 0; k < 4; k++)
-                        {
-                            bp[k] = bt2[16 * hh + 4 * q + k];
-                            cp[k] = ct2[16 * hh + 4 * q + k];
-                        }
-#pragma unroll
-                        for (int b = 0; b < 8; b++)
-                        {
-                            const double beta =
-                                (b & 1) ? bp[b >> 1].y : bp[b >> 1].x;
-                            const double ctn =
-                                (b & 1) ? cp[b >> 1].y : cp[b >> 1].x;
-                            if (!(FIRST && q == 0 && b == 0 && hh == 0))
-                            {
-                                const double by = RR ? beta * (rho2 * y)
-                                                     : beta * y;
-                                const double z = fma(tq, x, -by);
-                                y = x;
-                                x = z;
-                            }
-                            // round(v) in two's complement from the mantissa
-                            // of v + 1.5 2^52; the exponent field checks
-                            // |v| < 2^51
-                            const double tv = fma(x, ctn, TC_MAGIC);
-                            const unsigned lo = (unsigned)__double2loint(tv);
-                            const unsigned hw = (unsigned)__double2hiint(tv);
-                            ov |= hw ^ 0x43300000u;
-                            const unsigned hi = hw - 0x43380000u;
-                            if (b & 1)
-                            {
-                                loO[b >> 1] = lo;
-                                hiO[b >> 1] = hi;
-                            }
-                            else
-                            {
-                                loE[b >> 1] = lo;
-                                hiE[b >> 1] = hi;
-                            }
-                        }
-                        unsigned wd[TC_D];
-                        tc_transpose4(loE, hiE, wd);
-#pragma unroll
-                        for (int d = 0; d < TC_D; d++)
-                            wE[d][q] = wd[d];
-                        tc_transpose4(loO, hiO, wd);
-#pragma unroll
-                        for (int d = 0; d < TC_D; d++)
-                            wO[d][q] = wd[d];
-                    }
-                    const int off = tc_tile_off(tid, 16 * hh);
-#pragma unroll
-                    for (int d = 0; d < TC_D; d++)
-                    {
-                        *reinterpret_cast<uint4 *>(at + d * TC_ATILE + off) =
-                            make_uint4(wE[d][0], wE[d][1], wE[d][2], wE[d][3]);
-                        *reinterpret_cast<uint4 *>(at + (TC_D + d) * TC_ATILE +
-                                                   off) =
-                            make_uint4(wO[d][0], wO[d][1], wO[d][2], wO[d][3]);
-                    }
+                    if (j == 0)
+                        prep(std::integral_constant<bool, true>{});
+                    else
+                        prep(std::integral_constant<bool, false>{});
                 }
-            };
-            if (wok)
-            {
-                if (j == 0)
-                    prep(std::integral_constant<bool, true>{});
                 else
-                    prep(std::integral_constant<bool, false>{});
-            }
-            range_err |= ov >> 20;
-            if (any_scaled)
-            {
-                if (valid && leg_fixup(x, y, E))
                 {
-                    x *= rs;
-                    y *= rs;
+                    bad = true;
+                    *sAbort = 1;
                 }
-                any_scaled = __syncthreads_or(E != 0);
+                range_err |= ov >> 20;
+                if (any_scaled)
+                {
+                    if (valid && leg_fixup(x, y, E))
+                    {
+                        x *= rs;
+                        y *= rs;
+                    }
+                    any_scaled = tc_prep_or(E != 0);
+                }
+                fence_proxy_async_smem();
+                mbar_arrive(&bar_a[sa]);
             }
-            // operand tiles complete: hand them to the tensor cores
-            fence_proxy_async_smem();
-            tc_fence_before();
-            const bool all_ok = __syncthreads_and(wok) != 0;
-            tc_fence_after();
-            if (!all_ok)
+            // a uniform decision to stop (a wait of some thread gave up)
+            if (tc_prep_or(bad || *sAbort))
+                break;
+        }
+        if (range_err)
+            atomicOr(A.status, DEV_ERR_TC_RANGE);
+    }
+    else if (warp == 4)
+    {
+        // ================= producer =================
+        if (lane == 0)
+        {
+            unsigned long long g = 0;
+            for (unsigned long long k = 0;; k++)
             {
-                ok = false;
+                const unsigned long long item = sQ[k % TC_RING];
+                if (item >= (unsigned long long)A.nitems || *sAbort)
+                    break;
+                const long long m =
+                    (long long)(item / (unsigned long long)A.ntiles);
+                const int nch = (int)((N - m + TC_CH) / TC_CH);
+                bool ok = true;
+                for (int j = 0; j < nch && ok; j++, g++)
+                {
+                    const int sa = (int)(g & 1), sb = (int)(g % TC_NB);
+                    ok = mbar_wait_bounded(&bar_a[sa],
+                                           (unsigned)((g >> 1) & 1),
+                                           A.status) &&
+                         mbar_wait_bounded(&bar_b[sb],
+                                           (unsigned)((g / TC_NB) & 1),
+                                           A.status);
+                    // the accumulators are free (cleared by the epilogue of
+                    // the previous item, or at the start)
+                    if (ok && j == 0)
+                        ok = mbar_wait_bounded(bar_free, (unsigned)(k & 1),
+                                               A.status);
+                    if (!ok || *sAbort)
+                    {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t da0 =
+                        tc_sdesc(smem_u32(sA + sa * TC_ASTAGE));
+                    const uint64_t db0 =
+                        tc_sdesc(smem_u32(sB + sb * TC_BSTAGE));
+#pragma unroll
+                    for (int pp = 0; pp < 2; pp++)
+#pragma unroll
+                        for (int ia = 0; ia < TC_D; ia++)
+                        {
+                            // Legendre digit ia against the stack of
+                            // coefficient digits jb >= j0: block jb lands in
+                            // the accumulator of level ia + jb - TC_LMIN
+                            const int j0 = ia < TC_LMIN ? TC_LMIN - ia : 0;
+                            const int n = TC_COLS * (TC_D - j0);
+                            const uint64_t da =
+                                da0 + (uint64_t)(((pp * TC_D + ia) *
+                                                  TC_ATILE) >>
+                                                 4);
+                            const uint64_t db =
+                                db0 + (uint64_t)(((pp * TC_D + j0) *
+                                                  TC_BTILE) >>
+                                                 4);
+                            const uint32_t d =
+                                tmem + (uint32_t)((pp * TC_NLEV + ia + j0 -
+                                                   TC_LMIN) *
+                                                  TC_COLS);
+                            const uint32_t idesc =
+                                (ia == TC_D - 1 ? TC_IDESC_S : TC_IDESC_U) |
+                                ((uint32_t)(n >> 3) << 17);
+                            tc_mma(d, da, db, idesc, 1u);
+                        }
+                    tc_commit(&bar_m[sa]);
+                    if (j == nch - 1)
+                        tc_commit(bar_acc);
+                    // chunk g + TC_AHEAD + 1 goes to the stage of chunk
+                    // g - 1, whose MMAs are the latest on that barrier
+                    if (g >= 1 &&
+                        !mbar_wait_bounded(&bar_m[(g - 1) & 1],
+                                           (unsigned)(((g - 1) >> 1) & 1),
+                                           A.status))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    issue_next(g + TC_AHEAD + 1);
+                }
+                if (!ok)
+                {
+                    *sAbort = 1;
+                    break;
+                }
+            }
+            // the last commit: all MMAs of this CTA are complete before the
+            // accumulators are released
+            if (g > 0)
+                mbar_wait_bounded(&bar_m[(g - 1) & 1],
+                                  (unsigned)(((g - 1) >> 1) & 1), A.status);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ================= epilogue =================
+        const int quarter = warp & 3;
+        const int half = (warp - 5) >> 2;                 // columns half
+        const int row = quarter * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+        // clear this warp's half of the accumulator columns
+        auto clear = [&]() {
+            const uint32_t hb = lane_base + (uint32_t)(half * 16);
+#pragma unroll 1
+            for (int pl = 0; pl < 2 * TC_NLEV; pl++)
+                tc_st_zero16(hb + (uint32_t)(pl * TC_COLS));
+            tc_wait_st();
+        };
+        clear();
+        tc_fence_before();
+        mbar_arrive(bar_free);
+        for (unsigned long long k = 0;; k++)
+        {
+            const unsigned long long item = sQ[k % TC_RING];
+            if (__any_sync(0xffffffffu,
+                           item >= (unsigned long long)A.nitems || *sAbort))
+                break;
+            bool eok = mbar_wait_bounded(bar_acc, (unsigned)(k & 1),
+                                         A.status);
+            eok = __all_sync(0xffffffffu, eok);
+            if (!eok)
+            {
+                *sAbort = 1;
                 break;
             }
-            if (tid == 0)
-            {
-                // per parity and Legendre digit ia: one MMA against the
-                // stack of coefficient digits jb >= j0 (contiguous tiles,
-                // N = 32 (7 - j0) rows) whose 32-column blocks land in the
-                // accumulators of levels ia + jb - TC_LMIN
-                const uint64_t da0 = tc_sdesc(smem_u32(at));
-                const uint64_t db0 = tc_sdesc(smem_u32(sB + sb * TC_BSTAGE));
-#pragma unroll
-                for (int par = 0; par < 2; par++)
-#pragma unroll
-                    for (int ia = 0; ia < TC_D; ia++)
-                    {
-                        const int j0 = ia < TC_LMIN ? TC_LMIN - ia : 0;
-                        const int n = TC_COLS * (TC_D - j0);
-                        const uint64_t da =
-                            da0 + (uint64_t)(((par * TC_D + ia) * TC_ATILE) >>
-                                             4);
-                        const uint64_t db =
-                            db0 + (uint64_t)(((par * TC_D + j0) * TC_BTILE) >>
-                                             4);
-                        const uint32_t d =
-                            tmem + (uint32_t)((par * TC_NLEV + ia + j0 -
-                                               TC_LMIN) * TC_COLS);
-                        const uint32_t idesc =
-                            (ia == TC_D - 1 ? TC_IDESC_S : TC_IDESC_U) |
-                            ((uint32_t)(n >> 3) << 17);
-                        tc_mma(d, da, db, idesc, 1u);
-                    }
-                tc_commit(&bar_m[sa]);
-            }
-        }
-        if (!ok)
-            break;
-
-        // ---- epilogue: recombine the levels, north / south, write ----
-        const bool eok = mbar_wait_bounded(&bar_m[(g - 1) & 1],
-                                           (unsigned)(((g - 1) >> 1) & 1),
-                                           A.status);
-        if (!__syncthreads_and(eok))
-        {
-            ok = false;
-            break;
-        }
-        tc_fence_after();
-        const double cpack = m == 0 ? 1.0 : 0.5;
-        const double rsi = pow2i(eA - 105);
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-        int rown = -1, rows = -1;
-        if (valid)
-        {
-            rown = A.row_n[p];
-            rows = A.row_s[p];
-        }
-#pragma unroll 1
-        for (int cb = 0; cb < TC_COLS / 8; cb++)
-        {
-            double tot[2][8];
-#pragma unroll
-            for (int par = 0; par < 2; par++)
-            {
-                int v[TC_NLEV][8];
-#pragma unroll
-                for (int L = 0; L < TC_NLEV; L++)
-                    tc_ld8(lane_base +
-                               (uint32_t)((par * TC_NLEV + L) * TC_COLS +
-                                          cb * 8),
-                           v[L]);
-                tc_wait_ld();
-#pragma unroll
-                for (int c = 0; c < 8; c++)
-                {
-                    double s = 0.0;
-#pragma unroll
-                    for (int L = TC_NLEV - 1; L >= 0; L--)
-                        s = fma(i2d_exact(v[L][c]), pow2i(8 * (L + TC_LMIN)),
-                                s);
-                    tot[par][c] = s;
-                }
-            }
+            tc_fence_after();
+            const long long m =
+                (long long)(item / (unsigned long long)A.ntiles);
+            const int tile = (int)(item % (unsigned long long)A.ntiles);
+            const int p = tile * TC_M + row;
+            const bool valid = p < np;
+            double u = 1.0, rh = 1.0;
+            int rown = -1, rows = -1;
             if (valid)
             {
+                u = A.u[p];
+                if (RR)
+                    rh = A.rho[p];
+                rown = A.row_n[p];
+                rows = A.row_s[p];
+            }
+            double bnd = sqrt(2.0 * (double)N + 1.0);
+            if (u > 0.0)
+                bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
+            if (RR && rh > 1.0)
+                bnd *= pow(rh, (double)(N + 1));
+            const int eA = expo_of(bnd) + 1;
+            const double cpack = m == 0 ? 1.0 : 0.5;
+            const double rsi = pow2i(eA - 105);
+#pragma unroll 1
+            for (int cb = 2 * half; cb < 2 * half + 2; cb++)
+            {
+                double tot[2][8];
 #pragma unroll
-                for (int k = 0; k < 4; k++)
+                for (int pp = 0; pp < 2; pp++)
                 {
-                    const int set = cb * 4 + k;
-                    if (set >= A.nsets)
-                        break;
-                    const double fc = pow2i(sEcol[2 * set]) * rsi;
-                    const double fs = pow2i(sEcol[2 * set + 1]) * rsi;
-                    const double w = cpack * A.mur[set];
-                    const double ac = (tot[0][2 * k] + tot[1][2 * k]) * fc;
-                    const double as = (tot[0][2 * k + 1] + tot[1][2 * k + 1]) *
-                                      fs;
-                    double2 *o = A.out[set];
-                    if (rown >= 0 && rown < A.nlat)
-                        o[(size_t)rown * A.ldf + m] =
-                            make_double2(w * ac, -(w * as));
-                    if (rows >= 0 && rows < A.nlat)
+                    int v[TC_NLEV][8];
+#pragma unroll
+                    for (int L = 0; L < TC_NLEV; L++)
+                        tc_ld8(lane_base +
+                                   (uint32_t)((pp * TC_NLEV + L) * TC_COLS +
+                                              cb * 8),
+                               v[L]);
+                    tc_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < 8; c++)
                     {
-                        const double bc =
-                            (tot[0][2 * k] - tot[1][2 * k]) * fc;
-                        const double bs =
-                            (tot[0][2 * k + 1] - tot[1][2 * k + 1]) * fs;
-                        o[(size_t)rows * A.ldf + m] =
-                            make_double2(w * bc, -(w * bs));
+                        double s2 = 0.0;
+#pragma unroll
+                        for (int L = TC_NLEV - 1; L >= 0; L--)
+                            s2 = fma(i2d_exact(v[L][c]),
+                                     pow2i(8 * (L + TC_LMIN)), s2);
+                        tot[pp][c] = s2;
+                    }
+                }
+                if (valid)
+                {
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++)
+                    {
+                        const int set = cb * 4 + kk;
+                        if (set >= A.nsets)
+                            break;
+                        const int ec = __ldg(&A.ecol[m * TC_COLS + 2 * set]);
+                        const int es =
+                            __ldg(&A.ecol[m * TC_COLS + 2 * set + 1]);
+                        const double fc = pow2i(ec) * rsi;
+                        const double fs = pow2i(es) * rsi;
+                        const double wgt = cpack * A.mur[set];
+                        double2 *o = A.out[set];
+                        if (rown >= 0 && rown < A.nlat)
+                            o[(size_t)rown * A.ldf + m] = make_double2(
+                                wgt * ((tot[0][2 * kk] + tot[1][2 * kk]) * fc),
+                                -(wgt * ((tot[0][2 * kk + 1] +
+                                          tot[1][2 * kk + 1]) *
+                                         fs)));
+                        if (rows >= 0 && rows < A.nlat)
+                            o[(size_t)rows * A.ldf + m] = make_double2(
+                                wgt * ((tot[0][2 * kk] - tot[1][2 * kk]) * fc),
+                                -(wgt * ((tot[0][2 * kk + 1] -
+                                          tot[1][2 * kk + 1]) *
+                                         fs)));
                     }
                 }
             }
+            clear();
+            tc_fence_before();
+            mbar_arrive(bar_free);
         }
-        // the next item's MMAs overwrite the accumulators
-        tc_fence_before();
-        __syncthreads();
     }
-    if (range_err)
-        atomicOr(A.status, DEV_ERR_TC_RANGE);
-    // all MMAs of this CTA have completed (epilogue wait) unless a wait
-    // gave up; in that case wait once more for the last commit, bounded
-    if (!ok && g > 0)
-        mbar_wait_bounded(&bar_m[(g - 1) & 1], (unsigned)(((g - 1) >> 1) & 1),
-                          A.status);
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -696,9 +871,10 @@ __global__ void __launch_bounds__(128, 1) k_shs_tc(ShsTcArgs A)
 
 size_t shs_tc_smem_bytes()
 {
-    return 2 * TC_ASTAGE + 3 * TC_BSTAGE + 7 * TC_CH * sizeof(double) +
-           5 * sizeof(uint64_t) + 4 * sizeof(uint32_t) +
-           TC_COLS * sizeof(int) + sizeof(unsigned long long) + 64;
+    return 2 * TC_ASTAGE + TC_NB * TC_BSTAGE +
+           (2 * TC_NB + 1) * TC_CH * sizeof(double) +
+           (TC_NB + 6) * sizeof(uint64_t) + 4 * sizeof(uint32_t) +
+           8 * sizeof(unsigned long long) + 64;
 }
 
 size_t shs_tc_chunk_bytes()
@@ -737,7 +913,7 @@ cudaError_t launch_shs_tc(const ShsTcArgs &A, bool rr, int grid,
                                  (int)smem);
         if (e != cudaSuccess)
             return e;
-        k_shs_tc<true><<<grid, 128, smem, st>>>(A);
+        k_shs_tc<true><<<grid, TC_THREADS, smem, st>>>(A);
     }
     else
     {
@@ -746,7 +922,7 @@ cudaError_t launch_shs_tc(const ShsTcArgs &A, bool rr, int grid,
                                  (int)smem);
         if (e != cudaSuccess)
             return e;
-        k_shs_tc<false><<<grid, 128, smem, st>>>(A);
+        k_shs_tc<false><<<grid, TC_THREADS, smem, st>>>(A);
     }
     return cudaGetLastError();
 }
