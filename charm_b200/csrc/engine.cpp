@@ -1415,6 +1415,10 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
     const int ntiles = (np + 127) / 128;
+    double *seed_x = nullptr;
+    CB_TRY(dbuf(c, "tc_seed_x", (size_t)(N + 1) * np, &seed_x));
+    int2 *seed_e = nullptr;
+    CB_TRY(dbuf(c, "tc_seed_e", (size_t)(N + 1) * np, &seed_e));
 
     for (size_t j0 = 0; j0 < nsets; j0 += SHS_TC_SETS)
     {
@@ -1471,6 +1475,13 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         }
         A.counter = d_counter;
         A.status = d_status;
+        A.seed_x = seed_x;
+        A.seed_e = seed_e;
+        if (j0 == 0)
+        {
+            Scope sc(c, TIMER_PREP);
+            CB_CUDA(launch_tc_seeds(A, !G.r_eq, seed_x, seed_e, c.stream), st);
+        }
         const int grid = (int)std::min<long long>(A.nitems,
                                                   (long long)c.num_sms);
         {

@@ -280,6 +280,10 @@ struct ShsTcArgs
     const int *ecol;
     const double *t, *u, *rho;
     const int *row_n, *row_s;
+    // per (order m, pair p) at m * npairs + p: the seed R~_mm in the
+    // fixed-point scale (or its mantissa while scaled) and (E, eA)
+    const double *seed_x;
+    const int2 *seed_e;
     int nlat, ldf;
     int nsets;
     double2 *out[SHS_TC_SETS];            // lumped coefficients [nlat][ldf]
@@ -294,6 +298,8 @@ cudaError_t launch_tc_ctab(long long nmax, int ld, const double2 *tb,
                            const double *tc, double *btp, double *ctp,
                            cudaStream_t st);
 cudaError_t launch_tc_prep(const ShsTcPrep &P, cudaStream_t st);
+cudaError_t launch_tc_seeds(const ShsTcArgs &A, bool rr, double *seed_x,
+                            int2 *seed_e, cudaStream_t st);
 cudaError_t launch_shs_tc(const ShsTcArgs &A, bool rr, int grid,
                           cudaStream_t st);
 cudaError_t launch_tables_f32(long long nmax, const double *r,

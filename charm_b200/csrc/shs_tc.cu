@@ -25,12 +25,9 @@
 // 34 digit pairs per degree tile and parity; 8 levels x 2 parities x 32
 // columns = all 512 TMEM columns of the SM.
 //
-// The bound 2^eA of a latitude and order is min(sqrt(2N + 1),
-// 6 (m + 1)^(1/4) / sqrt(cos lat)) (times (R/r)^(N+1) below the sphere):
-// |P_nm| <= sqrt(2n + 1) holds for the geodetic normalisation, and
-// sqrt(cos lat) |P_nm| stays below 4.2 (m + 1)^(1/4) for all n, m <= 2190
-// (evaluated on 190 latitudes; the maxima sit at the turning points).  A
-// value outside the grid sets DEV_ERR_TC_RANGE and the call fails.
+// The fixed-point grid of the Legendre values of each (order, latitude) is
+// chosen from a bound of |P_nm| (k_tc_seeds); a value outside it sets
+// DEV_ERR_TC_RANGE and the call fails.
 //
 // Pipeline per CTA (one latitude pair per TMEM lane): the coefficient digit
 // tiles and the recurrence tables of a 64-degree chunk arrive by bulk
@@ -319,6 +316,40 @@ __global__ void k_tc_ctab(long long nmax, int ld, const double2 *__restrict__ tb
     }
 }
 
+// Seeds of every (order, latitude pair), once per call: the sectorial value
+// R~_mm (leg.cuh), its binary exponent E while below the double range, and
+// the exponent eA of the fixed-point grid of that latitude and order, i.e.
+// 2^eA > min(sqrt(2N + 1), 6 (m + 1)^(1/4) / sqrt(cos lat)) (times (R/r)^(N+1)
+// below the sphere): |P_nm| <= sqrt(2n + 1) holds for the geodetic
+// normalisation, and sqrt(cos lat) |P_nm| stays below 4.2 (m + 1)^(1/4) for
+// all n, m <= 2190 (evaluated on 190 latitudes).  Values in range are
+// stored already multiplied by 2^(51 - eA).
+template <bool RR>
+__global__ void k_tc_seeds(ShsTcArgs A, double *seed_x, int2 *seed_e)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long np = A.npairs;
+    if (idx >= (A.nmax + 1) * np)
+        return;
+    const long long m = idx / np;
+    const int p = (int)(idx % np);
+    const double u = A.u[p];
+    const double rh = RR ? A.rho[p] : 1.0;
+    double x;
+    int E;
+    leg_seed(A.sg[2 * m], u, rh, RR, m, 0, x, E);
+    double bnd = sqrt(2.0 * (double)A.nmax + 1.0);
+    if (u > 0.0)
+        bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
+    if (RR && rh > 1.0)
+        bnd *= pow(rh, (double)(A.nmax + 1));
+    const int eA = expo_of(bnd) + 1;
+    if (E == 0)
+        x *= pow2i(51 - eA);
+    seed_x[idx] = x;
+    seed_e[idx] = make_int2(E, eA);
+}
+
 // ---------------------------------------------------------------------------
 // The contraction kernel
 // ---------------------------------------------------------------------------
@@ -470,6 +501,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
         const int row = tid;
         unsigned long long g = 0;
         unsigned range_err = 0u;
+        // seed, exponents and geometry of an item's latitude pair
+        double nx_x = 0.0, nx_t = 0.0, nx_rh = 1.0;
+        int2 nx_e = make_int2(0, 0);
+        bool have_next = false;
+        auto load_seed = [&](unsigned long long it) {
+            const long long mm = (long long)(it / (unsigned long long)A.ntiles);
+            const int pp = (int)(it % (unsigned long long)A.ntiles) * TC_M + row;
+            nx_x = 0.0;
+            nx_t = 0.0;
+            nx_rh = 1.0;
+            nx_e = make_int2(0, 0);
+            if (pp < np)
+            {
+                const long long i = mm * (long long)np + pp;
+                nx_x = A.seed_x[i];
+                nx_e = A.seed_e[i];
+                nx_t = A.t[pp];
+                if (RR)
+                    nx_rh = A.rho[pp];
+            }
+        };
         for (unsigned long long k = 0;; k++)
         {
             // the same id for all 128 threads (written before the barrier
@@ -483,24 +535,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
             const int tile = (int)(item % (unsigned long long)A.ntiles);
             const int p = tile * TC_M + row;
             const bool valid = p < np;
-            const double t = valid ? A.t[p] : 0.0;
-            const double u = valid ? A.u[p] : 1.0;
-            const double rh = (RR && valid) ? A.rho[p] : 1.0;
-            const double tq = RR ? t * rh : t;
-            const double rho2 = rh * rh;
-            double x = 0.0, y = 0.0;
-            int E = 0;
-            if (valid)
-                leg_seed(A.sg[2 * m], u, rh, RR, m, 0, x, E);
-            double bnd = sqrt(2.0 * (double)N + 1.0);
-            if (u > 0.0)
-                bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
-            if (RR && rh > 1.0)
-                bnd *= pow(rh, (double)(N + 1));
-            const int eA = expo_of(bnd) + 1;
+            // this item's seed (prefetched during the previous item's last
+            // chunk, or loaded now for the first item)
+            if (!have_next)
+                load_seed(item);
+            const double tq = RR ? nx_t * nx_rh : nx_t;
+            const double rho2 = nx_rh * nx_rh;
+            double x = nx_x, y = 0.0;
+            int E = nx_e.x;
+            const int eA = nx_e.y;
+            have_next = false;
             const double rs = pow2i(51 - eA);
-            if (E == 0)
-                x *= rs;
             bool any_scaled = tc_prep_or(E != 0);
             const long long ncol = N - m + 1;
             const int nch = (int)((ncol + TC_CH - 1) / TC_CH);
@@ -526,6 +571,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                 }
                 if (j + 1 < nch)
                     mul_next = A.tmul[m * A.ldmul + j + 1];
+                else if (wok)
+                {
+                    // the next item's id was published before this chunk's
+                    // load barrier: fetch its seeds while this chunk runs
+                    const unsigned long long nit = sQ[(k + 1) % TC_RING];
+                    if (nit < (unsigned long long)A.nitems)
+                    {
+                        load_seed(nit);
+                        have_next = true;
+                    }
+                }
                 unsigned char *at = sA + sa * TC_ASTAGE;
                 const double2 *bt2 =
                     reinterpret_cast<const double2 *>(sBt + sb * TC_CH);
@@ -779,22 +835,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
             const int tile = (int)(item % (unsigned long long)A.ntiles);
             const int p = tile * TC_M + row;
             const bool valid = p < np;
-            double u = 1.0, rh = 1.0;
-            int rown = -1, rows = -1;
+            int rown = -1, rows = -1, eA = 0;
             if (valid)
             {
-                u = A.u[p];
-                if (RR)
-                    rh = A.rho[p];
                 rown = A.row_n[p];
                 rows = A.row_s[p];
+                eA = A.seed_e[m * (long long)np + p].y;
             }
-            double bnd = sqrt(2.0 * (double)N + 1.0);
-            if (u > 0.0)
-                bnd = fmin(bnd, 6.0 * sqrt(sqrt((double)m + 1.0)) / sqrt(u));
-            if (RR && rh > 1.0)
-                bnd *= pow(rh, (double)(N + 1));
-            const int eA = expo_of(bnd) + 1;
             const double cpack = m == 0 ? 1.0 : 0.5;
             const double rsi = pow2i(eA - 105);
 #pragma unroll 1
@@ -888,6 +935,18 @@ cudaError_t launch_tc_ctab(long long nmax, int ld, const double2 *tb,
 {
     k_tc_ctab<<<(unsigned)(nmax + 1), 128, 0, st>>>(nmax, ld, tb, tc, btp,
                                                     ctp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_seeds(const ShsTcArgs &A, bool rr, double *seed_x,
+                            int2 *seed_e, cudaStream_t st)
+{
+    const long long n = (A.nmax + 1) * (long long)A.npairs;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (rr)
+        k_tc_seeds<true><<<blocks, 256, 0, st>>>(A, seed_x, seed_e);
+    else
+        k_tc_seeds<false><<<blocks, 256, 0, st>>>(A, seed_x, seed_e);
     return cudaGetLastError();
 }
 
