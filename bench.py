@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--nmax", type=int, default=2190)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch-i8", action="store_true",
+                    help="skip the batched split-precision section")
     ap.add_argument("--no-n10800", action="store_true",
                     help="skip the nmax 10800 round trip")
     ap.add_argument("--workload", default="roundtrip",
@@ -263,6 +265,8 @@ def run_ours(args):
 
     f32 = single_precision(L, err, pnt, N, c, s, d_f, stream, flush,
                            args.steps)
+    bi8 = None if args.no_batch_i8 else batched_split_precision(
+        L, err, pnt, N, dev, peak, args.steps)
     hi = None if args.no_n10800 else ultra_high_degree(L, err, dev, stream,
                                                         flush, peak)
 
@@ -351,6 +355,8 @@ def run_ours(args):
         "clocks": clk,
     }
     line["f32"] = f32
+    if bi8 is not None:
+        line["batch_i8"] = bi8
     if hi is not None:
         line["nmax10800"] = hi
     if not args.no_cpu_baseline:
@@ -427,6 +433,94 @@ def single_precision(L, err, pnt, N, c, s, d_f64, stream, flush, steps):
                           "fft_total_per_step": ms[3] / steps},
             "field_rel_rms_vs_fp64": e_field,
             "round_trip_rel_rms": e_rt}
+
+
+def batched_split_precision(L, err, pnt, N, dev, peak, steps, nsets=16):
+    """Synthesis of nsets Kaula coefficient sets of degree N on the GL grid:
+    the FP64 batched path (charm_b200_shs_point_batch_dev, the plain FP64
+    kernels) against the split-precision one (..._batch_i8_dev: INT8 digit
+    products on the tensor cores, FP64 recombination), same inputs, device
+    resident.  Reports per-call and per-kernel times, sets/s, the largest
+    per-set relative RMS difference, the INT8 tensor-core rate (ops per MMA
+    as issued: 2 x 128 x 2176 x 32 per 64-degree chunk and latitude tile)
+    and the FP64-equivalent rate (12 flops per (n, m, latitude pair) unit
+    and set, as the synthesis roofline)."""
+    import torch
+    from charm_b200.workloads import GM, R_EARTH, kaula, rel_rms
+    P = ct.c_void_p
+    for f in (L.charm_b200_shs_point_batch_dev,
+              L.charm_b200_shs_point_batch_i8_dev):
+        f.argtypes = [P, ct.c_size_t, ct.POINTER(ct.c_ulong),
+                      ct.POINTER(ct.c_ulong), ct.POINTER(ct.c_double),
+                      ct.c_double, ct.POINTER(ct.c_void_p),
+                      ct.POINTER(ct.c_void_p), ct.c_int,
+                      ct.POINTER(ct.c_void_p), P]
+    npts = pnt.lat.size * pnt.lon.size
+    cs = [kaula(N, 6000 + j) for j in range(nsets)]
+    dc = [torch.from_numpy(c).to(dev) for c, _ in cs]
+    ds = [torch.from_numpy(s).to(dev) for _, s in cs]
+    o64 = [torch.empty(npts, dtype=torch.float64, device=dev)
+           for _ in range(nsets)]
+    o8 = [torch.empty(npts, dtype=torch.float64, device=dev)
+          for _ in range(nsets)]
+    nm = (ct.c_ulong * nsets)(*([N] * nsets))
+    mu = (ct.c_double * nsets)(*([GM] * nsets))
+    pc = (ct.c_void_p * nsets)(*[t.data_ptr() for t in dc])
+    ps = (ct.c_void_p * nsets)(*[t.data_ptr() for t in ds])
+
+    def run(fn, outs):
+        pf = (ct.c_void_p * nsets)(*[t.data_ptr() for t in outs])
+        fn(ct.cast(pnt._Point, P), nsets, nm, nm, mu, R_EARTH, pc, ps, 0, pf,
+           ct.cast(err, P))
+        if not L.charm_err_isempty(err):
+            raise RuntimeError(ct.string_at(err.contents.msg).decode())
+
+    res = {}
+    for name, fn, outs in (("fp64", L.charm_b200_shs_point_batch_dev, o64),
+                           ("i8", L.charm_b200_shs_point_batch_i8_dev, o8)):
+        run(fn, outs)               # tables, buffers
+        torch.cuda.synchronize()
+        L.charm_b200_timing(1)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            run(fn, outs)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) / steps
+        ms = (ct.c_double * 7)()
+        cnt = (ct.c_ulonglong * 7)()
+        L.charm_b200_timing_read(ms, cnt, 7, None, None)
+        L.charm_b200_timing(0)
+        res[name] = {"s_per_batch": wall, "sets_per_s": nsets / wall,
+                     "legendre_kernel_ms": ms[0] / steps,
+                     "row_transforms_ms": ms[3] / steps,
+                     "prep_ms": ms[5] / steps}
+    worst = max(rel_rms(a.cpu().numpy(), b.cpu().numpy())
+                for a, b in zip(o8, o64))
+    np_ = (pnt.lat.size + 1) // 2
+    ntiles = (np_ + 127) // 128
+    chunks = sum((N - m + 64) // 64 for m in range(N + 1))
+    int8_ops = 2.0 * 128 * 2176 * 32 * chunks * ntiles
+    units = (N + 1) * (N + 2) / 2 * np_ * nsets
+    k8 = res["i8"]["legendre_kernel_ms"] * 1e-3
+    k64 = res["fp64"]["legendre_kernel_ms"] * 1e-3
+    out = {
+        "workload": "%d Kaula sets of nmax %d, potential on the GL grid "
+                    "(%d x %d), r = R" % (nsets, N, pnt.lat.size,
+                                          pnt.lon.size),
+        "fp64_batch": res["fp64"], "i8_batch": res["i8"],
+        "speedup_sets_per_s": res["fp64"]["s_per_batch"] /
+        res["i8"]["s_per_batch"],
+        "speedup_legendre_kernel": k64 / k8,
+        "max_set_rel_rms_vs_fp64": worst,
+        "tensor_int8_tops": int8_ops / k8 / 1e12,
+        "tensor_int8_frac_of_nominal_4500": int8_ops / k8 / 1e12 / 4500.0,
+        "fp64_equivalent_tflops": units * 12.0 / k8 / 1e12,
+        "fp64_equivalent_frac_of_fp64_peak": (units * 12.0 / k8 / 1e12 / peak
+                                              if peak > 0 else None),
+    }
+    del dc, ds, o64, o8
+    torch.cuda.empty_cache()
+    return out
 
 
 def ultra_high_degree(L, err, dev, stream, flush, peak, steps=2):
@@ -739,6 +833,47 @@ def run_batch(args):
                 total_units += T * (pnt.lat.size // 2 + 1)
             del dc, ds, out
             torch.cuda.empty_cache()
+    # the potential of the same 64 sets: FP64 batch against the
+    # split-precision batch (tensor cores), each parity group in one call
+    L.charm_b200_shs_point_batch_i8_dev.argtypes = \
+        L.charm_b200_shs_point_batch_dev.argtypes
+    pot = {"fp64_s": 0.0, "i8_s": 0.0, "worst_rel_rms": 0.0}
+    from charm_b200.workloads import rel_rms
+    for pnt, idx in groups:
+        npts = pnt.lat.size * pnt.lon.size
+        n = len(idx)
+        cs = [kaula(int(nm[j]), 4000 + j) for j in idx]
+        dc = [torch.from_numpy(c).cuda() for c, _ in cs]
+        ds = [torch.from_numpy(s).cuda() for _, s in cs]
+        nmv = (ct.c_ulong * n)(*[int(nm[j]) for j in idx])
+        muv = (ct.c_double * n)(*([GM] * n))
+        pc = (ct.c_void_p * n)(*[t.data_ptr() for t in dc])
+        ps = (ct.c_void_p * n)(*[t.data_ptr() for t in ds])
+        outs = {}
+        for name, fn in (("fp64", L.charm_b200_shs_point_batch_dev),
+                         ("i8", L.charm_b200_shs_point_batch_i8_dev)):
+            out = [torch.empty(npts, dtype=torch.float64, device="cuda")
+                   for _ in idx]
+            pf = (ct.c_void_p * n)(*[t.data_ptr() for t in out])
+            for rep in range(2):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                fn(ct.cast(pnt._Point, P), n, nmv, nmv, muv, R_EARTH, pc, ps,
+                   0, pf, ct.cast(err, P))
+                check()
+                torch.cuda.synchronize()
+                if rep == 1:
+                    pot[name + "_s"] += time.perf_counter() - t0
+            outs[name] = out
+        for a, b in zip(outs["i8"], outs["fp64"]):
+            pot["worst_rel_rms"] = max(pot["worst_rel_rms"],
+                                       rel_rms(a.cpu().numpy(),
+                                               b.cpu().numpy()))
+        del dc, ds, outs
+        torch.cuda.empty_cache()
+    pot["speedup"] = pot["fp64_s"] / pot["i8_s"]
+    pot["i8_sets_per_s"] = 64.0 / pot["i8_s"]
+    pot["fp64_sets_per_s"] = 64.0 / pot["fp64_s"]
     line = {
         "workload": "64 coefficient sets, nmax U(90, 2160), potential + grad1 "
                     "+ grad2 (10 quantities) at r = R + 250 km, DH1 / DH2 grids "
@@ -747,6 +882,7 @@ def run_batch(args):
         "single_calls_s": t_single, "single_sets_per_s": 64.0 / t_single,
         "speedup": t_single / t_batch,
         "units_n_m_pair": total_units,
+        "potential_fp64_vs_split_precision": pot,
         "dtype": "f64", "data": "synthetic (seeds 4999, 4000 + j)",
     }
     L.charm_err_free(err)

@@ -1389,16 +1389,27 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
                                c.stream), st);
         c.tcp_nmax = (long long)N;
     }
+    // sets in order of decreasing degree, so that each launch of up to
+    // SHS_TC_SETS sets stops at a degree close to all of its sets'
+    std::vector<size_t> ord(nsets);
+    for (size_t j = 0; j < nsets; j++)
+        ord[j] = j;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+        return nmax_v[a] > nmax_v[b];
+    });
     // chunks of 64 degrees per order, and where each order's tiles start
+    // (for the largest degree; a launch of lower degree uses a prefix of
+    // the same layout rebuilt for its own degree)
     std::vector<long long> h0(N + 2);
-    h0[0] = 0;
-    for (unsigned long m = 0; m <= N; m++)
-        h0[m + 1] = h0[m] + (long long)((N - m + 64) / 64);
-    const long long nchunks = h0[N + 1];
+    auto chunk_layout = [&](unsigned long Ng) {
+        h0[0] = 0;
+        for (unsigned long m = 0; m <= Ng; m++)
+            h0[m + 1] = h0[m] + (long long)((Ng - m + 64) / 64);
+        return h0[Ng + 1];
+    };
+    const long long nchunks = chunk_layout(N);
     long long *d_chunk0 = nullptr;
     CB_TRY(dbuf(c, "tc_chunk0", h0.size(), &d_chunk0));
-    CB_CUDA(cudaMemcpyAsync(d_chunk0, h0.data(), h0.size() * sizeof(long long),
-                            cudaMemcpyHostToDevice, c.stream), st);
     int *d_ecol = nullptr;
     CB_TRY(dbuf(c, "tc_ecol", (size_t)(N + 1) * 32, &d_ecol));
     void *bdig = nullptr;
@@ -1423,15 +1434,21 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
     for (size_t j0 = 0; j0 < nsets; j0 += SHS_TC_SETS)
     {
         const int nb = (int)std::min<size_t>(SHS_TC_SETS, nsets - j0);
+        const unsigned long Ng = nmax_v[ord[j0]];   // largest of the launch
+        chunk_layout(Ng);
+        CB_CUDA(cudaMemcpyAsync(d_chunk0, h0.data(),
+                                (Ng + 2) * sizeof(long long),
+                                cudaMemcpyHostToDevice, c.stream), st);
         ShsTcPrep P{};
-        P.nmax = (long long)N;
+        P.nmax = (long long)Ng;
         P.nsets = nb;
         for (int b = 0; b < nb; b++)
         {
-            P.set_nmax[b] = (long long)nmax_v[j0 + b];
-            P.shc_nmax[b] = (long long)shc_nmax_v[j0 + b];
-            P.c[b] = d_c[j0 + b];
-            P.s[b] = d_s[j0 + b];
+            const size_t jj = ord[j0 + b];
+            P.set_nmax[b] = (long long)nmax_v[jj];
+            P.shc_nmax[b] = (long long)shc_nmax_v[jj];
+            P.c[b] = d_c[jj];
+            P.s[b] = d_s[jj];
         }
         P.chunk0 = d_chunk0;
         P.ecol = d_ecol;
@@ -1448,9 +1465,10 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
                                 c.stream), st);
         ShsTcArgs A{};
         A.nmax = (long long)N;
+        A.nmax_sets = (long long)Ng;
         A.npairs = np;
         A.ntiles = ntiles;
-        A.nitems = (long long)(N + 1) * ntiles;
+        A.nitems = (long long)(Ng + 1) * ntiles;
         A.tb = tab.tb;
         A.tmul = tab.tmul;
         A.ldmul = tab.ldmul;
@@ -1471,7 +1489,7 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         for (int b = 0; b < nb; b++)
         {
             A.out[b] = lc + (size_t)b * per_set;
-            A.mur[b] = mu_v[j0 + b] / R;
+            A.mur[b] = mu_v[ord[j0 + b]] / R;
         }
         A.counter = d_counter;
         A.status = d_status;
@@ -1491,7 +1509,8 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         }
         for (int b = 0; b < nb; b++)
         {
-            double *dst = d_f[j0 + b];
+            const size_t jj = ord[j0 + b];
+            double *dst = d_f[jj];
             double2 *src = lc + (size_t)b * per_set;
             if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
             {
@@ -1501,7 +1520,7 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
                 R2.ldx = (long long)nlon;
                 R2.X = src;
                 R2.ldX = ldf;
-                R2.kmax = (int)nmax_v[j0 + b];
+                R2.kmax = (int)nmax_v[jj];
                 Scope sc(c, TIMER_FFT);
                 CB_CUDA(launch_rfft(R2, true, c.stream), st);
             }

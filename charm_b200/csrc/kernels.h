@@ -251,7 +251,7 @@ constexpr int SHS_TC_SETS = 16;
 // set s), and the column exponents ecol[m][32].
 struct ShsTcPrep
 {
-    long long nmax;                       // table degree (largest set)
+    long long nmax;                       // largest degree of the launch
     int nsets;
     long long set_nmax[SHS_TC_SETS];
     long long shc_nmax[SHS_TC_SETS];      // layout of each set's triangle
@@ -265,10 +265,11 @@ struct ShsTcPrep
 
 struct ShsTcArgs
 {
-    long long nmax;
+    long long nmax;                       // degree of the tables
+    long long nmax_sets;                  // largest degree of the launch
     int npairs;
     int ntiles;                           // tiles of 128 latitude pairs
-    long long nitems;                     // (nmax + 1) * ntiles
+    long long nitems;                     // (nmax_sets + 1) * ntiles
     const double2 *tb;                    // recurrence tables (leg.cuh)
     const double *tmul;
     int ldmul;

@@ -441,7 +441,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
         fence_mbar_init();
         *sAbort = 0;
     }
-    const long long N = A.nmax;
+    // degrees of this launch's sets (<= the tables' A.nmax): work items,
+    // chunks and digit tiles stop here
+    const long long N = A.nmax_sets;
     const int np = A.npairs;
 
     // ---- load cursor (producer lane 0) ----
