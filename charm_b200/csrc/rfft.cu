@@ -29,6 +29,7 @@
 // output is sum_k X_k e^(+2 pi i k n / L) over the Hermitian spectrum, and
 // the analysis output is X_k = sum_n x_n e^(-2 pi i k n / L), k <= kmax.
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -285,20 +286,207 @@ __device__ __forceinline__ void fft_m(double2 *s,
                             p == last ? bh_last : nullptr);
 }
 
+// ---- the same transform with the whole plan known at compile time ----
+// (the lengths the grids of nmax about 2160..2190 use: M = 4608, 9216).
+// Radices, strides, thread counts and butterfly ranges become constants,
+// so the index arithmetic of every pass folds away.
+struct CtPlan
+{
+    int n8, n4, n2, n3;
+};
+
+// passes of radix 8, then 4, then 2, then 3, as the run-time plan
+constexpr CtPlan ct_plan(int M)
+{
+    int a = 0, b = 0, n = M;
+    while (n % 2 == 0)
+    {
+        n /= 2;
+        a++;
+    }
+    while (n % 3 == 0)
+    {
+        n /= 3;
+        b++;
+    }
+    int p8 = a / 3, p4 = 0, p2 = 0;
+    if (a % 3 == 2)
+        p4 = 1;
+    else if (a % 3 == 1)
+    {
+        if (p8 > 0)
+        {
+            p8--;
+            p4 = 2;
+        }
+        else
+            p2 = 1;
+    }
+    return CtPlan{p8, p4, p2, b};
+}
+
+constexpr int ct_npass(int M)
+{
+    return ct_plan(M).n8 + ct_plan(M).n4 + ct_plan(M).n2 + ct_plan(M).n3;
+}
+
+constexpr int ct_radix(int M, int p)
+{
+    const CtPlan q = ct_plan(M);
+    if (p < q.n8)
+        return 8;
+    p -= q.n8;
+    if (p < q.n4)
+        return 4;
+    p -= q.n4;
+    if (p < q.n2)
+        return 2;
+    return 3;
+}
+
+constexpr int ct_ns(int M, int p)
+{
+    int ns = 1;
+    for (int i = 0; i < p; i++)
+        ns *= ct_radix(M, i);
+    return ns;
+}
+
+// read-only load that stays after the barrier before it (a volatile asm is
+// not moved across the barrier's), so the twiddles of later passes are
+// not hoisted into registers ahead of time
+__device__ __forceinline__ double2 ld_tw(const double2 *p)
+{
+    double2 v;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(v.x), "=d"(v.y)
+                 : "l"(p));
+    return v;
+}
+
+template <int R, int V, int M, int NS, bool FIRST, bool BH, class Src>
+__device__ __forceinline__ void stockham_ct(double2 *s,
+                                            const double2 *__restrict__ tw,
+                                            int tid, const Src &src,
+                                            const double2 *__restrict__ bh)
+{
+    constexpr int T = M / V;
+    constexpr int BPT = (V + R - 1) / R;
+    constexpr int nb = M / R;
+    constexpr int step = M / (NS * R);
+    constexpr int ld_stride = nb + (nb >> 3);
+    constexpr int st_stride = (NS == 1) ? 1 : NS + (NS >> 3);
+    double2 v[BPT][R];
+#pragma unroll
+    for (int c = 0; c < BPT; c++)
+    {
+        const int j = tid + c * T;
+        if (j < nb)
+        {
+            if constexpr (FIRST)
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    v[c][r] = src(j + r * nb);
+            }
+            else
+            {
+                const int k = j % NS;
+                double2 wp[R];
+                wp[1] = ld_tw(&tw[k * step]);
+                twiddle_powers<R>(wp);
+                const int b = pidx(j);
+                v[c][0] = s[b];
+#pragma unroll
+                for (int r = 1; r < R; r++)
+                    v[c][r] = cmul(s[b + r * ld_stride], wp[r]);
+            }
+            dft<R>(v[c]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < BPT; c++)
+    {
+        const int j = tid + c * T;
+        if (j < nb)
+        {
+            const int k = j % NS;
+            const int d = (j / NS) * NS * R + k;
+            const int b = pidx(d);
+            if constexpr (BH)
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    s[b + r * st_stride] =
+                        conj2(cmul(v[c][r], ld_tw(&bh[d + r * NS])));
+            }
+            else
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    s[b + r * st_stride] = v[c][r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// passes P.. of FFT_M (compile-time plan); the last one multiplies by bh
+// when given
+template <int V, int M, int P, class Src>
+__device__ __forceinline__ void fft_ct(double2 *s,
+                                       const double2 *__restrict__ tw, int tid,
+                                       const Src &src,
+                                       const double2 *__restrict__ bh_last)
+{
+    if constexpr (P < ct_npass(M))
+    {
+        constexpr int R = ct_radix(M, P);
+        constexpr int NS = ct_ns(M, P);
+        if constexpr (P == ct_npass(M) - 1)
+        {
+            if (bh_last)
+                stockham_ct<R, V, M, NS, P == 0, true>(s, tw, tid, src,
+                                                       bh_last);
+            else
+                stockham_ct<R, V, M, NS, P == 0, false>(s, tw, tid, src,
+                                                        nullptr);
+        }
+        else
+            stockham_ct<R, V, M, NS, P == 0, false>(s, tw, tid, src, nullptr);
+        fft_ct<V, M, P + 1>(s, tw, tid, src, bh_last);
+    }
+}
+
 // Complex DFT of length H of the sequence z(0..H), zero-padded to M when
 // Bluestein is used; `pre` returns z_j already multiplied by the chirp
 // (Bluestein) and 0 for j >= H.  On return the DFT value k is dft_h_out(k).
-template <int V, class Pre>
+template <int V, int MC, class Pre>
 __device__ __forceinline__ void dft_h(double2 *s, const RfftArgs &A, int tid,
                                       int T, const Pre &pre)
 {
-    if (A.direct)
+    if constexpr (MC > 0)
     {
-        fft_m<V>(s, A.tw, A.M, A.npass, tid, T, pre, nullptr);
-        return;
+        // plan fixed at compile time (A.M == MC)
+        if (A.direct)
+        {
+            fft_ct<V, MC, 0>(s, A.tw, tid, pre, nullptr);
+            return;
+        }
+        fft_ct<V, MC, 0>(s, A.tw, tid, pre, A.bh);
+        fft_ct<V, MC, 0>(s, A.tw, tid, SrcSmem{s}, nullptr);
     }
-    fft_m<V>(s, A.tw, A.M, A.npass, tid, T, pre, A.bh);
-    fft_m<V>(s, A.tw, A.M, A.npass, tid, T, SrcSmem{s}, nullptr);
+    else
+    {
+        if (A.direct)
+        {
+            fft_m<V>(s, A.tw, A.M, A.npass, tid, T, pre, nullptr);
+            return;
+        }
+        fft_m<V>(s, A.tw, A.M, A.npass, tid, T, pre, A.bh);
+        fft_m<V>(s, A.tw, A.M, A.npass, tid, T, SrcSmem{s}, nullptr);
+    }
 }
 
 // value k (< H) of the length-H DFT after dft_h
@@ -388,7 +576,7 @@ struct SrcKernel
 // Analysis direction: real rows x[row][0..L) -> X[row][0..kmax]; one CTA
 // per row (a loop over rows would let the compiler hoist every pass's
 // twiddles out of it and run out of registers).
-template <int V, int NR, bool F32>
+template <int V, int NR, bool F32, int MC>
 __global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
 {
     extern __shared__ __align__(16) double2 s[];
@@ -400,13 +588,13 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
         const float *xf = reinterpret_cast<const float *>(A.x);
         SrcRowF src{reinterpret_cast<const float2 *>(xf + row * A.ldx),
                     A.direct ? nullptr : A.w, H};
-        dft_h<V>(s, A, tid, T, src);
+        dft_h<V, MC>(s, A, tid, T, src);
     }
     else
     {
         SrcRow src{reinterpret_cast<const double2 *>(A.x + row * A.ldx),
                    A.direct ? nullptr : A.w, H};
-        dft_h<V>(s, A, tid, T, src);
+        dft_h<V, MC>(s, A, tid, T, src);
     }
     double2 *X = A.X + row * A.ldX;
     for (int k = tid; k <= A.kmax; k += T)
@@ -422,7 +610,7 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
 }
 
 // Synthesis direction: X[row][0..kmax] (zero above) -> real rows x[row].
-template <int V, int NR, bool F32>
+template <int V, int NR, bool F32, int MC>
 __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
 {
     extern __shared__ __align__(16) double2 s[];
@@ -430,7 +618,7 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
     const long long row = blockIdx.x;
     SrcSpectrum src{A.X + row * A.ldX, A.direct ? nullptr : A.w, A.ht, A.H,
                     A.kmax};
-    dft_h<V>(s, A, tid, T, src);
+    dft_h<V, MC>(s, A, tid, T, src);
     if constexpr (F32)
     {
         float *xf = reinterpret_cast<float *>(A.x);
@@ -514,11 +702,20 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
 
 cudaError_t rfft_set_smem(size_t smem)
 {
-    const void *fns[] = {(const void *)k_rfft_fwd<16, 96, false>,
-                         (const void *)k_rfft_inv<16, 96, false>,
-                         (const void *)k_rfft_fwd<16, 96, true>,
-                         (const void *)k_rfft_inv<16, 96, true>,
-                         (const void *)k_rfft_kernel_spectrum<16, 96>};
+    const void *fns[] = {
+        (const void *)k_rfft_fwd<16, 96, false, 0>,
+        (const void *)k_rfft_inv<16, 96, false, 0>,
+        (const void *)k_rfft_fwd<16, 96, true, 0>,
+        (const void *)k_rfft_inv<16, 96, true, 0>,
+        (const void *)k_rfft_fwd<16, 96, false, 4608>,
+        (const void *)k_rfft_inv<16, 96, false, 4608>,
+        (const void *)k_rfft_fwd<16, 96, true, 4608>,
+        (const void *)k_rfft_inv<16, 96, true, 4608>,
+        (const void *)k_rfft_fwd<16, 96, false, 9216>,
+        (const void *)k_rfft_inv<16, 96, false, 9216>,
+        (const void *)k_rfft_fwd<16, 96, true, 9216>,
+        (const void *)k_rfft_inv<16, 96, true, 9216>,
+        (const void *)k_rfft_kernel_spectrum<16, 96>};
     for (const void *f : fns)
     {
         cudaError_t e = cudaFuncSetAttribute(
@@ -536,17 +733,28 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         return cudaSuccess;
     const size_t smem = rfft_smem_bytes(A.M);
     const int T = A.M / 16;
-    if (A.f32_rows)
-    {
-        if (inverse)
-            k_rfft_inv<16, 96, true><<<grid, T, smem, st>>>(A);
+    // the grids' common lengths with the plan fixed at compile time
+    auto go = [&](auto mc) {
+        constexpr int MC = decltype(mc)::value;
+        constexpr int NR = 96;
+        if (A.f32_rows)
+        {
+            if (inverse)
+                k_rfft_inv<16, NR, true, MC><<<grid, T, smem, st>>>(A);
+            else
+                k_rfft_fwd<16, NR, true, MC><<<grid, T, smem, st>>>(A);
+        }
+        else if (inverse)
+            k_rfft_inv<16, NR, false, MC><<<grid, T, smem, st>>>(A);
         else
-            k_rfft_fwd<16, 96, true><<<grid, T, smem, st>>>(A);
-    }
-    else if (inverse)
-        k_rfft_inv<16, 96, false><<<grid, T, smem, st>>>(A);
+            k_rfft_fwd<16, NR, false, MC><<<grid, T, smem, st>>>(A);
+    };
+    if (A.M == 4608)
+        go(std::integral_constant<int, 4608>{});
+    else if (A.M == 9216)
+        go(std::integral_constant<int, 9216>{});
     else
-        k_rfft_fwd<16, 96, false><<<grid, T, smem, st>>>(A);
+        go(std::integral_constant<int, 0>{});
     return cudaGetLastError();
 }
 
