@@ -74,25 +74,41 @@ class Clocks:
          "clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
+    # A timed region of a few milliseconds is shorter than the sampling
+    # interval: the caller runs the same work untimed for SETTLE_S just
+    # before it and keeps the samples of [settle start, region end], a
+    # window in which the GPU does nothing else.
+    SETTLE_S = 0.3
+
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []             # (host time, fields)
         self.proc = None
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi is running once its first line has arrived
+        t = time.perf_counter()
+        while not self.rows and time.perf_counter() - t < 5.0:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.perf_counter(),
+                              [x.strip() for x in line.split(",")]))
+
+    def mark(self, t0, t1):
+        self.t0, self.t1 = t0, t1
 
     def stop(self):
         if self.proc is None:
@@ -103,12 +119,14 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.th.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        rows = [r for t, r in self.rows
+                if self.t0 is None or self.t0 <= t <= self.t1]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in rows:
             if len(r) < 9:
                 continue
             for nm, v in zip(names, r[5:9]):
@@ -116,7 +134,10 @@ class Clocks:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(rows),
+                "window_s": ((self.t1 - self.t0)
+                             if self.t0 is not None else None),
+                "interval_ms": 50}
 
 
 # ---------------------------------------------------------------------------
@@ -199,6 +220,11 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
+    # the same round trip, untimed, so that the clock samples see this load
+    t_region0 = time.perf_counter()
+    while time.perf_counter() - t_region0 < Clocks.SETTLE_S:
+        step_dev()
+        torch.cuda.synchronize()
     L.charm_b200_timing(1)
     per_step = []
     for _ in range(args.steps):
@@ -219,6 +245,7 @@ def run_ours(args):
     fe = ct.c_ulonglong()
     L.charm_b200_timing_read(ms, cnt, 7, ct.byref(kl), ct.byref(fe))
     L.charm_b200_timing(0)
+    clocks.mark(t_region0, time.perf_counter())
     clk = clocks.stop()
     total_ms = max_over_ranks(float(sum(per_step)), dev)
     if dist is not None:
