@@ -11,6 +11,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
@@ -56,6 +57,10 @@ struct Context
     int device = -1;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
+    // host <-> device copies of grid bands, overlapped with the kernels on
+    // `stream` (events order the two)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t band_ev[8] = {};
     std::map<std::string, DevBuf> bufs;
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
@@ -189,6 +194,12 @@ Status init(Context &c)
     c.num_sms = prop.multiProcessorCount;
     if (!c.stream)
         CB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), st);
+    if (!c.copy_stream)
+        CB_CUDA(cudaStreamCreateWithFlags(&c.copy_stream,
+                                          cudaStreamNonBlocking), st);
+    for (cudaEvent_t &e : c.band_ev)
+        if (!e)
+            CB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), st);
     c.ready = true;
     return st;
 }
@@ -785,6 +796,72 @@ Status coef_to_device(Context &c, const CoefIn &in, unsigned long nmax,
 // ---------------------------------------------------------------------------
 // Grid synthesis
 // ---------------------------------------------------------------------------
+// Rows of the latitude pairs [p0, p1) as two contiguous ranges: north rows
+// [r[0], r[1]) and mirror rows [r[2], r[3]) (empty when there are none).
+// False when they do not form two disjoint contiguous ranges.
+bool band_rows(const Pairs &P, int p0, int p1, int nlat, int r[4])
+{
+    int nmin = nlat, nmx = -1, nn = 0, smin = nlat, smx = -1, ns = 0;
+    for (int p = p0; p < p1; p++)
+    {
+        const int a = P.row_n[p], b = P.row_s[p];
+        if (a >= 0 && a < nlat)
+        {
+            nmin = std::min(nmin, a);
+            nmx = std::max(nmx, a);
+            nn++;
+        }
+        if (b >= 0 && b < nlat)
+        {
+            smin = std::min(smin, b);
+            smx = std::max(smx, b);
+            ns++;
+        }
+    }
+    if (nn == 0 || nmx - nmin + 1 != nn)
+        return false;
+    r[0] = nmin;
+    r[1] = nmx + 1;
+    r[2] = r[3] = 0;
+    if (ns > 0)
+    {
+        if (smx - smin + 1 != ns || !(smx < nmin || smin > nmx))
+            return false;
+        r[2] = smin;
+        r[3] = smx + 1;
+    }
+    return true;
+}
+
+// Bands of consecutive tiles (or tile groups) for the overlap of the grid's
+// host copies with the kernels: nb bands of units [u0, u1) of `units`, each
+// unit covering `per` latitude pairs; their row ranges in `rows`.  Returns
+// the number of bands, 1 when the rows do not split into contiguous
+// ranges.
+int grid_bands(const Pairs &P, int nlat, int units, int per, int nb,
+               std::vector<std::array<int, 6>> &bands)
+{
+    const int np = (int)P.row_n.size();
+    bands.clear();
+    nb = std::max(1, std::min(nb, units));
+    if (nb < 2)
+        return 1;
+    for (int b = 0; b < nb; b++)
+    {
+        const int u0 = (int)((long long)b * units / nb);
+        const int u1 = (int)((long long)(b + 1) * units / nb);
+        const int p0 = std::min(np, u0 * per), p1 = std::min(np, u1 * per);
+        int r[4];
+        if (p1 <= p0 || !band_rows(P, p0, p1, nlat, r))
+        {
+            bands.clear();
+            return 1;
+        }
+        bands.push_back({u0, u1, r[0], r[1], r[2], r[3]});
+    }
+    return nb;
+}
+
 Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
                 unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
                 double **f, double *d_f)
@@ -926,6 +1003,70 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     A.polar_thr = polar_threshold(nmax);
     A.counter = d_counter;
     A.status = d_status;
+    // Host output through the row transform: bands of latitude tiles, each
+    // band's rows copied to the host (copy stream) while the next band is
+    // synthesised; the sums of every item are the same as in one launch.
+    std::vector<std::array<int, 6>> bands;
+    const int nband =
+        (!d_f && rf) ? grid_bands(P, (int)nlat, ntiles, 32 * K,
+                                  ntiles >= 6 ? 3 : 2, bands)
+                     : 1;
+    if (nband > 1)
+    {
+        unsigned long long *bcnt = nullptr;
+        CB_TRY(dbuf(c, "band_counters", 8, &bcnt));
+        CB_CUDA(cudaMemsetAsync(bcnt, 0, 8 * sizeof(unsigned long long),
+                                c.stream), st);
+        for (int b = 0; b < nband; b++)
+        {
+            const auto &bd = bands[b];
+            ShsGridArgs Ab = A;
+            Ab.tile0 = bd[0];
+            Ab.ntiles = bd[1] - bd[0];
+            Ab.nitems = (long long)(nmax + 1) * Ab.ntiles;
+            Ab.counter = bcnt + b;
+            const int gb = (int)std::min<long long>((Ab.nitems + 3) / 4,
+                                                    (long long)c.num_sms * 8);
+            {
+                Scope sc(c, TIMER_SHS);
+                CB_CUDA(launch_shs_grid(Ab, kgrad, dr, dlat, !r_eq, K,
+                                        std::max(gb, 1), c.stream), st);
+            }
+            for (int q = 0; q < npar; q++)
+                for (int h = 0; h < 2; h++)
+                {
+                    const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
+                    if (r1 <= r0)
+                        continue;
+                    RfftArgs R = *rf;
+                    R.nrows = r1 - r0;
+                    R.x = fg + ((size_t)q * nlat + r0) * nlon;
+                    R.ldx = (long long)nlon;
+                    R.X = lc + ((size_t)q * nlat + r0) * ldf;
+                    R.ldX = ldf;
+                    R.kmax = (int)nmax;
+                    Scope sc(c, TIMER_FFT);
+                    CB_CUDA(launch_rfft(R, true, c.stream), st);
+                }
+            CB_CUDA(cudaEventRecord(c.band_ev[b], c.stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[b], 0), st);
+            for (int q = 0; q < npar; q++)
+                for (int h = 0; h < 2; h++)
+                {
+                    const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
+                    if (r1 > r0)
+                        CB_CUDA(cudaMemcpyAsync(
+                                    f[q] + (size_t)r0 * nlon,
+                                    fg + ((size_t)q * nlat + r0) * nlon,
+                                    (size_t)(r1 - r0) * nlon * 8,
+                                    cudaMemcpyDeviceToHost, c.copy_stream),
+                                st);
+                }
+        }
+        CB_CUDA(cudaStreamSynchronize(c.copy_stream), st);
+        return finish(c, d_status);
+    }
+
     int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                         (long long)c.num_sms * 8);
     {
@@ -2016,49 +2157,8 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     Tabs tab;
     CB_TRY(tables(c, (long long)nmax, &tab));
 
-    // grid on the device and r2c along the parallels
-    const double *fg = d_fin;
-    if (!fg)
-    {
-        double *tmp = nullptr;
-        CB_TRY(dbuf(c, "fgrid", nlat * nlon, &tmp));
-        CB_CUDA(cudaMemcpyAsync(tmp, f_host, nlat * nlon * 8,
-                                cudaMemcpyHostToDevice, c.stream), st);
-        fg = tmp;
-    }
-    const int ldF = (int)(nlon / 2 + 1);
-    double2 *F = nullptr;
-    CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
-    const RfftArgs *rf = nullptr;
-    if (reinterpret_cast<uintptr_t>(fg) % 16 == 0)
-        CB_TRY(row_fft(c, (long long)nlon, &rf));
-    if (rf)
-    {
-        RfftArgs R = *rf;
-        R.nrows = (long long)nlat;
-        R.x = const_cast<double *>(fg);
-        R.ldx = (long long)nlon;
-        R.X = F;
-        R.ldX = ldF;
-        R.kmax = (int)nmax;
-        Scope sc(c, TIMER_FFT);
-        CB_CUDA(launch_rfft(R, false, c.stream), st);
-    }
-    else
-    {
-        cufftHandle h;
-        CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
-        Scope sc(c, TIMER_FFT, false);
-        if (cufftExecD2Z(h, const_cast<double *>(fg),
-                         reinterpret_cast<cufftDoubleComplex *>(F)) !=
-            CUFFT_SUCCESS)
-        {
-            st.code = CHARM_EFUNCARG;
-            st.msg = "cuFFT D2Z failed";
-            return st;
-        }
-    }
-
+    // work decomposition: K latitude pairs per lane, tiles of 32 K pairs,
+    // groups of tiles whose partial sums are added in fixed order
     unsigned *d_status;
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
@@ -2072,6 +2172,35 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     G = (ntiles + tpg - 1) / tpg;
     double2 *part = nullptr;
     CB_TRY(dbuf(c, "sha_part", (size_t)G * T, &part));
+
+    // grid on the device and r2c along the parallels
+    const double *fg = d_fin;
+    double *fdev = nullptr;
+    if (!fg)
+    {
+        CB_TRY(dbuf(c, "fgrid", nlat * nlon, &fdev));
+        fg = fdev;
+    }
+    const int ldF = (int)(nlon / 2 + 1);
+    double2 *F = nullptr;
+    CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
+    const RfftArgs *rf = nullptr;
+    if (reinterpret_cast<uintptr_t>(fg) % 16 == 0)
+        CB_TRY(row_fft(c, (long long)nlon, &rf));
+    auto rows_fft = [&](int r0, int r1) -> Status {
+        Status s2;
+        RfftArgs R = *rf;
+        R.nrows = (long long)(r1 - r0);
+        R.x = const_cast<double *>(fg) + (size_t)r0 * nlon;
+        R.ldx = (long long)nlon;
+        R.X = F + (size_t)r0 * ldF;
+        R.ldX = ldF;
+        R.kmax = (int)nmax;
+        Scope sc(c, TIMER_FFT);
+        CB_CUDA(launch_rfft(R, false, c.stream), s2);
+        return s2;
+    };
+
     ShaGridArgs A{};
     A.nmax = (long long)nmax;
     A.npairs = np;
@@ -2095,9 +2224,82 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     A.polar_thr = polar_threshold(nmax);
     A.counter = d_counter;
     A.status = d_status;
-    int grid = (int)std::min<long long>((A.nitems + 3) / 4,
-                                        (long long)c.num_sms * 8);
+
+    // Host input through the row transform: bands of tile groups; band b's
+    // rows are copied (copy stream) while band b - 1 is transformed and
+    // analysed.  The partial sums of every group are the same as in one
+    // launch.
+    std::vector<std::array<int, 6>> bands;
+    const int nband = (fdev && rf) ? grid_bands(P, (int)nlat, (int)G,
+                                                32 * K * tpg,
+                                                G >= 3 ? 3 : 2, bands)
+                                   : 1;
+    if (nband > 1)
     {
+        unsigned long long *bcnt = nullptr;
+        CB_TRY(dbuf(c, "band_counters", 8, &bcnt));
+        CB_CUDA(cudaMemsetAsync(bcnt, 0, 8 * sizeof(unsigned long long),
+                                c.stream), st);
+        // the copy stream starts after everything before it on the stream
+        // (buffers in use by an earlier call)
+        CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
+        CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+        for (int b = 0; b < nband; b++)
+        {
+            const auto &bd = bands[b];
+            for (int h = 0; h < 2; h++)
+            {
+                const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
+                if (r1 > r0)
+                    CB_CUDA(cudaMemcpyAsync(fdev + (size_t)r0 * nlon,
+                                            f_host + (size_t)r0 * nlon,
+                                            (size_t)(r1 - r0) * nlon * 8,
+                                            cudaMemcpyHostToDevice,
+                                            c.copy_stream),
+                            st);
+            }
+            CB_CUDA(cudaEventRecord(c.band_ev[b], c.copy_stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[b], 0), st);
+            for (int h = 0; h < 2; h++)
+            {
+                const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
+                if (r1 > r0)
+                    CB_TRY(rows_fft(r0, r1));
+            }
+            ShaGridArgs Ab = A;
+            Ab.group0 = bd[0];
+            Ab.ngroups = bd[1] - bd[0];
+            Ab.nitems = (long long)(nmax + 1) * Ab.ngroups;
+            Ab.counter = bcnt + b;
+            const int gb = (int)std::min<long long>((Ab.nitems + 3) / 4,
+                                                    (long long)c.num_sms * 8);
+            Scope sc(c, TIMER_SHA);
+            CB_CUDA(launch_sha_grid(Ab, K, std::max(gb, 1), c.stream), st);
+        }
+    }
+    else
+    {
+        if (fdev)
+            CB_CUDA(cudaMemcpyAsync(fdev, f_host, nlat * nlon * 8,
+                                    cudaMemcpyHostToDevice, c.stream), st);
+        if (rf)
+            CB_TRY(rows_fft(0, (int)nlat));
+        else
+        {
+            cufftHandle h;
+            CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
+            Scope sc(c, TIMER_FFT, false);
+            if (cufftExecD2Z(h, const_cast<double *>(fg),
+                             reinterpret_cast<cufftDoubleComplex *>(F)) !=
+                CUFFT_SUCCESS)
+            {
+                st.code = CHARM_EFUNCARG;
+                st.msg = "cuFFT D2Z failed";
+                return st;
+            }
+        }
+        int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                            (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
         CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
     }

@@ -37,7 +37,8 @@ struct ShsGridArgs
 {
     long long nmax;
     int npairs;            // evaluated latitudes (north rows of the pairs)
-    int ntiles;            // latitude tiles per order
+    int ntiles;            // latitude tiles per order in this launch
+    int tile0;             // first tile of this launch
     long long nitems;      // (nmax + 1) * ntiles
     const double2 *tb;     // (beta_n, e_n / a_n) per (n, m), order-major
     const double *tmul;    // chunk entry multipliers [m][chunk]
@@ -71,7 +72,8 @@ struct ShaGridArgs
     long long nmax;
     int npairs;
     int ntiles;            // latitude tiles per order
-    int ngroups;           // tile groups per order (partial sums)
+    int ngroups;           // tile groups per order in this launch
+    int group0;            // first group of this launch (partial sums)
     int tiles_per_group;
     long long nitems;      // (nmax + 1) * ngroups
     const double2 *tb;

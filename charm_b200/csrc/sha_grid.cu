@@ -133,7 +133,8 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
         if (item >= (unsigned long long)A.nitems)
             break;
         const long long m = (long long)(item / (unsigned long long)A.ngroups);
-        const int g = (int)(item % (unsigned long long)A.ngroups);
+        const int g =
+            A.group0 + (int)(item % (unsigned long long)A.ngroups);
         const long long c0 = tri_col0(N, m);
         const long long ncol = N - m + 1;
         const int nchunks = (int)((ncol + LEG_CHUNK - 1) / LEG_CHUNK);

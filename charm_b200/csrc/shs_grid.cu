@@ -93,7 +93,8 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
             local = item - (unsigned long long)bs.item0;
         }
         const long long m = (long long)(local / (unsigned long long)A.ntiles);
-        const int tile = (int)(local % (unsigned long long)A.ntiles);
+        const int tile =
+            A.tile0 + (int)(local % (unsigned long long)A.ntiles);
         const double sigma = A.sg[2 * m];
 
         // ---- geometry and seeds of this lane's latitude pairs ----------

@@ -1,0 +1,77 @@
+"""Host-array entry points with the grid copied in bands: charm_shs_point
+copies the rows of each band of latitude tiles to the host while the next
+band is synthesised, charm_sha_point copies band b while band b - 1 is
+transformed and analysed.  Every work item computes the same sums as in one
+launch, so the results equal those of the device-array entry points bit for
+bit."""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from charm_b200.workloads import GM, R_EARTH, kaula
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    import charm_b200 as cb
+    from charm_b200._lib import _libcharm as L
+    P = ct.c_void_p
+    L.charm_b200_shs_point_dev.argtypes = [
+        P, ct.c_ulong, ct.c_double, ct.c_double, P, P, ct.c_ulong, ct.c_int,
+        ct.c_uint, ct.c_uint, ct.c_uint, P, P]
+    L.charm_b200_sha_point_dev.argtypes = [
+        P, P, ct.c_ulong, ct.c_double, ct.c_double, ct.c_ulong, P, P, P]
+    return torch, cb, L
+
+
+def device_shs(env, p, c, s, N):
+    torch, cb, L = env
+    dc = torch.from_numpy(c).cuda()
+    ds = torch.from_numpy(s).cuda()
+    f = torch.empty(p.lat.size * p.lon.size, dtype=torch.float64,
+                    device="cuda")
+    err = L.charm_err_init()
+    L.charm_b200_shs_point_dev(ct.cast(p._Point, ct.c_void_p), N, GM,
+                               R_EARTH, dc.data_ptr(), ds.data_ptr(), N, 0, 0,
+                               0, 0, f.data_ptr(), ct.cast(err, ct.c_void_p))
+    assert L.charm_err_isempty(err)
+    L.charm_err_free(err)
+    return f.cpu().numpy().reshape(p.lat.size, p.lon.size)
+
+
+def device_sha(env, p, f, N):
+    torch, cb, L = env
+    df = torch.from_numpy(np.ascontiguousarray(f).ravel()).cuda()
+    T = (N + 1) * (N + 2) // 2
+    oc = torch.empty(T, dtype=torch.float64, device="cuda")
+    os_ = torch.empty(T, dtype=torch.float64, device="cuda")
+    err = L.charm_err_init()
+    L.charm_b200_sha_point_dev(ct.cast(p._Point, ct.c_void_p), df.data_ptr(),
+                               N, GM, R_EARTH, N, oc.data_ptr(),
+                               os_.data_ptr(), ct.cast(err, ct.c_void_p))
+    assert L.charm_err_isempty(err)
+    L.charm_err_free(err)
+    return oc.cpu().numpy(), os_.cpu().numpy()
+
+
+@pytest.mark.parametrize("grid,N,h", [("GL", 2190, 0.0), ("GL", 601, 0.0),
+                                      ("DH1", 800, 0.0), ("DH2", 700, 3e4)])
+def test_host_paths_equal_device_paths(env, grid, N, h):
+    torch, cb, L = env
+    ctor = {"GL": cb.PointGridGL, "DH1": cb.PointGridDH1,
+            "DH2": cb.PointGridDH2}[grid]
+    p = ctor(N, R_EARTH + h)
+    c, s = kaula(N, 880 + N)
+    shc = cb.Shc(N, GM, R_EARTH, c, s)
+    f_host = cb.shs_point(p, shc, N)
+    f_dev = device_shs(env, p, c, s, N)
+    assert np.array_equal(f_host, f_dev)
+    if h == 0.0:
+        out = cb.sha_point(p, f_host, N, GM, R_EARTH)
+        oc, os_ = device_sha(env, p, f_host, N)
+        assert np.array_equal(out.c, oc)
+        assert np.array_equal(out.s, os_)
