@@ -384,6 +384,12 @@ def run_ours(args):
     line["f32"] = f32
     if bi8 is not None:
         line["batch_i8"] = bi8
+    # the synthesis autotuner's choices (tile of latitude pairs per lane)
+    L.charm_b200_autotune_report.restype = ct.c_size_t
+    L.charm_b200_autotune_report.argtypes = [ct.c_char_p, ct.c_size_t]
+    rbuf = ct.create_string_buffer(8192)
+    L.charm_b200_autotune_report(rbuf, 8192)
+    line["autotune"] = rbuf.value.decode().splitlines()
     if hi is not None:
         line["nmax10800"] = hi
     if not args.no_cpu_baseline:

@@ -4,6 +4,7 @@
 // 0.4.9 (files cited per function) so that callers see the same behaviour;
 // the numerical work is delegated to the GPU engine (engine.cpp).
 #include <cfloat>
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -705,6 +706,22 @@ void charm_b200_shs_point_batch_dev(const charm_point *pnt, size_t nsets,
     report(err, __func__,
            cb::shs_point_batch_dev(pnt, nsets, nmax, shc_nmax, mu, r, d_c,
                                    d_s, kgrad, d_f));
+}
+
+// The synthesis autotuner's choices: copies up to n - 1 characters of the
+// report (one line per problem shape: kernel, shape, chosen K and the
+// measured milliseconds of every candidate) into buf; returns the full
+// length.
+size_t charm_b200_autotune_report(char *buf, size_t n)
+{
+    const std::string r = cb::autotune_report();
+    if (buf && n > 0)
+    {
+        const size_t k = std::min(n - 1, r.size());
+        std::memcpy(buf, r.data(), k);
+        buf[k] = '\0';
+    }
+    return r.size();
 }
 
 // Split-precision batched synthesis: the same call with the degree sums on

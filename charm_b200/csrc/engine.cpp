@@ -67,6 +67,12 @@ struct Context
     long long tab_nmax = -1;     // recurrence tables of this maximum degree
     long long tab32_nmax = -1;   // single-precision tables of this degree
     long long tcp_nmax = -1;     // padded ct_n rows of the tensor-core path
+    // autotuned latitude pairs per lane of the synthesis kernel, per
+    // (kgrad, dr, dlat, r != R, nmax, pairs); value and the measured ms of
+    // each candidate
+    std::map<std::tuple<int, int, int, int, long long, int>,
+             std::pair<int, std::vector<std::pair<int, float>>>>
+        tuned;
     std::map<std::tuple<int, int, long long>, cufftHandle> plans;
     std::map<long long, RfftArgs> rffts;   // row transforms by row length
     std::map<long long, void *> rfft_mem;  // their tables
@@ -691,6 +697,81 @@ int choose_k_sha(long long npairs)
     return 4;
 }
 
+// Autotuner of the synthesis kernel's latitude pairs per lane (the tile is
+// 32 K pairs): on the first call of a problem shape every candidate runs
+// once on the call's own data, timed with CUDA events on the library
+// stream, and the fastest is kept for the process.  The sums of a latitude
+// pair do not depend on K, so the choice changes no result.  Shapes with
+// nmax < 256 and CHARM_B200_AUTOTUNE=0 keep the built-in choice.
+bool autotune_on()
+{
+    static const bool on = [] {
+        const char *e = std::getenv("CHARM_B200_AUTOTUNE");
+        return !(e && std::strcmp(e, "0") == 0);
+    }();
+    return on;
+}
+
+Status tune_shs_k(Context &c, const ShsGridArgs &A0, int kgrad, int dr,
+                  int dlat, bool rr, int np, int *K)
+{
+    Status st;
+    const auto key = std::make_tuple(kgrad, dr, dlat, rr ? 1 : 0, A0.nmax, np);
+    auto it = c.tuned.find(key);
+    if (it != c.tuned.end())
+    {
+        *K = it->second.first;
+        return st;
+    }
+    if (!autotune_on() || A0.nmax < 256 || A0.nsets > 0)
+        return st;
+    std::vector<int> cands = kgrad >= 1 || dlat > 0 ? std::vector<int>{1, 2}
+                                                    : std::vector<int>{1, 2, 4};
+    cudaEvent_t e0 = ev_get(c), e1 = ev_get(c);
+    std::vector<std::pair<int, float>> meas;
+    int best = *K;
+    float best_ms = 0.0f;
+    // one untimed launch first (first-use costs of the module, caches)
+    cands.insert(cands.begin(), *K);
+    bool warm = true;
+    for (int k : cands)
+    {
+        ShsGridArgs A = A0;
+        A.ntiles = (np + 32 * k - 1) / (32 * k);
+        A.nitems = (long long)(A.nmax + 1) * A.ntiles;
+        const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                                  (long long)c.num_sms * 8);
+        CB_CUDA(cudaMemsetAsync(A.counter, 0, sizeof(unsigned long long),
+                                c.stream), st);
+        CB_CUDA(cudaEventRecord(e0, c.stream), st);
+        CB_CUDA(launch_shs_grid(A, kgrad, dr, dlat, rr, k, std::max(grid, 1),
+                                c.stream), st);
+        CB_CUDA(cudaEventRecord(e1, c.stream), st);
+        CB_CUDA(cudaEventSynchronize(e1), st);
+        float ms = 0.0f;
+        CB_CUDA(cudaEventElapsedTime(&ms, e0, e1), st);
+        c.launches++;
+        if (warm)
+        {
+            warm = false;
+            continue;
+        }
+        meas.emplace_back(k, ms);
+        if (best_ms == 0.0f || ms < best_ms)
+        {
+            best_ms = ms;
+            best = k;
+        }
+    }
+    c.ev_pool.push_back(e0);
+    c.ev_pool.push_back(e1);
+    CB_CUDA(cudaMemsetAsync(A0.counter, 0, sizeof(unsigned long long),
+                            c.stream), st);
+    c.tuned[key] = std::make_pair(best, meas);
+    *K = best;
+    return st;
+}
+
 Status finish(Context &c, unsigned *d_status)
 {
     Status st;
@@ -977,8 +1058,8 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
 
-    const int K = choose_k(kgrad, dlat, np);
-    const int ntiles = (np + 32 * K - 1) / (32 * K);
+    int K = choose_k(kgrad, dlat, np);
+    int ntiles = (np + 32 * K - 1) / (32 * K);
     ShsGridArgs A{};
     A.nmax = (long long)nmax;
     A.npairs = np;
@@ -1003,6 +1084,19 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     A.polar_thr = polar_threshold(nmax);
     A.counter = d_counter;
     A.status = d_status;
+    // autotuned tile (first call of this shape)
+    {
+        int Kt = K;
+        CB_TRY(tune_shs_k(c, A, kgrad, dr, dlat, !r_eq, np, &Kt));
+        if (Kt != K)
+        {
+            K = Kt;
+            ntiles = (np + 32 * K - 1) / (32 * K);
+            A.ntiles = ntiles;
+            A.nitems = (long long)(nmax + 1) * ntiles;
+        }
+    }
+
     // Host output through the row transform: bands of latitude tiles, each
     // band's rows copied to the host (copy stream) while the next band is
     // synthesised; the sums of every item are the same as in one launch.
@@ -2734,6 +2828,32 @@ Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
     CB_TRY(init(g_ctx));
     return shs_batch(g_ctx, pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
                      kgrad, d_f);
+}
+
+// The autotuner's choices so far, one line per problem shape.
+std::string autotune_report()
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    std::string out;
+    for (const auto &kv : g_ctx.tuned)
+    {
+        const auto &k = kv.first;
+        out += "k_shs_grid kgrad=" + std::to_string(std::get<0>(k)) +
+               " dr=" + std::to_string(std::get<1>(k)) +
+               " dlat=" + std::to_string(std::get<2>(k)) +
+               " rr=" + std::to_string(std::get<3>(k)) +
+               " nmax=" + std::to_string(std::get<4>(k)) +
+               " pairs=" + std::to_string(std::get<5>(k)) +
+               " K=" + std::to_string(kv.second.first) + " ms:";
+        for (const auto &m : kv.second.second)
+        {
+            char b[64];
+            snprintf(b, sizeof b, " %d:%.4f", m.first, (double)m.second);
+            out += b;
+        }
+        out += "\n";
+    }
+    return out;
 }
 
 Status shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,

@@ -68,6 +68,9 @@ Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
                            double r, const double *const *d_c,
                            const double *const *d_s, int kgrad,
                            double *const *d_f);
+// The autotuner's choices so far (one line per problem shape).
+std::string autotune_report();
+
 // The potential of the batch with the degree sums on the tensor cores
 // (INT8 digit products, FP64 recombination).
 Status shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,

@@ -245,6 +245,17 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_dev(
     const double *const *d_c, const double *const *d_s, int kgrad,
     double *const *d_f, charm_err *err);
 
+/* The synthesis kernel's autotuner (no counterpart in CHarm): on the first
+ * call of a problem shape (derivative kind, nmax >= 256, latitude pairs, on
+ * or off the reference sphere) the latitude pairs per lane of the grid
+ * synthesis are chosen by timing every candidate once; the results do not
+ * depend on the choice.  CHARM_B200_AUTOTUNE=0 keeps the built-in choice.
+ * Copies up to n - 1 characters of a report of the choices so far (one line
+ * per shape: chosen K, measured ms of each candidate) into buf and returns
+ * the report's full length. */
+CHARM_EXTERN size_t CHARM_CDECL charm_b200_autotune_report(char *buf,
+                                                            size_t n);
+
 /* charm_b200_shs_point_batch_dev with the degree sums of every (order,
  * 128-latitude tile) on the tensor cores for up to 16 sets at once (no
  * counterpart in CHarm): the Legendre values and the coefficients become
