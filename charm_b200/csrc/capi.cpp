@@ -708,6 +708,69 @@ void charm_b200_shs_point_batch_dev(const charm_point *pnt, size_t nsets,
                                    d_s, kgrad, d_f));
 }
 
+// A batched synthesis captured into a CUDA graph (no CHarm counterpart):
+// the checks of the batched entry points, then one plain call and the
+// captured one.
+void *charm_b200_shs_point_batch_graph(const charm_point *pnt, size_t nsets,
+                                       const unsigned long *nmax,
+                                       const unsigned long *shc_nmax,
+                                       const double *mu, double r,
+                                       const double *const *d_c,
+                                       const double *const *d_s, int kgrad,
+                                       double *const *d_f,
+                                       int split_precision, charm_err *err)
+{
+    if (kgrad < 0 || kgrad > 3 || (split_precision && kgrad != 0))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"kgrad\" must be 0..3 (0 with split precision).");
+        return nullptr;
+    }
+    if (!(pnt->type == CHARM_CRD_POINT_GRID ||
+          is_quad_type(pnt->type)))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The batched synthesis works on grids (\"pnt->type\").");
+        return nullptr;
+    }
+    for (size_t j = 0; j < nsets; j++)
+        if (nmax[j] > shc_nmax[j])
+        {
+            char msg[CHARM_ERR_MAX_MSG];
+            snprintf(msg, sizeof msg,
+                     "Set %zu: \"nmax = %lu\" cannot be larger than the "
+                     "degree of its coefficients \"%lu\".",
+                     j, nmax[j], shc_nmax[j]);
+            SET_ERR(err, CHARM_EFUNCARG, msg);
+            return nullptr;
+        }
+    if (nsets == 0 || pnt->npoint == 0)
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "Nothing to capture (no sets or points).");
+        return nullptr;
+    }
+    void *g = nullptr;
+    report(err, __func__,
+           cb::batch_graph_create(pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
+                                  kgrad, d_f, split_precision, &g));
+    return g;
+}
+
+void charm_b200_graph_launch(void *graph, charm_err *err)
+{
+    if (!graph)
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "\"graph\" is NULL.");
+        return;
+    }
+    report(err, __func__, cb::batch_graph_launch(graph));
+}
+
+void charm_b200_graph_free(void *graph)
+{
+    cb::batch_graph_free(graph);
+}
+
 // The synthesis autotuner's choices: copies up to n - 1 characters of the
 // report (one line per problem shape: kernel, shape, chosen K and the
 // measured milliseconds of every candidate) into buf; returns the full

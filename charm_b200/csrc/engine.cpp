@@ -67,6 +67,11 @@ struct Context
     long long tab_nmax = -1;     // recurrence tables of this maximum degree
     long long tab32_nmax = -1;   // single-precision tables of this degree
     long long tcp_nmax = -1;     // padded ct_n rows of the tensor-core path
+    // stream capture into a CUDA graph (batch_graph_create): host
+    // synchronisations are skipped, small host uploads go through pinned
+    // buffers owned by the graph
+    bool capturing = false;
+    std::vector<void *> capture_pins;
     // autotuned latitude pairs per lane of the synthesis kernel, per
     // (kgrad, dr, dlat, r != R, nmax, pairs); value and the measured ms of
     // each candidate
@@ -214,6 +219,12 @@ Status buf(Context &c, const std::string &name, size_t bytes, void **out)
 {
     Status st;
     DevBuf &b = c.bufs[name];
+    if (b.bytes < bytes && c.capturing)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "device buffer \"" + name + "\" grew during graph capture";
+        return st;
+    }
     if (b.bytes < bytes)
     {
         if (b.p)
@@ -252,6 +263,15 @@ Status dbuf(Context &c, const std::string &name, size_t count, T **out)
 Status pinned(Context &c, size_t bytes, void **out)
 {
     Status st;
+    if (c.capturing)
+    {
+        // a buffer of its own, read by the graph at every replay
+        void *p = nullptr;
+        CB_CUDA(cudaMallocHost(&p, std::max<size_t>(bytes, 16)), st);
+        c.capture_pins.push_back(p);
+        *out = p;
+        return st;
+    }
     if (c.pinned_bytes < bytes)
     {
         if (c.pinned)
@@ -266,6 +286,25 @@ Status pinned(Context &c, size_t bytes, void **out)
         c.pinned_bytes = want;
     }
     *out = c.pinned;
+    return st;
+}
+
+// Upload of a small host array; while capturing through a graph-owned
+// pinned copy (the graph reads it at every replay).
+Status h2d_small(Context &c, void *dst, const void *src, size_t bytes)
+{
+    Status st;
+    if (!c.capturing)
+    {
+        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice,
+                                c.stream), st);
+        return st;
+    }
+    void *hp = nullptr;
+    CB_TRY(pinned(c, bytes, &hp));
+    std::memcpy(hp, src, bytes);
+    CB_CUDA(cudaMemcpyAsync(dst, hp, bytes, cudaMemcpyHostToDevice, c.stream),
+            st);
     return st;
 }
 
@@ -775,6 +814,8 @@ Status tune_shs_k(Context &c, const ShsGridArgs &A0, int kgrad, int dr,
 Status finish(Context &c, unsigned *d_status)
 {
     Status st;
+    if (c.capturing)
+        return st;   // read by batch_graph_launch after each replay
     unsigned h_status = 0;
     CB_CUDA(cudaMemcpyAsync(&h_status, d_status, sizeof(unsigned),
                             cudaMemcpyDeviceToHost, c.stream), st);
@@ -1485,9 +1526,7 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                 hsets[b].polar_thr = polar_threshold(nmax_v[j]);
                 items += (long long)(nmax_v[j] + 1) * ntiles;
             }
-            CB_CUDA(cudaMemcpyAsync(dsets, hsets.data(),
-                                    nb * sizeof(BatchSet),
-                                    cudaMemcpyHostToDevice, c.stream), st);
+            CB_TRY(h2d_small(c, dsets, hsets.data(), nb * sizeof(BatchSet)));
             if (!rf)
                 CB_CUDA(cudaMemsetAsync(lc, 0, nb * per_set, c.stream), st);
             CB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long),
@@ -1572,8 +1611,10 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                     }
                 }
             // the set descriptors and the lumped buffer are reused by the
-            // next sub-batch: wait for this one
-            CB_CUDA(cudaStreamSynchronize(c.stream), st);
+            // next sub-batch: wait for this one (stream order suffices
+            // inside a captured graph, whose uploads have their own copies)
+            if (!c.capturing)
+                CB_CUDA(cudaStreamSynchronize(c.stream), st);
         }
     }
     (void)ncomp;
@@ -1671,9 +1712,8 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         const int nb = (int)std::min<size_t>(SHS_TC_SETS, nsets - j0);
         const unsigned long Ng = nmax_v[ord[j0]];   // largest of the launch
         chunk_layout(Ng);
-        CB_CUDA(cudaMemcpyAsync(d_chunk0, h0.data(),
-                                (Ng + 2) * sizeof(long long),
-                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_TRY(h2d_small(c, d_chunk0, h0.data(),
+                         (Ng + 2) * sizeof(long long)));
         ShsTcPrep P{};
         P.nmax = (long long)Ng;
         P.nsets = nb;
@@ -1781,7 +1821,9 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
             }
         }
         // the digit tiles and the lumped buffer are reused by the next group
-        CB_CUDA(cudaStreamSynchronize(c.stream), st);
+        // (stream order suffices inside a captured graph)
+        if (!c.capturing)
+            CB_CUDA(cudaStreamSynchronize(c.stream), st);
     }
     return finish(c, d_status);
 }
@@ -2828,6 +2870,116 @@ Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
     CB_TRY(init(g_ctx));
     return shs_batch(g_ctx, pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
                      kgrad, d_f);
+}
+
+// ---------------------------------------------------------------------------
+// Batched synthesis captured into a CUDA graph
+// ---------------------------------------------------------------------------
+struct BatchGraph
+{
+    cudaGraphExec_t exec = nullptr;
+    std::vector<void *> pins;
+};
+
+Status batch_graph_create(const charm_point *pnt, size_t nsets,
+                          const unsigned long *nmax,
+                          const unsigned long *shc_nmax, const double *mu,
+                          double r, const double *const *d_c,
+                          const double *const *d_s, int kgrad,
+                          double *const *d_f, int split, void **out)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    Context &c = g_ctx;
+    Status st;
+    *out = nullptr;
+    CB_TRY(init(c));
+    auto run = [&]() {
+        return split ? shs_batch_tc(c, pnt, nsets, nmax, shc_nmax, mu, r, d_c,
+                                    d_s, d_f)
+                     : shs_batch(c, pnt, nsets, nmax, shc_nmax, mu, r, d_c,
+                                 d_s, kgrad, d_f);
+    };
+    // a plain call first: checks the arguments, builds every table, plan,
+    // buffer and tuned choice the captured call then finds in place
+    CB_TRY(run());
+    const bool timing = c.timing;
+    c.timing = false;
+    c.capturing = true;
+    c.capture_pins.clear();
+    cudaGraph_t g = nullptr;
+    Status s2;
+    cudaError_t e = cudaStreamBeginCapture(c.stream,
+                                           cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess)
+    {
+        s2 = run();
+        e = cudaStreamEndCapture(c.stream, &g);
+    }
+    c.capturing = false;
+    c.timing = timing;
+    std::vector<void *> pins;
+    pins.swap(c.capture_pins);
+    auto drop = [&]() {
+        for (void *p : pins)
+            cudaFreeHost(p);
+        if (g)
+            cudaGraphDestroy(g);
+    };
+    if (!s2.ok())
+    {
+        drop();
+        return s2;
+    }
+    if (e != cudaSuccess)
+    {
+        drop();
+        st.code = CHARM_EFUNCARG;
+        st.msg = std::string("stream capture failed: ") + cudaGetErrorString(e);
+        return st;
+    }
+    BatchGraph *G = new BatchGraph;
+    e = cudaGraphInstantiate(&G->exec, g, 0);
+    cudaGraphDestroy(g);
+    g = nullptr;
+    if (e != cudaSuccess)
+    {
+        drop();
+        delete G;
+        st.code = CHARM_EFUNCARG;
+        st.msg = std::string("graph instantiation failed: ") +
+                 cudaGetErrorString(e);
+        return st;
+    }
+    G->pins.swap(pins);
+    *out = G;
+    return st;
+}
+
+Status batch_graph_launch(void *h)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    Context &c = g_ctx;
+    Status st;
+    BatchGraph *G = static_cast<BatchGraph *>(h);
+    CB_CUDA(cudaGraphLaunch(G->exec, c.stream), st);
+    c.launches++;
+    void *p = nullptr;
+    CB_TRY(buf(c, "status", 256, &p));
+    return finish(c, static_cast<unsigned *>(p));
+}
+
+void batch_graph_free(void *h)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    BatchGraph *G = static_cast<BatchGraph *>(h);
+    if (!G)
+        return;
+    cudaStreamSynchronize(g_ctx.stream);
+    if (G->exec)
+        cudaGraphExecDestroy(G->exec);
+    for (void *p : G->pins)
+        cudaFreeHost(p);
+    delete G;
 }
 
 // The autotuner's choices so far, one line per problem shape.

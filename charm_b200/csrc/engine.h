@@ -68,6 +68,18 @@ Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,
                            double r, const double *const *d_c,
                            const double *const *d_s, int kgrad,
                            double *const *d_f);
+// A batched synthesis call (FP64 batch or, split != 0, the split-precision
+// one) captured into a CUDA graph; launch replays it on the same device
+// buffers and checks the kernels' status word.
+Status batch_graph_create(const charm_point *pnt, size_t nsets,
+                          const unsigned long *nmax,
+                          const unsigned long *shc_nmax, const double *mu,
+                          double r, const double *const *d_c,
+                          const double *const *d_s, int kgrad,
+                          double *const *d_f, int split, void **out);
+Status batch_graph_launch(void *graph);
+void batch_graph_free(void *graph);
+
 // The autotuner's choices so far (one line per problem shape).
 std::string autotune_report();
 

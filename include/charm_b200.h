@@ -245,6 +245,24 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_dev(
     const double *const *d_c, const double *const *d_s, int kgrad,
     double *const *d_f, charm_err *err);
 
+/* A batched synthesis captured into a CUDA graph (no counterpart in CHarm):
+ * split_precision 0 captures charm_b200_shs_point_batch_dev, 1 captures
+ * charm_b200_shs_point_batch_i8_dev (kgrad 0), with these arguments.  The
+ * call runs once plainly (checks, tables, buffers, tuned choices), then once
+ * under stream capture; returns the graph's handle, or NULL with err set.
+ * charm_b200_graph_launch replays the whole call (every launch, copy and
+ * row transform of it) on the same device buffers, whose contents the
+ * caller may change between launches, and reports the kernels' status;
+ * charm_b200_graph_free releases the graph. */
+CHARM_EXTERN void *CHARM_CDECL charm_b200_shs_point_batch_graph(
+    const charm_point *pnt, size_t nsets, const unsigned long *nmax,
+    const unsigned long *shc_nmax, const double *mu, double r,
+    const double *const *d_c, const double *const *d_s, int kgrad,
+    double *const *d_f, int split_precision, charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_b200_graph_launch(void *graph,
+                                                      charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_b200_graph_free(void *graph);
+
 /* The synthesis kernel's autotuner (no counterpart in CHarm): on the first
  * call of a problem shape (derivative kind, nmax >= 256, latitude pairs, on
  * or off the reference sphere) the latitude pairs per lane of the grid
