@@ -1744,7 +1744,6 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         A.npairs = np;
         A.ntiles = ntiles;
         A.nitems = (long long)(Ng + 1) * ntiles;
-        A.tb = tab.tb;
         A.tmul = tab.tmul;
         A.ldmul = tab.ldmul;
         A.sg = tab.sg;

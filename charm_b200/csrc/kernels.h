@@ -272,8 +272,7 @@ struct ShsTcArgs
     int npairs;
     int ntiles;                           // tiles of 128 latitude pairs
     long long nitems;                     // (nmax_sets + 1) * ntiles
-    const double2 *tb;                    // recurrence tables (leg.cuh)
-    const double *tmul;
+    const double *tmul;                   // recurrence tables (leg.cuh)
     int ldmul;
     const double *sg;
     const double *btp;                    // beta_n rows of ldmul * 64

@@ -61,7 +61,9 @@ constexpr int TC_ASTAGE = 2 * TC_D * TC_ATILE;         // 57344
 constexpr int TC_BSTAGE = 2 * TC_D * TC_BTILE;         // 14336
 constexpr int TC_CH = 64;                              // degrees per chunk
 constexpr int TC_NB = 4;           // coefficient / table stages
-constexpr int TC_AHEAD = TC_NB - 2;   // chunks loaded ahead of the MMAs' next
+// the producer loads chunk g + TC_AHEAD + 1 once the MMAs of chunk g - 1
+// (the last user of that stage) are complete
+constexpr int TC_AHEAD = TC_NB - 2;
 constexpr unsigned TC_TMEM_COLS = 512;
 // offset of the balanced digits of the coefficients: sum_{i<7} 128 256^i
 constexpr unsigned long long TC_BIAS = 0x0080808080808080ull;
