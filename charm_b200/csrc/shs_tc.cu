@@ -15,28 +15,31 @@
 //     B_int = round(B 2^(54 - eB)),  2^eB > max_n |B| of that column,
 // each written in base 256 with seven digits: A_int in two's complement
 // (digits 0..5 unsigned, the top digit signed), taken straight from the
-// mantissa of A 2^(51 - eA) + 1.5 2^52 (one FP64 add, no conversion
-// instruction); B_int with balanced digits in [-128, 127] (the bytes of
+// mantissa of x c~_n + 1.5 2^52 (one FMA on the recurrence value x already
+// carrying 2^(51 - eA), no conversion instruction); B_int with balanced
+// digits in [-128, 127] (the bytes of
 // B_int + sum_i 128 256^i, minus 128), so that every dropped product has
 // zero mean.  The digit products a_i b_j are exact in the INT32
 // accumulators of tcgen05.mma kind::i8; products of level s = i + j are
 // summed in one accumulator and weighted by 256^s in FP64 afterwards.
 // Levels below 5 are dropped: they hold about 2^-53 of a typical term.
-// 34 digit pairs per degree tile and parity; 8 levels x 2 parities x 32
-// columns = all 512 TMEM columns of the SM.
+// 34 digit pairs per degree tile and parity, issued as 7 MMAs (one per
+// Legendre digit against the stack of coefficient digits it meets, N =
+// 64..224); 8 levels x 2 parities x 32 columns = all 512 TMEM columns.
 //
 // The fixed-point grid of the Legendre values of each (order, latitude) is
 // chosen from a bound of |P_nm| (k_tc_seeds); a value outside it sets
 // DEV_ERR_TC_RANGE and the call fails.
 //
-// Pipeline per CTA (one latitude pair per TMEM lane): the coefficient digit
-// tiles and the recurrence tables of a 64-degree chunk arrive by bulk
-// copies, two chunks ahead (four stages, streamed across work items); 256
-// threads run the rescaled recurrence of leg.cuh in FP64, cut the values
-// into digits and store them as the K-major operand tiles (two stages); a
-// producer warp issues the 14 MMAs of the chunk and commits them to an
-// mbarrier, so the tensor cores work on chunk j while the threads prepare
-// chunk j + 1.
+// Pipeline per CTA (one latitude pair per TMEM lane; warp roles at
+// k_shs_tc): the coefficient digit tiles and the recurrence tables of a
+// 64-degree chunk arrive by bulk copies, three chunks ahead of the MMAs
+// (four stages, streamed across work items); 128 threads run the rescaled
+// recurrence of leg.cuh in FP64, cut the values into digits and store them
+// as the K-major operand tiles (two stages); a producer lane issues the 14
+// MMAs of the chunk and commits them to an mbarrier, so the tensor cores
+// work on chunk j while the threads prepare chunk j + 1; epilogue warps
+// drain an item's accumulators while the next item is prepared.
 #include <cstdint>
 #include <type_traits>
 
