@@ -125,7 +125,117 @@ __device__ __forceinline__ void dft3(double2 *v)
     v[2] = sub2(h, q);
 }
 
-template <int R>
+// cos and sin of pi/8, 2 pi/9, 4 pi/9, 8 pi/9
+constexpr double C16 = 0.92387953251128675613;
+constexpr double S16 = 0.38268343236508977173;
+constexpr double C9A = 0.76604444311897803520;
+constexpr double S9A = 0.64278760968653932632;
+constexpr double C9B = 0.17364817766693034885;
+constexpr double S9B = 0.98480775301220805936;
+constexpr double C9D = -0.93969262078590838405;
+constexpr double S9D = 0.34202014332566873304;
+
+// 16 = 4 x 4 (n = 4 n1 + n2, k = k1 + 4 k2): DFTs of length 4 over n1,
+// twiddles exp(-2 pi i n2 k1 / 16), DFTs of length 4 over n2.  HZ: the
+// inputs v[8..15] are zero and are not read (the zero-padded half of a
+// Bluestein sequence).
+template <bool HZ>
+__device__ __forceinline__ void dft16(double2 *v)
+{
+    double2 a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++)
+    {
+        if constexpr (HZ)
+        {
+            const double2 x0 = v[n2], x1 = v[4 + n2];
+            a[n2][0] = add2(x0, x1);
+            a[n2][1] = add2(x0, mul_mi(x1));
+            a[n2][2] = sub2(x0, x1);
+            a[n2][3] = sub2(x0, mul_mi(x1));
+        }
+        else
+        {
+            a[n2][0] = v[n2];
+            a[n2][1] = v[4 + n2];
+            a[n2][2] = v[8 + n2];
+            a[n2][3] = v[12 + n2];
+            dft4(a[n2][0], a[n2][1], a[n2][2], a[n2][3]);
+        }
+    }
+    a[1][1] = cmul(a[1][1], make_double2(C16, -S16));
+    a[1][2] = make_double2((a[1][2].x + a[1][2].y) * RSQRT2,
+                           (a[1][2].y - a[1][2].x) * RSQRT2);
+    a[1][3] = cmul(a[1][3], make_double2(S16, -C16));
+    a[2][1] = make_double2((a[2][1].x + a[2][1].y) * RSQRT2,
+                           (a[2][1].y - a[2][1].x) * RSQRT2);
+    a[2][2] = mul_mi(a[2][2]);
+    a[2][3] = make_double2((a[2][3].y - a[2][3].x) * RSQRT2,
+                           -(a[2][3].x + a[2][3].y) * RSQRT2);
+    a[3][1] = cmul(a[3][1], make_double2(S16, -C16));
+    a[3][2] = make_double2((a[3][2].y - a[3][2].x) * RSQRT2,
+                           -(a[3][2].x + a[3][2].y) * RSQRT2);
+    a[3][3] = cmul(a[3][3], make_double2(-C16, S16));
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++)
+    {
+        dft4(a[0][k1], a[1][k1], a[2][k1], a[3][k1]);
+        v[k1] = a[0][k1];
+        v[k1 + 4] = a[1][k1];
+        v[k1 + 8] = a[2][k1];
+        v[k1 + 12] = a[3][k1];
+    }
+}
+
+// 9 = 3 x 3 (n = 3 n1 + n2, k = k1 + 3 k2), twiddles exp(-2 pi i n2 k1 / 9)
+__device__ __forceinline__ void dft9(double2 *v)
+{
+    double2 a[3][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; n2++)
+    {
+        a[n2][0] = v[n2];
+        a[n2][1] = v[3 + n2];
+        a[n2][2] = v[6 + n2];
+        dft3(a[n2]);
+    }
+    a[1][1] = cmul(a[1][1], make_double2(C9A, -S9A));
+    a[1][2] = cmul(a[1][2], make_double2(C9B, -S9B));
+    a[2][1] = cmul(a[2][1], make_double2(C9B, -S9B));
+    a[2][2] = cmul(a[2][2], make_double2(C9D, -S9D));
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++)
+    {
+        double2 b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+        dft3(b);
+        v[k1] = b[0];
+        v[k1 + 3] = b[1];
+        v[k1 + 6] = b[2];
+    }
+}
+
+// 18 = 2 x 9 by the prime-factor (Good-Thomas) map, no twiddles: input
+// n = (9 n1 + 2 n2) mod 18, output k = (9 k1 + 10 k2) mod 18
+__device__ __forceinline__ void dft18(double2 *v)
+{
+    double2 e[9], o[9];
+#pragma unroll
+    for (int n2 = 0; n2 < 9; n2++)
+    {
+        e[n2] = v[(2 * n2) % 18];
+        o[n2] = v[(9 + 2 * n2) % 18];
+    }
+    dft9(e);
+    dft9(o);
+#pragma unroll
+    for (int k2 = 0; k2 < 9; k2++)
+    {
+        v[(10 * k2) % 18] = add2(e[k2], o[k2]);
+        v[(9 + 10 * k2) % 18] = sub2(e[k2], o[k2]);
+    }
+}
+
+template <int R, bool HZ = false>
 __device__ __forceinline__ void dft(double2 *v)
 {
     if constexpr (R == 2)
@@ -134,24 +244,39 @@ __device__ __forceinline__ void dft(double2 *v)
         dft3(v);
     else if constexpr (R == 4)
         dft4(v[0], v[1], v[2], v[3]);
-    else
+    else if constexpr (R == 8)
         dft8(v);
+    else if constexpr (R == 9)
+        dft9(v);
+    else if constexpr (R == 16)
+        dft16<HZ>(v);
+    else
+    {
+        static_assert(R == 18, "radix");
+        dft18(v);
+    }
 }
 
-// w[r] = w[1]^r for r = 2..R-1 by at most three levels of products
+// w[r] = w[1]^r for r = 2..R-1: w[2^a] = w[2^(a-1)]^2 and
+// w[2^a + b] = w[2^a] w[b] (b < 2^a), at most log2 R + 1 products deep
+constexpr int hibit(int r)
+{
+    int h = 1;
+    while (2 * h <= r)
+        h *= 2;
+    return h;
+}
+
 template <int R>
 __device__ __forceinline__ void twiddle_powers(double2 *w)
 {
-    if constexpr (R >= 3)
-        w[2] = cmul(w[1], w[1]);
-    if constexpr (R >= 4)
-        w[3] = cmul(w[2], w[1]);
-    if constexpr (R == 8)
+#pragma unroll
+    for (int r = 2; r < R; r++)
     {
-        w[4] = cmul(w[2], w[2]);
-        w[5] = cmul(w[4], w[1]);
-        w[6] = cmul(w[4], w[2]);
-        w[7] = cmul(w[4], w[3]);
+        if (r == hibit(r))
+            w[r] = cmul(w[r / 2], w[r / 2]);
+        else
+            w[r] = cmul(w[hibit(r)], w[r - hibit(r)]);
     }
 }
 
@@ -289,59 +414,22 @@ __device__ __forceinline__ void fft_m(double2 *s,
 // ---- the same transform with the whole plan known at compile time ----
 // (the lengths the grids of nmax about 2160..2190 use: M = 4608, 9216).
 // Radices, strides, thread counts and butterfly ranges become constants,
-// so the index arithmetic of every pass folds away.
-struct CtPlan
-{
-    int n8, n4, n2, n3;
-};
-
-// passes of radix 8, then 4, then 2, then 3, as the run-time plan
-constexpr CtPlan ct_plan(int M)
-{
-    int a = 0, b = 0, n = M;
-    while (n % 2 == 0)
-    {
-        n /= 2;
-        a++;
-    }
-    while (n % 3 == 0)
-    {
-        n /= 3;
-        b++;
-    }
-    int p8 = a / 3, p4 = 0, p2 = 0;
-    if (a % 3 == 2)
-        p4 = 1;
-    else if (a % 3 == 1)
-    {
-        if (p8 > 0)
-        {
-            p8--;
-            p4 = 2;
-        }
-        else
-            p2 = 1;
-    }
-    return CtPlan{p8, p4, p2, b};
-}
-
+// so the index arithmetic of every pass folds away, and the larger
+// radices cut the number of barrier-separated passes through shared
+// memory: 4608 = 16 16 18 (three passes instead of five),
+// 9216 = 16 16 9 4 (four instead of six).  The first pass has radix 16
+// and every later stride is a multiple of 8, as the padded addressing
+// needs.
 constexpr int ct_npass(int M)
 {
-    return ct_plan(M).n8 + ct_plan(M).n4 + ct_plan(M).n2 + ct_plan(M).n3;
+    return M == 4608 ? 3 : 4;
 }
 
 constexpr int ct_radix(int M, int p)
 {
-    const CtPlan q = ct_plan(M);
-    if (p < q.n8)
-        return 8;
-    p -= q.n8;
-    if (p < q.n4)
-        return 4;
-    p -= q.n4;
-    if (p < q.n2)
-        return 2;
-    return 3;
+    if (M == 4608)
+        return p < 2 ? 16 : 18;
+    return p < 2 ? 16 : (p == 2 ? 9 : 4);
 }
 
 constexpr int ct_ns(int M, int p)
@@ -364,7 +452,10 @@ __device__ __forceinline__ double2 ld_tw(const double2 *p)
     return v;
 }
 
-template <int R, int V, int M, int NS, bool FIRST, bool BH, class Src>
+// HZ (first pass of a Bluestein sequence only): elements M/2.. are zero
+// (M >= 2H), so a butterfly's upper R/2 inputs are neither read nor added.
+template <int R, int V, int M, int NS, bool FIRST, bool BH, bool HZ,
+          class Src>
 __device__ __forceinline__ void stockham_ct(double2 *s,
                                             const double2 *__restrict__ tw,
                                             int tid, const Src &src,
@@ -375,7 +466,14 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
     constexpr int nb = M / R;
     constexpr int step = M / (NS * R);
     constexpr int ld_stride = nb + (nb >> 3);
-    constexpr int st_stride = (NS == 1) ? 1 : NS + (NS >> 3);
+    static_assert(nb % 8 == 0 && (NS == 1 || NS % 8 == 0), "padding");
+    static_assert(!FIRST || R % 8 == 0, "first pass radix");
+    static_assert(!HZ || (FIRST && R == 16), "zero half");
+    // padded offset of a butterfly's output r from its first one: the
+    // first pass writes R consecutive elements from a multiple of 8
+    auto st_off = [](int r) {
+        return NS == 1 ? r + (r >> 3) : r * (NS + (NS >> 3));
+    };
     double2 v[BPT][R];
 #pragma unroll
     for (int c = 0; c < BPT; c++)
@@ -386,7 +484,7 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
             if constexpr (FIRST)
             {
 #pragma unroll
-                for (int r = 0; r < R; r++)
+                for (int r = 0; r < (HZ ? R / 2 : R); r++)
                     v[c][r] = src(j + r * nb);
             }
             else
@@ -401,7 +499,7 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
                 for (int r = 1; r < R; r++)
                     v[c][r] = cmul(s[b + r * ld_stride], wp[r]);
             }
-            dft<R>(v[c]);
+            dft<R, HZ>(v[c]);
         }
     }
     __syncthreads();
@@ -418,14 +516,14 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
             {
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    s[b + r * st_stride] =
+                    s[b + st_off(r)] =
                         conj2(cmul(v[c][r], ld_tw(&bh[d + r * NS])));
             }
             else
             {
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    s[b + r * st_stride] = v[c][r];
+                    s[b + st_off(r)] = v[c][r];
             }
         }
     }
@@ -433,8 +531,8 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
 }
 
 // passes P.. of FFT_M (compile-time plan); the last one multiplies by bh
-// when given
-template <int V, int M, int P, class Src>
+// when given; HZ: the upper half of the input sequence is zero
+template <int V, int M, int P, bool HZ, class Src>
 __device__ __forceinline__ void fft_ct(double2 *s,
                                        const double2 *__restrict__ tw, int tid,
                                        const Src &src,
@@ -444,18 +542,20 @@ __device__ __forceinline__ void fft_ct(double2 *s,
     {
         constexpr int R = ct_radix(M, P);
         constexpr int NS = ct_ns(M, P);
+        constexpr bool Z = HZ && P == 0;
         if constexpr (P == ct_npass(M) - 1)
         {
             if (bh_last)
-                stockham_ct<R, V, M, NS, P == 0, true>(s, tw, tid, src,
-                                                       bh_last);
+                stockham_ct<R, V, M, NS, P == 0, true, Z>(s, tw, tid, src,
+                                                          bh_last);
             else
-                stockham_ct<R, V, M, NS, P == 0, false>(s, tw, tid, src,
-                                                        nullptr);
+                stockham_ct<R, V, M, NS, P == 0, false, Z>(s, tw, tid, src,
+                                                           nullptr);
         }
         else
-            stockham_ct<R, V, M, NS, P == 0, false>(s, tw, tid, src, nullptr);
-        fft_ct<V, M, P + 1>(s, tw, tid, src, bh_last);
+            stockham_ct<R, V, M, NS, P == 0, false, Z>(s, tw, tid, src,
+                                                       nullptr);
+        fft_ct<V, M, P + 1, HZ>(s, tw, tid, src, bh_last);
     }
 }
 
@@ -471,11 +571,11 @@ __device__ __forceinline__ void dft_h(double2 *s, const RfftArgs &A, int tid,
         // plan fixed at compile time (A.M == MC)
         if (A.direct)
         {
-            fft_ct<V, MC, 0>(s, A.tw, tid, pre, nullptr);
+            fft_ct<V, MC, 0, false>(s, A.tw, tid, pre, nullptr);
             return;
         }
-        fft_ct<V, MC, 0>(s, A.tw, tid, pre, A.bh);
-        fft_ct<V, MC, 0>(s, A.tw, tid, SrcSmem{s}, nullptr);
+        fft_ct<V, MC, 0, true>(s, A.tw, tid, pre, A.bh);
+        fft_ct<V, MC, 0, false>(s, A.tw, tid, SrcSmem{s}, nullptr);
     }
     else
     {
