@@ -454,8 +454,10 @@ __device__ __forceinline__ double2 ld_tw(const double2 *p)
 
 // HZ (first pass of a Bluestein sequence only): elements M/2.. are zero
 // (M >= 2H), so a butterfly's upper R/2 inputs are neither read nor added.
+// HO (last pass of Bluestein's second FFT only): outputs M/2.. are never
+// read (H <= M/2), so they are neither computed nor stored.
 template <int R, int V, int M, int NS, bool FIRST, bool BH, bool HZ,
-          class Src>
+          bool HO = false, class Src>
 __device__ __forceinline__ void stockham_ct(double2 *s,
                                             const double2 *__restrict__ tw,
                                             int tid, const Src &src,
@@ -469,6 +471,7 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
     static_assert(nb % 8 == 0 && (NS == 1 || NS % 8 == 0), "padding");
     static_assert(!FIRST || R % 8 == 0, "first pass radix");
     static_assert(!HZ || (FIRST && R == 16), "zero half");
+    static_assert(!HO || (NS * R == M && R % 2 == 0 && !BH), "half output");
     // padded offset of a butterfly's output r from its first one: the
     // first pass writes R consecutive elements from a multiple of 8
     auto st_off = [](int r) {
@@ -522,7 +525,7 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
             else
             {
 #pragma unroll
-                for (int r = 0; r < R; r++)
+                for (int r = 0; r < (HO ? R / 2 : R); r++)
                     s[b + st_off(r)] = v[c][r];
             }
         }
@@ -530,15 +533,17 @@ __device__ __forceinline__ void stockham_ct(double2 *s,
     __syncthreads();
 }
 
-// passes P.. of FFT_M (compile-time plan); the last one multiplies by bh
-// when given; HZ: the upper half of the input sequence is zero
-template <int V, int M, int P, bool HZ, class Src>
+// passes P..PEND-1 of FFT_M (compile-time plan); the FFT's last pass
+// multiplies by bh when given; HZ: the upper half of the input sequence
+// is zero; HO: only the lower half of the output is wanted
+template <int V, int M, int P, bool HZ, int PEND = ct_npass(M),
+          bool HO = false, class Src>
 __device__ __forceinline__ void fft_ct(double2 *s,
                                        const double2 *__restrict__ tw, int tid,
                                        const Src &src,
                                        const double2 *__restrict__ bh_last)
 {
-    if constexpr (P < ct_npass(M))
+    if constexpr (P < PEND)
     {
         constexpr int R = ct_radix(M, P);
         constexpr int NS = ct_ns(M, P);
@@ -549,13 +554,53 @@ __device__ __forceinline__ void fft_ct(double2 *s,
                 stockham_ct<R, V, M, NS, P == 0, true, Z>(s, tw, tid, src,
                                                           bh_last);
             else
-                stockham_ct<R, V, M, NS, P == 0, false, Z>(s, tw, tid, src,
-                                                           nullptr);
+                stockham_ct<R, V, M, NS, P == 0, false, Z, HO>(
+                    s, tw, tid, src, nullptr);
         }
         else
             stockham_ct<R, V, M, NS, P == 0, false, Z>(s, tw, tid, src,
                                                        nullptr);
-        fft_ct<V, M, P + 1, HZ>(s, tw, tid, src, bh_last);
+        fft_ct<V, M, P + 1, HZ, PEND, HO>(s, tw, tid, src, bh_last);
+    }
+}
+
+// The last pass of the second FFT_M of Bluestein's algorithm (compile-time
+// plan, even last radix) handed straight to its consumer: output
+// k = j + r M/R of butterfly j goes to out(k, value) for k < H <= M/2.
+// Nothing is stored in shared memory, so the pass needs no barrier.
+template <int V, int M, class Out>
+__device__ __forceinline__ void fft_ct_last_out(const double2 *s,
+                                                const double2 *__restrict__ tw,
+                                                int tid, int H, const Out &out)
+{
+    constexpr int P = ct_npass(M) - 1;
+    constexpr int R = ct_radix(M, P);
+    constexpr int NS = ct_ns(M, P);
+    static_assert(NS * R == M && R % 2 == 0, "last pass");
+    constexpr int T = M / V;
+    constexpr int BPT = (V + R - 1) / R;
+    constexpr int ld_stride = NS + (NS >> 3);
+#pragma unroll 1
+    for (int c = 0; c < BPT; c++)
+    {
+        const int j = tid + c * T;
+        if (j < NS)
+        {
+            double2 wp[R], v[R];
+            wp[1] = ld_tw(&tw[j]);
+            twiddle_powers<R>(wp);
+            const int b = pidx(j);
+            v[0] = s[b];
+#pragma unroll
+            for (int r = 1; r < R; r++)
+                v[r] = cmul(s[b + r * ld_stride], wp[r]);
+            dft<R>(v);
+            // H <= M/2: the outputs of the upper half are never used
+#pragma unroll
+            for (int r = 0; r < R / 2; r++)
+                if (j + r * NS < H)
+                    out(j + r * NS, v[r]);
+        }
     }
 }
 
@@ -568,14 +613,10 @@ __device__ __forceinline__ void dft_h(double2 *s, const RfftArgs &A, int tid,
 {
     if constexpr (MC > 0)
     {
-        // plan fixed at compile time (A.M == MC)
-        if (A.direct)
-        {
-            fft_ct<V, MC, 0, false>(s, A.tw, tid, pre, nullptr);
-            return;
-        }
+        // plan fixed at compile time (A.M == MC, Bluestein)
         fft_ct<V, MC, 0, true>(s, A.tw, tid, pre, A.bh);
-        fft_ct<V, MC, 0, false>(s, A.tw, tid, SrcSmem{s}, nullptr);
+        fft_ct<V, MC, 0, false, ct_npass(MC), true>(s, A.tw, tid, SrcSmem{s},
+                                                    nullptr);
     }
     else
     {
@@ -710,6 +751,24 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_fwd(RfftArgs A)
 }
 
 // Synthesis direction: X[row][0..kmax] (zero above) -> real rows x[row].
+// Output of the synthesis direction: x_2k + i x_2k+1 = conj of DFT value
+// k, which Bluestein's algorithm gives as w_k conj(second FFT output k).
+template <bool F32>
+struct OutRow
+{
+    void *x2;
+    const double2 *w;
+    __device__ __forceinline__ void operator()(int k, double2 v) const
+    {
+        const double2 z = cmul(__ldg(&w[k]), conj2(v));
+        if constexpr (F32)
+            reinterpret_cast<float2 *>(x2)[k] =
+                make_float2((float)z.x, (float)-z.y);
+        else
+            reinterpret_cast<double2 *>(x2)[k] = conj2(z);
+    }
+};
+
 template <int V, int NR, bool F32, int MC>
 __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
 {
@@ -718,6 +777,18 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
     const long long row = blockIdx.x;
     SrcSpectrum src{A.X + row * A.ldX, A.direct ? nullptr : A.w, A.ht, A.H,
                     A.kmax};
+    if constexpr (MC > 0)
+    {
+        // Bluestein with the second FFT's last pass writing the row
+        void *x2 = F32 ? (void *)(reinterpret_cast<float *>(A.x) +
+                                  row * A.ldx)
+                       : (void *)(A.x + row * A.ldx);
+        fft_ct<V, MC, 0, true>(s, A.tw, tid, src, A.bh);
+        fft_ct<V, MC, 0, false, ct_npass(MC) - 1>(s, A.tw, tid, SrcSmem{s},
+                                                  nullptr);
+        fft_ct_last_out<V, MC>(s, A.tw, tid, A.H, OutRow<F32>{x2, A.w});
+        return;
+    }
     dft_h<V, MC>(s, A, tid, T, src);
     if constexpr (F32)
     {
@@ -833,7 +904,8 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         return cudaSuccess;
     const size_t smem = rfft_smem_bytes(A.M);
     const int T = A.M / 16;
-    // the grids' common lengths with the plan fixed at compile time
+    // the grids' common Bluestein lengths with the plan fixed at compile
+    // time
     auto go = [&](auto mc) {
         constexpr int MC = decltype(mc)::value;
         constexpr int NR = 96;
@@ -849,7 +921,9 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         else
             k_rfft_fwd<16, NR, false, MC><<<grid, T, smem, st>>>(A);
     };
-    if (A.M == 4608)
+    if (A.direct)
+        go(std::integral_constant<int, 0>{});
+    else if (A.M == 4608)
         go(std::integral_constant<int, 4608>{});
     else if (A.M == 9216)
         go(std::integral_constant<int, 9216>{});
