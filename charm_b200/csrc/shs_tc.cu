@@ -58,6 +58,7 @@ constexpr int TC_COLS = 32;        // accumulator columns
 constexpr int TC_D = 7;            // digits per operand
 constexpr int TC_LMIN = 5;         // lowest product level kept
 constexpr int TC_NLEV = 2 * TC_D - 1 - TC_LMIN;        // 8
+static_assert(TC_NLEV == 8, "the epilogue groups the levels 3 + 3 + 2");
 constexpr int TC_ATILE = TC_M * 32;                    // bytes
 constexpr int TC_BTILE = TC_COLS * 32;                 // bytes
 constexpr int TC_ASTAGE = 2 * TC_D * TC_ATILE;         // 57344
@@ -156,12 +157,11 @@ __device__ __forceinline__ void tc_wait_st()
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
-// exact int32 -> double on the FP64 pipe: the bits 0x43300000:(v ^ 2^31)
-// are 2^52 + 2^31 + v
-__device__ __forceinline__ double i2d_exact(int v)
+// exact int64 -> double for |u| < 2^51 with one integer add and one DADD:
+// the bits 0x4338000000000000 + u are 1.5 2^52 + u
+__device__ __forceinline__ double l2d_exact(long long u)
 {
-    return __hiloint2double(0x43300000, v ^ (int)0x80000000) -
-           4503601774854144.0;
+    return __longlong_as_double(u + 0x4338000000000000LL) - TC_MAGIC;
 }
 
 // 2^e for |e| < 1000 (exact)
@@ -869,12 +869,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
 #pragma unroll
                     for (int c = 0; c < 8; c++)
                     {
-                        double s2 = 0.0;
-#pragma unroll
-                        for (int L = TC_NLEV - 1; L >= 0; L--)
-                            s2 = fma(i2d_exact(v[L][c]),
-                                     pow2i(8 * (L + TC_LMIN)), s2);
-                        tot[pp][c] = s2;
+                        // levels 0..2, 3..5 and 6..7 combined exactly in
+                        // 64-bit integers (|v| < 2^31: every group stays
+                        // below 2^48), then two FMAs
+                        const long long u0 = (long long)v[0][c] +
+                                             (long long)v[1][c] * 256LL +
+                                             (long long)v[2][c] * 65536LL;
+                        const long long u1 = (long long)v[3][c] +
+                                             (long long)v[4][c] * 256LL +
+                                             (long long)v[5][c] * 65536LL;
+                        const long long u2 = (long long)v[6][c] +
+                                             (long long)v[7][c] * 256LL;
+                        tot[pp][c] =
+                            fma(l2d_exact(u2), pow2i(8 * (6 + TC_LMIN)),
+                                fma(l2d_exact(u1), pow2i(8 * (3 + TC_LMIN)),
+                                    l2d_exact(u0) * pow2i(8 * TC_LMIN)));
                     }
                 }
                 if (valid)
