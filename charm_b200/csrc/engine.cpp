@@ -567,6 +567,78 @@ Status row_fft(Context &c, long long L, const RfftArgs **out)
     return st;
 }
 
+// Quarter-length plan for synthesis rows of length L = 4 Lq (DH2 grids:
+// L = 4 (nmax + 1)), or nullptr: two complex DFTs of length Lq per row
+// (rfft.cu, k_rfft_inv4), used where the half-length plan `half` needs
+// M = 9216 and Lq has the compile-time Bluestein plan M = 4608 (two CTAs
+// per SM instead of one).  Cached under the key -L.
+Status row_fft_quarter(Context &c, long long L, const RfftArgs *half,
+                       const RfftArgs **out)
+{
+    Status st;
+    *out = nullptr;
+    if (!half || half->M != 9216 || L % 4 != 0)
+        return st;
+    auto it = c.rffts.find(-L);
+    if (it != c.rffts.end())
+    {
+        *out = it->second.M > 0 ? &it->second : nullptr;
+        return st;
+    }
+    const long long Lq = L / 4;
+    RfftArgs A{};
+    if (!rfft_shape(2 * Lq, &A) || A.direct || A.M != 4608)
+    {
+        A.M = 0;
+        c.rffts[-L] = A;
+        return st;
+    }
+    const size_t nM = (size_t)A.M, nH = (size_t)A.H;
+    const size_t n_tab = nM + nH + nM + (nH + 1) + nH;
+    void *mem = nullptr;
+    CB_CUDA(cudaMalloc(&mem, n_tab * sizeof(double2)), st);
+    double2 *tw = static_cast<double2 *>(mem);
+    double2 *w = tw + nM;
+    double2 *bh = w + nH;
+    double2 *ht = bh + nM;
+    double2 *w4 = ht + nH + 1;
+    A.tw = tw;
+    A.w = w;
+    A.bh = bh;
+    A.ht = ht;
+    A.w4 = w4;
+    A.quarter = 1;
+    cudaError_t ce = rfft_set_smem(rfft_smem_bytes(9216));
+    if (ce == cudaSuccess)
+        ce = launch_rfft_tables(A, tw, w, ht, bh, c.stream);
+    if (ce == cudaSuccess)
+        ce = launch_rfft_w4(A.H, w4, c.stream);
+    if (ce == cudaSuccess)
+        ce = cudaStreamSynchronize(c.stream);
+    if (ce != cudaSuccess)
+    {
+        cudaFree(mem);
+        st.code = CHARM_EFUNCARG;
+        st.msg = std::string("row transform set-up failed: ") +
+                 cudaGetErrorString(ce);
+        return st;
+    }
+    c.launches += 3;
+    c.rffts[-L] = A;
+    c.rfft_mem[-L] = mem;
+    *out = &c.rffts[-L];
+    return st;
+}
+
+// The plan of a synthesis launch whose spectra stop at kmax: the
+// quarter-length one where it was set up and applies (kmax below its
+// length), else the half-length one.
+const RfftArgs *synth_plan(const RfftArgs *half, const RfftArgs *quarter,
+                           long long kmax)
+{
+    return (quarter && kmax < quarter->H) ? quarter : half;
+}
+
 // Triangle pointer of a charm_shc whose columns c[m] lie contiguously as in
 // src/shc/shc_init_chunk.c:126-145 (every charm_shc built by CHarm's
 // constructors), else null.
@@ -1087,9 +1159,12 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     double *fg = d_f;
     if (!fg)
         CB_TRY(dbuf(c, "fgrid", (size_t)npar * nlat * nlon, &fg));
-    const RfftArgs *rf = nullptr;
+    const RfftArgs *rf = nullptr, *rfq = nullptr;
     if (use_fft && reinterpret_cast<uintptr_t>(fg) % 16 == 0)
+    {
         CB_TRY(row_fft(c, (long long)nlon, &rf));
+        CB_TRY(row_fft_quarter(c, (long long)nlon, rf, &rfq));
+    }
     // the library transform reads the whole half spectrum; the row
     // transform reads orders <= nmax only
     if (use_fft && !rf && (size_t)ldf > nmax + 1)
@@ -1173,7 +1248,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
                     const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
                     if (r1 <= r0)
                         continue;
-                    RfftArgs R = *rf;
+                    RfftArgs R = *synth_plan(rf, rfq, (long long)nmax);
                     R.nrows = r1 - r0;
                     R.x = fg + ((size_t)q * nlat + r0) * nlon;
                     R.ldx = (long long)nlon;
@@ -1213,7 +1288,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     // longitude sums into the output grid(s)
     if (rf)
     {
-        RfftArgs R = *rf;
+        RfftArgs R = *synth_plan(rf, rfq, (long long)nmax);
         R.nrows = (long long)npar * nlat;
         R.x = fg;
         R.ldx = (long long)nlon;
@@ -1459,8 +1534,9 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                                     tab.tc, cs_all + (size_t)j * T, c.stream),
                 st);
     }
-    const RfftArgs *rf = nullptr;
+    const RfftArgs *rf = nullptr, *rfq = nullptr;
     CB_TRY(row_fft(c, (long long)nlon, &rf));
+    CB_TRY(row_fft_quarter(c, (long long)nlon, rf, &rfq));
     const int ldf = (int)(nlon / 2 + 1);
     const size_t grid_sz = nlat * nlon;
     unsigned *d_status;
@@ -1571,7 +1647,8 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                                    (size_t)q * nlat * ldf;
                     if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
                     {
-                        RfftArgs R2 = *rf;
+                        RfftArgs R2 = *synth_plan(
+                            rf, rfq, (long long)nmax_v[j0 + b]);
                         R2.nrows = (long long)nlat;
                         R2.x = dst;
                         R2.ldx = (long long)nlon;
@@ -1691,8 +1768,9 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
     void *bdig = nullptr;
     CB_TRY(buf(c, "tc_bdig", (size_t)nchunks * shs_tc_chunk_bytes(), &bdig));
 
-    const RfftArgs *rf = nullptr;
+    const RfftArgs *rf = nullptr, *rfq = nullptr;
     CB_TRY(row_fft(c, (long long)nlon, &rf));
+    CB_TRY(row_fft_quarter(c, (long long)nlon, rf, &rfq));
     const int ldf = (int)(nlon / 2 + 1);
     const size_t per_set = nlat * (size_t)ldf;
     const size_t bsz = std::min<size_t>(nsets, SHS_TC_SETS);
@@ -1788,7 +1866,7 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
             double2 *src = lc + (size_t)b * per_set;
             if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
             {
-                RfftArgs R2 = *rf;
+                RfftArgs R2 = *synth_plan(rf, rfq, (long long)nmax_v[jj]);
                 R2.nrows = (long long)nlat;
                 R2.x = dst;
                 R2.ldx = (long long)nlon;

@@ -192,6 +192,11 @@ struct RfftArgs
     long long ldX;
     int kmax;              // spectrum entries read (inverse) / written (forward)
     int f32_rows;          // 1: x points to float rows (converted on the fly)
+    // synthesis of rows of length 4H whose spectra stop below H (kmax < H):
+    // two complex DFTs of length H per row, each writing every other pair
+    // of the row (rfft.cu, k_rfft_inv4); w4 = exp(+2 pi i k / 4H), k < H
+    int quarter;
+    const double2 *w4;
 };
 
 // Size of the fixed device scratch of the allocation-free analysis
@@ -238,6 +243,7 @@ cudaError_t launch_fp64_probe(long long iters, int blocks, int threads,
                               double *sink, cudaStream_t st);
 cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
                         bool rr, int K, int grid, cudaStream_t st);
+cudaError_t launch_rfft_w4(int H, double2 *w4, cudaStream_t st);
 cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
                                double2 *ht, double2 *bh, cudaStream_t st);
 size_t rfft_smem_bytes(int M);

@@ -692,6 +692,48 @@ struct SrcSpectrum
     }
 };
 
+// Synthesis input of the quarter-length transform.  A row of length 4H
+// whose spectrum X stops below H gives, with a = X_k, b = conj X_H-k and
+// o = exp(2 pi i k / 4H),
+//   V_0[k] = (a + b) + i o (a - i b),
+//   V_1[k] = o^2 (a - b) + i o^3 (a + i b),
+// and the inverse DFT of length H of V_rho holds the pairs
+// (x_4q+2rho, x_4q+2rho+1) of the row (the four residues of the row index
+// mod 4, paired into two complex sequences).  Returns conj V_rho[k] times
+// the chirp, as SrcSpectrum.
+struct SrcQuarter
+{
+    const double2 *X;
+    const double2 *w;
+    const double2 *w4;
+    int H, kmax, rho;
+    __device__ __forceinline__ double2 operator()(int k) const
+    {
+        if (k >= H)
+            return make_double2(0.0, 0.0);
+        const int kh = H - k;
+        const double2 a = k <= kmax ? X[k] : make_double2(0.0, 0.0);
+        const double2 b =
+            (k >= 1 && kh <= kmax) ? conj2(X[kh]) : make_double2(0.0, 0.0);
+        const double2 o = __ldg(&w4[k]);
+        double2 v;
+        if (rho == 0)
+        {
+            const double2 t = cmul(o, add2(a, mul_mi(b)));
+            v = make_double2(a.x + b.x - t.y, a.y + b.y + t.x);
+        }
+        else
+        {
+            const double2 o2 = cmul(o, o);
+            const double2 o3 = cmul(o2, o);
+            const double2 u = cmul(o2, sub2(a, b));
+            const double2 t = cmul(o3, sub2(a, mul_mi(b)));
+            v = make_double2(u.x - t.y, u.y + t.x);
+        }
+        return cmul(conj2(v), __ldg(&w[k]));
+    }
+};
+
 // Bluestein kernel b_n = conj w_|n| on the circle of length M
 struct SrcKernel
 {
@@ -808,6 +850,50 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_inv(RfftArgs A)
     }
 }
 
+// Output of the quarter-length transform: the pair q of half rho of a row
+// is the conjugate of DFT value q (w_q conj of the second FFT's output q).
+struct OutRowQ
+{
+    double2 *x2;
+    const double2 *w;
+    int rho;
+    __device__ __forceinline__ void operator()(int q, double2 v) const
+    {
+        x2[2 * q + rho] = conj2(cmul(__ldg(&w[q]), conj2(v)));
+    }
+};
+
+// Synthesis of rows of length 4H with spectra below H: CTA 2 row + rho
+// computes half rho of the row (SrcQuarter), Bluestein with the plan fixed
+// at compile time.
+template <int V, int NR, int MC>
+__global__ void RFFT_BOUNDS(NR) k_rfft_inv4(RfftArgs A)
+{
+    extern __shared__ __align__(16) double2 s[];
+    const int tid = threadIdx.x;
+    const long long row = blockIdx.x >> 1;
+    const int rho = (int)(blockIdx.x & 1);
+    SrcQuarter src{A.X + row * A.ldX, A.w, A.w4, A.H, A.kmax, rho};
+    fft_ct<V, MC, 0, true>(s, A.tw, tid, src, A.bh);
+    fft_ct<V, MC, 0, false, ct_npass(MC) - 1>(s, A.tw, tid, SrcSmem{s},
+                                              nullptr);
+    fft_ct_last_out<V, MC>(
+        s, A.tw, tid, A.H,
+        OutRowQ{reinterpret_cast<double2 *>(A.x + row * A.ldx), A.w, rho});
+}
+
+// w4[k] = exp(2 pi i k / 4H), k < H
+__global__ void k_rfft_w4(int H, double2 *w4)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < H)
+    {
+        double sn, cs;
+        sincospi((double)k / (2.0 * (double)H), &sn, &cs);
+        w4[k] = make_double2(cs, sn);
+    }
+}
+
 // Tables of one transform length: twiddles exp(-2 pi i k / M), chirp
 // w_n = exp(-i pi n^2 / H) (n^2 reduced mod 2H in integers), and
 // ht_k = exp(-i pi k / H), k <= H.
@@ -871,6 +957,12 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
     return cudaGetLastError();
 }
 
+cudaError_t launch_rfft_w4(int H, double2 *w4, cudaStream_t st)
+{
+    k_rfft_w4<<<(H + 255) / 256, 256, 0, st>>>(H, w4);
+    return cudaGetLastError();
+}
+
 cudaError_t rfft_set_smem(size_t smem)
 {
     const void *fns[] = {
@@ -886,6 +978,7 @@ cudaError_t rfft_set_smem(size_t smem)
         (const void *)k_rfft_inv<16, 96, false, 9216>,
         (const void *)k_rfft_fwd<16, 96, true, 9216>,
         (const void *)k_rfft_inv<16, 96, true, 9216>,
+        (const void *)k_rfft_inv4<16, 96, 4608>,
         (const void *)k_rfft_kernel_spectrum<16, 96>};
     for (const void *f : fns)
     {
@@ -904,6 +997,15 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         return cudaSuccess;
     const size_t smem = rfft_smem_bytes(A.M);
     const int T = A.M / 16;
+    if (A.quarter)
+    {
+        // two CTAs per row (rfft plans set quarter only with M = 4608,
+        // double rows, synthesis)
+        if (!inverse || A.M != 4608 || A.f32_rows || A.direct)
+            return cudaErrorInvalidValue;
+        k_rfft_inv4<16, 96, 4608><<<2 * grid, T, smem, st>>>(A);
+        return cudaGetLastError();
+    }
     // the grids' common Bluestein lengths with the plan fixed at compile
     // time
     auto go = [&](auto mc) {

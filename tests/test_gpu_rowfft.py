@@ -5,7 +5,9 @@ CHARM_B200_ROW_FFT=library routes the longitude transforms through cuFFT
 instead; both compute the same unnormalised DFTs, so the outputs agree to a
 few units of rounding.  The grids cover every transform plan: direct
 mixed radix (H = 2^a 3^b, a >= 6), Bluestein for every other length up to
-M = 9216, and lengths where the row transform does not apply (H < 8)."""
+M = 9216, the quarter-length synthesis of rows of length 4L whose spectra
+stop below L (DH2 grids), and lengths where the row transform does not
+apply (H < 8)."""
 import os
 
 import numpy as np
@@ -43,8 +45,14 @@ def both(fn):
     ("GL", 287),    # H = 288 = 2^5 3^2, Bluestein M = 576
     ("GL", 360),    # H = 361 = 19^2, Bluestein M = 768
     ("DH1", 100),   # H = 101, Bluestein M = 256
-    ("DH2", 2190),  # H = 4382, Bluestein M = 9216, 16 values per thread
+    # DH2 rows of length 4 (N + 1): synthesis by two DFTs of length N + 1
+    # (Bluestein M = 4608) per row, analysis with H = 2 (N + 1), M = 9216
+    ("DH2", 2190),
+    ("DH2", 2160),
     ("GL", 2190),   # H = 2191, Bluestein M = 4608
+    # H = 4000, M = 9216 both ways: the spectrum reaches beyond a quarter
+    # of the row, so the quarter-length synthesis does not apply
+    ("GL", 3999),
     ("GL", 2),      # H = 3, library transform
 ])
 def test_row_transform_matches_library(cb, grid, N):
