@@ -553,7 +553,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
             const int eA = nx_e.y;
             have_next = false;
             const double rs = pow2i(51 - eA);
-            bool any_scaled = tc_prep_or(E != 0);
             const long long ncol = N - m + 1;
             const int nch = (int)((ncol + TC_CH - 1) / TC_CH);
             double mul_next = 1.0;
@@ -690,14 +689,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                     *sAbort = 1;
                 }
                 range_err |= ov >> 20;
-                if (any_scaled)
+                // scaled lanes renormalise on their own (no barrier: a
+                // lane's state does not depend on the others')
+                if (valid && E != 0 && leg_fixup(x, y, E))
                 {
-                    if (valid && leg_fixup(x, y, E))
-                    {
-                        x *= rs;
-                        y *= rs;
-                    }
-                    any_scaled = tc_prep_or(E != 0);
+                    x *= rs;
+                    y *= rs;
                 }
                 fence_proxy_async_smem();
                 mbar_arrive(&bar_a[sa]);
@@ -828,15 +825,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
             if (__any_sync(0xffffffffu,
                            item >= (unsigned long long)A.nitems || *sAbort))
                 break;
-            bool eok = mbar_wait_bounded(bar_acc, (unsigned)(k & 1),
-                                         A.status);
-            eok = __all_sync(0xffffffffu, eok);
-            if (!eok)
-            {
-                *sAbort = 1;
-                break;
-            }
-            tc_fence_after();
+            // the item's rows, grid exponent and column exponents (lane
+            // l: column l), loaded while the tensor cores finish its sums
             const long long m =
                 (long long)(item / (unsigned long long)A.ntiles);
             const int tile = (int)(item % (unsigned long long)A.ntiles);
@@ -849,6 +839,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                 rows = A.row_s[p];
                 eA = A.seed_e[m * (long long)np + p].y;
             }
+            const int ecl = __ldg(&A.ecol[m * TC_COLS + lane]);
+            bool eok = mbar_wait_bounded(bar_acc, (unsigned)(k & 1),
+                                         A.status);
+            eok = __all_sync(0xffffffffu, eok);
+            if (!eok)
+            {
+                *sAbort = 1;
+                break;
+            }
+            tc_fence_after();
             const double cpack = m == 0 ? 1.0 : 0.5;
             const double rsi = pow2i(eA - 105);
 #pragma unroll 1
@@ -886,6 +886,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                                     l2d_exact(u0) * pow2i(8 * TC_LMIN)));
                     }
                 }
+                if (cb == 2 * half + 1)
+                {
+                    // every accumulator of this warp has been read: clear
+                    // and release them before the item's outputs are written
+                    clear();
+                    tc_fence_before();
+                    mbar_arrive(bar_free);
+                }
+                int ecv[4], esv[4];
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++)
+                {
+                    ecv[kk] = __shfl_sync(0xffffffffu, ecl, 8 * cb + 2 * kk);
+                    esv[kk] =
+                        __shfl_sync(0xffffffffu, ecl, 8 * cb + 2 * kk + 1);
+                }
                 if (valid)
                 {
 #pragma unroll
@@ -894,9 +910,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                         const int set = cb * 4 + kk;
                         if (set >= A.nsets)
                             break;
-                        const int ec = __ldg(&A.ecol[m * TC_COLS + 2 * set]);
-                        const int es =
-                            __ldg(&A.ecol[m * TC_COLS + 2 * set + 1]);
+                        const int ec = ecv[kk];
+                        const int es = esv[kk];
                         const double fc = pow2i(ec) * rsi;
                         const double fs = pow2i(es) * rsi;
                         const double wgt = cpack * A.mur[set];
@@ -916,9 +931,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                     }
                 }
             }
-            clear();
-            tc_fence_before();
-            mbar_arrive(bar_free);
         }
     }
     tc_fence_before();
