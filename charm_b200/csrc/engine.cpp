@@ -703,6 +703,42 @@ Status download_tri(Context &c, const double *src, unsigned long shc_nmax,
     return st;
 }
 
+// Index of column m (C_mm) in an order-major triangle of degree N (CHarm's
+// layout, src/shc/shc_init_chunk.c:126-145).
+long long tri_start(long long N, long long m)
+{
+    return (m * (2 * N + 3 - m)) / 2;
+}
+
+// The columns m_lo <= m < m_hi of a device triangle of degree shc_nmax into
+// a charm_shc's host columns, on stream st.
+Status download_tri_orders(Context &c, const double *src,
+                           unsigned long shc_nmax, double *const *cols,
+                           long long m_lo, long long m_hi, cudaStream_t st)
+{
+    Status s2;
+    (void)c;
+    if (m_hi <= m_lo)
+        return s2;
+    const long long N = (long long)shc_nmax;
+    const double *base = contiguous_tri(cols, shc_nmax);
+    if (base)
+    {
+        const long long i0 = tri_start(N, m_lo), i1 = tri_start(N, m_hi);
+        CB_CUDA(cudaMemcpyAsync(const_cast<double *>(base) + i0, src + i0,
+                                (size_t)(i1 - i0) * 8, cudaMemcpyDeviceToHost,
+                                st),
+                s2);
+        return s2;
+    }
+    for (long long m = m_lo; m < m_hi; m++)
+        CB_CUDA(cudaMemcpyAsync(cols[m], src + tri_start(N, m),
+                                (size_t)(N + 1 - m) * 8,
+                                cudaMemcpyDeviceToHost, st),
+                s2);
+    return s2;
+}
+
 bool is_quad(int t)
 {
     return t == CHARM_CRD_POINT_GRID_GL || t == CHARM_CRD_POINT_GRID_DH1 ||
@@ -2381,6 +2417,12 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     long long slots = (long long)c.num_sms * 8 * 4;
     long long G = std::max<long long>(1, (2 * slots + nmax) / (nmax + 1));
     G = std::min<long long>(G, ntiles);
+    // a host grid is analysed in bands of tiles, overlapped with its copy:
+    // groups of single tiles (within 512 MB of partial sums) keep each
+    // band's launch balanced (shorter work items)
+    if (!d_fin)
+        G = std::max<long long>(
+            G, std::min<long long>(ntiles, (512LL << 20) / (16 * T)));
     int tpg = (int)((ntiles + G - 1) / G);
     G = (ntiles + tpg - 1) / tpg;
     double2 *part = nullptr;
@@ -2438,85 +2480,6 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     A.counter = d_counter;
     A.status = d_status;
 
-    // Host input through the row transform: bands of tile groups; band b's
-    // rows are copied (copy stream) while band b - 1 is transformed and
-    // analysed.  The partial sums of every group are the same as in one
-    // launch.
-    std::vector<std::array<int, 6>> bands;
-    const int nband = (fdev && rf) ? grid_bands(P, (int)nlat, (int)G,
-                                                32 * K * tpg,
-                                                G >= 3 ? 3 : 2, bands)
-                                   : 1;
-    if (nband > 1)
-    {
-        unsigned long long *bcnt = nullptr;
-        CB_TRY(dbuf(c, "band_counters", 8, &bcnt));
-        CB_CUDA(cudaMemsetAsync(bcnt, 0, 8 * sizeof(unsigned long long),
-                                c.stream), st);
-        // the copy stream starts after everything before it on the stream
-        // (buffers in use by an earlier call)
-        CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
-        CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
-        for (int b = 0; b < nband; b++)
-        {
-            const auto &bd = bands[b];
-            for (int h = 0; h < 2; h++)
-            {
-                const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
-                if (r1 > r0)
-                    CB_CUDA(cudaMemcpyAsync(fdev + (size_t)r0 * nlon,
-                                            f_host + (size_t)r0 * nlon,
-                                            (size_t)(r1 - r0) * nlon * 8,
-                                            cudaMemcpyHostToDevice,
-                                            c.copy_stream),
-                            st);
-            }
-            CB_CUDA(cudaEventRecord(c.band_ev[b], c.copy_stream), st);
-            CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[b], 0), st);
-            for (int h = 0; h < 2; h++)
-            {
-                const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
-                if (r1 > r0)
-                    CB_TRY(rows_fft(r0, r1));
-            }
-            ShaGridArgs Ab = A;
-            Ab.group0 = bd[0];
-            Ab.ngroups = bd[1] - bd[0];
-            Ab.nitems = (long long)(nmax + 1) * Ab.ngroups;
-            Ab.counter = bcnt + b;
-            const int gb = (int)std::min<long long>((Ab.nitems + 3) / 4,
-                                                    (long long)c.num_sms * 8);
-            Scope sc(c, TIMER_SHA);
-            CB_CUDA(launch_sha_grid(Ab, K, std::max(gb, 1), c.stream), st);
-        }
-    }
-    else
-    {
-        if (fdev)
-            CB_CUDA(cudaMemcpyAsync(fdev, f_host, nlat * nlon * 8,
-                                    cudaMemcpyHostToDevice, c.stream), st);
-        if (rf)
-            CB_TRY(rows_fft(0, (int)nlat));
-        else
-        {
-            cufftHandle h;
-            CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
-            Scope sc(c, TIMER_FFT, false);
-            if (cufftExecD2Z(h, const_cast<double *>(fg),
-                             reinterpret_cast<cufftDoubleComplex *>(F)) !=
-                CUFFT_SUCCESS)
-            {
-                st.code = CHARM_EFUNCARG;
-                st.msg = "cuFFT D2Z failed";
-                return st;
-            }
-        }
-        int grid = (int)std::min<long long>((A.nitems + 3) / 4,
-                                            (long long)c.num_sms * 8);
-        Scope sc(c, TIMER_SHA);
-        CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
-    }
-
     // rescaling from r0 to the coefficients' radius
     // (src/sha/sha_point.c:1088-1108 with src/shc/shc_rescale.c)
     const unsigned long sn = shc_nmax;
@@ -2546,6 +2509,155 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         CB_TRY(dbuf(c, "shc_out", (size_t)(2 * Ts), &dout));
         oc = dout;
         os = dout + Ts;
+    }
+
+    // Host input through the row transform: bands of tile groups; band b's
+    // rows are copied (copy stream) while band b - 1 is transformed and
+    // analysed.  The partial sums of every group are the same as in one
+    // launch.  With host outputs the last band runs in bands of orders,
+    // each reduced and copied to the host (copy stream) while the next one
+    // is analysed.
+    std::vector<std::array<int, 6>> bands;
+    const int nband = (fdev && rf) ? grid_bands(P, (int)nlat, (int)G,
+                                                32 * K * tpg,
+                                                G >= 3 ? 3 : 2, bands)
+                                   : 1;
+    bool ordered = false;
+    if (nband > 1)
+    {
+        // orders of the last band in up to four bands of about equal
+        // numbers of coefficients
+        std::vector<long long> mb{0};
+        if (!d_c)
+        {
+            const int nob = 4;
+            for (int k = 1; k < nob; k++)
+            {
+                long long m = mb.back();
+                while (m <= (long long)nmax &&
+                       tri_start((long long)nmax, m) < k * T / nob)
+                    m++;
+                if (m > mb.back() && m <= (long long)nmax)
+                    mb.push_back(m);
+            }
+        }
+        mb.push_back((long long)nmax + 1);
+        const int nob = (int)mb.size() - 1;
+        unsigned long long *bcnt = nullptr;
+        CB_TRY(dbuf(c, "band_counters", 16, &bcnt));
+        CB_CUDA(cudaMemsetAsync(bcnt, 0, 16 * sizeof(unsigned long long),
+                                c.stream), st);
+        // the copy stream starts after everything before it on the stream
+        // (buffers in use by an earlier call)
+        CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
+        CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+        for (int b = 0; b < nband; b++)
+        {
+            const auto &bd = bands[b];
+            for (int h = 0; h < 2; h++)
+            {
+                const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
+                if (r1 > r0)
+                    CB_CUDA(cudaMemcpyAsync(fdev + (size_t)r0 * nlon,
+                                            f_host + (size_t)r0 * nlon,
+                                            (size_t)(r1 - r0) * nlon * 8,
+                                            cudaMemcpyHostToDevice,
+                                            c.copy_stream),
+                            st);
+            }
+            CB_CUDA(cudaEventRecord(c.band_ev[b], c.copy_stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[b], 0), st);
+            for (int h = 0; h < 2; h++)
+            {
+                const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
+                if (r1 > r0)
+                    CB_TRY(rows_fft(r0, r1));
+            }
+            const bool split = b == nband - 1 && nob > 1;
+            for (int k = 0; k < (split ? nob : 1); k++)
+            {
+                ShaGridArgs Ab = A;
+                Ab.group0 = bd[0];
+                Ab.ngroups = bd[1] - bd[0];
+                Ab.m0 = split ? mb[k] : 0;
+                Ab.nitems = (long long)(split ? mb[k + 1] - mb[k]
+                                              : (long long)nmax + 1) *
+                            Ab.ngroups;
+                Ab.counter = bcnt + (split ? nband + k : b);
+                const int gb = (int)std::min<long long>(
+                    (Ab.nitems + 3) / 4, (long long)c.num_sms * 8);
+                {
+                    Scope sc(c, TIMER_SHA);
+                    CB_CUDA(launch_sha_grid(Ab, K, std::max(gb, 1), c.stream),
+                            st);
+                }
+                if (split)
+                {
+                    // these orders are complete: their coefficients (with
+                    // the zero orders above nmax after the last band)
+                    const long long m_hi =
+                        k == nob - 1 ? (long long)sn + 1 : mb[k + 1];
+                    Scope sc(c, TIMER_PREP);
+                    CB_CUDA(launch_sha_reduce_orders(
+                                (long long)nmax, (long long)sn, (int)G, T,
+                                part, tab.tc, dres, 1.0, oc, os, mb[k], m_hi,
+                                c.stream),
+                            st);
+                    CB_CUDA(cudaEventRecord(c.band_ev[3 + k], c.stream), st);
+                }
+            }
+            if (split)
+            {
+                // the copies after every launch, so that a copy to pageable
+                // memory, which returns only when it is done, holds back no
+                // launch
+                for (int k = 0; k < nob; k++)
+                {
+                    const long long m_hi =
+                        k == nob - 1 ? (long long)sn + 1 : mb[k + 1];
+                    CB_CUDA(cudaStreamWaitEvent(c.copy_stream,
+                                                c.band_ev[3 + k], 0),
+                            st);
+                    CB_TRY(download_tri_orders(c, oc, sn, hc, mb[k], m_hi,
+                                               c.copy_stream));
+                    CB_TRY(download_tri_orders(c, os, sn, hs, mb[k], m_hi,
+                                               c.copy_stream));
+                }
+                ordered = true;
+            }
+        }
+    }
+    else
+    {
+        if (fdev)
+            CB_CUDA(cudaMemcpyAsync(fdev, f_host, nlat * nlon * 8,
+                                    cudaMemcpyHostToDevice, c.stream), st);
+        if (rf)
+            CB_TRY(rows_fft(0, (int)nlat));
+        else
+        {
+            cufftHandle h;
+            CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
+            Scope sc(c, TIMER_FFT, false);
+            if (cufftExecD2Z(h, const_cast<double *>(fg),
+                             reinterpret_cast<cufftDoubleComplex *>(F)) !=
+                CUFFT_SUCCESS)
+            {
+                st.code = CHARM_EFUNCARG;
+                st.msg = "cuFFT D2Z failed";
+                return st;
+            }
+        }
+        int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                            (long long)c.num_sms * 8);
+        Scope sc(c, TIMER_SHA);
+        CB_CUDA(launch_sha_grid(A, K, std::max(grid, 1), c.stream), st);
+    }
+
+    if (ordered)
+    {
+        CB_CUDA(cudaStreamSynchronize(c.copy_stream), st);
+        return finish(c, d_status);
     }
     {
         Scope sc(c, TIMER_PREP);

@@ -74,6 +74,8 @@ struct ShaGridArgs
     int ntiles;            // latitude tiles per order
     int ngroups;           // tile groups per order in this launch
     int group0;            // first group of this launch (partial sums)
+    long long m0;          // first order of this launch (items: orders
+                           // m0, m0 + 1, ... times ngroups)
     int tiles_per_group;
     long long nitems;      // (nmax + 1) * ngroups
     const double2 *tb;
@@ -230,6 +232,13 @@ cudaError_t launch_sha_grid(const ShaGridArgs &A, int K, int grid,
 // points with their own radii
 cudaError_t launch_sha_points(const ShaGridArgs &A, int src, int K, int grid,
                               cudaStream_t st);
+// k_sha_reduce for the orders [m_lo, m_hi) only
+cudaError_t launch_sha_reduce_orders(long long nmax, long long shc_nmax,
+                                     int ngroups, long long T,
+                                     const double2 *part, const double *tc,
+                                     const double *rescale, double scale,
+                                     double *c, double *s, long long m_lo,
+                                     long long m_hi, cudaStream_t st);
 cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                               long long T, const double2 *part,
                               const double *tc, const double *rescale,

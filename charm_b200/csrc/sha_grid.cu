@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= (unsigned long long)A.nitems)
             break;
-        const long long m = (long long)(item / (unsigned long long)A.ngroups);
+        const long long m =
+            A.m0 + (long long)(item / (unsigned long long)A.ngroups);
         const int g =
             A.group0 + (int)(item % (unsigned long long)A.ngroups);
         const long long c0 = tri_col0(N, m);

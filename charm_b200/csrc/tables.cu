@@ -176,9 +176,9 @@ __global__ void k_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                              long long T, const double2 *__restrict__ part,
                              const double *__restrict__ tc,
                              const double *__restrict__ rescale, double scale,
-                             double *c, double *s)
+                             double *c, double *s, long long m_lo)
 {
-    long long m = blockIdx.x;
+    long long m = m_lo + blockIdx.x;
     if (m > shc_nmax)
         return;
     long long d0 = tri_col0(shc_nmax, m);
@@ -246,7 +246,21 @@ cudaError_t launch_sha_reduce(long long nmax, long long shc_nmax, int ngroups,
                               cudaStream_t st)
 {
     k_sha_reduce<<<(int)(shc_nmax + 1), 128, 0, st>>>(
-        nmax, shc_nmax, ngroups, T, part, tc, rescale, scale, c, s);
+        nmax, shc_nmax, ngroups, T, part, tc, rescale, scale, c, s, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sha_reduce_orders(long long nmax, long long shc_nmax,
+                                     int ngroups, long long T,
+                                     const double2 *part, const double *tc,
+                                     const double *rescale, double scale,
+                                     double *c, double *s, long long m_lo,
+                                     long long m_hi, cudaStream_t st)
+{
+    if (m_hi <= m_lo)
+        return cudaSuccess;
+    k_sha_reduce<<<(int)(m_hi - m_lo), 128, 0, st>>>(
+        nmax, shc_nmax, ngroups, T, part, tc, rescale, scale, c, s, m_lo);
     return cudaGetLastError();
 }
 

@@ -1,15 +1,18 @@
 """Host-array entry points with the grid copied in bands: charm_shs_point
 copies the rows of each band of latitude tiles to the host while the next
 band is synthesised, charm_sha_point copies band b while band b - 1 is
-transformed and analysed.  Every work item computes the same sums as in one
-launch, so the results equal those of the device-array entry points bit for
-bit."""
+transformed and analysed, and copies the coefficients to the host in bands
+of orders while the last band is analysed.  Synthesis work items compute the
+same sums as in one launch, so the grids equal those of the device-array
+entry point bit for bit.  The analysis of a host grid adds its partial sums
+in groups of single latitude tiles (the device-array entry point in larger
+groups), so its coefficients agree to rounding: 1e-14 relative RMS."""
 import ctypes as ct
 
 import numpy as np
 import pytest
 
-from charm_b200.workloads import GM, R_EARTH, kaula
+from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula
 
 pytestmark = pytest.mark.gpu
 
@@ -73,5 +76,8 @@ def test_host_paths_equal_device_paths(env, grid, N, h):
     if h == 0.0:
         out = cb.sha_point(p, f_host, N, GM, R_EARTH)
         oc, os_ = device_sha(env, p, f_host, N)
-        assert np.array_equal(out.c, oc)
-        assert np.array_equal(out.s, os_)
+        assert coef_rel_rms(out.c, out.s, oc, os_) <= 1e-14
+        # every coefficient, not only the RMS
+        scale = np.max(np.abs(np.concatenate([oc, os_])))
+        assert np.max(np.abs(out.c - oc)) <= 1e-13 * scale
+        assert np.max(np.abs(out.s - os_)) <= 1e-13 * scale
