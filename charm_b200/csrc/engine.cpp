@@ -710,6 +710,33 @@ long long tri_start(long long N, long long m)
     return (m * (2 * N + 3 - m)) / 2;
 }
 
+// The columns m_lo <= m < m_hi of a charm_shc's host columns into a device
+// triangle of degree shc_nmax, on stream st.
+Status upload_tri_orders(double *const *cols, unsigned long shc_nmax,
+                         double *dst, long long m_lo, long long m_hi,
+                         cudaStream_t st)
+{
+    Status s2;
+    if (m_hi <= m_lo)
+        return s2;
+    const long long N = (long long)shc_nmax;
+    const double *base = contiguous_tri(cols, shc_nmax);
+    if (base)
+    {
+        const long long i0 = tri_start(N, m_lo), i1 = tri_start(N, m_hi);
+        CB_CUDA(cudaMemcpyAsync(dst + i0, base + i0, (size_t)(i1 - i0) * 8,
+                                cudaMemcpyHostToDevice, st),
+                s2);
+        return s2;
+    }
+    for (long long m = m_lo; m < m_hi; m++)
+        CB_CUDA(cudaMemcpyAsync(dst + tri_start(N, m), cols[m],
+                                (size_t)(N + 1 - m) * 8,
+                                cudaMemcpyHostToDevice, st),
+                s2);
+    return s2;
+}
+
 // The columns m_lo <= m < m_hi of a device triangle of degree shc_nmax into
 // a charm_shc's host columns, on stream st.
 Status download_tri_orders(Context &c, const double *src,
@@ -857,6 +884,16 @@ bool autotune_on()
         return !(e && std::strcmp(e, "0") == 0);
     }();
     return on;
+}
+
+// True when tune_shs_k launches nothing for this shape (tuned already, or
+// not tuned at all), so that the call's coefficients need not all be on
+// the device before its first synthesis launch.
+bool shs_k_settled(Context &c, int kgrad, int dr, int dlat, bool rr,
+                   long long nmax, int np)
+{
+    const auto key = std::make_tuple(kgrad, dr, dlat, rr ? 1 : 0, nmax, np);
+    return c.tuned.count(key) > 0 || !autotune_on() || nmax < 256;
 }
 
 Status tune_shs_k(Context &c, const ShsGridArgs &A0, int kgrad, int dr,
@@ -1185,8 +1222,22 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
 
     Tabs tab;
     CB_TRY(tables(c, (long long)nmax, &tab));
+    // Host coefficients of a call whose grid goes to the host are uploaded
+    // later, in bands of orders overlapped with the synthesis of the first
+    // band of latitudes (when the call runs in bands), else all now.
     double2 *dcs = nullptr;
-    CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
+    double *raw = nullptr;
+    const long long Ts = (long long)(in.nmax + 1) * (in.nmax + 2) / 2;
+    bool coef_later =
+        !in.dc && !d_f &&
+        shs_k_settled(c, kgrad, dr, dlat, !r_eq, (long long)nmax, np);
+    if (coef_later)
+    {
+        CB_TRY(dbuf(c, "cs", (size_t)((nmax + 1) * (nmax + 2) / 2), &dcs));
+        CB_TRY(dbuf(c, "shc_in", (size_t)(2 * Ts), &raw));
+    }
+    else
+        CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
 
     // lumped coefficients
     const int ldf = use_fft ? (int)(nlon / 2 + 1) : (int)(nmax + 1);
@@ -1257,23 +1308,84 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
         (!d_f && rf) ? grid_bands(P, (int)nlat, ntiles, 32 * K,
                                   ntiles >= 6 ? 3 : 2, bands)
                      : 1;
+    if (coef_later && nband <= 1)
+    {
+        // no bands: every coefficient now
+        CB_TRY(upload_tri(c, in.hc, in.nmax, raw));
+        CB_TRY(upload_tri(c, in.hs, in.nmax, raw + Ts));
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_scale_cs((long long)nmax, (long long)in.nmax, raw,
+                                raw + Ts, tab.tc, dcs, c.stream),
+                st);
+        coef_later = false;
+    }
     if (nband > 1)
     {
         unsigned long long *bcnt = nullptr;
-        CB_TRY(dbuf(c, "band_counters", 8, &bcnt));
-        CB_CUDA(cudaMemsetAsync(bcnt, 0, 8 * sizeof(unsigned long long),
+        CB_TRY(dbuf(c, "band_counters", 16, &bcnt));
+        CB_CUDA(cudaMemsetAsync(bcnt, 0, 16 * sizeof(unsigned long long),
                                 c.stream), st);
+        // orders in up to four bands of about equal numbers of coefficients
+        std::vector<long long> mb{0};
+        if (coef_later)
+        {
+            const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
+            for (int k = 1; k < 4; k++)
+            {
+                long long m = mb.back();
+                while (m <= (long long)nmax &&
+                       tri_start((long long)nmax, m) < k * T / 4)
+                    m++;
+                if (m > mb.back() && m <= (long long)nmax)
+                    mb.push_back(m);
+            }
+            // the copy stream starts after everything before it on the
+            // stream; band k of the orders: copy (copy stream), then scale
+            CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+        }
+        mb.push_back((long long)nmax + 1);
+        const int nob = (int)mb.size() - 1;
+        if (coef_later)
+            for (int k = 0; k < nob; k++)
+            {
+                CB_TRY(upload_tri_orders(in.hc, in.nmax, raw, mb[k],
+                                         mb[k + 1], c.copy_stream));
+                CB_TRY(upload_tri_orders(in.hs, in.nmax, raw + Ts, mb[k],
+                                         mb[k + 1], c.copy_stream));
+                CB_CUDA(cudaEventRecord(c.band_ev[3 + k], c.copy_stream),
+                        st);
+            }
         for (int b = 0; b < nband; b++)
         {
             const auto &bd = bands[b];
-            ShsGridArgs Ab = A;
-            Ab.tile0 = bd[0];
-            Ab.ntiles = bd[1] - bd[0];
-            Ab.nitems = (long long)(nmax + 1) * Ab.ntiles;
-            Ab.counter = bcnt + b;
-            const int gb = (int)std::min<long long>((Ab.nitems + 3) / 4,
-                                                    (long long)c.num_sms * 8);
+            // the first band synthesises each band of orders as soon as its
+            // coefficients are on the device
+            const bool split = b == 0 && coef_later;
+            for (int k = 0; k < (split ? nob : 1); k++)
             {
+                if (split)
+                {
+                    CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[3 + k],
+                                                0),
+                            st);
+                    Scope sc(c, TIMER_PREP);
+                    CB_CUDA(launch_scale_cs_orders(
+                                (long long)nmax, (long long)in.nmax, raw,
+                                raw + Ts, tab.tc, dcs, mb[k], mb[k + 1],
+                                c.stream),
+                            st);
+                }
+                ShsGridArgs Ab = A;
+                Ab.tile0 = bd[0];
+                Ab.ntiles = bd[1] - bd[0];
+                Ab.m0 = split ? mb[k] : 0;
+                Ab.nitems = (long long)(split ? mb[k + 1] - mb[k]
+                                              : (long long)nmax + 1) *
+                            Ab.ntiles;
+                Ab.counter = bcnt + (split ? 8 + k : b);
+                const int gb = (int)std::min<long long>(
+                    (Ab.nitems + 3) / 4, (long long)c.num_sms * 8);
                 Scope sc(c, TIMER_SHS);
                 CB_CUDA(launch_shs_grid(Ab, kgrad, dr, dlat, !r_eq, K,
                                         std::max(gb, 1), c.stream), st);

@@ -39,6 +39,7 @@ struct ShsGridArgs
     int npairs;            // evaluated latitudes (north rows of the pairs)
     int ntiles;            // latitude tiles per order in this launch
     int tile0;             // first tile of this launch
+    long long m0;          // first order of this launch (single set)
     long long nitems;      // (nmax + 1) * ntiles
     const double2 *tb;     // (beta_n, e_n / a_n) per (n, m), order-major
     const double *tmul;    // chunk entry multipliers [m][chunk]
@@ -212,6 +213,12 @@ cudaError_t launch_tables(long long nmax, const double *r, const double *ri,
                           const double *smm, double2 *tb, double *tc,
                           double *tmul, int ldmul, double *sg,
                           cudaStream_t st);
+// k_scale_cs for the orders [m_lo, m_hi) only
+cudaError_t launch_scale_cs_orders(long long nmax, long long shc_nmax,
+                                   const double *c, const double *s,
+                                   const double *tc, double2 *cs,
+                                   long long m_lo, long long m_hi,
+                                   cudaStream_t st);
 cudaError_t launch_scale_cs(long long nmax, long long shc_nmax,
                             const double *c, const double *s,
                             const double *tc, double2 *cs, cudaStream_t st);

@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(128) k_shs_grid(ShsGridArgs A)
             polar_thr = bs.polar_thr;
             local = item - (unsigned long long)bs.item0;
         }
-        const long long m = (long long)(local / (unsigned long long)A.ntiles);
+        const long long m =
+            A.m0 + (long long)(local / (unsigned long long)A.ntiles);
         const int tile =
             A.tile0 + (int)(local % (unsigned long long)A.ntiles);
         const double sigma = A.sg[2 * m];

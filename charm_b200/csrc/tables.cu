@@ -127,9 +127,10 @@ __global__ void k_tables(long long nmax, const double *__restrict__ r,
 __global__ void k_scale_cs(long long nmax, long long shc_nmax,
                            const double *__restrict__ c,
                            const double *__restrict__ s,
-                           const double *__restrict__ tc, double2 *cs)
+                           const double *__restrict__ tc, double2 *cs,
+                           long long m_lo)
 {
-    long long m = blockIdx.x;
+    long long m = m_lo + blockIdx.x;
     if (m > nmax)
         return;
     long long c0 = tri_col0(nmax, m);
@@ -235,7 +236,21 @@ cudaError_t launch_scale_cs(long long nmax, long long shc_nmax,
                             const double *c, const double *s,
                             const double *tc, double2 *cs, cudaStream_t st)
 {
-    k_scale_cs<<<(int)(nmax + 1), 128, 0, st>>>(nmax, shc_nmax, c, s, tc, cs);
+    k_scale_cs<<<(int)(nmax + 1), 128, 0, st>>>(nmax, shc_nmax, c, s, tc, cs,
+                                                0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_cs_orders(long long nmax, long long shc_nmax,
+                                   const double *c, const double *s,
+                                   const double *tc, double2 *cs,
+                                   long long m_lo, long long m_hi,
+                                   cudaStream_t st)
+{
+    if (m_hi <= m_lo)
+        return cudaSuccess;
+    k_scale_cs<<<(int)(m_hi - m_lo), 128, 0, st>>>(nmax, shc_nmax, c, s, tc,
+                                                   cs, m_lo);
     return cudaGetLastError();
 }
 
