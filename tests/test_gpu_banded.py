@@ -81,3 +81,58 @@ def test_host_paths_equal_device_paths(env, grid, N, h):
         scale = np.max(np.abs(np.concatenate([oc, os_])))
         assert np.max(np.abs(out.c - oc)) <= 1e-13 * scale
         assert np.max(np.abs(out.s - os_)) <= 1e-13 * scale
+
+
+class ScatteredShc:
+    """A charm_shc whose columns C[m], S[m] are separate arrays (allowed by
+    CHarm's layout: one pointer per order), so that the copies go column by
+    column."""
+
+    def __init__(self, N, c, s):
+        from charm_b200._lib import _Shc
+        P = ct.POINTER(ct.c_double)
+        idx = [m * (2 * N + 3 - m) // 2 for m in range(N + 2)]
+        self.cc = [np.array(c[idx[m]:idx[m + 1]]) for m in range(N + 1)]
+        self.cs = [np.array(s[idx[m]:idx[m + 1]]) for m in range(N + 1)]
+        self.pc = (P * (N + 1))(*[a.ctypes.data_as(P) for a in self.cc])
+        self.ps = (P * (N + 1))(*[a.ctypes.data_as(P) for a in self.cs])
+        T = (N + 1) * (N + 2) // 2
+        self.st = _Shc(nmax=N, mu=GM, r=R_EARTH, nc=T, ns=T,
+                       c=ct.cast(self.pc, ct.POINTER(P)),
+                       s=ct.cast(self.ps, ct.POINTER(P)), owner=False,
+                       distributed=False)
+        self.ptr = ct.pointer(self.st)
+
+    def gather(self):
+        return np.concatenate(self.cc), np.concatenate(self.cs)
+
+
+def test_repeated_calls_and_scattered_columns(env):
+    """The second host call of a shape copies the coefficients in bands of
+    orders (the first one also runs the synthesis autotuner); a charm_shc
+    with one array per order is copied column by column.  Grids equal the
+    device-array path's bit for bit, coefficients agree to rounding."""
+    torch, cb, L = env
+    N = 600
+    p = cb.PointGridGL(N, R_EARTH)
+    c, s = kaula(N, 777)
+    f_dev = device_shs(env, p, c, s, N)
+    shc = cb.Shc(N, GM, R_EARTH, c, s)
+    for _ in range(3):
+        assert np.array_equal(cb.shs_point(p, shc, N), f_dev)
+    sc = ScatteredShc(N, c, s)
+    f = np.empty(p.lat.size * p.lon.size)
+    P = ct.POINTER(ct.c_double)
+    oc, os_ = device_sha(env, p, f_dev, N)
+    out = ScatteredShc(N, np.zeros_like(c), np.zeros_like(s))
+    fd = np.ascontiguousarray(f_dev).ravel()
+    for _ in range(2):
+        err = L.charm_err_init()
+        L.charm_shs_point(p._Point, sc.ptr, N, f.ctypes.data_as(P), err)
+        assert L.charm_err_isempty(err)
+        L.charm_sha_point(p._Point, fd.ctypes.data_as(P), N, out.ptr, err)
+        assert L.charm_err_isempty(err)
+        L.charm_err_free(err)
+        assert np.array_equal(f.reshape(p.lat.size, p.lon.size), f_dev)
+        gc, gs = out.gather()
+        assert coef_rel_rms(gc, gs, oc, os_) <= 1e-14
