@@ -60,6 +60,10 @@ struct Context
     // host <-> device copies of grid bands, overlapped with the kernels on
     // `stream` (events order the two)
     cudaStream_t copy_stream = nullptr;
+    // events between the compute and copy streams of the banded host-array
+    // calls: 0..2 the bands of latitude tiles (grid_bands gives at most
+    // three), 3..6 the bands of orders (at most four), 7 the start of the
+    // copy stream after the work already on the compute stream
     cudaEvent_t band_ev[8] = {};
     std::map<std::string, DevBuf> bufs;
     void *pinned = nullptr;
