@@ -743,12 +743,11 @@ Status upload_tri_orders(double *const *cols, unsigned long shc_nmax,
 
 // The columns m_lo <= m < m_hi of a device triangle of degree shc_nmax into
 // a charm_shc's host columns, on stream st.
-Status download_tri_orders(Context &c, const double *src,
-                           unsigned long shc_nmax, double *const *cols,
-                           long long m_lo, long long m_hi, cudaStream_t st)
+Status download_tri_orders(const double *src, unsigned long shc_nmax,
+                           double *const *cols, long long m_lo,
+                           long long m_hi, cudaStream_t st)
 {
     Status s2;
-    (void)c;
     if (m_hi <= m_lo)
         return s2;
     const long long N = (long long)shc_nmax;
@@ -2734,9 +2733,9 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                     CB_CUDA(cudaStreamWaitEvent(c.copy_stream,
                                                 c.band_ev[3 + k], 0),
                             st);
-                    CB_TRY(download_tri_orders(c, oc, sn, hc, mb[k], m_hi,
+                    CB_TRY(download_tri_orders(oc, sn, hc, mb[k], m_hi,
                                                c.copy_stream));
-                    CB_TRY(download_tri_orders(c, os, sn, hs, mb[k], m_hi,
+                    CB_TRY(download_tri_orders(os, sn, hs, mb[k], m_hi,
                                                c.copy_stream));
                 }
                 ordered = true;
