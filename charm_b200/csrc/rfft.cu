@@ -16,14 +16,20 @@
 //     a circular convolution of length M >= 2H - 1, M = 2^a 3^b, evaluated
 //     as FFT_M, a pointwise product with the precomputed FFT_M of the chirp,
 //     and a second FFT_M (conjugated in and out, which inverts it);
-//   * FFT_M by in-place Stockham autosort passes of radix 8, 4, 2 and 3:
-//     every thread holds V values across the barrier that separates the
-//     loads of a pass from its stores, so one buffer of M values suffices.
-//     The first pass reads its inputs straight from global memory (with the
-//     chirp applied), and the last pass of the first FFT applies the
-//     pointwise product as it stores.  Element i lives at i + i/8 in shared
-//     memory, which spreads the strided stores of the first pass over all
-//     banks.
+//   * FFT_M by in-place Stockham autosort passes (radix 8, 4, 2 and 3 in
+//     the run-time plans; 16, 16, 18 for M = 4608 and 16, 16, 9, 4 for
+//     M = 9216 in the compile-time ones): every thread holds V values
+//     across the barrier that separates the loads of a pass from its
+//     stores, so one buffer of M values suffices.  The first pass reads its
+//     inputs straight from global memory (with the chirp applied; the zero
+//     half of the chirped sequence is skipped), and the last pass of the
+//     first FFT applies the pointwise product as it stores.  In synthesis
+//     the last pass of the second FFT writes the row itself.  Element i
+//     lives at i + i/8 in shared memory, which spreads the strided stores
+//     of the first pass over the banks;
+//   * rows of length 4L whose spectra stop below L (DH2 synthesis): two
+//     complex DFTs of length L per row, each computing every other pair of
+//     the row (k_rfft_inv4, two CTAs per row).
 //
 // Both directions are unnormalised, as FFTW's and CHarm's: the synthesis
 // output is sum_k X_k e^(+2 pi i k n / L) over the Hermitian spectrum, and
