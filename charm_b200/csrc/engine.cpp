@@ -1,10 +1,13 @@
 // Host runtime of charm_b200 (see engine.h).
 //
-// One process-wide context per CUDA device: a stream, grow-only device
-// buffers, cached recurrence tables per maximum degree, cached cuFFT plans
-// and a pinned staging area for the small per-call arrays.  Calls are
-// serialised by a mutex.  Every call ends with a synchronisation of the
-// stream and a check of the device status word written by the kernels.
+// One process-wide context per CUDA device: a compute stream and a copy
+// stream (the host-array calls copy their grids and coefficients in bands
+// there, ordered against the kernels by events), grow-only device buffers,
+// cached recurrence tables per maximum degree, cached row-transform and
+// cuFFT plans and a pinned staging area for the small per-call arrays.
+// Calls are serialised by a mutex.  Every call ends with a synchronisation
+// of its streams and a check of the device status word written by the
+// kernels.
 #include "engine.h"
 
 #include <cuda_runtime.h>
