@@ -68,6 +68,8 @@ struct Context
     // three), 3..6 the bands of orders (at most four), 7 the start of the
     // copy stream after the work already on the compute stream
     cudaEvent_t band_ev[8] = {};
+    // page-locked copy of the device status word read at the end of a call
+    unsigned *h_status = nullptr;
     std::map<std::string, DevBuf> bufs;
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
@@ -218,6 +220,12 @@ Status init(Context &c)
     for (cudaEvent_t &e : c.band_ev)
         if (!e)
             CB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), st);
+    if (!c.h_status)
+    {
+        void *hp = nullptr;
+        CB_CUDA(cudaHostAlloc(&hp, 64, cudaHostAllocDefault), st);
+        c.h_status = static_cast<unsigned *>(hp);
+    }
     c.ready = true;
     return st;
 }
@@ -967,10 +975,13 @@ Status finish(Context &c, unsigned *d_status)
     Status st;
     if (c.capturing)
         return st;   // read by batch_graph_launch after each replay
-    unsigned h_status = 0;
-    CB_CUDA(cudaMemcpyAsync(&h_status, d_status, sizeof(unsigned),
+    // into page-locked memory, so the copy is queued like a kernel and the
+    // one synchronisation below covers both
+    *c.h_status = 0u;
+    CB_CUDA(cudaMemcpyAsync(c.h_status, d_status, sizeof(unsigned),
                             cudaMemcpyDeviceToHost, c.stream), st);
     CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    const unsigned h_status = *c.h_status;
     if (c.timing)
         resolve_timers(c);
     if (h_status)
@@ -3492,6 +3503,9 @@ void shutdown()
         cudaFreeHost(c.pinned);
     c.pinned = nullptr;
     c.pinned_bytes = 0;
+    if (c.h_status)
+        cudaFreeHost(c.h_status);
+    c.h_status = nullptr;
     c.tab_nmax = -1;
     c.ready = false;
 }
