@@ -48,6 +48,21 @@ bool nearly_equal(double a, double b, double eps)
     return d / std::max(aa, ba) <= eps;
 }
 
+// Every a[i] nearly_equal to ref: an exact scan first (the common case, a
+// grid on one sphere), the element-wise test only when that fails.
+bool all_nearly_equal(const double *a, size_t n, double ref, double eps)
+{
+    bool exact = true;
+    for (size_t i = 0; i < n; i++)
+        exact &= (a[i] == ref);
+    if (exact)
+        return true;
+    for (size_t i = 0; i < n; i++)
+        if (!nearly_equal(a[i], ref, eps))
+            return false;
+    return true;
+}
+
 struct DevBuf
 {
     void *p = nullptr;
@@ -1183,13 +1198,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
                    nearly_equal(pnt->lon[nlon - 1] + dlon_step, 2.0 * PI, thr);
 
     // r == R everywhere selects the faster kernels (shs_r_eq_rref.c)
-    bool r_eq = true;
-    for (size_t i = 0; i < nlat; i++)
-        if (!nearly_equal(pnt->r[i], in.r, thr))
-        {
-            r_eq = false;
-            break;
-        }
+    const bool r_eq = all_nearly_equal(pnt->r, nlat, in.r, thr);
     Pairs P;
     grid_pairs(pnt, thr2, true, P);
     if (!r_eq)
@@ -1221,8 +1230,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     for (int p = 0; p < np; p++)
     {
         double la = pnt->lat[P.row_n[p]];
-        ht[p] = std::sin(la);
-        hu[p] = std::cos(la);
+        sincos(la, &ht[p], &hu[p]);
         hrho[p] = r_eq ? 1.0 : in.r / pnt->r[P.row_n[p]];
         hrn[p] = P.row_n[p];
         hrs[p] = P.row_s[p];
@@ -1504,13 +1512,8 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
 {
     Status st;
     const size_t npt = pnt->nlat;
-    bool r_eq = true;
-    for (size_t i = 0; i < npt; i++)
-        if (!nearly_equal(pnt->r[i], in.r, charm_glob_threshold))
-        {
-            r_eq = false;
-            break;
-        }
+    const bool r_eq =
+        all_nearly_equal(pnt->r, npt, in.r, charm_glob_threshold);
     double mur;
     int dorder, npar;
     mur_dorder(in.mu, in.r, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
@@ -1610,13 +1613,7 @@ Status batch_geometry(Context &c, const charm_point *pnt, unsigned long N,
                  "(0, 2 pi / nlon, ..., nlon > 2 nmax).";
         return st;
     }
-    bool r_eq = true;
-    for (size_t i = 0; i < nlat; i++)
-        if (!nearly_equal(pnt->r[i], R, thr))
-        {
-            r_eq = false;
-            break;
-        }
+    const bool r_eq = all_nearly_equal(pnt->r, nlat, R, thr);
     Pairs &P = G->P;
     grid_pairs(pnt, thr2, true, P);
     if (!r_eq)
@@ -1639,8 +1636,7 @@ Status batch_geometry(Context &c, const charm_point *pnt, unsigned long N,
     for (int p = 0; p < np; p++)
     {
         double la = pnt->lat[P.row_n[p]];
-        ht[p] = std::sin(la);
-        hu[p] = std::cos(la);
+        sincos(la, &ht[p], &hu[p]);
         hrho[p] = r_eq ? 1.0 : R / pnt->r[P.row_n[p]];
         hrn[p] = P.row_n[p];
         hrs[p] = P.row_s[p];
@@ -2178,8 +2174,7 @@ Status shs_grid_f32(Context &c, const charm_point *pnt, unsigned long shc_nmax,
     for (int p = 0; p < np; p++)
     {
         double la = pnt->lat[P.row_n[p]];
-        ht[p] = std::sin(la);
-        hu[p] = std::cos(la);
+        sincos(la, &ht[p], &hu[p]);
         hrn[p] = P.row_n[p];
         hrs[p] = P.row_s[p];
     }
@@ -2282,8 +2277,7 @@ Status sha_grid_f32(Context &c, const charm_point *pnt, const float *d_f,
     for (int p = 0; p < np; p++)
     {
         double la = pnt->lat[P.row_n[p]];
-        ht[p] = std::sin(la);
-        hu[p] = std::cos(la);
+        sincos(la, &ht[p], &hu[p]);
         hcn[p] = cq * pnt->w[P.row_n[p]];
         hcs[p] = P.row_s[p] >= 0 ? cq * pnt->w[P.row_s[p]] : 0.0;
         hrn[p] = P.row_n[p];
@@ -2391,13 +2385,7 @@ Status sctr_adjoint(Context &c, const charm_point *pnt, const double *g_host,
 {
     Status st;
     const size_t npt = pnt->nlat;
-    bool r_eq = true;
-    for (size_t i = 0; i < npt; i++)
-        if (!nearly_equal(pnt->r[i], R, charm_glob_threshold))
-        {
-            r_eq = false;
-            break;
-        }
+    const bool r_eq = all_nearly_equal(pnt->r, npt, R, charm_glob_threshold);
     Tabs tab;
     CB_TRY(tables(c, (long long)nmax, &tab));
     double *dpts = nullptr;
@@ -2514,8 +2502,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     for (int p = 0; p < np; p++)
     {
         double la = pnt->lat[P.row_n[p]];
-        ht[p] = std::sin(la);
-        hu[p] = std::cos(la);
+        sincos(la, &ht[p], &hu[p]);
         hcn[p] = cq * pnt->w[P.row_n[p]];
         hcs[p] = P.row_s[p] >= 0 ? cq * pnt->w[P.row_s[p]] : 0.0;
         hrn[p] = P.row_n[p];
