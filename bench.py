@@ -9,7 +9,10 @@ One step = one SHS + SHA round trip.  "value" is seconds per round trip with
 the coefficients and the grid resident in HBM (device-timed with CUDA
 events on the library's stream, L2 flushed between steps by a 256 MiB
 write); "e2e" is the same round trip through the C ABI with pinned host
-buffers, host<->device copies included.  With --gpus N > 1 (torchrun) every
+buffers, host<->device copies included (with, measured after the timed
+region, each host-array call alone, the pinned copy bandwidths and the
+time the round trip's copies alone take at them).  With --gpus N > 1
+(torchrun) every
 rank runs its own round trips (replicas, no collective on the data path);
 value = max-over-ranks time / (N * K).
 
@@ -290,6 +293,42 @@ def run_ours(args):
     e2e_ms = max_over_ranks(f0.elapsed_time(f1), dev)
     rt_e2e = coef_rel_rms(oc.numpy(), os_.numpy(), c, s)
 
+    # where the end-to-end time goes (after the timed region): each
+    # host-array call alone (they return with their streams idle) and the
+    # pinned copy bandwidths that bound them
+    def call_ms(fn, reps=5):
+        ts = []
+        for _ in range(reps):
+            t1 = time.perf_counter()
+            fn()
+            check()
+            ts.append(time.perf_counter() - t1)
+        return 1e3 * float(np.median(ts))
+    shs_call_ms = call_ms(lambda: L.charm_shs_point(
+        pnt._Point, shc_in, N, ct.cast(hf.data_ptr(), P), err))
+    sha_call_ms = call_ms(lambda: L.charm_sha_point(
+        pnt._Point, ct.cast(hf.data_ptr(), P), N, shc_out, err))
+    d_tmp = torch.empty(nlat * nlon, dtype=torch.float64, device=dev)
+    copy_gbs = {}
+    for name, fn in (("h2d", lambda: d_tmp.copy_(hf, non_blocking=True)),
+                     ("d2h", lambda: hf.copy_(d_tmp, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record()
+        for _ in range(5):
+            fn()
+        c1.record()
+        c1.synchronize()
+        copy_gbs[name] = 5 * 8 * nlat * nlon / (c0.elapsed_time(c1) * 1e-3) / 1e9
+    del d_tmp
+    # synthesis: coefficients up, then the grid down; analysis: the grid
+    # up, then the coefficients down (neither pair can overlap)
+    coef_b, grid_b = 16 * T, 8 * nlat * nlon
+    copy_bound_ms = 1e3 * ((coef_b + grid_b) / (copy_gbs["h2d"] * 1e9) +
+                           (grid_b + coef_b) / (copy_gbs["d2h"] * 1e9))
+
     f32 = single_precision(L, err, pnt, N, c, s, d_f, stream, flush,
                            args.steps)
     bi8 = None if args.no_batch_i8 else batched_split_precision(
@@ -376,7 +415,10 @@ def run_ours(args):
                 "unit": "s",
                 "wall_s": wall / e2e_steps,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "round_trip_rel_rms": rt_e2e},
+                "round_trip_rel_rms": rt_e2e,
+                "shs_call_ms": shs_call_ms, "sha_call_ms": sha_call_ms,
+                "pinned_copy_gbs": copy_gbs,
+                "copy_bound_ms": copy_bound_ms},
         "gpu_launches": int(kl.value),
         "fft_execs": int(fe.value),
         "clocks": clk,
