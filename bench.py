@@ -16,9 +16,11 @@ time the round trip's copies alone take at them).  With --gpus N > 1
 rank runs its own round trips (replicas, no collective on the data path);
 value = max-over-ranks time / (N * K).
 
---impl reference times the CPU oracle (the restatement of CHarm's algorithm
-in oracle/, OpenMP on all host cores) on a bounded sample of latitude rows
-of the same workload, scaled to a full round trip.
+--impl reference times CHarm 0.4.9 itself on the host cores: its own
+sources compiled by oracle/build_ref.py (OpenMP, AVX-512 or AVX2, -O3
+-ffast-math, FFTW replaced by the FFTW-API shim of oracle/fftw_shim), every
+step the full round trip of the same workload through charm_shs_point and
+charm_sha_point.  It loads nothing of the charm_b200 package's library.
 """
 import argparse
 import ctypes as ct
@@ -384,14 +386,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (Kaula-decay coefficients, seed 2000)",
-        "config": {
-            "workload": "GL-grid SHS+SHA round trip, plain FP64",
-            "nmax": N, "grid": "%dx%d" % (nlat, nlon), "r": "R",
-            "GM": GM, "R": R_EARTH,
-            "l2": "flushed between steps (256 MiB write outside the timed "
-                  "events)",
-            "parallelism": "replicas" if ws > 1 else "single GPU",
-        },
+        "config": workload_config(N, nlat, nlon, ws),
         "round_trip_rel_rms": rt,
         "kernel_ms": {"shs_grid": shs_ms, "sha_grid": sha_ms,
                       "fft_total_per_step": ms[3] / args.steps,
@@ -435,7 +430,7 @@ def run_ours(args):
     if hi is not None:
         line["nmax10800"] = hi
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(N, c, s, sample_rows=None)
+        line["cpu_baseline"] = cpu_baseline(N, c, s)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -683,90 +678,136 @@ def profiled_traffic(kernel, N):
     return None
 
 
-def cpu_baseline(N, c, s, sample_rows=None, budget_s=20.0):
-    """Times the CPU oracle on a sample of latitude pairs of the GL grid and
-    scales the Legendre part to the full grid; the FFTs run over all rows.
-    Returns the cpu_baseline object (seconds per round trip)."""
-    from oracle import orc
+def host_cores():
+    """Host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def workload_config(N, nlat, nlon, ws):
+    """The config object of the round-trip workload, shared by both arms."""
     from charm_b200.workloads import GM, R_EARTH
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    p = orc.gl(N, R_EARTH)
-    shc = orc.Shc(N, GM, R_EARTH, c, s)
-    rows, mirrors, flags = orc.grid_rows(p)
-    npairs = len(rows)
-    if sample_rows is None:
-        # calibrate on 4 pairs, then size the sample to about budget_s
-        sel4 = np.linspace(0, npairs - 1, min(4, npairs)).astype(int)
-        one = np.ones(sel4.size)
+    return {
+        "workload": "GL-grid SHS+SHA round trip, plain FP64",
+        "nmax": N, "grid": "%dx%d" % (nlat, nlon), "r": "R",
+        "GM": GM, "R": R_EARTH,
+        "coefficients": "Kaula 1e-5 n^-2 / sqrt(2n+1), seed 2000",
+        "l2": "flushed between GPU steps (256 MiB write outside the timed "
+              "events); the grid (76.8 MB) and triangles exceed the host "
+              "caches",
+        "parallelism": "replicas" if ws > 1 else "single device",
+    }
+
+
+def charm_round_trips(N, c, s, steps, warmup, fft_share=True):
+    """Times CHarm 0.4.9 itself -- charm_shs_point then charm_sha_point of
+    the double-precision build in oracle/_ref (its own sources compiled with
+    OpenMP and AVX-512, or AVX2 where the host lacks AVX-512, -O3
+    -ffast-math), on the full GL grid of degree N at r = R, `warmup`
+    untimed and `steps` timed round trips, wall clock, all host threads.
+    Also times, once, the row FFTs CHarm makes in a round trip through the
+    same library's FFTW-API shim (analysis: one r2c per row in one thread,
+    as sha_point.c runs them; synthesis: one c2r per row, spread over the
+    threads by CHarm), so that the shim's share can be read off."""
+    cores = host_cores()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    from charm_b200.workloads import GM, R_EARTH, coef_rel_rms
+    from oracle import charm_ref
+    C = charm_ref.Charm("d")
+    pnt, lat, lon, w = C.grid(charm_ref.GL, N, R_EARTH)
+    shc = C.shc(N, GM, R_EARTH, c, s)
+    npt = lat.size * lon.size
+    shs_t, sha_t = [], []
+    c2 = s2 = None
+    for i in range(warmup + steps):
         t0 = time.perf_counter()
-        orc.lumped(shc, N, p.lat[rows[sel4]], one, one, flags[sel4], "pot")
-        per_pair = 2.0 * (time.perf_counter() - t0) / sel4.size
-        sample_rows = int(max(4, min(npairs, budget_s / max(per_pair, 1e-9))))
-    sel = np.linspace(0, npairs - 1, sample_rows).astype(int)
-    lat = p.lat[rows[sel]]
-    ones = np.ones(sel.size)
-    t0 = time.perf_counter()
-    a, b, a2, b2 = orc.lumped(shc, N, lat, ones, ones, flags[sel], "pot")
-    t_shs = time.perf_counter() - t0
-    nlon = p.lon.size
-    t0 = time.perf_counter()
-    fn = orc.lon_synthesis_fft(np.repeat(a[0][:1], p.lat.size, axis=0),
-                               np.repeat(b[0][:1], p.lat.size, axis=0), nlon,
-                               1.0)
-    t_fft1 = time.perf_counter() - t0
-    L = N + 1
-    amp = np.ascontiguousarray(a[0] + a2[0])
-    amm = np.ascontiguousarray(a[0] - a2[0])
-    bmp = np.ascontiguousarray(b[0] + b2[0])
-    bmm = np.ascontiguousarray(b[0] - b2[0])
-    cc = np.zeros(L * (L + 1) // 2)
-    ss = np.zeros_like(cc)
-    t0 = time.perf_counter()
-    orc.lib("d").orc_d_sha_contract(N, sel.size, orc._ptr(np.ascontiguousarray(lat)),
-                                    orc._ptr(amp), orc._ptr(amm), orc._ptr(bmp),
-                                    orc._ptr(bmm), orc._ptr(cc), orc._ptr(ss))
-    t_sha = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    np.fft.rfft(fn, axis=1)
-    t_fft2 = time.perf_counter() - t0
-    scale = npairs / sel.size
-    total = (t_shs + t_sha) * scale + t_fft1 + t_fft2
-    return {"value": total, "unit": "s", "cores": cores, "kind": "port",
-            "sample": "%d of %d latitude pairs of the nmax %d GL grid (Legendre "
-                      "sums scaled by %.1f; FFTs on all rows, numpy)" % (
-                          sel.size, npairs, N, scale),
-            "measured_s": t_shs + t_sha + t_fft1 + t_fft2}
+        f = C.shs_point(pnt, shc, N, npt)
+        t1 = time.perf_counter()
+        c2, s2 = C.sha_point(pnt, f, N, GM, R_EARTH)
+        t2 = time.perf_counter()
+        if i >= warmup:
+            shs_t.append(t1 - t0)
+            sha_t.append(t2 - t1)
+    rt = coef_rel_rms(c2, s2, c, s)
+    out = {"cores": cores, "lib": os.path.relpath(C.path, ROOT),
+           "avx512": charm_ref.cpu_has_avx512(),
+           "shs_s": float(np.mean(shs_t)), "sha_s": float(np.mean(sha_t)),
+           "round_trip_s": [a + b for a, b in zip(shs_t, sha_t)],
+           "round_trip_rel_rms": rt}
+    if fft_share:
+        L = C.L
+        vp = ct.c_void_p
+        for nm_, at in (("fftw_plan_dft_r2c_1d", [ct.c_int, vp, vp, ct.c_uint]),
+                        ("fftw_plan_dft_c2r_1d", [ct.c_int, vp, vp, ct.c_uint])):
+            getattr(L, nm_).argtypes = at
+            getattr(L, nm_).restype = vp
+        for nm_ in ("fftw_execute_dft_r2c", "fftw_execute_dft_c2r"):
+            getattr(L, nm_).argtypes = [vp, vp, vp]
+            getattr(L, nm_).restype = None
+        L.fftw_destroy_plan.argtypes = [vp]
+        nlon = lon.size
+        x = np.random.default_rng(0).standard_normal(nlon)
+        X = np.zeros(nlon // 2 + 1, np.complex128)
+        pr = L.fftw_plan_dft_r2c_1d(nlon, None, None, 1 << 6)
+        pc = L.fftw_plan_dft_c2r_1d(nlon, None, None, 1 << 6)
+        t0 = time.perf_counter()
+        for _ in range(lat.size):
+            L.fftw_execute_dft_r2c(pr, x.ctypes.data, X.ctypes.data)
+        t_r2c = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(lat.size):
+            L.fftw_execute_dft_c2r(pc, X.ctypes.data, x.ctypes.data)
+        t_c2r = time.perf_counter() - t0
+        L.fftw_destroy_plan(pr)
+        L.fftw_destroy_plan(pc)
+        out["fft_shim_s"] = {"sha_r2c_serial": t_r2c,
+                             "shs_c2r_one_thread": t_c2r,
+                             "shs_c2r_spread_over_threads": t_c2r / cores}
+    return out
+
+
+def cpu_baseline(N, c, s):
+    """The cpu_baseline object: CHarm itself on the same round trip (one
+    warm-up, three timed round trips, their median)."""
+    r = charm_round_trips(N, c, s, steps=3, warmup=1)
+    v = float(np.median(r["round_trip_s"]))
+    return {"value": v, "unit": "s", "cores": r["cores"], "kind": "reference",
+            "sample": "the full round trip (nmax %d GL grid), 1 warm-up + 3 "
+                      "timed, median" % N,
+            "detail": r}
 
 
 def run_reference(args):
-    ws, rank, local = dist_env()
+    """The reference arm: CHarm 0.4.9 (oracle/_ref) on the host cores,
+    every step the full round trip of the GPU arm's workload.  Under
+    torchrun only rank 0 runs and prints; the others exit."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from charm_b200.workloads import kaula
     N = args.nmax
     c, s = kaula(N, 2000)
-    times = []
-    cb = None
-    # each step a bounded sample: the whole run stays within about 3 min
-    budget = max(2.0, min(20.0, 180.0 / max(1, args.warmup + args.steps)))
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(N, c, s, budget_s=budget)
-        if i >= args.warmup:
-            times.append(cb["value"])
-    v = float(np.mean(times))
-    cb["value"] = v
+    r = charm_round_trips(N, c, s, steps=args.steps, warmup=args.warmup)
+    v = float(np.mean(r["round_trip_s"]))
     line = {
         "impl": "reference",
         "metric": METRIC, "value": v, "unit": "s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (Kaula-decay coefficients, seed 2000)",
-        "config": {"workload": "GL-grid SHS+SHA round trip, plain FP64",
-                   "nmax": N, "grid": "%dx%d" % (N + 1, 2 * (N + 1)), "r": "R"},
-        "cpu_baseline": cb,
+        "config": workload_config(N, N + 1, 2 * (N + 1), ws),
+        "round_trip_rel_rms": r["round_trip_rel_rms"],
+        "cpu_baseline": {"value": v, "unit": "s", "cores": r["cores"],
+                         "kind": "reference",
+                         "sample": "every step the full round trip: "
+                                   "charm_shs_point + charm_sha_point of "
+                                   "CHarm 0.4.9 (%s), wall clock" % r["lib"]},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference": r,
     }
     print(json.dumps(line), flush=True)
 

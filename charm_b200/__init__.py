@@ -2,16 +2,24 @@
 NVIDIA B200 (sm_100a).
 
 The C ABI lives in libcharm.so (include/charm_b200.h); this package exposes
-it to Python with PyHarm's names (see charm_b200.pyharm).  Importing fails
-loudly when libcharm.so has not been built.
+it to Python with PyHarm's names (see charm_b200.pyharm).  The library is
+loaded on first use of any of those names, and that fails loudly when
+libcharm.so has not been built.  `charm_b200.workloads` (the seeded
+synthetic inputs) needs no library.
 """
-from .pyharm import (CHarmError, GRID, GRID_DH1, GRID_DH2, GRID_GL, SCATTERED,
-                     PointGrid, PointGridDH1, PointGridDH2, PointGridGL,
-                     PointSctr, Shc, sha_point, shs_point, shs_point_grad1,
-                     shs_point_grad2, shs_point_guru)
-from ._lib import LIB_PATH
-
-__all__ = ["CHarmError", "GRID", "GRID_DH1", "GRID_DH2", "GRID_GL",
+_PYHARM = ("CHarmError", "GRID", "GRID_DH1", "GRID_DH2", "GRID_GL",
            "SCATTERED", "PointGrid", "PointGridDH1", "PointGridDH2",
            "PointGridGL", "PointSctr", "Shc", "sha_point", "shs_point",
-           "shs_point_grad1", "shs_point_grad2", "shs_point_guru", "LIB_PATH"]
+           "shs_point_grad1", "shs_point_grad2", "shs_point_guru")
+
+__all__ = list(_PYHARM) + ["LIB_PATH"]
+
+
+def __getattr__(name):
+    if name in _PYHARM:
+        from . import pyharm
+        return getattr(pyharm, name)
+    if name == "LIB_PATH":
+        from ._lib import LIB_PATH
+        return LIB_PATH
+    raise AttributeError("module 'charm_b200' has no attribute %r" % name)

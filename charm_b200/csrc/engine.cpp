@@ -206,15 +206,23 @@ void resolve_timers(Context &c)
 Status init(Context &c)
 {
     Status st;
-    if (c.ready)
-    {
-        int dev = -1;
-        cudaGetDevice(&dev);
-        if (dev == c.device)
-            return st;
-    }
     int dev = 0;
     CB_CUDA(cudaGetDevice(&dev), st);
+    if (c.ready)
+    {
+        if (dev == c.device)
+            return st;
+        // The streams, events, cached buffers, tables, transform plans and
+        // kernel attributes of the context belong to the device it was set
+        // up on: one device per process (one process per GPU, as the
+        // replicas run).
+        st.code = CHARM_EFUNCARG;
+        st.msg = "charm_b200 serves one device per process: it was set up on "
+                 "device " + std::to_string(c.device) +
+                 " and is now called with device " + std::to_string(dev) +
+                 " current.";
+        return st;
+    }
     cudaDeviceProp prop;
     CB_CUDA(cudaGetDeviceProperties(&prop, dev), st);
     if (prop.major < 10)
@@ -2854,14 +2862,17 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
         cudaError_t e = static_scratch_address(&p);
         if (e != cudaSuccess || !p)
         {
+            cudaGetLastError();
             st.code = CHARM_EFUNCARG;
             st.msg = std::string("cudaGetSymbolAddress of the static scratch "
                                  "failed: ") +
                      cudaGetErrorString(e);
             return st;
         }
-        sd.base = static_cast<unsigned char *>(p);
         CB_CUDA(rfft_set_smem(rfft_smem_bytes(9216)), st);
+        // recorded only once the whole set-up has succeeded, so that a
+        // failed set-up is retried by the next call
+        sd.base = static_cast<unsigned char *>(p);
     }
     const long long N = (long long)nmax;
     const size_t nlat = pnt->nlat, nlon = pnt->nlon;
@@ -2922,9 +2933,9 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
     {
         int s = !symm ? 0 : ((dh && p == 0) ? 0 : ((size_t)p < equator));
         int rs = s ? (int)(pnt_nlat - p - 1) : -1;
-        double la = pnt->lat[p];
-        hs.geo_d[p] = std::sin(la);
-        hs.geo_d[np + p] = std::cos(la);
+        // sincos, as sha_grid computes the same geometry, so that both
+        // paths see identical latitude terms
+        sincos(pnt->lat[p], &hs.geo_d[p], &hs.geo_d[np + p]);
         hs.geo_d[2 * np + p] = cq * pnt->w[p];
         hs.geo_d[3 * np + p] = rs >= 0 ? cq * pnt->w[rs] : 0.0;
         hs.geo_i[p] = p;
@@ -2988,6 +2999,11 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
     // recurrence tables (kept while nmax repeats)
     if (sd.tab_nmax != N)
     {
+        // the tables below overwrite the scratch: nothing cached stays
+        // valid if a copy or launch fails before they are complete
+        sd.tab_nmax = -1;
+        sd.fft_L = -1;
+        sd.fft_nmax = -1;
         for (long long k = 0; k <= 2 * N + 3; k++)
         {
             double w = std::sqrt((double)k);
@@ -3017,6 +3033,8 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
     RF.ht = reinterpret_cast<double2 *>(b + o_ht);
     if (sd.fft_L != (long long)nlon || sd.fft_nmax != N)
     {
+        sd.fft_L = -1;
+        sd.fft_nmax = -1;
         RfftArgs tmp = RF;
         CB_CUDA(launch_rfft_tables(tmp, const_cast<double2 *>(RF.tw),
                                    const_cast<double2 *>(RF.w),

@@ -345,7 +345,11 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_sctr_adjoint_dev(
  * CHARM_EFUNCARG and a message naming the limit.  The library serialises
  * these calls on its stream and returns after the stream is idle; kernels
  * of calls that overlap on the GPU (another process's context aside) would
- * race on the scratch.  The first call on a device performs the set-up
+ * race on the scratch.  The host-side staging of the call (latitude
+ * geometry and table sources, fixed arrays in engine.cpp) is one
+ * process-wide object as well: call it from one host thread at a time.
+ * Like the rest of the library it serves one device per process.  The
+ * first call on a device performs the set-up
  * (symbol address, kernel attributes, recurrence and transform tables) and
  * should precede any stream capture.  Only the scratch's status and
  * work-counter words must start at zero; each call clears them. */

@@ -2,7 +2,7 @@
 small fixtures under tests/golden/.
 
 Run once in a container that has the CHarm source tree (its path is the
-first argument, default /root/reference); the tests only read the .npz files
+first argument); the tests only read the .npz files
 this writes, so the GPU machine never needs the reference tree.
 
 Sources (CHarm 0.4.9):
@@ -54,7 +54,9 @@ GRAD_SUFFIX = re.compile(r"_(x|y|z|xx|xy|xz|yy|yz|zz|guru\d+)\.txt$")
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <CHarm source tree>")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     dbl = {}
     for name in sorted(os.listdir(os.path.join(ref, "data/tests/double"))):

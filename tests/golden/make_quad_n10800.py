@@ -11,11 +11,13 @@ takes the FFT path), of which 64 are compared.
 Coefficients: Kaula decay sigma_n = 1e-5 n^-2 (C00 = 1, degree 1 zero,
 S_n0 = 0), standard normals from numpy's default_rng(3000), the order-major
 triangle of charm_b200.workloads.kaula(10800, 3000, sqrt_scaling=False).
-The oracle sums in binary128 (oracle/orc.c built with -DORC_QUAD) and
-returns (hi, lo) float64 pairs.
+The values come from CHarm's own quad-precision build (charmq_shs_point of
+CHarm 0.4.9 compiled by oracle/build_ref.py, binary128 throughout, its FFT
+through oracle/fftw_shim), stored as (hi, lo) float64 pairs.
 
-Run from the repository root: python tests/golden/make_quad_n10800.py
-(about 5 minutes on 8 cores)."""
+Run from the repository root after `python oracle/build_ref.py --reference
+<CHarm source tree> --variants q`:
+    python tests/golden/make_quad_n10800.py     (a few minutes on 8 cores)"""
 import math
 import os
 import sys
@@ -50,37 +52,30 @@ def points():
 
 
 def main():
+    from oracle import charm_ref
     lat, lon_idx = points()
     c, s = kaula(NMAX, 3000, sqrt_scaling=False)
     L = NMAX + 1
+    nlon = 2 * L
     nrow = lat.size
-    cq = orc.q_from_dd(c)
-    sq = orc.q_from_dd(s)
-    latq = orc.q_from_dd(lat)
-    ones = orc.q_from_dd(np.ones(nrow))
-    out = [np.zeros((nrow * L, 2)) for _ in range(4)]
-    t0 = time.time()
-    orc.lib("q").orc_q_shs_lumped(
-        NMAX, NMAX, orc._ptr(cq), orc._ptr(sq), nrow, orc._ptr(latq),
-        orc._ptr(ones), orc._ptr(ones.copy()),
-        orc._ptr(np.zeros(nrow, np.int32)), 0, 0, 0, 0,
-        *[orc._ptr(o) for o in out])
-    t1 = time.time()
-    # longitudes j pi / (nmax + 1) and GM / R in binary128
+    Q = charm_ref.CharmQ()
+    # longitudes j pi / (nmax + 1) exact in binary128: CHarm checks that a
+    # grid's longitudes increase linearly within its quad threshold before
+    # it takes the FFT path (src/shs/shs_grd_point_fft_check.c)
     piq = orc.q_from_dd(np.array([math.pi]), np.array([1.2246467991473532e-16]))
     step = orc.q_arith("/", piq, orc.q_from_dd(np.array([float(L)])))
-    lonq = orc.q_arith("*", orc.q_from_dd(lon_idx.astype(np.float64)), step)
-    mur = orc.q_arith("/", orc.q_from_dd(np.array([GM])),
-                      orc.q_from_dd(np.array([R_EARTH])))
-    f = np.zeros((nrow * lon_idx.size, 2))
-    orc.lib("q").orc_q_lonsum(nrow, L, orc._ptr(out[0]), orc._ptr(out[1]),
-                              lon_idx.size, orc._ptr(lonq), orc._ptr(mur),
-                              orc._ptr(f))
-    hi, lo = orc.q_to_dd(f)
+    lonq = orc.q_arith("*", orc.q_from_dd(np.arange(nlon, dtype=np.float64)),
+                       step)
+    pnt = Q.point_raw(charm_ref.GRID, orc.q_from_dd(lat), lonq,
+                      orc.q_from_dd(np.full(nrow, R_EARTH)))
+    shc = Q.shc(NMAX, GM, R_EARTH, c, s)
+    t0 = time.time()
+    hi, lo = Q.shs_point(pnt, shc, NMAX, nrow * nlon)
+    hi = hi.reshape(nrow, nlon)[:, lon_idx]
+    lo = lo.reshape(nrow, nlon)[:, lon_idx]
     np.savez_compressed(OUT, nmax=NMAX, seed=3000, lat=lat, lon_idx=lon_idx,
-                        f_hi=hi.reshape(nrow, -1), f_lo=lo.reshape(nrow, -1))
-    print("lumped %.0f s, longitude sums %.0f s -> %s" % (
-        t1 - t0, time.time() - t1, OUT))
+                        f_hi=hi, f_lo=lo, source=np.array(Q.path.split("/")[-1]))
+    print("charmq_shs_point %.0f s -> %s" % (time.time() - t0, OUT))
 
 
 if __name__ == "__main__":
