@@ -61,7 +61,7 @@ def build(verbose=False):
         return LIB
     tmp = LIB + ".tmp"
     cmd = [nvcc()] + ARCH + ["-ccbin", HOST_CXX, "-shared", "-o", tmp] + objs + [
-        "-lcufft", "-lcudart"]
+        "-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

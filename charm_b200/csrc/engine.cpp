@@ -1,17 +1,18 @@
 // Host runtime of charm_b200 (see engine.h).
 //
-// One process-wide context per CUDA device: a compute stream and a copy
-// stream (the host-array calls copy their grids and coefficients in bands
-// there, ordered against the kernels by events), grow-only device buffers,
-// cached recurrence tables per maximum degree, cached row-transform and
-// cuFFT plans and a pinned staging area for the small per-call arrays.
+// One process-wide context, bound to the device it was set up on (one
+// device per process): a compute stream and a copy stream (the host-array
+// calls copy their grids and coefficients in bands there, ordered against
+// the kernels by events), grow-only device buffers, cached recurrence
+// tables per maximum degree, cached row-transform plans (rfft.cu, every
+// row length up to 147456 points; no library FFT) and a pinned staging
+// area for the small per-call arrays.
 // Calls are serialised by a mutex.  Every call ends with a synchronisation
 // of its streams and a check of the device status word written by the
 // kernels.
 #include "engine.h"
 
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <algorithm>
 #include <array>
@@ -102,7 +103,6 @@ struct Context
     std::map<std::tuple<int, int, int, int, long long, int>,
              std::pair<int, std::vector<std::pair<int, float>>>>
         tuned;
-    std::map<std::tuple<int, int, long long>, cufftHandle> plans;
     std::map<long long, RfftArgs> rffts;   // row transforms by row length
     std::map<long long, void *> rfft_mem;  // their tables
     std::recursive_mutex mtx;
@@ -113,7 +113,9 @@ struct Context
     double timer_ms[TIMER_COUNT] = {};
     unsigned long long timer_n[TIMER_COUNT] = {};
     unsigned long long launches = 0;   // kernels of this library
-    unsigned long long fft_execs = 0;  // cuFFT executions
+    // launches of library kernels (none: every transform is this
+    // library's own)
+    unsigned long long fft_execs = 0;
 };
 
 Context g_ctx;
@@ -431,56 +433,18 @@ Status tables(Context &c, long long nmax, Tabs *tab)
     return st;
 }
 
-Status plan(Context &c, cufftType type, int n, long long batch,
-            cufftHandle *out)
-{
-    Status st;
-    auto key = std::make_tuple((int)type, n, batch);
-    auto it = c.plans.find(key);
-    if (it != c.plans.end())
-    {
-        *out = it->second;
-        return st;
-    }
-    if (c.plans.size() >= 8)
-    {
-        cudaStreamSynchronize(c.stream);
-        for (auto &kv : c.plans)
-            cufftDestroy(kv.second);
-        c.plans.clear();
-    }
-    cufftHandle h;
-    int nn[1] = {n};
-    int nfc = n / 2 + 1;
-    int nc[1] = {nfc};
-    cufftResult r;
-    if (type == CUFFT_Z2D)
-        r = cufftPlanMany(&h, 1, nn, nc, 1, nfc, nn, 1, n, CUFFT_Z2D,
-                          (int)batch);
-    else
-        r = cufftPlanMany(&h, 1, nn, nn, 1, n, nc, 1, nfc, CUFFT_D2Z,
-                          (int)batch);
-    if (r != CUFFT_SUCCESS)
-    {
-        st.code = (r == CUFFT_ALLOC_FAILED) ? CHARM_EMEM : CHARM_EFUNCARG;
-        st.msg = "cuFFT plan creation failed (code " + std::to_string((int)r) +
-                 ")";
-        return st;
-    }
-    cufftSetStream(h, c.stream);
-    c.plans[key] = h;
-    *out = h;
-    return st;
-}
-
-// Shape of the shared-memory transform of rows of length L (rfft.cu):
-// H, M, V, direct and the passes of FFT_M, or false when it does not apply
-// (L odd, H < 8, or M beyond 9216, the shared memory of one CTA).
+// Shape of the transform of grid rows of length L (rfft.cu): the complex
+// length H (L / 2 for even rows, L for odd rows), the FFT length M, the
+// cluster size C (CTAs per row, each holding M / C values) and the passes
+// of the per-CTA FFT, or false when no plan exists (M / C would exceed
+// 9216 even with clusters of 16, i.e. H above 73728).
 bool rfft_shape(long long L, RfftArgs *out)
 {
+    constexpr long long MC_MAX = 9216;   // values in one CTA's shared memory
     RfftArgs A{};
     A.M = 0;
-    const long long H = L / 2;
+    A.C = 1;
+    A.V = 16;
     auto smooth = [](long long n, int *a, int *b) {
         *a = *b = 0;
         while (n > 1 && n % 2 == 0)
@@ -495,41 +459,60 @@ bool rfft_shape(long long L, RfftArgs *out)
         }
         return n == 1;
     };
-    int a = 0, b = 0;
-    if (L % 2 == 0 && H >= 8)
-    {
-        // transform lengths are 2^a 3^b with a >= 6: the passes then start
-        // with two of radix 8 and every stride is a multiple of 8 (rfft.cu)
-        if (smooth(H, &a, &b) && a >= 6 && H <= 9216)
-        {
-            A.M = (int)H;
-            A.direct = 1;
-        }
-        else
-        {
-            long long best = 0;
-            for (long long p2 = 64; p2 <= 9216; p2 *= 2)
-                for (long long m = p2; m <= 9216; m *= 3)
-                    if (m >= 2 * H - 1 && (best == 0 || m < best))
-                        best = m;
-            if (best > 0)
-            {
-                A.M = (int)best;
-                A.direct = 0;
-                smooth(best, &a, &b);
-            }
-        }
-    }
-    // 16 values per thread: M / 16 threads, two CTAs per SM up to
-    // M = 4608
-    A.V = 16;
-    if (A.M == 0)
+    // smallest 2^a 3^b >= need with a >= 6 (every per-CTA plan starts with
+    // two radix-8 passes and keeps its strides multiples of 8), <= MC_MAX
+    auto local_len = [&](long long need) {
+        long long best = 0;
+        for (long long p2 = 64; p2 <= MC_MAX; p2 *= 2)
+            for (long long m = p2; m <= MC_MAX; m *= 3)
+                if (m >= need && (best == 0 || m < best))
+                    best = m;
+        return best;
+    };
+    if (L < 1)
     {
         *out = A;
         return false;
     }
+    const bool odd = (L % 2) != 0;
+    const long long H = odd ? L : L / 2;
+    int a = 0, b = 0;
+    long long Mc = 0;
+    if (!odd && smooth(H, &a, &b) && a >= 6 && H <= MC_MAX)
+    {
+        A.direct = 1;
+        A.M = (int)H;
+        Mc = H;
+    }
+    else
+    {
+        // Bluestein: M = C Mc >= 2H - 1, the smallest M, then the fewest
+        // CTAs per row
+        const long long need = 2 * H - 1;
+        long long bestM = 0;
+        for (int C = 1; C <= 16; C *= 2)
+        {
+            const long long m = local_len((need + C - 1) / C);
+            if (m > 0 && (bestM == 0 || C * m < bestM))
+            {
+                bestM = C * m;
+                A.C = C;
+                Mc = m;
+            }
+        }
+        if (bestM == 0)
+        {
+            *out = A;
+            return false;
+        }
+        A.direct = 0;
+        A.M = (int)bestM;
+    }
+    smooth(Mc, &a, &b);
     A.H = (int)H;
-    // radix 8 passes, then 4, then 2 (powers of two), then 3
+    A.odd = odd ? 1 : 0;
+    // passes of the per-CTA FFT of length Mc: radix 8, then 4, then 2
+    // (powers of two), then 3
     int p8 = a / 3, p4 = 0, p2 = 0;
     if (a % 3 == 2)
         p4 = 1;
@@ -548,46 +531,74 @@ bool rfft_shape(long long L, RfftArgs *out)
     return true;
 }
 
-// Shared-memory transform of grid rows of length L (rfft.cu), or nullptr
-// when it does not apply: L odd, or a transform length M beyond 9216
-// (the shared memory of one CTA), or CHARM_B200_ROW_FFT=library.
+// Transform of grid rows of length L (rfft.cu), set up once per length:
+// fails with CHARM_EFUNCARG when no plan exists for L (rfft_shape) or the
+// plan's cluster shape cannot be scheduled on this device.
 Status row_fft(Context &c, long long L, const RfftArgs **out)
 {
     Status st;
     *out = nullptr;
-    const char *e = std::getenv("CHARM_B200_ROW_FFT");
-    if (e && std::strcmp(e, "library") == 0)
-        return st;
     auto it = c.rffts.find(L);
     if (it != c.rffts.end())
     {
-        *out = it->second.M > 0 ? &it->second : nullptr;
+        *out = &it->second;
         return st;
     }
     RfftArgs A{};
     if (!rfft_shape(L, &A))
     {
-        c.rffts[L] = A;
+        st.code = CHARM_EFUNCARG;
+        st.msg = "no longitude transform for grid rows of " +
+                 std::to_string(L) +
+                 " points (the limit is 147456 points per row).";
         return st;
     }
     const long long H = A.H;
     const size_t nM = (size_t)A.M, nH = (size_t)H;
-    const size_t n_tab = nM + (A.direct ? 0 : nH + nM) + nH + 1;
-    void *mem = nullptr;
-    CB_CUDA(cudaMalloc(&mem, n_tab * sizeof(double2)), st);
-    double2 *tw = static_cast<double2 *>(mem);
-    double2 *w = A.direct ? nullptr : tw + nM;
-    double2 *bh = A.direct ? nullptr : w + nH;
-    double2 *ht = A.direct ? tw + nM : bh + nM;
-    A.tw = tw;
-    A.w = w;
-    A.bh = bh;
-    A.ht = ht;
     // the largest transform of either width, so that no later plan needs
     // a different limit
-    cudaError_t ce = rfft_set_smem(rfft_smem_bytes(9216));
-    if (ce == cudaSuccess)
+    CB_CUDA(rfft_set_smem(rfft_smem_bytes(9216)), st);
+    void *mem = nullptr;
+    cudaError_t ce = cudaSuccess;
+    if (A.C > 1)
+    {
+        const int Mc = A.M / A.C;
+        if (rfftc_max_clusters(A.C, Mc) < 1)
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "the longitude transform of rows of " +
+                     std::to_string(L) + " points needs clusters of " +
+                     std::to_string(A.C) +
+                     " CTAs, which this device cannot schedule.";
+            return st;
+        }
+        // tw (Mc), twM (M), w (H), bh (M), ht (H + 1)
+        const size_t n_tab = (size_t)Mc + nM + nH + nM + nH + 1;
+        CB_CUDA(cudaMalloc(&mem, n_tab * sizeof(double2)), st);
+        double2 *tw = static_cast<double2 *>(mem);
+        double2 *twM = tw + Mc;
+        double2 *w = twM + nM;
+        double2 *bh = w + nH;
+        double2 *ht = bh + nM;
+        A.bh = bh;
+        ce = launch_rfftc_tables(A, tw, twM, w, ht, bh, c.stream);
+        c.launches += 3;
+    }
+    else
+    {
+        const size_t n_tab = nM + (A.direct ? 0 : nH + nM) + nH + 1;
+        CB_CUDA(cudaMalloc(&mem, n_tab * sizeof(double2)), st);
+        double2 *tw = static_cast<double2 *>(mem);
+        double2 *w = A.direct ? nullptr : tw + nM;
+        double2 *bh = A.direct ? nullptr : w + nH;
+        double2 *ht = A.direct ? tw + nM : bh + nM;
+        A.tw = tw;
+        A.w = w;
+        A.bh = bh;
+        A.ht = ht;
         ce = launch_rfft_tables(A, tw, w, ht, bh, c.stream);
+        c.launches += A.direct ? 1 : 2;
+    }
     if (ce == cudaSuccess)
         ce = cudaStreamSynchronize(c.stream);
     if (ce != cudaSuccess)
@@ -598,7 +609,6 @@ Status row_fft(Context &c, long long L, const RfftArgs **out)
                  cudaGetErrorString(ce);
         return st;
     }
-    c.launches += A.direct ? 1 : 2;
     c.rffts[L] = A;
     c.rfft_mem[L] = mem;
     *out = &c.rffts[L];
@@ -615,7 +625,7 @@ Status row_fft_quarter(Context &c, long long L, const RfftArgs *half,
 {
     Status st;
     *out = nullptr;
-    if (!half || half->M != 9216 || L % 4 != 0)
+    if (!half || half->M != 9216 || half->C != 1 || half->odd || L % 4 != 0)
         return st;
     auto it = c.rffts.find(-L);
     if (it != c.rffts.end())
@@ -625,7 +635,7 @@ Status row_fft_quarter(Context &c, long long L, const RfftArgs *half,
     }
     const long long Lq = L / 4;
     RfftArgs A{};
-    if (!rfft_shape(2 * Lq, &A) || A.direct || A.M != 4608)
+    if (!rfft_shape(2 * Lq, &A) || A.direct || A.M != 4608 || A.C != 1)
     {
         A.M = 0;
         c.rffts[-L] = A;
@@ -1277,19 +1287,24 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     double2 *lc = nullptr;
     CB_TRY(dbuf(c, "lumped", (size_t)npar * nlat * ldf, &lc));
     double *fg = d_f;
+    // the even-row transform stores pairs of doubles: a device output that
+    // is not on a 16-byte boundary is written through the aligned staging
+    // grid and copied once
+    double *f_dev_unaligned = nullptr;
+    if (fg && use_fft && nlon % 2 == 0 &&
+        reinterpret_cast<uintptr_t>(fg) % 16 != 0)
+    {
+        f_dev_unaligned = fg;
+        fg = nullptr;
+    }
     if (!fg)
         CB_TRY(dbuf(c, "fgrid", (size_t)npar * nlat * nlon, &fg));
     const RfftArgs *rf = nullptr, *rfq = nullptr;
-    if (use_fft && reinterpret_cast<uintptr_t>(fg) % 16 == 0)
+    if (use_fft)
     {
         CB_TRY(row_fft(c, (long long)nlon, &rf));
         CB_TRY(row_fft_quarter(c, (long long)nlon, rf, &rfq));
     }
-    // the library transform reads the whole half spectrum; the row
-    // transform reads orders <= nmax only
-    if (use_fft && !rf && (size_t)ldf > nmax + 1)
-        CB_CUDA(cudaMemsetAsync(lc, 0, (size_t)npar * nlat * ldf * 16,
-                                c.stream), st);
     unsigned *d_status;
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
@@ -1479,20 +1494,6 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
         Scope sc(c, TIMER_FFT);
         CB_CUDA(launch_rfft(R, true, c.stream), st);
     }
-    else if (use_fft)
-    {
-        cufftHandle h;
-        CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)npar * nlat, &h));
-        Scope sc(c, TIMER_FFT, false);
-        cufftResult r = cufftExecZ2D(
-            h, reinterpret_cast<cufftDoubleComplex *>(lc), fg);
-        if (r != CUFFT_SUCCESS)
-        {
-            st.code = CHARM_EFUNCARG;
-            st.msg = "cuFFT Z2D failed (code " + std::to_string((int)r) + ")";
-            return st;
-        }
-    }
     else
     {
         double *dlon_arr = nullptr;
@@ -1503,6 +1504,10 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
         CB_CUDA(launch_lon_direct(npar, (int)nlat, (int)nlon, (long long)nmax,
                                   lc, ldf, dlon_arr, fg, c.stream), st);
     }
+    if (f_dev_unaligned)
+        CB_CUDA(cudaMemcpyAsync(f_dev_unaligned, fg,
+                                (size_t)npar * nlat * nlon * 8,
+                                cudaMemcpyDeviceToDevice, c.stream), st);
     if (!d_f)
         for (int q = 0; q < npar; q++)
             CB_CUDA(cudaMemcpyAsync(f[q], fg + (size_t)q * nlat * nlon,
@@ -1772,8 +1777,6 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                 items += (long long)(nmax_v[j] + 1) * ntiles;
             }
             CB_TRY(h2d_small(c, dsets, hsets.data(), nb * sizeof(BatchSet)));
-            if (!rf)
-                CB_CUDA(cudaMemsetAsync(lc, 0, nb * per_set, c.stream), st);
             CB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long),
                                     c.stream), st);
             ShsGridArgs A{};
@@ -1814,7 +1817,7 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                                   (size_t)(kd.base + kd.slot[q]) * grid_sz;
                     double2 *src = lc + b * (per_set / sizeof(double2)) +
                                    (size_t)q * nlat * ldf;
-                    if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
+                    if (rf->odd || reinterpret_cast<uintptr_t>(dst) % 16 == 0)
                     {
                         RfftArgs R2 = *synth_plan(
                             rf, rfq, (long long)nmax_v[j0 + b]);
@@ -1832,28 +1835,10 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
                     }
                     else
                     {
-                        if (rf)
-                        {
-                            // the row transform reads orders <= nmax only;
-                            // the library one needs the rest zero
-                            st.code = CHARM_EFUNCARG;
-                            st.msg = "batched synthesis outputs must start "
-                                     "on a 16-byte boundary";
-                            return st;
-                        }
-                        cufftHandle h;
-                        CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)nlat,
-                                    &h));
-                        Scope sc(c, TIMER_FFT, false);
-                        if (cufftExecZ2D(h,
-                                         reinterpret_cast<cufftDoubleComplex *>(
-                                             src),
-                                         dst) != CUFFT_SUCCESS)
-                        {
-                            st.code = CHARM_EFUNCARG;
-                            st.msg = "cuFFT Z2D failed";
-                            return st;
-                        }
+                        st.code = CHARM_EFUNCARG;
+                        st.msg = "batched synthesis outputs must start on "
+                                 "a 16-byte boundary";
+                        return st;
                     }
                 }
             // the set descriptors and the lumped buffer are reused by the
@@ -1980,9 +1965,6 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
             Scope sc(c, TIMER_PREP);
             CB_CUDA(launch_tc_prep(P, c.stream), st);
         }
-        if (!rf)
-            CB_CUDA(cudaMemsetAsync(lc, 0, nb * per_set * sizeof(double2),
-                                    c.stream), st);
         CB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long),
                                 c.stream), st);
         ShsTcArgs A{};
@@ -2033,7 +2015,7 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
             const size_t jj = ord[j0 + b];
             double *dst = d_f[jj];
             double2 *src = lc + (size_t)b * per_set;
-            if (rf && reinterpret_cast<uintptr_t>(dst) % 16 == 0)
+            if (rf->odd || reinterpret_cast<uintptr_t>(dst) % 16 == 0)
             {
                 RfftArgs R2 = *synth_plan(rf, rfq, (long long)nmax_v[jj]);
                 R2.nrows = (long long)nlat;
@@ -2047,23 +2029,10 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
             }
             else
             {
-                if (rf)
-                {
-                    st.code = CHARM_EFUNCARG;
-                    st.msg = "batched synthesis outputs must start on a "
-                             "16-byte boundary";
-                    return st;
-                }
-                cufftHandle h;
-                CB_TRY(plan(c, CUFFT_Z2D, (int)nlon, (long long)nlat, &h));
-                Scope sc(c, TIMER_FFT, false);
-                if (cufftExecZ2D(h, reinterpret_cast<cufftDoubleComplex *>(src),
-                                 dst) != CUFFT_SUCCESS)
-                {
-                    st.code = CHARM_EFUNCARG;
-                    st.msg = "cuFFT Z2D failed";
-                    return st;
-                }
+                st.code = CHARM_EFUNCARG;
+                st.msg = "batched synthesis outputs must start on a 16-byte "
+                         "boundary";
+                return st;
             }
         }
         // the digit tiles and the lumped buffer are reused by the next group
@@ -2134,9 +2103,9 @@ Status f32_grid_checks(Context &c, const charm_point *pnt, unsigned long nmax,
                           charm_glob_threshold2))
             fft = false;
     *rf = nullptr;
-    if (fft)
+    if (fft && nlon % 2 == 0)
         CB_TRY(row_fft(c, (long long)nlon, rf));
-    if (!*rf)
+    if (!*rf || (*rf)->C > 1)
     {
         st.code = CHARM_EFUNCARG;
         st.msg = "The single-precision mode needs a grid whose longitudes "
@@ -2563,9 +2532,24 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     const int ldF = (int)(nlon / 2 + 1);
     double2 *F = nullptr;
     CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
+    // the transform loads pairs of doubles: a device grid that is not on a
+    // 16-byte boundary is copied once into the aligned staging grid
+    if (d_fin && reinterpret_cast<uintptr_t>(d_fin) % 16 != 0)
+    {
+        double *al = nullptr;
+        CB_TRY(dbuf(c, "fgrid", nlat * nlon, &al));
+        CB_CUDA(cudaMemcpyAsync(al, d_fin, nlat * nlon * 8,
+                                cudaMemcpyDeviceToDevice, c.stream), st);
+        fg = al;
+    }
     const RfftArgs *rf = nullptr;
-    if (reinterpret_cast<uintptr_t>(fg) % 16 == 0)
-        CB_TRY(row_fft(c, (long long)nlon, &rf));
+    CB_TRY(row_fft(c, (long long)nlon, &rf));
+    if (rf->odd)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "analysis grids have an even number of longitudes";
+        return st;
+    }
     auto rows_fft = [&](int r0, int r1) -> Status {
         Status s2;
         RfftArgs R = *rf;
@@ -2756,22 +2740,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         if (fdev)
             CB_CUDA(cudaMemcpyAsync(fdev, f_host, nlat * nlon * 8,
                                     cudaMemcpyHostToDevice, c.stream), st);
-        if (rf)
-            CB_TRY(rows_fft(0, (int)nlat));
-        else
-        {
-            cufftHandle h;
-            CB_TRY(plan(c, CUFFT_D2Z, (int)nlon, (long long)nlat, &h));
-            Scope sc(c, TIMER_FFT, false);
-            if (cufftExecD2Z(h, const_cast<double *>(fg),
-                             reinterpret_cast<cufftDoubleComplex *>(F)) !=
-                CUFFT_SUCCESS)
-            {
-                st.code = CHARM_EFUNCARG;
-                st.msg = "cuFFT D2Z failed";
-                return st;
-            }
-        }
+        CB_TRY(rows_fft(0, (int)nlat));
         int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                             (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
@@ -2893,7 +2862,7 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
         return st;
     }
     RfftArgs RF{};
-    if (!rfft_shape((long long)nlon, &RF))
+    if (!rfft_shape((long long)nlon, &RF) || RF.C > 1 || RF.odd)
     {
         st.code = CHARM_EFUNCARG;
         st.msg = "charm_b200_sha_point_dev_static: no shared-memory row "
@@ -3493,9 +3462,6 @@ void shutdown()
     if (!c.ready)
         return;
     cudaStreamSynchronize(c.stream);
-    for (auto &kv : c.plans)
-        cufftDestroy(kv.second);
-    c.plans.clear();
     for (auto &kv : c.rfft_mem)
         cudaFree(kv.second);
     c.rfft_mem.clear();

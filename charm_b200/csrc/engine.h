@@ -1,7 +1,6 @@
 // Host runtime of charm_b200: device context, buffer and plan caches, and
 // the call flows of grid synthesis, scattered synthesis and grid analysis.
-// Used by capi.cpp; independent of any framework (plain CUDA runtime and
-// cuFFT).
+// Used by capi.cpp; independent of any framework (plain CUDA runtime).
 #pragma once
 
 #include <string>
@@ -17,7 +16,7 @@ enum
     TIMER_SHS = 0,   // grid synthesis Legendre kernel
     TIMER_SHA = 1,   // grid analysis Legendre kernel
     TIMER_SCTR = 2,  // scattered synthesis kernel
-    TIMER_FFT = 3,   // cuFFT along the parallels
+    TIMER_FFT = 3,   // row transforms along the parallels (rfft.cu)
     TIMER_LON = 4,   // direct longitude sums (non-FFT grids)
     TIMER_PREP = 5,  // seeds, interleave, reductions, nodes
     TIMER_TABLES = 6,

@@ -200,6 +200,16 @@ struct RfftArgs
     // of the row (rfft.cu, k_rfft_inv4); w4 = exp(+2 pi i k / 4H), k < H
     int quarter;
     const double2 *w4;
+    // rows of odd length L (synthesis only): one complex DFT of length
+    // H = L by Bluestein, the row being its real part
+    int odd;
+    // transforms longer than one CTA's shared memory: a cluster of C CTAs
+    // per row, each holding M / C values (rfft.cu, k_rfftc_*); tw then has
+    // M / C entries (exp(-2 pi i k C / M)), twM the M twiddles
+    // exp(-2 pi i k / M), and bh is stored by residue: bh[q M/C + l] is
+    // the FFT_M value C l + q
+    int C;
+    const double2 *twM;
 };
 
 // Size of the fixed device scratch of the allocation-free analysis
@@ -265,6 +275,14 @@ cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
 size_t rfft_smem_bytes(int M);
 cudaError_t rfft_set_smem(size_t smem);
 cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st);
+// tables of a cluster plan (A.C > 1): tw (M / C), twM (M), w (H), ht
+// (H + 1) and the residue-ordered kernel spectrum bh (M)
+cudaError_t launch_rfftc_tables(RfftArgs &A, double2 *tw, double2 *twM,
+                                double2 *w, double2 *ht, double2 *bh,
+                                cudaStream_t st);
+// clusters of C CTAs with the largest shared memory that can be resident
+// at once (0: the cluster shape cannot be scheduled)
+int rfftc_max_clusters(int C, int Mc);
 
 // Batched grid synthesis with the degree sums on the tensor cores
 // (shs_tc.cu): up to SHS_TC_SETS coefficient sets per launch.

@@ -1,4 +1,5 @@
-// Longitude transforms of whole grid rows in shared memory.
+// Longitude transforms of whole grid rows in shared memory (one CTA, or a
+// cluster of CTAs, per row).
 //
 // CHarm hands every grid row to FFTW: a c2r transform of the lumped
 // coefficients in synthesis (src/shs/shs_grd_fft.c) and an r2c transform of
@@ -29,13 +30,23 @@
 //     of the first pass over the banks;
 //   * rows of length 4L whose spectra stop below L (DH2 synthesis): two
 //     complex DFTs of length L per row, each computing every other pair of
-//     the row (k_rfft_inv4, two CTAs per row).
+//     the row (k_rfft_inv4, two CTAs per row);
+//   * rows of odd length L (custom grids, synthesis only): one complex DFT
+//     of length L by Bluestein, the row being its real part
+//     (k_rfft_inv_odd);
+//   * transform lengths beyond one CTA's shared memory (M > 9216, e.g. the
+//     21602-point rows of the nmax 10800 GL grid, M = 24576): a cluster of
+//     C = 2..16 CTAs per row, each holding M / C values, with a radix-C
+//     step across the CTAs on either side of the per-CTA FFTs, read
+//     through distributed shared memory (k_rfftc_fwd / k_rfftc_inv).
 //
 // Both directions are unnormalised, as FFTW's and CHarm's: the synthesis
 // output is sum_k X_k e^(+2 pi i k n / L) over the Hermitian spectrum, and
 // the analysis output is X_k = sum_n x_n e^(-2 pi i k n / L), k <= kmax.
 #include <cstdint>
 #include <type_traits>
+
+#include <cooperative_groups.h>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -755,6 +766,87 @@ struct SrcKernel
     }
 };
 
+// Synthesis input of a row of odd length L: the Hermitian extension Y of
+// the spectrum (Y_k = X_k for k <= (L - 1)/2, conj X_L-k above, zero above
+// kmax, the imaginary part of X_0 ignored), conjugated and chirped; the row
+// is the real part of the inverse DFT of length H = L.
+struct SrcSpectrumOdd
+{
+    const double2 *X;
+    const double2 *w;
+    int H, kmax;
+    __device__ __forceinline__ double2 operator()(int k) const
+    {
+        if (k >= H)
+            return make_double2(0.0, 0.0);
+        double2 y = make_double2(0.0, 0.0);
+        if (2 * k < H)
+        {
+            if (k <= kmax)
+                y = X[k];
+            if (k == 0)
+                y.y = 0.0;
+        }
+        else if (H - k <= kmax)
+            y = conj2(X[H - k]);
+        return cmul(conj2(y), __ldg(&w[k]));
+    }
+};
+
+// ---- transforms longer than one CTA's shared memory ----
+// A cluster of C CTAs owns a row; CTA q holds Mc = M / C values.  FFT_M of
+// a sequence a is computed as
+//   y_q[i] = w_M^(i q) sum_k a[i + k Mc] w_C^(k q)    (radix-C decimation
+//            in frequency across the CTAs, folded into the loads of the
+//            first local pass), then FFT_Mc(y_q)[l] = FFT_M(a)[C l + q],
+// so every CTA holds one residue class of the spectrum, in which the
+// pointwise product of Bluestein's algorithm needs no exchange.  The second
+// FFT_M takes its input by residue classes (decimation in time): each CTA
+// transforms its class, U_q = FFT_Mc, and
+//   v_t = sum_q w_M^(q t) U_q[t mod Mc]
+// is gathered through distributed shared memory for the outputs t a CTA
+// writes.
+
+// Input of the first local pass of CTA q: a = src(0..M) vanishes from nz
+// on, so blocks k with k Mc >= nz are not read.
+template <class Src>
+struct SrcClusterDif
+{
+    Src src;
+    const double2 *twM;
+    int q, C, Mc, M, nz;
+    __device__ __forceinline__ double2 operator()(int i) const
+    {
+        double2 acc = src(i);
+        for (int k = 1; k < C && k * Mc < nz; k++)
+        {
+            const int kq = (k * q) % C;
+            acc = add2(acc, cmul(src(i + k * Mc), __ldg(&twM[kq * Mc])));
+        }
+        if (q == 0)
+            return acc;
+        const int e = (int)(((long long)i * q) % M);
+        return cmul(acc, __ldg(&twM[e]));
+    }
+};
+
+// v_t of the second FFT_M (t < M) from the residue transforms U_q held in
+// the shared memory of the cluster's CTAs.
+__device__ __forceinline__ double2 cluster_v(
+    const cooperative_groups::cluster_group &cl, double2 *s,
+    const double2 *__restrict__ twM, int C, int Mc, int M, int t)
+{
+    const int pj = pidx(t % Mc);
+    double2 acc = *cl.map_shared_rank(s + pj, 0);
+    for (int qq = 1; qq < C; qq++)
+    {
+        const double2 u = *cl.map_shared_rank(s + pj, qq);
+        const int e = (int)(((long long)qq * t) % M);
+        acc = add2(acc, cmul(u, __ldg(&twM[e])));
+    }
+    return acc;
+}
+
 } // namespace
 
 // Register cap NR: M / 16 <= 576 threads of 96 registers with V = 16 values
@@ -888,6 +980,130 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_inv4(RfftArgs A)
         OutRowQ{reinterpret_cast<double2 *>(A.x + row * A.ldx), A.w, rho});
 }
 
+// Synthesis of rows of odd length L = H: Bluestein over the whole row
+// (run-time plan), the row being the real part of the inverse DFT.
+template <int V, int NR>
+__global__ void RFFT_BOUNDS(NR) k_rfft_inv_odd(RfftArgs A)
+{
+    extern __shared__ __align__(16) double2 s[];
+    const int tid = threadIdx.x, T = blockDim.x;
+    const long long row = blockIdx.x;
+    SrcSpectrumOdd src{A.X + row * A.ldX, A.w, A.H, A.kmax};
+    dft_h<V, 0>(s, A, tid, T, src);
+    double *x = A.x + row * A.ldx;
+    for (int j = tid; j < A.H; j += T)
+        x[j] = dft_h_out(s, A, j).x;
+}
+
+// Analysis direction of a cluster plan (A.C CTAs per row, double rows).
+template <int V, int NR>
+__global__ void RFFT_BOUNDS(NR) k_rfftc_fwd(RfftArgs A)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) double2 s[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int C = A.C, q = (int)cl.block_rank(), H = A.H;
+    const int Mc = A.M / C;
+    const long long row = blockIdx.x / C;
+    SrcRow src{reinterpret_cast<const double2 *>(A.x + row * A.ldx), A.w, H};
+    SrcClusterDif<SrcRow> dif{src, A.twM, q, C, Mc, A.M, H};
+    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, A.bh + (size_t)q * Mc);
+    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, SrcSmem{s}, nullptr);
+    cl.sync();
+    // this CTA's share of the half spectrum X_0..X_kmax
+    const int nk = A.kmax + 1;
+    const int k0 = (int)((long long)nk * q / C);
+    const int k1 = (int)((long long)nk * (q + 1) / C);
+    double2 *X = A.X + row * A.ldX;
+    for (int k = k0 + tid; k < k1; k += T)
+    {
+        const int ka = (k == H) ? 0 : k;
+        const int kb = (k == 0) ? 0 : H - k;
+        const double2 va = cluster_v(cl, s, A.twM, C, Mc, A.M, ka);
+        const double2 vb = cluster_v(cl, s, A.twM, C, Mc, A.M, kb);
+        const double2 zk = cmul(__ldg(&A.w[ka]), conj2(va));
+        const double2 zh = conj2(cmul(__ldg(&A.w[kb]), conj2(vb)));
+        const double2 e = cmul(__ldg(&A.ht[k]), sub2(zk, zh));
+        const double2 sm = add2(zk, zh);
+        X[k] = make_double2(0.5 * (sm.x + e.y), 0.5 * (sm.y - e.x));
+    }
+    // no CTA leaves while another still reads its shared memory
+    cl.sync();
+}
+
+// Synthesis direction of a cluster plan: rows of even length (ODD false,
+// pairs x_2t + i x_2t+1 for t < H) or of odd length H (the real part).
+template <int V, int NR, bool ODD>
+__global__ void RFFT_BOUNDS(NR) k_rfftc_inv(RfftArgs A)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) double2 s[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int C = A.C, q = (int)cl.block_rank(), H = A.H;
+    const int Mc = A.M / C;
+    const long long row = blockIdx.x / C;
+    if constexpr (ODD)
+    {
+        SrcSpectrumOdd src{A.X + row * A.ldX, A.w, H, A.kmax};
+        SrcClusterDif<SrcSpectrumOdd> dif{src, A.twM, q, C, Mc, A.M, H};
+        fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, A.bh + (size_t)q * Mc);
+    }
+    else
+    {
+        SrcSpectrum src{A.X + row * A.ldX, A.w, A.ht, H, A.kmax};
+        SrcClusterDif<SrcSpectrum> dif{src, A.twM, q, C, Mc, A.M, H};
+        fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, A.bh + (size_t)q * Mc);
+    }
+    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, SrcSmem{s}, nullptr);
+    cl.sync();
+    const int t0 = (int)((long long)H * q / C);
+    const int t1 = (int)((long long)H * (q + 1) / C);
+    for (int t = t0 + tid; t < t1; t += T)
+    {
+        const double2 v = cluster_v(cl, s, A.twM, C, Mc, A.M, t);
+        const double2 z = cmul(__ldg(&A.w[t]), conj2(v));
+        if constexpr (ODD)
+            A.x[row * A.ldx + t] = z.x;
+        else
+            reinterpret_cast<double2 *>(A.x + row * A.ldx)[t] = conj2(z);
+    }
+    cl.sync();
+}
+
+// Residue-ordered FFT_M of the Bluestein kernel, times 1/M: CTA q
+// (blockIdx.x, no cluster needed) writes bh[q Mc + l] = FFT_M(b)[C l + q] / M.
+template <int V, int NR>
+__global__ void RFFT_BOUNDS(NR) k_rfftc_kspec(RfftArgs A, double2 *bh)
+{
+    extern __shared__ __align__(16) double2 s[];
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int C = A.C, q = (int)blockIdx.x;
+    const int Mc = A.M / C;
+    SrcClusterDif<SrcKernel> dif{SrcKernel{A.w, A.H, A.M}, A.twM, q, C, Mc,
+                                 A.M, A.M};
+    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, nullptr);
+    const double inv = 1.0 / (double)A.M;
+    for (int l = tid; l < Mc; l += T)
+    {
+        const double2 v = s[pidx(l)];
+        bh[(size_t)q * Mc + l] = make_double2(v.x * inv, v.y * inv);
+    }
+}
+
+// tw[k] = exp(-2 pi i k / n), k < n
+__global__ void k_rfft_twiddles(int n, double2 *tw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        double sn, cs;
+        sincospi(2.0 * (double)i / (double)n, &sn, &cs);
+        tw[i] = make_double2(cs, -sn);
+    }
+}
+
 // w4[k] = exp(2 pi i k / 4H), k < H
 __global__ void k_rfft_w4(int H, double2 *w4)
 {
@@ -985,7 +1201,12 @@ cudaError_t rfft_set_smem(size_t smem)
         (const void *)k_rfft_fwd<16, 96, true, 9216>,
         (const void *)k_rfft_inv<16, 96, true, 9216>,
         (const void *)k_rfft_inv4<16, 96, 4608>,
-        (const void *)k_rfft_kernel_spectrum<16, 96>};
+        (const void *)k_rfft_kernel_spectrum<16, 96>,
+        (const void *)k_rfft_inv_odd<16, 96>,
+        (const void *)k_rfftc_fwd<16, 96>,
+        (const void *)k_rfftc_inv<16, 96, false>,
+        (const void *)k_rfftc_inv<16, 96, true>,
+        (const void *)k_rfftc_kspec<16, 96>};
     for (const void *f : fns)
     {
         cudaError_t e = cudaFuncSetAttribute(
@@ -993,7 +1214,72 @@ cudaError_t rfft_set_smem(size_t smem)
         if (e != cudaSuccess)
             return e;
     }
+    // clusters of 16 CTAs (rows beyond 8 x 9216) are a non-portable size
+    const void *cfns[] = {(const void *)k_rfftc_fwd<16, 96>,
+                          (const void *)k_rfftc_inv<16, 96, false>,
+                          (const void *)k_rfftc_inv<16, 96, true>};
+    for (const void *f : cfns)
+    {
+        // where refused, plans with 16 CTAs fail their occupancy check
+        // (rfftc_max_clusters) instead
+        if (cudaFuncSetAttribute(
+                f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+            cudaGetLastError();
+    }
     return cudaSuccess;
+}
+
+int rfftc_max_clusters(int C, int Mc)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)C, 1, 1);
+    cfg.blockDim = dim3((unsigned)(Mc / 16), 1, 1);
+    cfg.dynamicSmemBytes = rfft_smem_bytes(Mc);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_rfftc_fwd<16, 96>, &cfg) !=
+        cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    int n2 = 0;
+    if (cudaOccupancyMaxActiveClusters(&n2, k_rfftc_inv<16, 96, false>,
+                                       &cfg) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    return n < n2 ? n : n2;
+}
+
+cudaError_t launch_rfftc_tables(RfftArgs &A, double2 *tw, double2 *twM,
+                                double2 *w, double2 *ht, double2 *bh,
+                                cudaStream_t st)
+{
+    const int Mc = A.M / A.C;
+    k_rfft_twiddles<<<(Mc + 255) / 256, 256, 0, st>>>(Mc, tw);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    const int n = (A.M > A.H + 1 ? A.M : A.H + 1);
+    k_rfft_tables<<<(n + 255) / 256, 256, 0, st>>>(A.H, A.M, twM, w, ht);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    A.tw = tw;
+    A.twM = twM;
+    A.w = w;
+    A.ht = ht;
+    k_rfftc_kspec<16, 96><<<A.C, Mc / 16, rfft_smem_bytes(Mc), st>>>(A, bh);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
@@ -1001,8 +1287,40 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
     const unsigned grid = (unsigned)A.nrows;
     if (grid == 0)
         return cudaSuccess;
+    if (A.C > 1)
+    {
+        // one cluster of A.C CTAs per row
+        if (A.f32_rows || A.quarter || A.direct || (!inverse && A.odd))
+            return cudaErrorInvalidValue;
+        const int Mc = A.M / A.C;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid * (unsigned)A.C, 1, 1);
+        cfg.blockDim = dim3((unsigned)(Mc / 16), 1, 1);
+        cfg.dynamicSmemBytes = rfft_smem_bytes(Mc);
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)A.C;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (!inverse)
+            return cudaLaunchKernelEx(&cfg, k_rfftc_fwd<16, 96>, A);
+        if (A.odd)
+            return cudaLaunchKernelEx(&cfg, k_rfftc_inv<16, 96, true>, A);
+        return cudaLaunchKernelEx(&cfg, k_rfftc_inv<16, 96, false>, A);
+    }
     const size_t smem = rfft_smem_bytes(A.M);
     const int T = A.M / 16;
+    if (A.odd)
+    {
+        // rows of odd length: synthesis only, Bluestein, run-time plan
+        if (!inverse || A.f32_rows || A.direct)
+            return cudaErrorInvalidValue;
+        k_rfft_inv_odd<16, 96><<<grid, T, smem, st>>>(A);
+        return cudaGetLastError();
+    }
     if (A.quarter)
     {
         // two CTAs per row (rfft plans set quarter only with M = 4608,

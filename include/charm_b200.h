@@ -331,7 +331,7 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_sctr_adjoint_dev(
 #define CHARM_B200_STATIC_SCRATCH_BYTES 33554432
 
 /* charm_b200_sha_point_dev that allocates nothing: no cudaMalloc, cudaFree,
- * pinned or heap memory and no allocating library routine (no cuFFT plan).
+ * pinned or heap memory and no allocating library routine.
  * No counterpart in CHarm; it serves callers that cannot allocate during
  * the call -- device memory owned by another allocator (a framework's
  * caching pool), or a loop that must not synchronise the device as
@@ -366,9 +366,11 @@ CHARM_EXTERN void *CHARM_CDECL charm_b200_stream(void);
 CHARM_EXTERN void CHARM_CDECL charm_b200_timing(int enable);
 
 /* Reads the accumulated timers: ms[i], count[i] for i < n (0 grid synthesis
- * kernel, 1 grid analysis kernel, 2 scattered synthesis kernel, 3 cuFFT, 4
- * direct longitude sums, 5 preparation kernels, 6 tables) and the number of
- * this library's kernel launches and of cuFFT executions since enabled.
+ * kernel, 1 grid analysis kernel, 2 scattered synthesis kernel, 3 row
+ * transforms, 4 direct longitude sums, 5 preparation kernels, 6 tables) and
+ * the number of this library's kernel launches and of library (non-charm)
+ * kernel launches since enabled; the latter stays 0, since every transform
+ * runs this library's own kernels.
  * Returns the number of timers available. */
 CHARM_EXTERN int CHARM_CDECL charm_b200_timing_read(
     double *ms, unsigned long long *count, int n,

@@ -1,23 +1,31 @@
-"""The shared-memory row transforms (rfft.cu) against cuFFT on the same
-lumped coefficients / grids, through the public synthesis and analysis.
+"""The longitude transforms (rfft.cu) against numpy's FFT in double
+precision and against CHarm, through the public synthesis and analysis.
 
-CHARM_B200_ROW_FFT=library routes the longitude transforms through cuFFT
-instead; both compute the same unnormalised DFTs, so the outputs agree to a
-few units of rounding.  The grids cover every transform plan: direct
-mixed radix (H = 2^a 3^b, a >= 6), Bluestein for every other length up to
-M = 9216, the quarter-length synthesis of rows of length 4L whose spectra
-stop below L (DH2 grids), and lengths where the row transform does not
-apply (H < 8)."""
-import os
+Every transform plan is covered:
+  * direct mixed radix (H = 2^a 3^b, a >= 6) and Bluestein with run-time
+    and compile-time plans in one CTA (M <= 9216);
+  * tiny rows (fewer than 16 points) and rows of odd length (one complex
+    DFT of the whole row by Bluestein);
+  * rows longer than one CTA's shared memory, transformed by clusters of
+    2, 4 and 8 CTAs (e.g. the 21602-point rows of the nmax 10800 GL grid
+    and the 43204-point rows of its DH2 grid);
+  * the quarter-length synthesis of DH2 rows whose spectra stop below L.
 
+Synthesis reference: the oracle's lumped coefficients of the same
+latitudes, summed along the parallels by numpy.fft.irfft (the role FFTW
+plays in CHarm, src/shs/shs_grd_fft.c).  Analysis reference: CHarm's own
+charm_sha_point (oracle/_ref), or the oracle's analysis (numpy.fft.rfft)
+where CHarm's build is absent."""
 import numpy as np
 import pytest
 
 from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula, rel_rms
+from oracle import charm_ref, orc
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-14
+TOL = 1e-13
+LATS = np.array([1.3, 0.7, -0.2, -1.1])
 
 
 @pytest.fixture(scope="module")
@@ -26,50 +34,95 @@ def cb():
     return charm_b200
 
 
-def both(fn):
-    old = os.environ.pop("CHARM_B200_ROW_FFT", None)
-    try:
-        a = fn()
-        os.environ["CHARM_B200_ROW_FFT"] = "library"
-        b = fn()
-    finally:
-        os.environ.pop("CHARM_B200_ROW_FFT", None)
-        if old is not None:
-            os.environ["CHARM_B200_ROW_FFT"] = old
-    return a, b
+def oracle_rows(lat, nlon, N, c, s):
+    """Synthesis on the points (lat x 2 pi j / nlon): oracle lumped
+    coefficients and numpy's inverse real FFT."""
+    lon = 2.0 * np.pi * np.arange(nlon) / nlon
+    p = orc.Point(orc.GRID, lat, lon, np.full(lat.size, R_EARTH))
+    return orc.shs_point(p, orc.Shc(N, GM, R_EARTH, c, s), N)[0]
+
+
+@pytest.mark.parametrize("nlon,N", [
+    (2, 0), (3, 1), (4, 1), (5, 2), (6, 2), (14, 6), (15, 7), (16, 7),
+    (21, 10),
+    (384, 120),      # H = 192 = 2^6 3, direct
+    (576, 200),      # H = 288, Bluestein M = 576
+    (722, 360),      # H = 361, Bluestein M = 768
+    (1001, 300),     # odd, Bluestein of the whole row, M = 2304
+    (4382, 700),     # H = 2191, compile-time plan M = 4608
+    (8000, 700),     # H = 4000, compile-time plan M = 9216
+    (8764, 700),     # 4 x 2191: quarter-length synthesis
+    (9218, 700),     # H = 4609: cluster of 2 CTAs, M = 10368
+    (9999, 500),     # odd, cluster of 4 CTAs, M = 20736
+    (21602, 800),    # H = 10801: cluster of 4 CTAs, M = 24576
+    (43204, 600),    # H = 21602: cluster of 8 CTAs, M = 49152
+])
+def test_synthesis_rows_against_numpy(cb, nlon, N):
+    c, s = kaula(N, 4242 + nlon)
+    lon = 2.0 * np.pi * np.arange(nlon) / nlon
+    p = cb.PointGrid(LATS, lon, np.full(LATS.size, R_EARTH))
+    f = cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s), N)
+    fo = oracle_rows(LATS, nlon, N, c, s)
+    assert rel_rms(f, fo) <= TOL
+    f00 = GM / R_EARTH
+    if N >= 2:
+        # the signal without the degree-0 term, against its own size
+        assert rel_rms(np.ravel(f) - f00, np.ravel(fo) - f00) <= 1e-9
+
+
+def test_synthesis_rows_nmax10800_against_numpy(cb):
+    """The north-star grid's row length at its full degree: 21602-point
+    rows carrying orders 0..10800 (cluster transform, M = 24576)."""
+    N = 10800
+    c, s = kaula(N, 3000, sqrt_scaling=False)
+    lat = LATS[:2]
+    nlon = 2 * (N + 1)
+    lon = np.arange(nlon) * (np.pi / (N + 1))
+    f = cb.shs_point(cb.PointGrid(lat, lon, np.full(lat.size, R_EARTH)),
+                     cb.Shc(N, GM, R_EARTH, c, s), N)
+    fo = oracle_rows(lat, nlon, N, c, s)
+    assert rel_rms(f, fo) <= TOL
+    f00 = GM / R_EARTH
+    assert rel_rms(np.ravel(f) - f00, np.ravel(fo) - f00) <= 1e-10
+
+
+def analysis_reference(kind, N, f):
+    if charm_ref.available("d"):
+        C = charm_ref.Charm("d")
+        k = {"GL": charm_ref.GL, "DH1": charm_ref.DH1, "DH2": charm_ref.DH2}[kind]
+        cp, lat, lon, w = C.grid(k, N, R_EARTH)
+        return C.sha_point(cp, np.ravel(f), N, GM, R_EARTH)
+    ctor = {"GL": lambda: orc.gl(N, R_EARTH),
+            "DH1": lambda: orc.dh(N, R_EARTH, orc.DH1),
+            "DH2": lambda: orc.dh(N, R_EARTH, orc.DH2)}[kind]
+    out = orc.sha_point(ctor(), f, N, GM, R_EARTH)
+    return out.c, out.s
 
 
 @pytest.mark.parametrize("grid,N", [
-    ("GL", 7),      # H = 8, Bluestein M = 64
-    ("GL", 191),    # H = 192 = 2^6 3, direct
-    ("GL", 287),    # H = 288 = 2^5 3^2, Bluestein M = 576
-    ("GL", 360),    # H = 361 = 19^2, Bluestein M = 768
-    ("DH1", 100),   # H = 101, Bluestein M = 256
-    # DH2 rows of length 4 (N + 1): synthesis by two DFTs of length N + 1
-    # (Bluestein M = 4608) per row, analysis with H = 2 (N + 1), M = 9216
-    ("DH2", 2190),
-    ("DH2", 2160),
-    ("GL", 2190),   # H = 2191, Bluestein M = 4608
-    # H = 4000, M = 9216 both ways: the spectrum reaches beyond a quarter
-    # of the row, so the quarter-length synthesis does not apply
-    ("GL", 3999),
-    ("GL", 2),      # H = 3, library transform
+    ("GL", 191),    # H = 192, direct
+    ("GL", 360),    # H = 361, run-time Bluestein plan
+    ("DH1", 100),   # H = 101
+    ("GL", 2190),   # H = 2191, compile-time plan M = 4608
+    ("DH2", 2190),  # H = 4382, compile-time plan M = 9216
+    ("GL", 4700),   # H = 4701, cluster of 2 CTAs, M = 10368
+    ("DH2", 2400),  # H = 4802, cluster of 2 CTAs, M = 10368
 ])
-def test_row_transform_matches_library(cb, grid, N):
+def test_analysis_rows(cb, grid, N):
+    """Analysis of a synthesised grid against CHarm's analysis of the same
+    grid values, and the round trip back to the coefficients."""
     ctor = {"GL": cb.PointGridGL, "DH1": cb.PointGridDH1,
             "DH2": cb.PointGridDH2}[grid]
-    c, s = kaula(N, 4242 + N)
+    c, s = kaula(N, 4300 + N)
     p = ctor(N, R_EARTH)
-    shc = cb.Shc(N, GM, R_EARTH, c, s)
-    f_row, f_lib = both(lambda: cb.shs_point(p, shc, N))
-    assert rel_rms(f_row, f_lib) <= TOL
-    a_row, a_lib = both(lambda: cb.sha_point(p, f_lib, N, GM, R_EARTH))
-    assert coef_rel_rms(a_row.c, a_row.s, a_lib.c, a_lib.s) <= TOL
-    # and the round trip closes through the row transforms alone
-    assert coef_rel_rms(a_row.c, a_row.s, c, s) <= 1e-12
+    f = cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s), N)
+    out = cb.sha_point(p, f, N, GM, R_EARTH)
+    cr, sr = analysis_reference(grid, N, f)
+    assert coef_rel_rms(out.c, out.s, cr, sr) <= TOL
+    assert coef_rel_rms(out.c, out.s, c, s) <= 1e-12
 
 
-def test_row_transform_zero_and_constant_rows(cb):
+def test_row_transform_constant_rows(cb):
     """A field that is constant along every row has one nonzero order."""
     N = 360
     c = np.zeros((N + 1) * (N + 2) // 2)
@@ -77,7 +130,5 @@ def test_row_transform_zero_and_constant_rows(cb):
     c[0] = 1.0
     c[2] = 0.25    # C20 (order-major triangle: m = 0 column first)
     p = cb.PointGridGL(N, R_EARTH)
-    f_row, f_lib = both(lambda: cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s),
-                                             N))
-    assert rel_rms(f_row, f_lib) <= TOL
-    assert np.max(np.ptp(f_row, axis=1)) <= 1e-14 * np.max(np.abs(f_row))
+    f = cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s), N)
+    assert np.max(np.ptp(f, axis=1)) <= 1e-14 * np.max(np.abs(f))
