@@ -1025,3 +1025,627 @@ double charm_b200_fp64_peak_tflops(void)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Single-precision ABI: CHarm's float build exports the same entry points
+// with the prefix charmf_ and float arrays (src/prec.h:84-86 with @P@ = f;
+// src/shs/shs.h.in:168-173, 239-244, 344-349, 428-435;
+// src/sha/sha.h.in:164-169; src/crd/crd.h.in:477-760;
+// src/shc/shc.h.in:423-602; src/err/err.h.in:236-294; src/glob/glob.c).
+// Argument checks restate the double-precision ones above.  The transforms
+// run on the single-precision kernels where they serve the call (potential
+// on grids with FFT longitudes, nmax <= 2200, every row at the
+// coefficients' radius), otherwise on the FP64 path with the results
+// rounded to float.  Float inputs convert to double exactly; during a call
+// the comparison thresholds are the float build's (charmf_glob_threshold*),
+// as CHarm's float build applies them.
+// ---------------------------------------------------------------------------
+#include <vector>
+
+extern "C"
+{
+
+CHARM_EXTERN float charmf_glob_threshold = 100.0f * FLT_EPSILON;
+CHARM_EXTERN float charmf_glob_threshold2 = 100000.0f * FLT_EPSILON;
+CHARM_EXTERN unsigned long charmf_glob_polar_optimization_a1 = 100;
+CHARM_EXTERN float charmf_glob_polar_optimization_a2 = -1.0f;
+
+charmf_err *charmf_err_init(void) { return charm_err_init(); }
+void charmf_err_free(charmf_err *err) { charm_err_free(err); }
+void charmf_err_reset(charmf_err *err) { charm_err_reset(err); }
+void charmf_err_handler(charmf_err *err, _Bool terminate)
+{
+    charm_err_handler(err, terminate);
+}
+_Bool charmf_err_isempty(const charmf_err *err)
+{
+    return charm_err_isempty(err);
+}
+
+charmf_point *charmf_crd_point_init(int type, size_t nlat, size_t nlon,
+                                    float *lat, float *lon, float *r)
+{
+    if (!is_point_type(type))
+        return NULL;
+    if (type == CHARM_CRD_POINT_SCATTERED && nlat != nlon)
+        return NULL;
+    charmf_point *p = (charmf_point *)malloc(sizeof(charmf_point));
+    if (!p)
+        return NULL;
+    p->lat = p->lon = p->r = p->w = NULL;
+    if (nlat > 0)
+    {
+        p->lat = lat;
+        p->r = r;
+    }
+    if (nlon > 0)
+        p->lon = lon;
+    p->nlat = nlat;
+    p->nlon = nlon;
+    p->npoint = type == CHARM_CRD_POINT_SCATTERED ? nlat
+                                                  : (is_grid_type(type)
+                                                         ? nlat * nlon
+                                                         : 0);
+    p->type = type;
+    p->owner = 0;
+    p->distributed = 0;
+    return p;
+}
+
+static charmf_point *pointf_alloc(int type, size_t nlat, size_t nlon,
+                                  bool zero)
+{
+    if (!is_point_type(type))
+        return NULL;
+    if (type == CHARM_CRD_POINT_SCATTERED && nlat != nlon)
+        return NULL;
+    float *lat = NULL, *lon = NULL, *r = NULL, *w = NULL;
+    auto al = [&](size_t n) -> float * {
+        return zero ? (float *)calloc(n, sizeof(float))
+                    : (float *)malloc(n * sizeof(float));
+    };
+    charmf_point *p = NULL;
+    if (nlat > 0)
+    {
+        lat = al(nlat);
+        r = al(nlat);
+        if (!lat || !r)
+            goto FAIL;
+    }
+    if (nlon > 0)
+    {
+        lon = al(nlon);
+        if (!lon)
+            goto FAIL;
+    }
+    p = charmf_crd_point_init(type, nlat, nlon, lat, lon, r);
+    if (!p)
+        goto FAIL;
+    if (is_quad_type(type))
+    {
+        w = al(nlat > 0 ? nlat : 1);
+        if (!w)
+            goto FAIL;
+        p->w = w;
+    }
+    p->owner = 1;
+    return p;
+FAIL:
+    free(lat);
+    free(lon);
+    free(r);
+    free(w);
+    free(p);
+    return NULL;
+}
+
+charmf_point *charmf_crd_point_malloc(int type, size_t nlat, size_t nlon)
+{
+    return pointf_alloc(type, nlat, nlon, false);
+}
+
+charmf_point *charmf_crd_point_calloc(int type, size_t nlat, size_t nlon)
+{
+    return pointf_alloc(type, nlat, nlon, true);
+}
+
+void charmf_crd_point_free(charmf_point *pnt)
+{
+    if (!pnt)
+        return;
+    if (pnt->owner)
+    {
+        free(pnt->lat);
+        free(pnt->lon);
+        free(pnt->r);
+        free(pnt->w);
+    }
+    free(pnt);
+}
+
+void charmf_crd_point_gl_shape(unsigned long nmax, size_t *nlat, size_t *nlon)
+{
+    charm_crd_point_gl_shape(nmax, nlat, nlon);
+}
+
+void charmf_crd_point_dh1_shape(unsigned long nmax, size_t *nlat,
+                                size_t *nlon)
+{
+    charm_crd_point_dh1_shape(nmax, nlat, nlon);
+}
+
+void charmf_crd_point_dh2_shape(unsigned long nmax, size_t *nlat,
+                                size_t *nlon)
+{
+    charm_crd_point_dh2_shape(nmax, nlat, nlon);
+}
+
+// the double-precision grid (nodes from the GPU Newton iteration), rounded
+static charmf_point *quad_gridf(int type, unsigned long nmax, float r)
+{
+    charm_point *d = quad_grid(type, nmax, (double)r);
+    if (!d)
+        return NULL;
+    charmf_point *p = pointf_alloc(type, d->nlat, d->nlon, false);
+    if (p)
+    {
+        for (size_t i = 0; i < d->nlat; i++)
+        {
+            p->lat[i] = (float)d->lat[i];
+            p->r[i] = r;
+            p->w[i] = (float)d->w[i];
+        }
+        for (size_t j = 0; j < d->nlon; j++)
+            p->lon[j] = (float)d->lon[j];
+    }
+    charm_crd_point_free(d);
+    return p;
+}
+
+charmf_point *charmf_crd_point_gl(unsigned long nmax, float r)
+{
+    return quad_gridf(CHARM_CRD_POINT_GRID_GL, nmax, r);
+}
+
+charmf_point *charmf_crd_point_dh1(unsigned long nmax, float r)
+{
+    return quad_gridf(CHARM_CRD_POINT_GRID_DH1, nmax, r);
+}
+
+charmf_point *charmf_crd_point_dh2(unsigned long nmax, float r)
+{
+    return quad_gridf(CHARM_CRD_POINT_GRID_DH2, nmax, r);
+}
+
+charmf_shc *charmf_shc_init(unsigned long nmax, float mu, float r, float *c,
+                            float *s)
+{
+    if (r <= 0.0f)
+        return NULL;
+    charmf_shc *h = (charmf_shc *)malloc(sizeof(charmf_shc));
+    if (!h)
+        return NULL;
+    h->nmax = nmax;
+    h->mu = mu;
+    h->r = r;
+    size_t nmax1 = (size_t)nmax + 1;
+    size_t len = ((nmax1 + 1) * nmax1) / 2;
+    h->nc = h->ns = len;
+    h->owner = 0;
+    h->distributed = 0;
+    h->c = (float **)malloc(nmax1 * sizeof(float *));
+    h->s = (float **)malloc(nmax1 * sizeof(float *));
+    if (!h->c || !h->s)
+    {
+        free(h->c);
+        free(h->s);
+        free(h);
+        return NULL;
+    }
+    size_t idx = 0;
+    for (size_t m = 0; m <= nmax; m++)
+    {
+        h->c[m] = c + idx;
+        h->s[m] = s + idx;
+        idx += nmax1 - m;
+    }
+    return h;
+}
+
+static charmf_shc *shcf_alloc(unsigned long nmax, float mu, float r,
+                              bool zero)
+{
+    size_t nmax1 = (size_t)nmax + 1;
+    size_t len = ((nmax1 + 1) * nmax1) / 2;
+    float *c = zero ? (float *)calloc(len, sizeof(float))
+                    : (float *)malloc(len * sizeof(float));
+    float *s = zero ? (float *)calloc(len, sizeof(float))
+                    : (float *)malloc(len * sizeof(float));
+    charmf_shc *h = NULL;
+    if (!c || !s)
+        goto FAIL;
+    h = charmf_shc_init(nmax, mu, r, c, s);
+    if (!h)
+        goto FAIL;
+    h->owner = 1;
+    return h;
+FAIL:
+    free(c);
+    free(s);
+    return NULL;
+}
+
+charmf_shc *charmf_shc_malloc(unsigned long nmax, float mu, float r)
+{
+    return shcf_alloc(nmax, mu, r, false);
+}
+
+charmf_shc *charmf_shc_calloc(unsigned long nmax, float mu, float r)
+{
+    return shcf_alloc(nmax, mu, r, true);
+}
+
+void charmf_shc_free(charmf_shc *shcs)
+{
+    if (!shcs)
+        return;
+    if (shcs->owner && shcs->c && shcs->s)
+    {
+        free(shcs->c[0]);
+        free(shcs->s[0]);
+    }
+    free(shcs->c);
+    free(shcs->s);
+    free(shcs);
+}
+
+} // extern "C"
+
+namespace
+{
+
+// the float build's thresholds in force for the duration of a call
+struct FloatThresholds
+{
+    double t1, t2, a2;
+    unsigned long a1;
+    FloatThresholds()
+        : t1(charm_glob_threshold), t2(charm_glob_threshold2),
+          a2(charm_glob_polar_optimization_a2),
+          a1(charm_glob_polar_optimization_a1)
+    {
+        charm_glob_threshold = (double)charmf_glob_threshold;
+        charm_glob_threshold2 = (double)charmf_glob_threshold2;
+        charm_glob_polar_optimization_a1 = charmf_glob_polar_optimization_a1;
+        charm_glob_polar_optimization_a2 =
+            (double)charmf_glob_polar_optimization_a2;
+    }
+    ~FloatThresholds()
+    {
+        charm_glob_threshold = t1;
+        charm_glob_threshold2 = t2;
+        charm_glob_polar_optimization_a1 = a1;
+        charm_glob_polar_optimization_a2 = a2;
+    }
+};
+
+// a charm_point over double copies of a charmf_point's arrays
+struct PointD
+{
+    charm_point p{};
+    std::vector<double> lat, lon, r, w;
+    explicit PointD(const charmf_point *f)
+    {
+        auto cp = [](const float *src, size_t n, std::vector<double> &dst) {
+            if (src)
+                dst.assign(src, src + n);
+        };
+        cp(f->lat, f->nlat, lat);
+        cp(f->lon, f->nlon, lon);
+        cp(f->r, f->nlat, r);
+        cp(f->w, f->nlat, w);
+        p.type = f->type;
+        p.nlat = f->nlat;
+        p.nlon = f->nlon;
+        p.npoint = f->npoint;
+        p.lat = lat.empty() ? nullptr : lat.data();
+        p.lon = lon.empty() ? nullptr : lon.data();
+        p.r = r.empty() ? nullptr : r.data();
+        p.w = w.empty() ? nullptr : w.data();
+        p.owner = 0;
+        p.distributed = 0;
+    }
+};
+
+// a charm_shc over a contiguous double copy of a charmf_shc's triangle
+struct ShcD
+{
+    charm_shc h{};
+    std::vector<double> c, s;
+    std::vector<double *> cp, sp;
+    explicit ShcD(const charmf_shc *f, bool copy = true)
+    {
+        const size_t n1 = (size_t)f->nmax + 1;
+        c.assign(n1 * (n1 + 1) / 2, 0.0);
+        s.assign(c.size(), 0.0);
+        cp.resize(n1);
+        sp.resize(n1);
+        size_t idx = 0;
+        for (size_t m = 0; m < n1; m++)
+        {
+            if (copy)
+                for (size_t k = 0; k < n1 - m; k++)
+                {
+                    c[idx + k] = (double)f->c[m][k];
+                    s[idx + k] = (double)f->s[m][k];
+                }
+            cp[m] = c.data() + idx;
+            sp[m] = s.data() + idx;
+            idx += n1 - m;
+        }
+        h.nmax = f->nmax;
+        h.mu = (double)f->mu;
+        h.r = (double)f->r;
+        h.nc = h.ns = c.size();
+        h.c = cp.data();
+        h.s = sp.data();
+        h.owner = 0;
+        h.distributed = 0;
+    }
+};
+
+// contiguous float copy of a charmf_shc's triangle
+void gather_tri(const charmf_shc *f, std::vector<float> &c,
+                std::vector<float> &s)
+{
+    const size_t n1 = (size_t)f->nmax + 1;
+    c.resize(n1 * (n1 + 1) / 2);
+    s.resize(c.size());
+    size_t idx = 0;
+    for (size_t m = 0; m < n1; m++)
+    {
+        std::memcpy(c.data() + idx, f->c[m], (n1 - m) * sizeof(float));
+        std::memcpy(s.data() + idx, f->s[m], (n1 - m) * sizeof(float));
+        idx += n1 - m;
+    }
+}
+
+bool check_nmax_f(const charmf_shc *shcs, unsigned long nmax, charm_err *err,
+                  const char *what, const char *func)
+{
+    if (nmax > shcs->nmax)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg,
+                 "Maximum harmonic degree of the %s \"nmax = %lu\" cannot be "
+                 "larger than maximum harmonic degree of spherical harmonic "
+                 "coefficients \"shcs->nmax = %lu\".",
+                 what, nmax, shcs->nmax);
+        err_set(err, __FILE__, __LINE__, func, CHARM_EFUNCARG, msg);
+        return false;
+    }
+    return true;
+}
+
+// synthesis of npar components on the FP64 path, rounded into f[q]
+void shs_f_fp64(const charmf_point *pnt, const charmf_shc *shcs,
+                unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
+                int npar, float **f, charm_err *err, const char *func)
+{
+    PointD dp(pnt);
+    ShcD dh(shcs);
+    std::vector<std::vector<double>> out(npar,
+                                         std::vector<double>(pnt->npoint));
+    std::vector<double *> fp(npar);
+    for (int q = 0; q < npar; q++)
+        fp[q] = out[q].data();
+    cb::Status st = cb::shs_point(&dp.p, &dh.h, nmax, kgrad, dr, dlat, dlon,
+                                  fp.data());
+    if (!st.ok())
+    {
+        err_set(err, __FILE__, __LINE__, func, st.code, st.msg.c_str());
+        return;
+    }
+    for (int q = 0; q < npar; q++)
+        for (size_t i = 0; i < pnt->npoint; i++)
+            f[q][i] = (float)out[q][i];
+}
+
+bool check_type_shs_f(const charmf_point *pnt, charm_err *err,
+                      const char *func)
+{
+    if (pnt->type != CHARM_CRD_POINT_SCATTERED && !is_grid_type(pnt->type))
+    {
+        err_set(err, __FILE__, __LINE__, func, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic synthesis "
+                "of point values.");
+        return false;
+    }
+    if (pnt->type == CHARM_CRD_POINT_SCATTERED && pnt->nlat != pnt->nlon)
+    {
+        err_set(err, __FILE__, __LINE__, func, CHARM_EFUNCARG,
+                "The number of latitudes and longitudes in the \"pnt\" "
+                "structure must be the same to perform point-wise spherical "
+                "harmonic synthesis.");
+        return false;
+    }
+    return true;
+}
+
+} // namespace
+
+extern "C"
+{
+
+void charmf_shs_point(const charmf_point *pnt, const charmf_shc *shcs,
+                      unsigned long nmax, float *f, charmf_err *err)
+{
+    if (!check_nmax_f(shcs, nmax, err, "synthesis", __func__))
+        return;
+    if (!check_type_shs_f(pnt, err, __func__))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    FloatThresholds thr;
+    PointD dp(pnt);
+    if (cb::f32_serves(&dp.p, nmax, (double)shcs->r))
+    {
+        std::vector<float> c, s;
+        gather_tri(shcs, c, s);
+        report(err, __func__,
+               cb::shs_point_f32_host(&dp.p, shcs->nmax, (double)shcs->mu,
+                                      (double)shcs->r, c.data(), s.data(),
+                                      nmax, f));
+        return;
+    }
+    float *fp[1] = {f};
+    shs_f_fp64(pnt, shcs, nmax, 0, 0, 0, 0, 1, fp, err, __func__);
+}
+
+void charmf_shs_point_grad1(const charmf_point *pnt, const charmf_shc *shcs,
+                            unsigned long nmax, float **f, charmf_err *err)
+{
+    if (!check_nmax_f(shcs, nmax, err, "synthesis", __func__))
+        return;
+    if (!check_type_shs_f(pnt, err, __func__))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    FloatThresholds thr;
+    shs_f_fp64(pnt, shcs, nmax, 1, 1, 1, 1, 3, f, err, __func__);
+    if (!charm_err_isempty(err))
+        return;
+    // src/shs/shs_point_gradn.c:133-145
+    float *fx = f[2], *fy = f[0], *fz = f[1];
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = fz;
+}
+
+void charmf_shs_point_grad2(const charmf_point *pnt, const charmf_shc *shcs,
+                            unsigned long nmax, float **f, charmf_err *err)
+{
+    if (!check_nmax_f(shcs, nmax, err, "synthesis", __func__))
+        return;
+    if (!check_type_shs_f(pnt, err, __func__))
+        return;
+    if (pnt->npoint == 0)
+        return;
+    FloatThresholds thr;
+    shs_f_fp64(pnt, shcs, nmax, 2, 2, 2, 2, 6, f, err, __func__);
+    if (!charm_err_isempty(err))
+        return;
+    // src/shs/shs_point_gradn.c:146-165
+    float *fxx = f[5], *fxy = f[2], *fxz = f[4];
+    float *fyy = f[0], *fyz = f[1], *fzz = f[3];
+    f[0] = fxx;
+    f[1] = fxy;
+    f[2] = fxz;
+    f[3] = fyy;
+    f[4] = fyz;
+    f[5] = fzz;
+}
+
+void charmf_shs_point_guru(const charmf_point *pnt, const charmf_shc *shcs,
+                           unsigned long nmax, unsigned dr, unsigned dlat,
+                           unsigned dlon, float *f, charmf_err *err)
+{
+    if (!check_nmax_f(shcs, nmax, err, "synthesis", __func__))
+        return;
+    if ((int)dr < 0 || (int)dlat < 0 || (int)dlon < 0 || dr + dlat + dlon > 2)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg,
+                 "The sum \"dr + dlat + dlon\" is \"%d\", but it cannot be "
+                 "larger than \"%d\".",
+                 (int)(dr + dlat + dlon), 2);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (pnt->npoint == 0)
+        return;
+    if (!check_type_shs_f(pnt, err, __func__))
+        return;
+    FloatThresholds thr;
+    float *fp[1] = {f};
+    shs_f_fp64(pnt, shcs, nmax, 0, (int)dr, (int)dlat, (int)dlon, 1, fp, err,
+               __func__);
+}
+
+void charmf_sha_point(const charmf_point *pnt, const float *f,
+                      unsigned long nmax, charmf_shc *shcs, charmf_err *err)
+{
+    if (!check_nmax_f(shcs, nmax, err, "analysis", __func__))
+        return;
+    if (!is_quad_type(pnt->type))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic analysis of "
+                "point data values.");
+        return;
+    }
+    FloatThresholds thr;
+    const double r0 = (double)pnt->r[0];
+    for (size_t i = 1; i < pnt->nlat; i++)
+    {
+        if (!nearly_equal((double)pnt->r[i], r0, charm_glob_threshold))
+        {
+            SET_ERR(err, CHARM_EFUNCARG,
+                    "All spherical radii in \"pnt->r\" must be equal.");
+            return;
+        }
+    }
+    unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                 ? (unsigned long)pnt->nlat - 1
+                                 : ((unsigned long)pnt->nlat - 2) / 2;
+    if (nmax > nmax_grd)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The input data grid \"pnt\" was created for a maximum degree "
+                "that is not high enough to recover harmonics up to the "
+                "specified maximum degree of the analysis.");
+        return;
+    }
+    PointD dp(pnt);
+    const size_t n1 = (size_t)shcs->nmax + 1;
+    if (cb::f32_serves(&dp.p, nmax, (double)shcs->r))
+    {
+        std::vector<float> c(n1 * (n1 + 1) / 2, 0.0f), s(c.size(), 0.0f);
+        cb::Status st = cb::sha_point_f32_host(
+            &dp.p, f, nmax, (double)shcs->mu, (double)shcs->r, shcs->nmax,
+            c.data(), s.data());
+        report(err, __func__, st);
+        if (!st.ok())
+            return;
+        size_t idx = 0;
+        for (size_t m = 0; m < n1; m++)
+        {
+            for (size_t k = 0; k < n1 - m; k++)
+            {
+                const bool keep = m + k <= nmax;
+                shcs->c[m][k] = keep ? c[idx + k] : 0.0f;
+                shcs->s[m][k] = keep ? s[idx + k] : 0.0f;
+            }
+            idx += n1 - m;
+        }
+        return;
+    }
+    ShcD dh(shcs, false);
+    std::vector<double> fd(f, f + pnt->npoint);
+    cb::Status st = cb::sha_point(&dp.p, fd.data(), nmax, &dh.h);
+    report(err, __func__, st);
+    if (!st.ok())
+        return;
+    size_t idx = 0;
+    for (size_t m = 0; m < n1; m++)
+    {
+        for (size_t k = 0; k < n1 - m; k++)
+        {
+            shcs->c[m][k] = (float)dh.c[idx + k];
+            shcs->s[m][k] = (float)dh.s[idx + k];
+        }
+        idx += n1 - m;
+    }
+}
+
+} // extern "C"

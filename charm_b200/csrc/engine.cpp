@@ -3330,6 +3330,68 @@ Status sha_point_dev_f32(const charm_point *pnt, const float *d_f,
     return sha_grid_f32(g_ctx, pnt, d_f, nmax, mu, r, shc_nmax, d_c, d_s);
 }
 
+bool f32_serves(const charm_point *pnt, unsigned long nmax, double R)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    if (!init(g_ctx).ok())
+        return false;
+    if (pnt->type == CHARM_CRD_POINT_SCATTERED || pnt->npoint == 0)
+        return false;
+    const RfftArgs *rf = nullptr;
+    Status st = f32_grid_checks(g_ctx, pnt, nmax, R, &rf);
+    return st.ok();
+}
+
+Status shs_point_f32_host(const charm_point *pnt, unsigned long shc_nmax,
+                          double mu, double r, const float *c, const float *s,
+                          unsigned long nmax, float *f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    Context &cx = g_ctx;
+    CB_TRY(init(cx));
+    Status st;
+    const size_t T = (size_t)(shc_nmax + 1) * (shc_nmax + 2) / 2;
+    const size_t npt = pnt->nlat * pnt->nlon;
+    float *dc = nullptr, *ds = nullptr, *df = nullptr;
+    CB_TRY(dbuf(cx, "f32h_c", T, &dc));
+    CB_TRY(dbuf(cx, "f32h_s", T, &ds));
+    CB_TRY(dbuf(cx, "f32h_f", npt, &df));
+    CB_CUDA(cudaMemcpyAsync(dc, c, T * 4, cudaMemcpyHostToDevice, cx.stream),
+            st);
+    CB_CUDA(cudaMemcpyAsync(ds, s, T * 4, cudaMemcpyHostToDevice, cx.stream),
+            st);
+    CB_TRY(shs_grid_f32(cx, pnt, shc_nmax, mu, r, dc, ds, nmax, df));
+    CB_CUDA(cudaMemcpyAsync(f, df, npt * 4, cudaMemcpyDeviceToHost,
+                            cx.stream), st);
+    CB_CUDA(cudaStreamSynchronize(cx.stream), st);
+    return st;
+}
+
+Status sha_point_f32_host(const charm_point *pnt, const float *f,
+                          unsigned long nmax, double mu, double r,
+                          unsigned long shc_nmax, float *c, float *s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    Context &cx = g_ctx;
+    CB_TRY(init(cx));
+    Status st;
+    const size_t T = (size_t)(shc_nmax + 1) * (shc_nmax + 2) / 2;
+    const size_t npt = pnt->nlat * pnt->nlon;
+    float *dc = nullptr, *ds = nullptr, *df = nullptr;
+    CB_TRY(dbuf(cx, "f32h_c", T, &dc));
+    CB_TRY(dbuf(cx, "f32h_s", T, &ds));
+    CB_TRY(dbuf(cx, "f32h_f", npt, &df));
+    CB_CUDA(cudaMemcpyAsync(df, f, npt * 4, cudaMemcpyHostToDevice,
+                            cx.stream), st);
+    CB_TRY(sha_grid_f32(cx, pnt, df, nmax, mu, r, shc_nmax, dc, ds));
+    CB_CUDA(cudaMemcpyAsync(c, dc, T * 4, cudaMemcpyDeviceToHost, cx.stream),
+            st);
+    CB_CUDA(cudaMemcpyAsync(s, ds, T * 4, cudaMemcpyDeviceToHost, cx.stream),
+            st);
+    CB_CUDA(cudaStreamSynchronize(cx.stream), st);
+    return st;
+}
+
 Status shs_point_sctr_adjoint(const charm_point *pnt, const double *g,
                               unsigned long nmax, charm_shc *shcs)
 {

@@ -100,6 +100,18 @@ Status sha_point_dev_f32(const charm_point *pnt, const float *d_f,
                          unsigned long nmax, double mu, double r,
                          unsigned long shc_nmax, float *d_c, float *d_s);
 
+// The same mode with float host arrays (the charmf_* ABI): whether the
+// single-precision kernels serve a call (grid with FFT longitudes and an
+// even row length, nmax <= 2200, every row at r = R), and the calls
+// themselves (contiguous float triangles of degree shc_nmax, float grid).
+bool f32_serves(const charm_point *pnt, unsigned long nmax, double R);
+Status shs_point_f32_host(const charm_point *pnt, unsigned long shc_nmax,
+                          double mu, double r, const float *c, const float *s,
+                          unsigned long nmax, float *f);
+Status sha_point_f32_host(const charm_point *pnt, const float *f,
+                          unsigned long nmax, double mu, double r,
+                          unsigned long shc_nmax, float *c, float *s);
+
 // Adjoint of the scattered-point potential synthesis with respect to the
 // coefficients: shcs->c, shcs->s (degree shcs->nmax, zero above nmax)
 // receive sum_i g_i d f_i / d C_nm and d f_i / d S_nm for the model

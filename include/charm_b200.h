@@ -358,6 +358,123 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev_static(
     double r, unsigned long shc_nmax, double *d_c, double *d_s,
     charm_err *err);
 
+/* ------------------------------------------------------------------------
+ * Single-precision ABI: the entry points of CHarm's float build
+ * (src/prec.h:84-86 with @P@ = f, RDT = float): the same structures with
+ * float arrays, the same functions with the prefix charmf_.  The transforms
+ * run on the single-precision kernels where they serve the call (the
+ * potential on grids with FFT longitudes, nmax <= 2200, every row at the
+ * coefficients' radius); every other call (gradients, scattered points,
+ * higher degrees) runs the FP64 path and rounds its results to float.  The
+ * comparison thresholds of a charmf_ call are charmf_glob_threshold and
+ * charmf_glob_threshold2 (src/glob/glob.c with EPS = FLT_EPSILON).
+ * ------------------------------------------------------------------------ */
+/* err.h.in: the error structure has no precision-dependent member */
+typedef charm_err charmf_err;
+
+/* crd.h.in:125-300 with RDT = float */
+typedef struct
+{
+    int type;
+    size_t nlat;
+    size_t nlon;
+    size_t npoint;
+    float *lat;
+    float *lon;
+    float *r;
+    float *w;
+    _Bool owner;
+    _Bool distributed;
+} charmf_point;
+
+/* shc.h.in:139-381 with RDT = float */
+typedef struct
+{
+    unsigned long nmax;
+    float mu;
+    float r;
+    size_t nc;
+    size_t ns;
+    float **c;
+    float **s;
+    _Bool owner;
+    _Bool distributed;
+} charmf_shc;
+
+/* glob.h.in (float build) */
+CHARM_EXTERN extern float charmf_glob_threshold;
+CHARM_EXTERN extern float charmf_glob_threshold2;
+CHARM_EXTERN extern unsigned long charmf_glob_polar_optimization_a1;
+CHARM_EXTERN extern float charmf_glob_polar_optimization_a2;
+
+/* err.h.in:236-294 */
+CHARM_EXTERN charmf_err *CHARM_CDECL charmf_err_init(void);
+CHARM_EXTERN void CHARM_CDECL charmf_err_free(charmf_err *err);
+CHARM_EXTERN void CHARM_CDECL charmf_err_reset(charmf_err *err);
+CHARM_EXTERN void CHARM_CDECL charmf_err_handler(charmf_err *err,
+                                                  _Bool terminate);
+CHARM_EXTERN _Bool CHARM_CDECL charmf_err_isempty(const charmf_err *err);
+
+/* crd.h.in:477-760 */
+CHARM_EXTERN charmf_point *CHARM_CDECL charmf_crd_point_malloc(int type,
+                                                               size_t nlat,
+                                                               size_t nlon);
+CHARM_EXTERN charmf_point *CHARM_CDECL charmf_crd_point_calloc(int type,
+                                                               size_t nlat,
+                                                               size_t nlon);
+CHARM_EXTERN charmf_point *CHARM_CDECL charmf_crd_point_init(
+    int type, size_t nlat, size_t nlon, float *lat, float *lon, float *r);
+CHARM_EXTERN void CHARM_CDECL charmf_crd_point_free(charmf_point *pnt);
+CHARM_EXTERN charmf_point *CHARM_CDECL charmf_crd_point_gl(unsigned long nmax,
+                                                           float r);
+CHARM_EXTERN charmf_point *CHARM_CDECL charmf_crd_point_dh1(unsigned long nmax,
+                                                            float r);
+CHARM_EXTERN charmf_point *CHARM_CDECL charmf_crd_point_dh2(unsigned long nmax,
+                                                            float r);
+CHARM_EXTERN void CHARM_CDECL charmf_crd_point_gl_shape(unsigned long nmax,
+                                                        size_t *nlat,
+                                                        size_t *nlon);
+CHARM_EXTERN void CHARM_CDECL charmf_crd_point_dh1_shape(unsigned long nmax,
+                                                         size_t *nlat,
+                                                         size_t *nlon);
+CHARM_EXTERN void CHARM_CDECL charmf_crd_point_dh2_shape(unsigned long nmax,
+                                                         size_t *nlat,
+                                                         size_t *nlon);
+
+/* shc.h.in:423-602 */
+CHARM_EXTERN charmf_shc *CHARM_CDECL charmf_shc_malloc(unsigned long nmax,
+                                                       float mu, float r);
+CHARM_EXTERN charmf_shc *CHARM_CDECL charmf_shc_calloc(unsigned long nmax,
+                                                       float mu, float r);
+CHARM_EXTERN charmf_shc *CHARM_CDECL charmf_shc_init(unsigned long nmax,
+                                                     float mu, float r,
+                                                     float *c, float *s);
+CHARM_EXTERN void CHARM_CDECL charmf_shc_free(charmf_shc *shcs);
+
+/* shs.h.in:168-173, 239-244, 344-349, 428-435; sha.h.in:164-169 */
+CHARM_EXTERN void CHARM_CDECL charmf_shs_point(const charmf_point *pnt,
+                                               const charmf_shc *shcs,
+                                               unsigned long nmax, float *f,
+                                               charmf_err *err);
+CHARM_EXTERN void CHARM_CDECL charmf_shs_point_grad1(const charmf_point *pnt,
+                                                     const charmf_shc *shcs,
+                                                     unsigned long nmax,
+                                                     float **f,
+                                                     charmf_err *err);
+CHARM_EXTERN void CHARM_CDECL charmf_shs_point_grad2(const charmf_point *pnt,
+                                                     const charmf_shc *shcs,
+                                                     unsigned long nmax,
+                                                     float **f,
+                                                     charmf_err *err);
+CHARM_EXTERN void CHARM_CDECL charmf_shs_point_guru(
+    const charmf_point *pnt, const charmf_shc *shcs, unsigned long nmax,
+    unsigned dr, unsigned dlat, unsigned dlon, float *f, charmf_err *err);
+CHARM_EXTERN void CHARM_CDECL charmf_sha_point(const charmf_point *pnt,
+                                               const float *f,
+                                               unsigned long nmax,
+                                               charmf_shc *shcs,
+                                               charmf_err *err);
+
 /* The CUDA stream the library runs on (a cudaStream_t), or NULL when no
  * usable device is present. */
 CHARM_EXTERN void *CHARM_CDECL charm_b200_stream(void);

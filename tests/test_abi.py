@@ -16,8 +16,9 @@ HEADER = os.path.join(ROOT, "include", "charm_b200.h")
 def declared_symbols():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    funcs = re.findall(r"CHARM_EXTERN[^;(]*?\b(charm_\w+)\s*\(", text)
-    data = re.findall(r"CHARM_EXTERN\s+extern\s+[\w ]+?\b(charm_\w+)\s*;", text)
+    funcs = re.findall(r"CHARM_EXTERN[^;(]*?\b(charmf?_\w+)\s*\(", text)
+    data = re.findall(r"CHARM_EXTERN\s+extern\s+[\w ]+?\b(charmf?_\w+)\s*;",
+                      text)
     return sorted(set(funcs)), sorted(set(data))
 
 
@@ -26,9 +27,16 @@ def test_exports_everything_declared():
     lib = ct.CDLL(LIB_PATH)
     funcs, data = declared_symbols()
     assert len(funcs) >= 24
-    assert set(data) == {"charm_glob_threshold", "charm_glob_threshold2",
-                         "charm_glob_polar_optimization_a1",
-                         "charm_glob_polar_optimization_a2"}
+    glob = {"glob_threshold", "glob_threshold2",
+            "glob_polar_optimization_a1", "glob_polar_optimization_a2"}
+    assert set(data) == {p + g for p in ("charm_", "charmf_") for g in glob}
+    # the float build's entry points (CHarm src/prec.h:84-86, @P@ = f)
+    for name in ("shs_point", "shs_point_grad1", "shs_point_grad2",
+                 "shs_point_guru", "sha_point", "shc_init", "shc_malloc",
+                 "shc_calloc", "shc_free", "crd_point_gl", "crd_point_dh1",
+                 "crd_point_dh2", "crd_point_init", "crd_point_free",
+                 "err_init", "err_free", "err_isempty"):
+        assert "charmf_" + name in funcs, name
     for name in funcs + data:
         assert hasattr(lib, name), name
 
@@ -42,6 +50,52 @@ def test_globals_default_values():
                              "charm_glob_polar_optimization_a1").value == 100
     assert ct.c_double.in_dll(_libcharm,
                               "charm_glob_polar_optimization_a2").value == -1.0
+
+
+def test_float_globals_and_layouts():
+    """charmf_glob_* hold the float build's defaults (src/glob/glob.c with
+    EPS = FLT_EPSILON), and charmf_point / charmf_shc have CHarm's float
+    layouts (RDT = float)."""
+    from charm_b200._lib import _libcharm
+    feps = np.finfo(np.float32).eps
+    assert ct.c_float.in_dll(_libcharm, "charmf_glob_threshold").value == \
+        np.float32(100 * feps)
+    assert ct.c_float.in_dll(_libcharm, "charmf_glob_threshold2").value == \
+        np.float32(1e5 * feps)
+
+    class PointF(ct.Structure):
+        _fields_ = [("type", ct.c_int), ("nlat", ct.c_size_t),
+                    ("nlon", ct.c_size_t), ("npoint", ct.c_size_t),
+                    ("lat", ct.POINTER(ct.c_float)),
+                    ("lon", ct.POINTER(ct.c_float)),
+                    ("r", ct.POINTER(ct.c_float)),
+                    ("w", ct.POINTER(ct.c_float)),
+                    ("owner", ct.c_bool), ("distributed", ct.c_bool)]
+
+    class ShcF(ct.Structure):
+        _fields_ = [("nmax", ct.c_ulong), ("mu", ct.c_float),
+                    ("r", ct.c_float), ("nc", ct.c_size_t),
+                    ("ns", ct.c_size_t),
+                    ("c", ct.POINTER(ct.POINTER(ct.c_float))),
+                    ("s", ct.POINTER(ct.POINTER(ct.c_float))),
+                    ("owner", ct.c_bool), ("distributed", ct.c_bool)]
+    L = _libcharm
+    L.charmf_shc_calloc.restype = ct.POINTER(ShcF)
+    L.charmf_shc_calloc.argtypes = [ct.c_ulong, ct.c_float, ct.c_float]
+    L.charmf_shc_free.argtypes = [ct.POINTER(ShcF)]
+    h = L.charmf_shc_calloc(10, 3.5, 2.0)
+    assert h.contents.nmax == 10 and h.contents.mu == 3.5 and \
+        h.contents.r == 2.0 and h.contents.nc == 66 and h.contents.owner
+    # column m starts m (2 nmax + 3 - m) / 2 floats into the triangle
+    base = ct.cast(h.contents.c[0], ct.c_void_p).value
+    assert ct.cast(h.contents.c[3], ct.c_void_p).value - base == 4 * 30
+    L.charmf_shc_free(h)
+    L.charmf_crd_point_calloc.restype = ct.POINTER(PointF)
+    L.charmf_crd_point_calloc.argtypes = [ct.c_int, ct.c_size_t, ct.c_size_t]
+    L.charmf_crd_point_free.argtypes = [ct.POINTER(PointF)]
+    p = L.charmf_crd_point_calloc(3, 5, 12)     # GL type: weights too
+    assert p.contents.npoint == 60 and bool(p.contents.w)
+    L.charmf_crd_point_free(p)
 
 
 def test_struct_layouts():

@@ -110,3 +110,29 @@ def test_f32_rejects_unsupported(env):
     q = cb.PointSctr(lat, lon[:16], np.full(16, R_EARTH))
     f, msg = shs32(env, q, c, s, N)
     assert msg is not None and "grids only" in msg
+
+
+def test_f32_and_f64_against_quad_oracle_nmax2190(env):
+    """nmax 2190 (Kaula, seed 2000, r = R) at 16 GL latitudes x 128 GL
+    longitudes against CHarm's quad-precision build (fixture made by
+    tests/golden/make_quad_n2190.py): the FP64 path to a relative RMS of
+    1e-14 of the whole potential; the single-precision mode to 1e-6 of the
+    whole potential (measured: a few 1e-8) -- its degree-0 term alone
+    (GM / R = 6.25e7) sets the scale of the float rounding."""
+    import os
+    torch, cb, L = env
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                             "golden", "shs_gl2190_quad16.npz"))
+    N = int(z["nmax"])
+    ref = z["f_hi"] + z["f_lo"]
+    idx = z["lon_idx"]
+    c, s = kaula(N, int(z["seed"]))
+    nlon = 2 * (N + 1)
+    lon = np.arange(nlon) * (np.pi / (N + 1))
+    p = cb.PointGrid(z["lat"], lon, np.full(z["lat"].size, R_EARTH))
+    f64 = cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s), N)[:, idx]
+    assert rel_rms(f64, ref) <= 1e-14
+    f32, msg = shs32(env, p, c, s, N)
+    assert msg is None, msg
+    f32 = f32.cpu().numpy().astype(np.float64).reshape(-1, nlon)[:, idx]
+    assert rel_rms(f32, ref) <= 1e-6
