@@ -61,6 +61,14 @@ def parse():
                          "round trip")
     ap.add_argument("--npoint", type=int, default=10_000_000)
     ap.add_argument("--cg-iters", type=int, default=20)
+    ap.add_argument("--no-batch-dh", action="store_true",
+                    help="skip the 64-set DH section")
+    ap.add_argument("--no-sctr", action="store_true",
+                    help="skip the scattered-point section")
+    ap.add_argument("--sctr-points", type=int, default=1_000_000,
+                    help="points of the scattered section of the default "
+                         "line (the full workload: --workload sctr-cg)")
+    ap.add_argument("--sctr-iters", type=int, default=2)
     return ap.parse_args()
 
 
@@ -337,6 +345,9 @@ def run_ours(args):
         L, err, pnt, N, dev, peak, args.steps)
     hi = None if args.no_n10800 else ultra_high_degree(L, err, dev, stream,
                                                         flush, peak)
+    n360 = nmax360_round_trip()
+    bdh = None if args.no_batch_dh else batch_dh(single_calls=False)
+    sct = None if args.no_sctr else scattered(args.sctr_points, args.sctr_iters)
 
     if rank != 0:
         if dist is not None:
@@ -429,6 +440,11 @@ def run_ours(args):
     line["autotune"] = rbuf.value.decode().splitlines()
     if hi is not None:
         line["nmax10800"] = hi
+    line["nmax360"] = n360
+    if bdh is not None:
+        line["batch_dh"] = bdh
+    if sct is not None:
+        line["scattered"] = sct
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, c, s)
     print(json.dumps(line), flush=True)
@@ -812,18 +828,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_sctr_cg(args):
-    """Scattered points: nmax 2160 Kaula coefficients (seed 5000), points
-    uniform on the sphere with heights 0-9000 m (seed 5001), observations
-    A c + N(0, (1e-3 rms)^2) (seed 5002); times one synthesis, one adjoint
-    and a CGLS fit from zero, and reports the fit's misfit and coefficient
-    error.  One GPU; prints one JSON line."""
+def scattered(npt=10_000_000, cg_iters=20):
+    """Scattered points: nmax 2160 Kaula coefficients (seed 5000), `npt`
+    points uniform on the sphere with heights 0-9000 m (seed 5001),
+    observations A c + N(0, (1e-3 rms)^2) (seed 5002); times one synthesis,
+    one adjoint (with its dot-product identity <A c, y> = <c, A^T y>) and a
+    CGLS fit from zero of `cg_iters` iterations, and reports the fit's
+    misfit and coefficient error.  Returns a dict."""
     import torch
-    torch.cuda.set_device(0)
     import charm_b200 as cb
     from charm_b200 import autograd as ag
     from charm_b200.workloads import GM, R_EARTH, kaula
-    N, npt = 2160, args.npoint
+    N = 2160
     rng = np.random.default_rng(5001)
     lat = np.arcsin(rng.uniform(-1.0, 1.0, npt))
     lon = rng.uniform(0.0, 2.0 * np.pi, npt)
@@ -840,6 +856,7 @@ def run_sctr_cg(args):
         torch.cuda.synchronize()
         return out, time.perf_counter() - t0
 
+    ag._synthesis(dc, ds, p, N, GM, R_EARTH)    # tables, buffers
     truth, t_fwd = timed(lambda: ag._synthesis(dc, ds, p, N, GM, R_EARTH))
     rms = float(torch.sqrt(torch.mean(truth * truth)))
     noise = np.random.default_rng(5002).standard_normal(npt) * (1e-3 * rms)
@@ -847,45 +864,122 @@ def run_sctr_cg(args):
     (gc, gs), t_adj = timed(lambda: ag._adjoint(obs, p, N, GM, R_EARTH))
     lhs = float(torch.dot(truth, obs))
     rhs = float(torch.dot(dc, gc) + torch.dot(ds, gs))
-    (xc, xs, hist), t_cg = timed(
-        lambda: ag.cgls(p, obs, N, GM, R_EARTH, iters=args.cg_iters))
-    T = c.size
-    units = T * npt
-    num = torch.linalg.norm(torch.cat([xc - dc, xs - ds]))
-    den = torch.linalg.norm(torch.cat([dc, ds]))
-    line = {
+    out = {
         "workload": "scattered synthesis + adjoint + CGLS, nmax %d, %d points "
-                    "(heights 0-9000 m), %d iterations" % (N, npt, args.cg_iters),
-        "forward_s": t_fwd, "adjoint_s": t_adj, "cgls_s": t_cg,
-        "forward_tflops_alg": units * 12.0 / t_fwd / 1e12,
-        "adjoint_tflops_alg": units * 8.0 / t_adj / 1e12,
+                    "(heights 0-9000 m), %d iterations" % (N, npt, cg_iters),
+        "forward_s": t_fwd, "adjoint_s": t_adj,
+        "forward_tflops_alg": c.size * npt * 8.0 / t_fwd / 1e12,
+        "adjoint_tflops_alg": c.size * npt * 8.0 / t_adj / 1e12,
+        "flops_per_unit": "8 per (n, m, point): recurrence 2 mul + 1 FMA, "
+                          "two FMA (src/shs/shs_point_sctr.c)",
         "dot_product_rel": abs(lhs - rhs) / abs(lhs),
-        "misfit_first_last": [hist[0], hist[-1]],
-        "noise_norm": float(np.linalg.norm(noise)),
-        "coef_rel_error": float(num / den),
         "dtype": "f64", "data": "synthetic (seeds 5000, 5001, 5002)",
     }
-    print(json.dumps(line), flush=True)
+    if cg_iters > 0:
+        (xc, xs, hist), t_cg = timed(
+            lambda: ag.cgls(p, obs, N, GM, R_EARTH, iters=cg_iters))
+        num = torch.linalg.norm(torch.cat([xc - dc, xs - ds]))
+        den = torch.linalg.norm(torch.cat([dc, ds]))
+        out.update({"cgls_s": t_cg,
+                    "misfit_first_last": [hist[0], hist[-1]],
+                    "noise_norm": float(np.linalg.norm(noise)),
+                    "coef_rel_error": float(num / den)})
+    return out
 
 
-def run_batch(args):
+def run_sctr_cg(args):
+    """The scattered workload alone; prints one JSON line.  One GPU."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(scattered(args.npoint, args.cg_iters)), flush=True)
+
+
+def nmax360_round_trip(steps=10):
+    """The nmax 360 GL round trip (361 x 722 grid, seed 1000): device time
+    per round trip through the device entry points and CHarm's own time on
+    the host cores for the same round trip."""
+    import torch
+    import charm_b200 as cb
+    from charm_b200._lib import _libcharm as L
+    from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula
+    N = 360
+    c, s = kaula(N, 1000)
+    pnt = cb.PointGridGL(N, R_EARTH)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_c = torch.from_numpy(c).to(dev)
+    d_s = torch.from_numpy(s).to(dev)
+    d_f = torch.empty(pnt.lat.size * pnt.lon.size, dtype=torch.float64,
+                      device=dev)
+    o_c = torch.empty_like(d_c)
+    o_s = torch.empty_like(d_s)
+    err = L.charm_err_init()
+    stream = torch.cuda.ExternalStream(L.charm_b200_stream())
+
+    def step():
+        L.charm_b200_shs_point_dev(ct.cast(pnt._Point, ct.c_void_p), N, GM,
+                                   R_EARTH, d_c.data_ptr(), d_s.data_ptr(), N,
+                                   0, 0, 0, 0, d_f.data_ptr(),
+                                   ct.cast(err, ct.c_void_p))
+        L.charm_b200_sha_point_dev(ct.cast(pnt._Point, ct.c_void_p),
+                                   d_f.data_ptr(), N, GM, R_EARTH, N,
+                                   o_c.data_ptr(), o_s.data_ptr(),
+                                   ct.cast(err, ct.c_void_p))
+        if not L.charm_err_isempty(err):
+            raise RuntimeError(ct.string_at(err.contents.msg).decode())
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    for _ in range(steps):
+        step()
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    rt = coef_rel_rms(o_c.cpu().numpy(), o_s.cpu().numpy(), c, s)
+    L.charm_err_free(err)
+    out = {"workload": "GL-grid SHS+SHA round trip, plain FP64, nmax 360, "
+                       "grid 361x722 (seed 1000)",
+           "ms_per_round_trip": ms, "steps": steps,
+           "round_trip_rel_rms": rt}
+    try:
+        r = charm_round_trips(N, c, s, steps=5, warmup=1, fft_share=False)
+        out["charm_cpu_ms_per_round_trip"] = 1e3 * float(
+            np.median(r["round_trip_s"]))
+        out["charm_cpu_cores"] = r["cores"]
+    except (OSError, RuntimeError) as e:
+        out["charm_cpu"] = "unavailable: %s" % e
+    return out
+
+
+def batch_dh(single_calls=True, oracle_rows=6):
     """64 coefficient sets, nmax_j uniform in 90..2160 (numpy default_rng
     4999), Kaula coefficients (seeds 4000 + j), synthesised at r = R + 250 km
     with the potential, grad1 and grad2 (ten quantities): even sets on the
     DH1 grid and odd sets on the DH2 grid of their largest degree.  Times
-    the batched entry point (groups of 8 sets per call, bounded by the
-    output memory) against one call per set and derivative kind on the same
-    grids; prints one JSON line.  One GPU."""
+    the batched FP64 entry point (groups of 8 sets per call, bounded by the
+    output memory), optionally one call per set and derivative kind, and the
+    potential of all 64 sets through the FP64 batch and the split-precision
+    batch (tensor cores).  Errors per component: the batched FP64 output of
+    the lowest-degree set of each grid against the CPU oracle on
+    `oracle_rows` of its rows, and the split-precision potential against the
+    FP64 batch (all sets) and the oracle (those rows).  Returns a dict."""
     import torch
-    torch.cuda.set_device(0)
     import charm_b200 as cb
     from charm_b200._lib import _libcharm as L
-    from charm_b200.workloads import GM, R_EARTH, kaula
+    from charm_b200.workloads import GM, R_EARTH, kaula, rel_rms
+    from oracle import orc
     P = ct.c_void_p
     L.charm_b200_shs_point_batch_dev.argtypes = [
         P, ct.c_size_t, ct.POINTER(ct.c_ulong), ct.POINTER(ct.c_ulong),
         ct.POINTER(ct.c_double), ct.c_double, ct.POINTER(ct.c_void_p),
         ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p), P]
+    L.charm_b200_shs_point_batch_i8_dev.argtypes = \
+        L.charm_b200_shs_point_batch_dev.argtypes
     L.charm_b200_shs_point_dev.argtypes = [
         P, ct.c_ulong, ct.c_double, ct.c_double, P, P, ct.c_ulong, ct.c_int,
         ct.c_uint, ct.c_uint, ct.c_uint, P, P]
@@ -897,23 +991,27 @@ def run_batch(args):
             raise RuntimeError(ct.string_at(err.contents.msg).decode())
 
     h = 250e3
+    names = ["V", "Vx", "Vy", "Vz", "Vxx", "Vxy", "Vxz", "Vyy", "Vyz", "Vzz"]
     groups = []
     for parity, ctor in ((0, cb.PointGridDH1), (1, cb.PointGridDH2)):
         idx = [j for j in range(64) if j % 2 == parity]
         Ng = int(max(nm[j] for j in idx))
         groups.append((ctor(Ng, R_EARTH + h), idx))
+    coefs = {j: kaula(int(nm[j]), 4000 + j) for j in range(64)}
     total_units = 0.0
     t_batch = 0.0
     t_single = 0.0
     G = 8
+    probe = {}     # set -> (grid, rows, [10 x (rows, nlon)]) of the FP64 batch
     for pnt, idx in groups:
         npts = pnt.lat.size * pnt.lon.size
+        jmin = min(idx, key=lambda j: nm[j])
+        rows = np.linspace(1, pnt.lat.size - 2, oracle_rows).astype(int)
         for g0 in range(0, len(idx), G):
             sel = idx[g0:g0 + G]
             n = len(sel)
-            cs = [kaula(int(nm[j]), 4000 + j) for j in sel]
-            dc = [torch.from_numpy(c).cuda() for c, _ in cs]
-            ds = [torch.from_numpy(s).cuda() for _, s in cs]
+            dc = [torch.from_numpy(coefs[j][0]).cuda() for j in sel]
+            ds = [torch.from_numpy(coefs[j][1]).cuda() for j in sel]
             out = [torch.empty(10 * npts, dtype=torch.float64, device="cuda")
                    for _ in sel]
             nmv = (ct.c_ulong * n)(*[int(nm[j]) for j in sel])
@@ -931,23 +1029,29 @@ def run_batch(args):
                 torch.cuda.synchronize()
                 if rep == 1:
                     t_batch += time.perf_counter() - t0
-            # one call per set and kind (potential, grad1, grad2); the
-            # first pass, untimed, takes each shape's one-time costs (tables,
-            # the synthesis autotuner), as the batched call's warm-up does
-            for rep in range(2):
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                for b, j in enumerate(sel):
-                    for kg, d, off in ((0, 0, 0), (1, 1, 1), (2, 2, 4)):
-                        L.charm_b200_shs_point_dev(
-                            ct.cast(pnt._Point, P), int(nm[j]), GM, R_EARTH,
-                            dc[b].data_ptr(), ds[b].data_ptr(), int(nm[j]),
-                            kg, d, d, d, out[b].data_ptr() + off * npts * 8,
-                            ct.cast(err, P))
-                        check()
-                torch.cuda.synchronize()
-                if rep == 1:
-                    t_single += time.perf_counter() - t0
+            if jmin in sel:
+                o = out[sel.index(jmin)].view(10, pnt.lat.size, pnt.lon.size)
+                probe[jmin] = (pnt, rows, o[:, rows, :].cpu().numpy())
+            if single_calls:
+                # one call per set and kind (potential, grad1, grad2); the
+                # first pass, untimed, takes each shape's one-time costs
+                # (tables, the synthesis autotuner), as the batched call's
+                # warm-up does
+                for rep in range(2):
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    for b, j in enumerate(sel):
+                        for kg, d, off in ((0, 0, 0), (1, 1, 1), (2, 2, 4)):
+                            L.charm_b200_shs_point_dev(
+                                ct.cast(pnt._Point, P), int(nm[j]), GM,
+                                R_EARTH, dc[b].data_ptr(), ds[b].data_ptr(),
+                                int(nm[j]), kg, d, d, d,
+                                out[b].data_ptr() + off * npts * 8,
+                                ct.cast(err, P))
+                            check()
+                    torch.cuda.synchronize()
+                    if rep == 1:
+                        t_single += time.perf_counter() - t0
             for j in sel:
                 T = (int(nm[j]) + 1) * (int(nm[j]) + 2) / 2
                 total_units += T * (pnt.lat.size // 2 + 1)
@@ -955,16 +1059,13 @@ def run_batch(args):
             torch.cuda.empty_cache()
     # the potential of the same 64 sets: FP64 batch against the
     # split-precision batch (tensor cores), each parity group in one call
-    L.charm_b200_shs_point_batch_i8_dev.argtypes = \
-        L.charm_b200_shs_point_batch_dev.argtypes
-    pot = {"fp64_s": 0.0, "i8_s": 0.0, "worst_rel_rms": 0.0}
-    from charm_b200.workloads import rel_rms
+    pot = {"fp64_s": 0.0, "i8_s": 0.0, "worst_rel_rms_vs_fp64": 0.0}
+    i8_probe = {}
     for pnt, idx in groups:
         npts = pnt.lat.size * pnt.lon.size
         n = len(idx)
-        cs = [kaula(int(nm[j]), 4000 + j) for j in idx]
-        dc = [torch.from_numpy(c).cuda() for c, _ in cs]
-        ds = [torch.from_numpy(s).cuda() for _, s in cs]
+        dc = [torch.from_numpy(coefs[j][0]).cuda() for j in idx]
+        ds = [torch.from_numpy(coefs[j][1]).cuda() for j in idx]
         nmv = (ct.c_ulong * n)(*[int(nm[j]) for j in idx])
         muv = (ct.c_double * n)(*([GM] * n))
         pc = (ct.c_void_p * n)(*[t.data_ptr() for t in dc])
@@ -986,27 +1087,59 @@ def run_batch(args):
                     pot[name + "_s"] += time.perf_counter() - t0
             outs[name] = out
         for a, b in zip(outs["i8"], outs["fp64"]):
-            pot["worst_rel_rms"] = max(pot["worst_rel_rms"],
-                                       rel_rms(a.cpu().numpy(),
-                                               b.cpu().numpy()))
+            pot["worst_rel_rms_vs_fp64"] = max(
+                pot["worst_rel_rms_vs_fp64"],
+                rel_rms(a.cpu().numpy(), b.cpu().numpy()))
+        for j in idx:
+            if j in probe:
+                rows = probe[j][1]
+                o = outs["i8"][idx.index(j)].view(pnt.lat.size, pnt.lon.size)
+                i8_probe[j] = o[rows, :].cpu().numpy()
         del dc, ds, outs
         torch.cuda.empty_cache()
     pot["speedup"] = pot["fp64_s"] / pot["i8_s"]
     pot["i8_sets_per_s"] = 64.0 / pot["i8_s"]
     pot["fp64_sets_per_s"] = 64.0 / pot["fp64_s"]
-    line = {
-        "workload": "64 coefficient sets, nmax U(90, 2160), potential + grad1 "
-                    "+ grad2 (10 quantities) at r = R + 250 km, DH1 / DH2 grids "
-                    "of the largest degree, plain FP64",
-        "batched_s": t_batch, "batched_sets_per_s": 64.0 / t_batch,
-        "single_calls_s": t_single, "single_sets_per_s": 64.0 / t_single,
-        "speedup": t_single / t_batch,
+    # per-component errors against the oracle
+    comp = {}
+    for j, (pnt, rows, vals) in probe.items():
+        c, s = coefs[j]
+        po = orc.Point(orc.GRID, pnt.lat[rows], pnt.lon,
+                       np.full(rows.size, R_EARTH + h))
+        shc = orc.Shc(int(nm[j]), GM, R_EARTH, c, s)
+        ref = (orc.shs_point(po, shc, int(nm[j]), "pot") +
+               orc.shs_point(po, shc, int(nm[j]), "grad1") +
+               orc.shs_point(po, shc, int(nm[j]), "grad2"))
+        e = {nm_: rel_rms(vals[q], ref[q]) for q, nm_ in enumerate(names)}
+        e["V_split_precision"] = rel_rms(i8_probe[j], ref[0])
+        comp["set%d_nmax%d_%s" % (j, int(nm[j]),
+                                  "dh1" if j % 2 == 0 else "dh2")] = e
+    L.charm_err_free(err)
+    out = {
+        "workload": "64 coefficient sets, nmax U(90, 2160) (rng 4999), "
+                    "potential + grad1 + grad2 (10 quantities) at r = R + "
+                    "250 km, DH1 / DH2 grids of the largest degree",
+        "fp64_batched_10q_s": t_batch,
+        "fp64_batched_10q_sets_per_s": 64.0 / t_batch,
         "units_n_m_pair": total_units,
         "potential_fp64_vs_split_precision": pot,
+        "rel_rms_vs_oracle_per_component": comp,
+        "oracle_rows_per_set": oracle_rows,
         "dtype": "f64", "data": "synthetic (seeds 4999, 4000 + j)",
     }
-    L.charm_err_free(err)
-    print(json.dumps(line), flush=True)
+    if single_calls:
+        out["single_calls_10q_s"] = t_single
+        out["single_calls_10q_sets_per_s"] = 64.0 / t_single
+        out["batched_speedup_over_single_calls"] = t_single / t_batch
+    return out
+
+
+def run_batch(args):
+    """The batched DH workload alone (batch_dh with single calls); prints
+    one JSON line.  One GPU."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(batch_dh(single_calls=True)), flush=True)
 
 
 def main():
