@@ -989,6 +989,53 @@ void charm_b200_sha_point_dev_static(const charm_point *pnt,
                                     d_s));
 }
 
+// Latitude-band analysis of a sharded transform: no CHarm counterpart (the
+// reference's MPI build distributes latitude chunks, src/mpi, and reduces
+// the coefficients, src/shc/shc_block_set_coeffs.c:80-86); the checks are
+// charm_b200_sha_point_dev's.
+void charm_b200_sha_point_dev_band(const charm_point *pnt, const double *d_f,
+                                   unsigned long nmax, double mu, double r,
+                                   unsigned long shc_nmax, int pair0,
+                                   int pair1, double *d_c, double *d_s,
+                                   charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (!is_quad_type(pnt->type))
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"pnt->type\" for spherical harmonic analysis of "
+                "point data values.");
+        return;
+    }
+    unsigned long nmax_grd = pnt->type == CHARM_CRD_POINT_GRID_GL
+                                 ? (unsigned long)pnt->nlat - 1
+                                 : ((unsigned long)pnt->nlat - 2) / 2;
+    if (nmax > nmax_grd)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "The input data grid \"pnt\" was created for a maximum degree "
+                "that is not high enough to recover harmonics up to the "
+                "specified maximum degree of the analysis.");
+        return;
+    }
+    report(err, __func__,
+           cb::sha_point_dev_band(pnt, d_f, nmax, mu, r, shc_nmax, pair0,
+                                  pair1, d_c, d_s));
+}
+
+int charm_b200_grid_pairs(const charm_point *pnt, int *row_n, int *row_s,
+                          int cap)
+{
+    if (!pnt || !is_grid_type(pnt->type))
+        return 0;
+    return cb::grid_pair_rows(pnt, row_n, row_s, cap);
+}
+
 void *charm_b200_stream(void)
 {
     return cb::stream_handle();

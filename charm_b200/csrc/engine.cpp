@@ -2447,10 +2447,13 @@ Status sctr_adjoint(Context &c, const charm_point *pnt, const double *g_host,
 // ---------------------------------------------------------------------------
 // Grid analysis
 // ---------------------------------------------------------------------------
+// pair0 / pair1: with pair1 >= 0, only the latitude pairs [pair0, pair1)
+// of the grid's pairing (grid_pairs) enter the sums (a band of one
+// latitude-band-sharded analysis; device grids only).
 Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                 const double *d_fin, unsigned long nmax, double mu, double R,
                 unsigned long shc_nmax, double *const *hc, double *const *hs,
-                double *d_c, double *d_s)
+                double *d_c, double *d_s, int pair0 = 0, int pair1 = -1)
 {
     Status st;
     const size_t nlat = pnt->nlat, nlon = pnt->nlon;
@@ -2466,6 +2469,44 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
 
     Pairs P;
     grid_pairs(pnt, charm_glob_threshold2, true, P);
+    const bool band = pair1 >= 0;
+    // rows of the band's northern and southern members, [lo, hi)
+    int band_n0 = 0, band_n1 = 0, band_s0 = 0, band_s1 = 0;
+    if (band)
+    {
+        if (!d_fin || pair0 < 0 || pair0 > pair1 ||
+            pair1 > (int)P.row_n.size())
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "latitude band [" + std::to_string(pair0) + ", " +
+                     std::to_string(pair1) + ") outside the grid's " +
+                     std::to_string(P.row_n.size()) +
+                     " latitude pairs (or a host grid)";
+            return st;
+        }
+        P.row_n.assign(P.row_n.begin() + pair0, P.row_n.begin() + pair1);
+        P.row_s.assign(P.row_s.begin() + pair0, P.row_s.begin() + pair1);
+        band_n0 = band_s0 = (int)nlat;
+        for (size_t p = 0; p < P.row_n.size(); p++)
+        {
+            band_n0 = std::min(band_n0, P.row_n[p]);
+            band_n1 = std::max(band_n1, P.row_n[p] + 1);
+            if (P.row_s[p] >= 0 && P.row_s[p] < (int)nlat)
+            {
+                band_s0 = std::min(band_s0, P.row_s[p]);
+                band_s1 = std::max(band_s1, P.row_s[p] + 1);
+            }
+        }
+        if (P.row_n.empty())
+        {
+            // an empty band contributes nothing
+            const size_t T = (size_t)(shc_nmax + 1) * (shc_nmax + 2) / 2;
+            CB_CUDA(cudaMemsetAsync(d_c, 0, T * 8, c.stream), st);
+            CB_CUDA(cudaMemsetAsync(d_s, 0, T * 8, c.stream), st);
+            CB_CUDA(cudaStreamSynchronize(c.stream), st);
+            return st;
+        }
+    }
     const int np = (int)P.row_n.size();
     size_t geo_bytes = (size_t)np * (4 * 8 + 2 * 4);
     void *hp = nullptr;
@@ -2740,7 +2781,14 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         if (fdev)
             CB_CUDA(cudaMemcpyAsync(fdev, f_host, nlat * nlon * 8,
                                     cudaMemcpyHostToDevice, c.stream), st);
-        CB_TRY(rows_fft(0, (int)nlat));
+        if (band)
+        {
+            CB_TRY(rows_fft(band_n0, band_n1));
+            if (band_s1 > band_s0)
+                CB_TRY(rows_fft(band_s0, band_s1));
+        }
+        else
+            CB_TRY(rows_fft(0, (int)nlat));
         int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                             (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
@@ -3149,6 +3197,32 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
                     nullptr, d_c, d_s);
+}
+
+Status sha_point_dev_band(const charm_point *pnt, const double *d_f,
+                          unsigned long nmax, double mu, double r,
+                          unsigned long shc_nmax, int pair0, int pair1,
+                          double *d_c, double *d_s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
+                    nullptr, d_c, d_s, pair0, pair1 < pair0 ? pair0 : pair1);
+}
+
+int grid_pair_rows(const charm_point *pnt, int *row_n, int *row_s, int cap)
+{
+    Pairs P;
+    grid_pairs(pnt, charm_glob_threshold2, true, P);
+    const int np = (int)P.row_n.size();
+    for (int p = 0; p < np && p < cap; p++)
+    {
+        if (row_n)
+            row_n[p] = P.row_n[p];
+        if (row_s)
+            row_s[p] = P.row_s[p] < (int)pnt->nlat ? P.row_s[p] : -1;
+    }
+    return np;
 }
 
 Status shs_point_batch_dev(const charm_point *pnt, size_t nsets,

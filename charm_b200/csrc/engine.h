@@ -56,6 +56,18 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
                      unsigned long nmax, double mu, double r,
                      unsigned long shc_nmax, double *d_c, double *d_s);
 
+// One latitude band of a sharded analysis: the contribution of the
+// latitude pairs [pair0, pair1) of the grid's pairing to the coefficients
+// (linear in the grid, so the bands' outputs sum to sha_point_dev's).
+Status sha_point_dev_band(const charm_point *pnt, const double *d_f,
+                          unsigned long nmax, double mu, double r,
+                          unsigned long shc_nmax, int pair0, int pair1,
+                          double *d_c, double *d_s);
+// The latitude pairs of a grid as the transforms group them: row_n[p] and
+// the mirror row row_s[p] (-1: none); returns their number (fills at most
+// cap entries).
+int grid_pair_rows(const charm_point *pnt, int *row_n, int *row_s, int cap);
+
 // Batched synthesis of nsets coefficient sets (degree shc_nmax[j], maximum
 // degree nmax[j], scaling mu[j], common reference radius r; device
 // triangles d_c[j], d_s[j]) on one grid with FFT longitudes; kgrad 0, 1, 2

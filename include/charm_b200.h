@@ -475,6 +475,25 @@ CHARM_EXTERN void CHARM_CDECL charmf_sha_point(const charmf_point *pnt,
                                                charmf_shc *shcs,
                                                charmf_err *err);
 
+/* Latitude-band sharding of one transform over several GPUs (one process
+ * per GPU; the reference's MPI build distributes latitude chunks, src/mpi,
+ * and sums the coefficients, src/shc/shc_block_set_coeffs.c:80-86; no
+ * single-call counterpart in CHarm).  charm_b200_grid_pairs lists the
+ * latitude pairs of a grid as the transforms group them (row_n[p] and its
+ * mirror row row_s[p], -1 when it has none; at most cap entries written)
+ * and returns their number.  charm_b200_sha_point_dev_band is
+ * charm_b200_sha_point_dev restricted to the pairs [pair0, pair1): the
+ * contribution of those rows of d_f (the other rows are not read) to the
+ * coefficients, so that the bands of a partition of the pairs sum to the
+ * whole analysis. */
+CHARM_EXTERN int CHARM_CDECL charm_b200_grid_pairs(const charm_point *pnt,
+                                                   int *row_n, int *row_s,
+                                                   int cap);
+CHARM_EXTERN void CHARM_CDECL charm_b200_sha_point_dev_band(
+    const charm_point *pnt, const double *d_f, unsigned long nmax, double mu,
+    double r, unsigned long shc_nmax, int pair0, int pair1, double *d_c,
+    double *d_s, charm_err *err);
+
 /* The CUDA stream the library runs on (a cudaStream_t), or NULL when no
  * usable device is present. */
 CHARM_EXTERN void *CHARM_CDECL charm_b200_stream(void);
