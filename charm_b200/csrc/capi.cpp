@@ -720,10 +720,9 @@ void *charm_b200_shs_point_batch_graph(const charm_point *pnt, size_t nsets,
                                        double *const *d_f,
                                        int split_precision, charm_err *err)
 {
-    if (kgrad < 0 || kgrad > 3 || (split_precision && kgrad != 0))
+    if (kgrad < 0 || kgrad > 3)
     {
-        SET_ERR(err, CHARM_EFUNCARG,
-                "\"kgrad\" must be 0..3 (0 with split precision).");
+        SET_ERR(err, CHARM_EFUNCARG, "\"kgrad\" must be 0..3.");
         return nullptr;
     }
     if (!(pnt->type == CHARM_CRD_POINT_GRID ||
@@ -788,7 +787,7 @@ size_t charm_b200_autotune_report(char *buf, size_t n)
 }
 
 // Split-precision batched synthesis: the same call with the degree sums on
-// the tensor cores.  kgrad 0 (the potential).
+// the tensor cores, kgrad 0..3 as the FP64 batch.
 void charm_b200_shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
                                        const unsigned long *nmax,
                                        const unsigned long *shc_nmax,
@@ -797,11 +796,9 @@ void charm_b200_shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
                                        const double *const *d_s, int kgrad,
                                        double *const *d_f, charm_err *err)
 {
-    if (kgrad != 0)
+    if (kgrad < 0 || kgrad > 3)
     {
-        SET_ERR(err, CHARM_EFUNCARG,
-                "The split-precision batched synthesis computes the "
-                "potential (\"kgrad = 0\").");
+        SET_ERR(err, CHARM_EFUNCARG, "\"kgrad\" must be 0, 1, 2 or 3.");
         return;
     }
     if (!(pnt->type == CHARM_CRD_POINT_GRID ||
@@ -826,7 +823,7 @@ void charm_b200_shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
         return;
     report(err, __func__,
            cb::shs_point_batch_i8_dev(pnt, nsets, nmax, shc_nmax, mu, r, d_c,
-                                      d_s, d_f));
+                                      d_s, kgrad, d_f));
 }
 
 // Single-precision mode: no CHarm counterpart at this ABI level (CHarm's

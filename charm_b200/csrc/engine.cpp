@@ -1860,13 +1860,20 @@ Status shs_batch(Context &c, const charm_point *pnt, size_t nsets,
 // the lumped coefficients of all sets for every (order, 128-pair tile) and
 // the row transforms follow per set.  Same grids and outputs as
 // shs_batch's kgrad 0.
+// kgrad 0: the potential, SHS_TC_SETS sets per launch; kgrad 1, 2 or 3:
+// the gradient families (shs_tc.cu), SHS_TC_GRAD_SETS sets per launch, of
+// which grad1 (kgrad 1), grad2 (2) or all ten quantities (3) are written,
+// in the batched FP64 path's component order.
 Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
                     const unsigned long *nmax_v,
                     const unsigned long *shc_nmax_v, const double *mu_v,
                     double R, const double *const *d_c,
-                    const double *const *d_s, double *const *d_f)
+                    const double *const *d_s, double *const *d_f,
+                    int kgrad = 0)
 {
     Status st;
+    const bool grad = kgrad != 0;
+    const size_t per_launch = grad ? SHS_TC_GRAD_SETS : SHS_TC_SETS;
     const size_t nlat = pnt->nlat, nlon = pnt->nlon;
     unsigned long N = 0;
     for (size_t j = 0; j < nsets; j++)
@@ -1926,10 +1933,29 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
     CB_TRY(row_fft(c, (long long)nlon, &rf));
     CB_TRY(row_fft_quarter(c, (long long)nlon, rf, &rfq));
     const int ldf = (int)(nlon / 2 + 1);
-    const size_t per_set = nlat * (size_t)ldf;
-    const size_t bsz = std::min<size_t>(nsets, SHS_TC_SETS);
+    const size_t per_q = nlat * (size_t)ldf;
+    const size_t per_set = (grad ? 10 : 1) * per_q;
+    const size_t bsz = std::min<size_t>(nsets, per_launch);
     double2 *lc = nullptr;
     CB_TRY(dbuf(c, "batch_lumped", bsz * per_set, &lc));
+    // lumped array q of a set -> component slot of the caller's output
+    // (V; grad1 l r p -> y z x; grad2 ll lr lp rr rp pp -> yy yz xy zz xz
+    // xx, CHarm's order after src/shs/shs_point_gradn.c:133-165), or -1
+    int slot[10];
+    for (int q = 0; q < 10; q++)
+        slot[q] = -1;
+    {
+        const int s1[3] = {1, 2, 0}, s2[6] = {3, 4, 1, 5, 2, 0};
+        if (kgrad == 0 || kgrad == 3)
+            slot[0] = 0;
+        for (int q = 0; q < 3; q++)
+            if (kgrad == 1 || kgrad == 3)
+                slot[1 + q] = (kgrad == 3 ? 1 : 0) + s1[q];
+        for (int q = 0; q < 6; q++)
+            if (kgrad == 2 || kgrad == 3)
+                slot[4 + q] = (kgrad == 3 ? 4 : 0) + s2[q];
+    }
+    const size_t grid_sz = nlat * nlon;
     unsigned *d_status;
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
@@ -1939,9 +1965,9 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
     int2 *seed_e = nullptr;
     CB_TRY(dbuf(c, "tc_seed_e", (size_t)(N + 1) * np, &seed_e));
 
-    for (size_t j0 = 0; j0 < nsets; j0 += SHS_TC_SETS)
+    for (size_t j0 = 0; j0 < nsets; j0 += per_launch)
     {
-        const int nb = (int)std::min<size_t>(SHS_TC_SETS, nsets - j0);
+        const int nb = (int)std::min<size_t>(per_launch, nsets - j0);
         const unsigned long Ng = nmax_v[ord[j0]];   // largest of the launch
         chunk_layout(Ng);
         CB_TRY(h2d_small(c, d_chunk0, h0.data(),
@@ -1961,6 +1987,7 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         P.ecol = d_ecol;
         P.bdig = static_cast<unsigned char *>(bdig);
         P.status = d_status;
+        P.grad = grad ? 1 : 0;
         {
             Scope sc(c, TIMER_PREP);
             CB_CUDA(launch_tc_prep(P, c.stream), st);
@@ -1998,6 +2025,8 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         A.status = d_status;
         A.seed_x = seed_x;
         A.seed_e = seed_e;
+        A.grad = grad ? 1 : 0;
+        A.Rref = R;
         if (j0 == 0)
         {
             Scope sc(c, TIMER_PREP);
@@ -2013,26 +2042,32 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
         for (int b = 0; b < nb; b++)
         {
             const size_t jj = ord[j0 + b];
-            double *dst = d_f[jj];
-            double2 *src = lc + (size_t)b * per_set;
-            if (rf->odd || reinterpret_cast<uintptr_t>(dst) % 16 == 0)
+            for (int q = 0; q < (grad ? 10 : 1); q++)
             {
-                RfftArgs R2 = *synth_plan(rf, rfq, (long long)nmax_v[jj]);
-                R2.nrows = (long long)nlat;
-                R2.x = dst;
-                R2.ldx = (long long)nlon;
-                R2.X = src;
-                R2.ldX = ldf;
-                R2.kmax = (int)nmax_v[jj];
-                Scope sc(c, TIMER_FFT);
-                CB_CUDA(launch_rfft(R2, true, c.stream), st);
-            }
-            else
-            {
-                st.code = CHARM_EFUNCARG;
-                st.msg = "batched synthesis outputs must start on a 16-byte "
-                         "boundary";
-                return st;
+                const int sl = grad ? slot[q] : 0;
+                if (sl < 0)
+                    continue;
+                double *dst = d_f[jj] + (size_t)sl * grid_sz;
+                double2 *src = lc + (size_t)b * per_set + (size_t)q * per_q;
+                if (rf->odd || reinterpret_cast<uintptr_t>(dst) % 16 == 0)
+                {
+                    RfftArgs R2 = *synth_plan(rf, rfq, (long long)nmax_v[jj]);
+                    R2.nrows = (long long)nlat;
+                    R2.x = dst;
+                    R2.ldx = (long long)nlon;
+                    R2.X = src;
+                    R2.ldX = ldf;
+                    R2.kmax = (int)nmax_v[jj];
+                    Scope sc(c, TIMER_FFT);
+                    CB_CUDA(launch_rfft(R2, true, c.stream), st);
+                }
+                else
+                {
+                    st.code = CHARM_EFUNCARG;
+                    st.msg = "batched synthesis outputs must start on a "
+                             "16-byte boundary";
+                    return st;
+                }
             }
         }
         // the digit tiles and the lumped buffer are reused by the next group
@@ -3261,7 +3296,7 @@ Status batch_graph_create(const charm_point *pnt, size_t nsets,
     CB_TRY(init(c));
     auto run = [&]() {
         return split ? shs_batch_tc(c, pnt, nsets, nmax, shc_nmax, mu, r, d_c,
-                                    d_s, d_f)
+                                    d_s, d_f, kgrad)
                      : shs_batch(c, pnt, nsets, nmax, shc_nmax, mu, r, d_c,
                                  d_s, kgrad, d_f);
     };
@@ -3378,12 +3413,13 @@ Status shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
                               const unsigned long *nmax,
                               const unsigned long *shc_nmax, const double *mu,
                               double r, const double *const *d_c,
-                              const double *const *d_s, double *const *d_f)
+                              const double *const *d_s, int kgrad,
+                              double *const *d_f)
 {
     std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
     CB_TRY(init(g_ctx));
     return shs_batch_tc(g_ctx, pnt, nsets, nmax, shc_nmax, mu, r, d_c, d_s,
-                        d_f);
+                        d_f, kgrad);
 }
 
 Status shs_point_dev_f32(const charm_point *pnt, unsigned long shc_nmax,

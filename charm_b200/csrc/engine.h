@@ -94,13 +94,15 @@ void batch_graph_free(void *graph);
 // The autotuner's choices so far (one line per problem shape).
 std::string autotune_report();
 
-// The potential of the batch with the degree sums on the tensor cores
-// (INT8 digit products, FP64 recombination).
+// The batch with the degree sums on the tensor cores (INT8 digit products,
+// FP64 recombination): kgrad 0 the potential, 1 grad1, 2 grad2, 3 all ten
+// quantities (as shs_point_batch_dev).
 Status shs_point_batch_i8_dev(const charm_point *pnt, size_t nsets,
                               const unsigned long *nmax,
                               const unsigned long *shc_nmax, const double *mu,
                               double r, const double *const *d_c,
-                              const double *const *d_s, double *const *d_f);
+                              const double *const *d_s, int kgrad,
+                              double *const *d_f);
 
 // Single-precision potential synthesis / analysis on grids whose rows admit
 // the shared-memory row transform, every row at r = R; float coefficient

@@ -287,6 +287,10 @@ int rfftc_max_clusters(int C, int Mc);
 // Batched grid synthesis with the degree sums on the tensor cores
 // (shs_tc.cu): up to SHS_TC_SETS coefficient sets per launch.
 constexpr int SHS_TC_SETS = 16;
+// with the gradients (ten quantities per set): five coefficient families
+// (C and S each) per set in the 32 accumulator columns
+constexpr int SHS_TC_GRAD_SETS = 3;
+constexpr int SHS_TC_FAMILIES = 5;
 
 // Coefficient digit tiles of a batch: per order m and 64-degree chunk,
 // [parity][digit][32 columns x 32 bytes] (columns 2 s, 2 s + 1 = C, S of
@@ -303,6 +307,9 @@ struct ShsTcPrep
     int *ecol;
     unsigned char *bdig;
     unsigned *status;
+    // 0: columns (C, S) per set; 1: the gradient families of shs_tc.cu,
+    // column 10 set + 2 family + (0: C, 1: S)
+    int grad;
 };
 
 struct ShsTcArgs
@@ -329,9 +336,15 @@ struct ShsTcArgs
     int nlat, ldf;
     int nsets;
     double2 *out[SHS_TC_SETS];            // lumped coefficients [nlat][ldf]
+                                          // ([10][nlat][ldf] with grad)
     double mur[SHS_TC_SETS];              // GM / R per set
     unsigned long long *counter;
     unsigned *status;
+    // 1: potential, grad1 and grad2 of SHS_TC_GRAD_SETS sets (ten lumped
+    // arrays per set in the order V, grad1 l r p, grad2 ll lr lp rr rp pp;
+    // GM / R^(k+1) = mur / Rref^k for the derivatives of order k)
+    int grad;
+    double Rref;
 };
 
 size_t shs_tc_smem_bytes();

@@ -46,6 +46,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "leg.cuh"
+#include "synth.cuh"
 
 namespace cb
 {
@@ -137,6 +138,15 @@ __device__ __forceinline__ void tc_ld8(uint32_t taddr, int (&v)[8])
                  : "r"(taddr));
 }
 
+// 2 consecutive accumulator columns of this warp's 32 lanes (the column
+// offset is even)
+__device__ __forceinline__ void tc_ld2(uint32_t taddr, int (&v)[2])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                 : "=r"(v[0]), "=r"(v[1])
+                 : "r"(taddr));
+}
+
 __device__ __forceinline__ void tc_wait_ld()
 {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
@@ -149,6 +159,15 @@ __device__ __forceinline__ void tc_st_zero16(uint32_t taddr)
     asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
                  "{%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
                  "%1, %1};" ::"r"(taddr), "r"(z)
+                 : "memory");
+}
+
+// zeros into 2 consecutive accumulator columns (even offset)
+__device__ __forceinline__ void tc_st_zero2(uint32_t taddr)
+{
+    const unsigned z = 0u;
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %1};"
+                 ::"r"(taddr), "r"(z)
                  : "memory");
 }
 
@@ -238,6 +257,69 @@ __global__ void k_tc_colexp(ShsTcPrep P)
     }
 }
 
+// The coefficient families of the gradients.  With A_n = P_nm (R/r)^(n+1)
+// the Legendre operand and X = C or S of one set, the potential, grad1 and
+// grad2 need, per latitude, the sums over n of A_n times
+//   f = 0: X_n,  1: n X_n,  2: n (n + 1) X_n,
+//   f = 3: e_(n+1) X_(n+1),  4: n e_(n+1) X_(n+1),
+// e_n = sqrt((n - m)(n + m)(2n + 1) / (2n - 1)) (src/leg/leg_func_enm.c):
+// cos(lat) dP_n/dlat = e_n P_n-1 - n sin(lat) P_n shifts the first term to
+// the Legendre index n - 1 (families 3, 4), and the Legendre equation
+// d2P_n/dlat2 = tan(lat) dP_n/dlat - (n (n + 1) - m^2 / cos^2(lat)) P_n
+// gives the second derivatives -- the per-degree relations CHarm's
+// kernels (src/shs/shs_point_kernel.c:1639-1946) and shs_grid.cu use.
+// src[n] = X_nm, nset the set's degree.
+__device__ __forceinline__ double tc_family(int f, long long m, long long n,
+                                            const double *src, long long nset)
+{
+    const double nd = (double)n;
+    if (f <= 2)
+    {
+        if (n > nset)
+            return 0.0;
+        const double x = src[n];
+        return f == 0 ? x : (f == 1 ? nd * x : (nd * (nd + 1.0)) * x);
+    }
+    const long long n1 = n + 1;
+    if (n1 > nset)
+        return 0.0;
+    const double n1d = (double)n1, md = (double)m;
+    const double e = sqrt(((n1d - md) * (n1d + md)) * (2.0 * n1d + 1.0) /
+                          (2.0 * n1d - 1.0));
+    const double x = e * src[n1];
+    return f == 3 ? x : nd * x;
+}
+
+// Column exponents of the gradient families: column 10 set + 2 f + (C, S),
+// one warp per column.
+__global__ void k_tc_colexp_grad(ShsTcPrep P)
+{
+    const long long m = blockIdx.x;
+    const int col = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (m > P.nmax)
+        return;
+    const int set = col / (2 * SHS_TC_FAMILIES);
+    const int f = (col % (2 * SHS_TC_FAMILIES)) >> 1;
+    const bool is_s = col & 1;
+    double mx = 0.0;
+    if (set < P.nsets && m <= P.set_nmax[set] && !(is_s && m == 0))
+    {
+        const long long s0 = tri_col0(P.shc_nmax[set], m);
+        const double *src = (is_s ? P.s[set] : P.c[set]) + s0 - m;
+        for (long long n = m + lane; n <= P.set_nmax[set]; n += 32)
+            mx = fmax(mx, fabs(tc_family(f, m, n, src, P.set_nmax[set])));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0)
+    {
+        P.ecol[m * TC_COLS + col] = mx > 0.0 ? max(expo_of(mx) + 1, -900) : 0;
+        if (!isfinite(mx))
+            atomicOr(P.status, DEV_ERR_BAD_ARGS);
+    }
+}
+
 // Digit tiles of every (order, chunk): [parity][digit][32 columns x 32 B].
 // One block per order, thread = (parity, column, 16-degree half).
 __global__ void __launch_bounds__(128) k_tc_bdigits(ShsTcPrep P)
@@ -247,7 +329,9 @@ __global__ void __launch_bounds__(128) k_tc_bdigits(ShsTcPrep P)
         return;
     const int t = threadIdx.x;
     const int p = t >> 6, col = (t >> 1) & 31, h = t & 1;
-    const int set = col >> 1;
+    // potential: columns (C, S) per set; gradients: 10 per set
+    const int set = P.grad ? col / (2 * SHS_TC_FAMILIES) : (col >> 1);
+    const int fam = P.grad ? (col % (2 * SHS_TC_FAMILIES)) >> 1 : 0;
     const bool is_s = col & 1;
     const bool active = set < P.nsets && m <= P.set_nmax[set] &&
                         !(is_s && m == 0);
@@ -274,7 +358,8 @@ __global__ void __launch_bounds__(128) k_tc_bdigits(ShsTcPrep P)
             {
                 const int k = 16 * h + 4 * q + b;
                 const long long n = m + j * TC_CH + 2 * k + p;
-                double v = (n <= nset) ? src[n] * sc : 0.0;
+                double v =
+                    (n <= nset) ? tc_family(fam, m, n, src, nset) * sc : 0.0;
                 unsigned long long y =
                     (unsigned long long)__double2ll_rn(v) + TC_BIAS;
                 lo[b] = (unsigned)y;
@@ -398,7 +483,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
                  : "memory");
 }
 
-template <bool RR>
+template <bool RR, bool GRAD>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -851,6 +936,156 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
             tc_fence_after();
             const double cpack = m == 0 ? 1.0 : 0.5;
             const double rsi = pow2i(eA - 105);
+            if constexpr (GRAD)
+            {
+                // potential, grad1 and grad2 from the five families of
+                // each set (tc_family): half 0 of the warps takes sets 0 and
+                // 2, half 1 set 1
+                const double t = valid ? A.t[p] : 0.0;
+                const double u = valid ? A.u[p] : 1.0;
+                const double rho = (RR && valid) ? A.rho[p] : 1.0;
+                const double ur = u > 0.0 ? 1.0 / u : 0.0;
+                const double u2 = ur * ur;
+                const double md = (double)m;
+                const size_t qs = (size_t)A.nlat * (size_t)A.ldf;
+#pragma unroll 1
+                for (int set = half; set < A.nsets; set += 2)
+                {
+                    // [parity][family][C, S], scaled to the coefficients
+                    double V[2][SHS_TC_FAMILIES][2];
+#pragma unroll 1
+                    for (int f = 0; f < SHS_TC_FAMILIES; f++)
+                    {
+                        const int col = 2 * SHS_TC_FAMILIES * set + 2 * f;
+#pragma unroll
+                        for (int pp = 0; pp < 2; pp++)
+                        {
+                            int v[TC_NLEV][2];
+#pragma unroll
+                            for (int L = 0; L < TC_NLEV; L++)
+                                tc_ld2(lane_base +
+                                           (uint32_t)((pp * TC_NLEV + L) *
+                                                          TC_COLS +
+                                                      col),
+                                       v[L]);
+                            tc_wait_ld();
+#pragma unroll
+                            for (int cs = 0; cs < 2; cs++)
+                            {
+                                const long long u0 =
+                                    (long long)v[0][cs] +
+                                    (long long)v[1][cs] * 256LL +
+                                    (long long)v[2][cs] * 65536LL;
+                                const long long u1 =
+                                    (long long)v[3][cs] +
+                                    (long long)v[4][cs] * 256LL +
+                                    (long long)v[5][cs] * 65536LL;
+                                const long long uu2 =
+                                    (long long)v[6][cs] +
+                                    (long long)v[7][cs] * 256LL;
+                                V[pp][f][cs] = fma(
+                                    l2d_exact(uu2), pow2i(8 * (6 + TC_LMIN)),
+                                    fma(l2d_exact(u1),
+                                        pow2i(8 * (3 + TC_LMIN)),
+                                        l2d_exact(u0) * pow2i(8 * TC_LMIN)));
+                            }
+                        }
+                        const int ec = __shfl_sync(0xffffffffu, ecl, col);
+                        const int es = __shfl_sync(0xffffffffu, ecl, col + 1);
+                        const double fc = pow2i(ec) * rsi;
+                        const double fs = pow2i(es) * rsi;
+#pragma unroll
+                        for (int pp = 0; pp < 2; pp++)
+                        {
+                            V[pp][f][0] *= fc;
+                            V[pp][f][1] *= fs;
+                        }
+                    }
+                    // this warp is the only reader of the set's columns
+                    // (for its lanes): zero them for the next item
+#pragma unroll 1
+                    for (int pl = 0; pl < 2 * TC_NLEV; pl++)
+#pragma unroll
+                        for (int f = 0; f < SHS_TC_FAMILIES; f++)
+                            tc_st_zero2(lane_base +
+                                        (uint32_t)(pl * TC_COLS +
+                                                   2 * SHS_TC_FAMILIES * set +
+                                                   2 * f));
+                    if (!valid)
+                        continue;
+                    const double mur0 = A.mur[set];
+                    const double mur1 = mur0 / A.Rref;
+                    const double mur2 = mur1 / A.Rref;
+                    double2 *o = A.out[set];
+#pragma unroll 1
+                    for (int hh = 0; hh < 2; hh++)
+                    {
+                        const int row = hh == 0 ? rown : rows;
+                        if (row < 0 || row >= A.nlat)
+                            continue;
+                        // the families at this latitude: P_n(-t) =
+                        // (-1)^(n - m) P_n(t) for the southern member
+                        const double sg = hh == 0 ? 1.0 : -1.0;
+                        const double tt = hh == 0 ? t : -t;
+                        double a2[6], b2[6];
+#pragma unroll
+                        for (int cs = 0; cs < 2; cs++)
+                        {
+                            const double f0 = V[0][0][cs] + sg * V[1][0][cs];
+                            const double fn = V[0][1][cs] + sg * V[1][1][cs];
+                            const double fnn = V[0][2][cs] + sg * V[1][2][cs];
+                            const double fe = V[0][3][cs] + sg * V[1][3][cs];
+                            const double fke = V[0][4][cs] + sg * V[1][4][cs];
+                            const double dp = (rho * fe - tt * fn) * ur;
+                            double *q = cs == 0 ? a2 : b2;
+                            q[0] = f0;                       // P
+                            q[1] = fn + f0;                  // (n + 1) P
+                            q[2] = dp;                       // dP
+                            q[3] = fnn + 2.0 * (fn + f0);    // (n+1)(n+2) P
+                            q[4] = (rho * (fke + 2.0 * fe) - tt * fnn) * ur;
+                            q[5] = fma(tt * ur, dp,
+                                       fma(md * md, u2 * f0, -fnn));   // ddP
+                        }
+                        const size_t at = (size_t)row * A.ldf + m;
+                        const double w0 = cpack * mur0;
+                        o[at] = make_double2(w0 * a2[0], -(w0 * b2[0]));
+                        // grad1: (R/r)^(n+2), order l, r, p
+                        double a1[3], b1[3];
+#pragma unroll
+                        for (int q = 0; q < 3; q++)
+                        {
+                            a1[q] = rho * a2[q];
+                            b1[q] = rho * b2[q];
+                        }
+                        lumped_post<1, 0, 3>(a1, b1, md, ur, u2, tt * ur, 0);
+                        const double w1 = cpack * mur1;
+#pragma unroll
+                        for (int q = 0; q < 3; q++)
+                            o[(1 + q) * qs + at] =
+                                make_double2(w1 * a1[q], -(w1 * b1[q]));
+                        // grad2: (R/r)^(n+3), order ll lr lp rr rp pp
+                        const double r2 = rho * rho;
+#pragma unroll
+                        for (int q = 0; q < 6; q++)
+                        {
+                            a2[q] *= r2;
+                            b2[q] *= r2;
+                        }
+                        lumped_post<2, 0, 6>(a2, b2, md, ur, u2, tt * ur, 0);
+                        const double w2 = cpack * mur2;
+#pragma unroll
+                        for (int q = 0; q < 6; q++)
+                            o[(4 + q) * qs + at] =
+                                make_double2(w2 * a2[q], -(w2 * b2[q]));
+                    }
+                }
+                // the columns this warp read are zero again: release them
+                tc_wait_st();
+                tc_fence_before();
+                mbar_arrive(bar_free);
+            }
+            else
+            {
 #pragma unroll 1
             for (int cb = 2 * half; cb < 2 * half + 2; cb++)
             {
@@ -931,6 +1166,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_shs_tc(ShsTcArgs A)
                     }
                 }
             }
+            }
         }
     }
     tc_fence_before();
@@ -980,7 +1216,10 @@ cudaError_t launch_tc_seeds(const ShsTcArgs &A, bool rr, double *seed_x,
 
 cudaError_t launch_tc_prep(const ShsTcPrep &P, cudaStream_t st)
 {
-    k_tc_colexp<<<(unsigned)(P.nmax + 1), 512, 0, st>>>(P);
+    if (P.grad)
+        k_tc_colexp_grad<<<(unsigned)(P.nmax + 1), 32 * TC_COLS, 0, st>>>(P);
+    else
+        k_tc_colexp<<<(unsigned)(P.nmax + 1), 512, 0, st>>>(P);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return e;
@@ -992,26 +1231,17 @@ cudaError_t launch_shs_tc(const ShsTcArgs &A, bool rr, int grid,
                           cudaStream_t st)
 {
     const size_t smem = shs_tc_smem_bytes();
-    cudaError_t e;
-    if (rr)
-    {
-        e = cudaFuncSetAttribute(k_shs_tc<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
+    auto go = [&](auto kern) {
+        cudaError_t e = cudaFuncSetAttribute(
+            kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess)
             return e;
-        k_shs_tc<true><<<grid, TC_THREADS, smem, st>>>(A);
-    }
-    else
-    {
-        e = cudaFuncSetAttribute(k_shs_tc<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess)
-            return e;
-        k_shs_tc<false><<<grid, TC_THREADS, smem, st>>>(A);
-    }
-    return cudaGetLastError();
+        kern<<<grid, TC_THREADS, smem, st>>>(A);
+        return cudaGetLastError();
+    };
+    if (A.grad)
+        return rr ? go(k_shs_tc<true, true>) : go(k_shs_tc<false, true>);
+    return rr ? go(k_shs_tc<true, false>) : go(k_shs_tc<false, false>);
 }
 
 } // namespace cb

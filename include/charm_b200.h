@@ -247,7 +247,7 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_dev(
 
 /* A batched synthesis captured into a CUDA graph (no counterpart in CHarm):
  * split_precision 0 captures charm_b200_shs_point_batch_dev, 1 captures
- * charm_b200_shs_point_batch_i8_dev (kgrad 0), with these arguments.  The
+ * charm_b200_shs_point_batch_i8_dev, with these arguments.  The
  * call runs once plainly (checks, tables, buffers, tuned choices), then once
  * under stream capture; returns the graph's handle, or NULL with err set.
  * charm_b200_graph_launch replays the whole call (every launch, copy and
@@ -280,7 +280,13 @@ CHARM_EXTERN size_t CHARM_CDECL charm_b200_autotune_report(char *buf,
  * 54-bit fixed-point integers, cut into seven 8-bit digits whose products
  * are summed exactly in INT32 (tcgen05 kind::i8) and recombined in FP64.
  * Agrees with the FP64 path to a relative RMS of about 1e-15 per set.
- * kgrad must be 0 (the potential); the polar optimisation must be off. */
+ * kgrad as charm_b200_shs_point_batch_dev: 0 the potential; 1, 2 and 3
+ * (grad1, grad2, all ten quantities) contract the same Legendre values
+ * against five coefficient families per set (C_n, n C_n, n (n + 1) C_n,
+ * e_n+1 C_n+1, n e_n+1 C_n+1 and the same of S), from which the derivative
+ * terms follow by the per-degree relations of CHarm's kernels
+ * (src/shs/shs_point_kernel.c:1639-1946), 3 sets per launch.  The polar
+ * optimisation must be off. */
 CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_i8_dev(
     const charm_point *pnt, size_t nsets, const unsigned long *nmax,
     const unsigned long *shc_nmax, const double *mu, double r,

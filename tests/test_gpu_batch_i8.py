@@ -42,10 +42,11 @@ def run(env, fn, pnt, sets, r, kgrad=0):
     dc = (ct.c_void_p * n)()
     ds = (ct.c_void_p * n)()
     df = (ct.c_void_p * n)()
+    ncomp = {0: 1, 1: 3, 2: 6, 3: 10}.get(kgrad, 1)
     for j, (N, c, s, _) in enumerate(sets):
         tc = torch.from_numpy(c).cuda()
         ts = torch.from_numpy(s).cuda()
-        tf = torch.full((pnt.lat.size * pnt.lon.size,), np.nan,
+        tf = torch.full((ncomp * pnt.lat.size * pnt.lon.size,), np.nan,
                         dtype=torch.float64, device="cuda")
         keep += [tc, ts]
         outs.append(tf)
@@ -60,6 +61,8 @@ def run(env, fn, pnt, sets, r, kgrad=0):
     if msg is not None:
         return None, msg
     shape = (pnt.lat.size, pnt.lon.size)
+    if kgrad:
+        shape = (ncomp,) + shape
     return [o.cpu().numpy().reshape(shape) for o in outs], None
 
 
@@ -123,9 +126,79 @@ def test_i8_below_the_sphere(env):
     compare(env, p, make_sets(950, [120, 80, 120]), R_EARTH)
 
 
-def test_i8_rejects_gradients(env):
+NAMES = {1: ["x", "y", "z"], 2: ["xx", "xy", "xz", "yy", "yz", "zz"],
+         3: ["V", "x", "y", "z", "xx", "xy", "xz", "yy", "yz", "zz"]}
+
+
+def interior(pnt):
+    """Rows off the poles: the x / y components are singular at a pole
+    (CHarm's tests zero them there, tests/check_shs_point_all.c:229-300)."""
+    return np.cos(pnt.lat) > 1e-8
+
+
+@pytest.mark.parametrize("grid,N,h,kgrad", [
+    ("GL", 300, 0.0, 3),
+    ("DH2", 200, 250e3, 3),      # the batched workload's height, pole row
+    ("DH1", 150, -5000.0, 1),
+    ("GL", 129, 1000.0, 2),
+])
+def test_i8_gradients_against_fp64(env, grid, N, h, kgrad):
+    """grad1 / grad2 / all ten quantities through the gradient families on
+    the tensor cores, 4 sets (launches of 3 and 1), each component against
+    the FP64 batch's, relative to that component's RMS off the poles."""
+    torch, cb, L = env
+    ctor = {"GL": cb.PointGridGL, "DH1": cb.PointGridDH1,
+            "DH2": cb.PointGridDH2}[grid]
+    p = ctor(N, R_EARTH + h)
+    sets = make_sets(970 + N, [N, N // 2, N - 1, 3])
+    ref, msg = run(env, L.charm_b200_shs_point_batch_dev, p, sets, R_EARTH,
+                   kgrad)
+    assert msg is None, msg
+    got, msg = run(env, L.charm_b200_shs_point_batch_i8_dev, p, sets, R_EARTH,
+                   kgrad)
+    assert msg is None, msg
+    keep = interior(p)
+    worst = {}
+    for (Ns, *_), g, f in zip(sets, got, ref):
+        for q, name in enumerate(NAMES[kgrad]):
+            a, b = g[q][keep], f[q][keep]
+            assert np.all(np.isfinite(a)), (Ns, name)
+            e = rel_rms(a, b)
+            worst[name] = max(worst.get(name, 0.0), e)
+            assert e <= 1e-12, (Ns, name, e)
+        # the non-singular components on the pole rows too
+        for q, name in enumerate(NAMES[kgrad]):
+            if name in ("V", "z", "zz"):
+                assert rel_rms(g[q], f[q]) <= 1e-12, (Ns, name)
+    print(grid, N, kgrad, {k: "%.1e" % v for k, v in worst.items()})
+
+
+def test_i8_gradients_against_oracle(env):
+    """All ten quantities of one set at nmax 120 on the DH2 grid at
+    R + 250 km against the CPU oracle on 6 interior rows."""
+    from oracle import orc
+    torch, cb, L = env
+    N, h = 120, 250e3
+    p = cb.PointGridDH2(N, R_EARTH + h)
+    sets = make_sets(990, [N])
+    got, msg = run(env, L.charm_b200_shs_point_batch_i8_dev, p, sets, R_EARTH,
+                   3)
+    assert msg is None, msg
+    rows = np.linspace(3, p.lat.size - 4, 6).astype(int)
+    po = orc.Point(orc.GRID, p.lat[rows], p.lon,
+                   np.full(rows.size, R_EARTH + h))
+    N_, c, s, mu = sets[0]
+    shc = orc.Shc(N, mu, R_EARTH, c, s)
+    ref = (orc.shs_point(po, shc, N, "pot") + orc.shs_point(po, shc, N, "grad1")
+           + orc.shs_point(po, shc, N, "grad2"))
+    for q, name in enumerate(NAMES[3]):
+        e = rel_rms(got[0][q][rows], np.reshape(ref[q], (rows.size, -1)))
+        assert e <= 1e-12, (name, e)
+
+
+def test_i8_rejects_bad_kgrad(env):
     torch, cb, L = env
     p = cb.PointGridGL(30, R_EARTH)
     _, msg = run(env, L.charm_b200_shs_point_batch_i8_dev, p,
-                 make_sets(960, [30]), R_EARTH, kgrad=1)
+                 make_sets(960, [30]), R_EARTH, kgrad=4)
     assert msg is not None and "kgrad" in msg
