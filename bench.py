@@ -1003,6 +1003,9 @@ def batch_dh(single_calls=True, oracle_rows=6):
     t_single = 0.0
     G = 8
     probe = {}     # set -> (grid, rows, [10 x (rows, nlon)]) of the FP64 batch
+    probe8 = {}    # the same of the split-precision batch
+    worst8 = {}    # component -> largest relative RMS split vs FP64
+    t_batch8 = 0.0
     for pnt, idx in groups:
         npts = pnt.lat.size * pnt.lon.size
         jmin = min(idx, key=lambda j: nm[j])
@@ -1032,6 +1035,36 @@ def batch_dh(single_calls=True, oracle_rows=6):
             if jmin in sel:
                 o = out[sel.index(jmin)].view(10, pnt.lat.size, pnt.lon.size)
                 probe[jmin] = (pnt, rows, o[:, rows, :].cpu().numpy())
+            # the same ten quantities with the degree sums on the tensor
+            # cores (split precision, 3 sets per launch), compared per
+            # component off the poles (x / y components are singular there)
+            out8 = [torch.empty(10 * npts, dtype=torch.float64, device="cuda")
+                    for _ in sel]
+            pf8 = (ct.c_void_p * n)(*[t.data_ptr() for t in out8])
+            for rep in range(2):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                L.charm_b200_shs_point_batch_i8_dev(
+                    ct.cast(pnt._Point, P), n, nmv, nmv, muv, R_EARTH, pc, ps,
+                    3, pf8, ct.cast(err, P))
+                check()
+                torch.cuda.synchronize()
+                if rep == 1:
+                    t_batch8 += time.perf_counter() - t0
+            keep = torch.from_numpy(np.cos(pnt.lat) > 1e-8).cuda()
+            for b in range(n):
+                a8 = out8[b].view(10, pnt.lat.size, pnt.lon.size)
+                a64 = out[b].view(10, pnt.lat.size, pnt.lon.size)
+                for q, nm_ in enumerate(names):
+                    d = (a8[q][keep] - a64[q][keep]).double()
+                    r_ = a64[q][keep].double()
+                    e = float(torch.sqrt(torch.mean(d * d)) /
+                              torch.sqrt(torch.mean(r_ * r_)))
+                    worst8[nm_] = max(worst8.get(nm_, 0.0), e)
+            if jmin in sel:
+                o8 = out8[sel.index(jmin)].view(10, pnt.lat.size, pnt.lon.size)
+                probe8[jmin] = o8[:, rows, :].cpu().numpy()
+            del out8
             if single_calls:
                 # one call per set and kind (potential, grad1, grad2); the
                 # first pass, untimed, takes each shape's one-time costs
@@ -1111,7 +1144,8 @@ def batch_dh(single_calls=True, oracle_rows=6):
                orc.shs_point(po, shc, int(nm[j]), "grad1") +
                orc.shs_point(po, shc, int(nm[j]), "grad2"))
         e = {nm_: rel_rms(vals[q], ref[q]) for q, nm_ in enumerate(names)}
-        e["V_split_precision"] = rel_rms(i8_probe[j], ref[0])
+        e["split_precision"] = {nm_: rel_rms(probe8[j][q], ref[q])
+                                for q, nm_ in enumerate(names)}
         comp["set%d_nmax%d_%s" % (j, int(nm[j]),
                                   "dh1" if j % 2 == 0 else "dh2")] = e
     L.charm_err_free(err)
@@ -1121,6 +1155,10 @@ def batch_dh(single_calls=True, oracle_rows=6):
                     "250 km, DH1 / DH2 grids of the largest degree",
         "fp64_batched_10q_s": t_batch,
         "fp64_batched_10q_sets_per_s": 64.0 / t_batch,
+        "split_precision_batched_10q_s": t_batch8,
+        "split_precision_batched_10q_sets_per_s": 64.0 / t_batch8,
+        "split_precision_speedup_10q": t_batch / t_batch8,
+        "split_vs_fp64_rel_rms_per_component_off_poles": worst8,
         "units_n_m_pair": total_units,
         "potential_fp64_vs_split_precision": pot,
         "rel_rms_vs_oracle_per_component": comp,
