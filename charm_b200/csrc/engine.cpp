@@ -2707,6 +2707,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                                                 G >= 3 ? 3 : 2, bands)
                                    : 1;
     bool ordered = false;
+    bool fused = false;   // the analysis kernel reduced the groups itself
     if (nband > 1)
     {
         // orders of the last band in up to four bands of about equal
@@ -2824,6 +2825,27 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         }
         else
             CB_TRY(rows_fft(0, (int)nlat));
+        // one launch over all groups: the last group of each order to
+        // finish sums the order's partial columns (no separate reduction
+        // pass over the partial sums)
+        unsigned *mcount = nullptr;
+        CB_TRY(dbuf(c, "sha_mcount", (size_t)nmax + 1, &mcount));
+        CB_CUDA(cudaMemsetAsync(mcount, 0, ((size_t)nmax + 1) * sizeof(unsigned),
+                                c.stream), st);
+        if (sn > nmax)
+        {
+            const size_t Tn = (size_t)(sn + 1) * (sn + 2) / 2;
+            CB_CUDA(cudaMemsetAsync(oc, 0, Tn * 8, c.stream), st);
+            CB_CUDA(cudaMemsetAsync(os, 0, Tn * 8, c.stream), st);
+        }
+        A.m_count = mcount;
+        A.tc = tab.tc;
+        A.rescale = dres;
+        A.scale = 1.0;
+        A.shc_nmax = (long long)sn;
+        A.out_c = oc;
+        A.out_s = os;
+        fused = true;
         int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                             (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
@@ -2835,6 +2857,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         CB_CUDA(cudaStreamSynchronize(c.copy_stream), st);
         return finish(c, d_status);
     }
+    if (!fused)
     {
         Scope sc(c, TIMER_PREP);
         CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T,
