@@ -399,13 +399,28 @@ __global__ void k_lon_direct(int npar, int nlat, int nlon, long long nmax,
     long long qi = idx / nlon;
     const double2 *row = lc + qi * ldf;
     double lj = lon[j];
+    // cos(m lon), sin(m lon) by rotation through lon from one order to the
+    // next -- the recurrence over the orders that CHarm's PSLR path runs
+    // over the longitudes (src/shs/shs_grd_lr.c, shs_grd_lr2.c: 2 cos(m
+    // dlon) d_j-1 - d_j-2) -- restarted from the exact angle
+    // (sincos_mlon) every 64 orders, so that the rounding of the rotations
+    // cannot accumulate over more than 64 steps
+    double s1, c1;
+    sincos(lj, &s1, &c1);
     double acc = 0.0;
-    for (long long m = 0; m <= nmax; m++)
+    for (long long m0 = 0; m0 <= nmax; m0 += 64)
     {
         double ss, cc;
-        sincos_mlon((double)m, lj, &ss, &cc);
-        double2 v = row[m];
-        acc = fma(v.x, cc, fma(v.y, ss, acc));
+        sincos_mlon((double)m0, lj, &ss, &cc);
+        const long long m1 = m0 + 63 < nmax ? m0 + 63 : nmax;
+        for (long long m = m0; m <= m1; m++)
+        {
+            const double2 v = row[m];
+            acc = fma(v.x, cc, fma(v.y, ss, acc));
+            const double cn = fma(cc, c1, -(ss * s1));
+            ss = fma(ss, c1, cc * s1);
+            cc = cn;
+        }
     }
     f[idx] = acc;
 }

@@ -150,6 +150,29 @@ def test_custom_grid_direct_longitudes(cb):
     assert rel_rms(f, fo) <= TOL
 
 
+def test_custom_grid_longitude_recurrence_high_degree(cb):
+    """A regional grid (longitudes 10..60 degrees, no FFT) at nmax 1500:
+    the longitude sums run the rotation recurrence over 1501 orders
+    (restarted every 64), against the oracle's direct sums and against
+    CHarm's own PSLR path (src/shs/shs_grd_lr.c) where its build exists."""
+    from oracle import charm_ref
+    N = 1500
+    c, s = kaula(N, 37)
+    lat = np.deg2rad(np.linspace(50.0, 30.0, 12))
+    lon = np.deg2rad(np.linspace(10.0, 60.0, 301))
+    r = np.full(lat.size, R_EARTH)
+    f = cb.shs_point(cb.PointGrid(lat, lon, r), cb.Shc(N, GM, R_EARTH, c, s), N)
+    fo = orc.shs_point(orc.Point(orc.GRID, lat, lon, r), ora_shc(N, c, s), N)[0]
+    assert rel_rms(f, fo) <= TOL
+    f00 = GM / R_EARTH
+    assert rel_rms(np.ravel(f) - f00, np.ravel(fo) - f00) <= 1e-9
+    if charm_ref.available("d"):
+        C = charm_ref.Charm("d")
+        fr = C.shs_point(C.point(charm_ref.GRID, lat, lon, r),
+                         C.shc(N, GM, R_EARTH, c, s), N, lat.size * lon.size)
+        assert rel_rms(f, fr) <= TOL
+
+
 @pytest.mark.parametrize("N", [2190])
 def test_round_trip_large(cb, N):
     """Config 2: nmax 2190 on GL 2191 x 4382 -- SHA(SHS(c)) recovers c."""
