@@ -94,7 +94,14 @@ def _structs(flt):
                     ("c", ct.POINTER(ct.POINTER(flt))),
                     ("s", ct.POINTER(ct.POINTER(flt))),
                     ("owner", ct.c_bool), ("distributed", ct.c_bool)]
-    return Err, Point, Shc
+
+    class Cell(ct.Structure):
+        _fields_ = [("type", ct.c_int), ("nlat", ct.c_size_t),
+                    ("nlon", ct.c_size_t), ("ncell", ct.c_size_t),
+                    ("latmin", ct.POINTER(flt)), ("latmax", ct.POINTER(flt)),
+                    ("lonmin", ct.POINTER(flt)), ("lonmax", ct.POINTER(flt)),
+                    ("r", ct.POINTER(flt)), ("owner", ct.c_bool)]
+    return Err, Point, Shc, Cell
 
 
 class Charm:
@@ -113,7 +120,7 @@ class Charm:
         self.pre = pre
         flt = {"d": ct.c_double, "f": ct.c_float, "q": _F128}[prec]
         self.flt = flt
-        self.Err, self.Point, self.Shc = _structs(flt)
+        self.Err, self.Point, self.Shc, self.Cell = _structs(flt)
         P, UL, SZ = ct.POINTER, ct.c_ulong, ct.c_size_t
         sig = {
             "err_init": ([], P(self.Err)),
@@ -135,6 +142,13 @@ class Charm:
                                None),
             "sha_point": ([P(self.Point), P(flt), UL, P(self.Shc),
                            P(self.Err)], None),
+            "crd_cell_init": ([ct.c_int, SZ, SZ, P(flt), P(flt), P(flt),
+                               P(flt), P(flt)], P(self.Cell)),
+            "crd_cell_free": ([P(self.Cell)], None),
+            "shs_cell": ([P(self.Cell), P(self.Shc), UL, P(flt),
+                          P(self.Err)], None),
+            "sha_cell": ([P(self.Cell), P(flt), UL, ct.c_int, P(self.Shc),
+                          P(self.Err)], None),
         }
         if prec != "q":
             sig["shc_init"] = ([UL, flt, flt, P(flt), P(flt)], P(self.Shc))
@@ -232,6 +246,35 @@ class Charm:
         out = self.shc(nmax, mu, r, c, s)
         f = np.ascontiguousarray(f, self._np())
         self.fn("sha_point")(_p(pnt), self._ptr(f), nmax, out.ptr, self.err)
+        self.check()
+        return out.keep[0].copy(), out.keep[1].copy()
+
+    def cell(self, ctype, latmin, latmax, lonmin, lonmax, r):
+        """charm_crd_cell_init over caller arrays (kept alive on the
+        returned object)."""
+        t = self._np()
+        arrs = [np.ascontiguousarray(a, t) for a in
+                (latmin, latmax, lonmin, lonmax, r)]
+        c = self.fn("crd_cell_init")(ctype, arrs[0].size, arrs[2].size,
+                                     *[self._ptr(a) for a in arrs])
+        if not c:
+            raise RuntimeError("CHarm crd_cell_init failed")
+        return _Owned(c, tuple(arrs), self.fn("crd_cell_free"))
+
+    def shs_cell(self, cell, shcs, nmax, ncell):
+        f = np.empty(ncell, self._np())
+        self.fn("shs_cell")(_p(cell), _p(shcs), nmax, self._ptr(f), self.err)
+        self.check()
+        return f
+
+    def sha_cell(self, cell, f, nmax, mu, r):
+        """Approximate-quadrature analysis (CHARM_SHA_CELL_AQ) into a fresh
+        triangle of degree nmax; returns (c, s)."""
+        T = (nmax + 1) * (nmax + 2) // 2
+        out = self.shc(nmax, mu, r, np.zeros(T), np.zeros(T))
+        f = np.ascontiguousarray(f, self._np())
+        self.fn("sha_cell")(_p(cell), self._ptr(f), nmax, 0, out.ptr,
+                            self.err)
         self.check()
         return out.keep[0].copy(), out.keep[1].copy()
 

@@ -801,6 +801,478 @@ void ORC(sha_contract)(unsigned long nmax, size_t nrow, const real *lat,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Block-mean values in cells: latitude integrals of the Legendre functions  */
+/* ------------------------------------------------------------------------ */
+/* Un-normalised Legendre recurrence P_n = e_n t P_n-1 - f_n P_n-2,
+ * src/leg/leg_pol_en_fn.c:14-38 (arrays of nmax + 1 entries). */
+static void leg_en_fn(unsigned long nmax, real *en, real *fn)
+{
+    en[0] = fn[0] = 0;
+    if (nmax == 0)
+        return;
+    en[1] = fn[1] = 0;
+    for (unsigned long n = 2; n <= nmax; n++)
+    {
+        en[n] = (real)(2 * n - 1) / (real)n;
+        fn[n] = (real)(n - 1) / (real)n;
+    }
+}
+
+/* Coefficients of the integral recurrences, src/leg/leg_func_gm_hm.c:14-45:
+ * I_mm = g_m I_m-2,m-2 + (t2 P_mm(t2) - t1 P_mm(t1)) / (m + 1) and
+ * I_nm = h_n b_nm I_n-2,m - a_nm / (n + 1) (u2^2 P_n-1,m(t2) - ...). */
+static void leg_gm_hm(unsigned long nmax, const real *r, const real *ri,
+                      real *gm, real *hm)
+{
+    for (unsigned long n = 0; n <= nmax && n < 3; n++)
+        gm[n] = 0;
+    for (unsigned long n = 3; n <= nmax; n++)
+        gm[n] = (real)1 / (real)(2 * n + 2) * r[n] * r[2 * n + 1] *
+                r[2 * n - 1] * ri[n - 1];
+    for (unsigned long n = 0; n <= nmax; n++)
+        hm[n] = (real)((long)n - 2) / (real)(n + 1);
+}
+
+/* X-number state of one latitude's recurrence over the degrees and its
+ * tesseral step (PNM_TESSERAL_XNUM, src/leg/leg_func_xnum.h), the same
+ * arithmetic as the loop of shs_kernel above.  Returns P_n,m as an
+ * F-number (zero below the X-number range). */
+typedef struct
+{
+    real x, y;
+    int64_t ix, iy;
+    int ds;
+} xrec_t;
+
+static inline real xrec_sectorial(xrec_t *s, const real *ps,
+                                  const int64_t *ips, unsigned long m)
+{
+    s->x = ps[m - 1];
+    s->ix = ips[m - 1];
+    s->y = 0;
+    s->iy = 0;
+    s->ds = 0;
+    return x2f(s->x, s->ix);
+}
+
+static inline real xrec_semisectorial(xrec_t *s, real t, real anm)
+{
+    s->y = s->x;
+    s->iy = s->ix;
+    s->x = (anm * t) * s->y;
+    s->ix = s->iy;
+    xnorm(&s->x, &s->ix);
+    return x2f(s->x, s->ix);
+}
+
+static inline real xrec_tesseral(xrec_t *s, real t, real anm, real bnm)
+{
+    real pnm2;
+    if (s->ds)
+    {
+        pnm2 = (anm * t) * s->x - bnm * s->y;
+        s->y = s->x;
+        s->x = pnm2;
+        return pnm2;
+    }
+    int64_t ixy = s->ix - s->iy, iz;
+    real z;
+    if (ixy == 0)
+    {
+        z = (anm * t) * s->x - bnm * s->y;
+        iz = s->ix;
+    }
+    else if (ixy == 1)
+    {
+        z = (anm * t) * s->x - bnm * (s->y * BIGI);
+        iz = s->ix;
+    }
+    else if (ixy == -1)
+    {
+        z = (anm * t) * (s->x * BIGI) - bnm * s->y;
+        iz = s->iy;
+    }
+    else if (ixy > 1)
+    {
+        z = (anm * t) * s->x;
+        iz = s->ix;
+    }
+    else
+    {
+        z = -bnm * s->y;
+        iz = s->iy;
+    }
+    xnorm(&z, &iz);
+    s->y = s->x;
+    s->iy = s->ix;
+    s->x = z;
+    s->ix = iz;
+    pnm2 = x2f(z, iz);
+    if (s->ix == 0 && s->iy == 0)
+        s->ds = 1;
+    return pnm2;
+}
+
+/* I_mm of one cell row for m = 0..nmax (imm[0] unused), the sectorial
+ * integrals of src/sha/sha_cell.c:586-660 (and the imm0..imm2 state that
+ * src/shs/shs_cell_kernel.c:229-268 carries over the orders). */
+static void cell_imm(unsigned long nmax, real latmin, real latmax, real t1,
+                     real u1, real t2, real u2, const real *ps1,
+                     const int64_t *ips1, const real *ps2,
+                     const int64_t *ips2, const real *gm, real *imm)
+{
+    imm[0] = 0;
+    for (unsigned long m = 1; m <= nmax; m++)
+    {
+        real p1 = x2f(ps1[m - 1], ips1[m - 1]);
+        real p2 = x2f(ps2[m - 1], ips2[m - 1]);
+        if (m == 1)
+            imm[m] = (RROOT3 / (real)2) *
+                     ((t2 * u2 - (RPI_2 - latmax)) -
+                      (t1 * u1 - (RPI_2 - latmin)));
+        else if (m == 2)
+            imm[m] = (RSQRT((real)15) / (real)6) *
+                     (t2 * ((real)3 - t2 * t2) - t1 * ((real)3 - t1 * t1));
+        else
+            imm[m] = gm[m] * imm[m - 2] +
+                     ((real)1 / (real)(m + 1)) * (t2 * p2 - t1 * p1);
+    }
+}
+
+/* Public: lumped coefficients of the cell synthesis, the latitude integrals
+ * of src/shs/shs_cell_kernel.c:68-470 for every row and order:
+ *   a_m = sum_n (R/r)^(n+1) I_nm C_nm,  b_m likewise with S_nm,
+ * a2, b2 for the mirror row [-latmax, -latmin] ((-1)^(n+m) I_nm) when
+ * symm[i].  Outputs [nrow][nmax+1]; orders skipped by the polar
+ * optimisation (thr >= 0: m - nmax cos(latmin) > thr) are zero. */
+void ORC(cell_lumped)(unsigned long nmax, unsigned long shc_nmax,
+                      const real *c, const real *s, size_t nrow,
+                      const real *latmin, const real *latmax, const real *rr,
+                      const real *rr2, const int *symm, double polar_thr,
+                      real *a, real *b, real *a2, real *b2)
+{
+    init_consts();
+    size_t L = nmax + 1;
+    real *r = calloc(2 * nmax + 6, sizeof(real));
+    real *ri = calloc(2 * nmax + 6, sizeof(real));
+    real *dm = calloc(nmax + 2, sizeof(real));
+    real *en = calloc(nmax + 3, sizeof(real));
+    real *fn = calloc(nmax + 3, sizeof(real));
+    real *gm = calloc(nmax + 2, sizeof(real));
+    real *hm = calloc(nmax + 2, sizeof(real));
+    leg_r_ri(nmax, r, ri);
+    leg_dm(nmax, r, ri, dm);
+    leg_en_fn(nmax + 1, en, fn);
+    leg_gm_hm(nmax, r, ri, gm, hm);
+    size_t *col = malloc((shc_nmax + 1) * sizeof(size_t));
+    size_t idx = 0;
+    for (unsigned long m = 0; m <= shc_nmax; m++)
+    {
+        col[m] = idx;
+        idx += shc_nmax + 1 - m;
+    }
+    memset(a, 0, nrow * L * sizeof(real));
+    memset(b, 0, nrow * L * sizeof(real));
+    memset(a2, 0, nrow * L * sizeof(real));
+    memset(b2, 0, nrow * L * sizeof(real));
+
+#pragma omp parallel
+    {
+        real *anm = calloc(nmax + 2, sizeof(real));
+        real *bnm = calloc(nmax + 2, sizeof(real));
+        real *ps1 = calloc(nmax + 1, sizeof(real));
+        real *ps2 = calloc(nmax + 1, sizeof(real));
+        int64_t *ips1 = calloc(nmax + 1, sizeof(int64_t));
+        int64_t *ips2 = calloc(nmax + 1, sizeof(int64_t));
+        real *imm = calloc(nmax + 1, sizeof(real));
+#pragma omp for schedule(dynamic)
+        for (size_t i = 0; i < nrow; i++)
+        {
+            real t1 = RSIN(latmin[i]), u1 = RCOS(latmin[i]);
+            real t2 = RSIN(latmax[i]), u2 = RCOS(latmax[i]);
+            leg_prepare(u1, dm, nmax, ps1, ips1);
+            leg_prepare(u2, dm, nmax, ps2, ips2);
+            cell_imm(nmax, latmin[i], latmax[i], t1, u1, t2, u2, ps1, ips1,
+                     ps2, ips2, gm, imm);
+            const int sy = symm[i];
+            const real ratio = rr[i], ratio2 = sy ? rr2[i] : (real)0;
+            real ratiom = ratio, ratio2m = ratio2;
+            real *ar = a + i * L, *br = b + i * L;
+            real *a2r = a2 + i * L, *b2r = b2 + i * L;
+            for (unsigned long m = 0; m <= nmax;
+                 m++, ratiom *= ratio, ratio2m *= ratio2)
+            {
+                if (polar_thr >= 0.0 &&
+                    (real)polar_thr < (real)m - (real)nmax * u1)
+                    continue;
+                leg_anm_bnm(nmax, m, r, ri, anm, bnm);
+                const real *cm = c + col[m], *sm = s + col[m];
+                real ration = ratiom, ratio2n = ratio2m;
+                real A = 0, B = 0, A2 = 0, B2 = 0;
+                if (m == 0)
+                {
+                    /* zonal: un-normalised P_n and
+                     * I_n0 = (P_n+1 - P_n-1) / sqrt(2n+1),
+                     * shs_cell_kernel.c:97-175 */
+                    real p0a = 1, p0b = 1, p1a = t1, p1b = t2;
+                    real in0 = t2 - t1;
+                    real v = in0 * cm[0];
+                    A = ration * v;
+                    ration *= ratio;
+                    if (sy)
+                    {
+                        A2 = ratio2n * v;
+                        ratio2n *= ratio2;
+                    }
+                    int even = 0;
+                    for (unsigned long n = 1; n <= nmax; n++, even = !even)
+                    {
+                        real p2a = en[n + 1] * (t1 * p1a) - fn[n + 1] * p0a;
+                        real p2b = en[n + 1] * (t2 * p1b) - fn[n + 1] * p0b;
+                        in0 = ri[2 * n + 1] * ((p2b - p0b) - (p2a - p0a));
+                        v = in0 * cm[n];
+                        A = A + ration * v;
+                        ration *= ratio;
+                        if (sy)
+                        {
+                            A2 = even ? A2 + ratio2n * v : A2 - ratio2n * v;
+                            ratio2n *= ratio2;
+                        }
+                        p0a = p1a;
+                        p1a = p2a;
+                        p0b = p1b;
+                        p1b = p2b;
+                    }
+                }
+                else
+                {
+                    xrec_t s1, s2;
+                    real q1 = xrec_sectorial(&s1, ps1, ips1, m);
+                    real q2 = xrec_sectorial(&s2, ps2, ips2, m);
+                    real inm0 = imm[m];
+                    real vc = inm0 * cm[0], vs = inm0 * sm[0];
+                    A = ration * vc;
+                    B = ration * vs;
+                    ration *= ratio;
+                    if (sy)
+                    {
+                        A2 = ratio2n * vc;
+                        B2 = ratio2n * vs;
+                        ratio2n *= ratio2;
+                    }
+                    if (m < nmax)
+                    {
+                        real pm1 = q1, pm2 = q2; /* P_mm */
+                        q1 = xrec_semisectorial(&s1, t1, anm[m + 1]);
+                        q2 = xrec_semisectorial(&s2, t2, anm[m + 1]);
+                        real inm1 = -((anm[m + 1] / (real)(m + 2)) *
+                                      ((u2 * u2) * pm2 - (u1 * u1) * pm1));
+                        vc = inm1 * cm[1];
+                        vs = inm1 * sm[1];
+                        A = A + ration * vc;
+                        B = B + ration * vs;
+                        ration *= ratio;
+                        if (sy)
+                        {
+                            A2 = A2 - ratio2n * vc;
+                            B2 = B2 - ratio2n * vs;
+                            ratio2n *= ratio2;
+                        }
+                        int even = 1;
+                        for (unsigned long n = m + 2; n <= nmax;
+                             n++, even = !even)
+                        {
+                            real pa = q1, pb = q2; /* P_n-1,m */
+                            q1 = xrec_tesseral(&s1, t1, anm[n], bnm[n]);
+                            q2 = xrec_tesseral(&s2, t2, anm[n], bnm[n]);
+                            real inm2 = (hm[n] * bnm[n]) * inm0 -
+                                        (anm[n] / (real)(n + 1)) *
+                                        ((u2 * u2) * pb - (u1 * u1) * pa);
+                            inm0 = inm1;
+                            inm1 = inm2;
+                            vc = inm2 * cm[n - m];
+                            vs = inm2 * sm[n - m];
+                            A = A + ration * vc;
+                            B = B + ration * vs;
+                            ration *= ratio;
+                            if (sy)
+                            {
+                                if (even)
+                                {
+                                    A2 = A2 + ratio2n * vc;
+                                    B2 = B2 + ratio2n * vs;
+                                }
+                                else
+                                {
+                                    A2 = A2 - ratio2n * vc;
+                                    B2 = B2 - ratio2n * vs;
+                                }
+                                ratio2n *= ratio2;
+                            }
+                        }
+                    }
+                }
+                ar[m] = A;
+                br[m] = B;
+                a2r[m] = A2;
+                b2r[m] = B2;
+            }
+        }
+        free(anm);
+        free(bnm);
+        free(ps1);
+        free(ps2);
+        free(ips1);
+        free(ips2);
+        free(imm);
+    }
+    free(r);
+    free(ri);
+    free(dm);
+    free(en);
+    free(fn);
+    free(gm);
+    free(hm);
+    free(col);
+}
+
+/* Public: the Legendre contraction of the cell analysis,
+ * src/sha/sha_cell.c:560-1110.  amp, amm, bmp, bmm [nrow][nmax+1] are the
+ * longitude-integrated Fourier sums of each row (and its mirror) as formed
+ * at sha_cell.c:790-840; C_nm, S_nm accumulate into the order-major
+ * triangles c, s of degree nmax (zeroed by the caller), before the
+ * 1 / (4 pi) r / mu factor. */
+void ORC(cell_contract)(unsigned long nmax, size_t nrow, const real *latmin,
+                        const real *latmax, const real *amp, const real *amm,
+                        const real *bmp, const real *bmm, double polar_thr,
+                        real *c, real *s)
+{
+    init_consts();
+    size_t L = nmax + 1;
+    real *r = calloc(2 * nmax + 6, sizeof(real));
+    real *ri = calloc(2 * nmax + 6, sizeof(real));
+    real *dm = calloc(nmax + 2, sizeof(real));
+    real *en = calloc(nmax + 3, sizeof(real));
+    real *fn = calloc(nmax + 3, sizeof(real));
+    real *gm = calloc(nmax + 2, sizeof(real));
+    real *hm = calloc(nmax + 2, sizeof(real));
+    leg_r_ri(nmax, r, ri);
+    leg_dm(nmax, r, ri, dm);
+    leg_en_fn(nmax + 1, en, fn);
+    leg_gm_hm(nmax, r, ri, gm, hm);
+    size_t *col = malloc((nmax + 1) * sizeof(size_t));
+    size_t idx = 0;
+    for (unsigned long m = 0; m <= nmax; m++)
+    {
+        col[m] = idx;
+        idx += nmax + 1 - m;
+    }
+    real *geo = malloc(nrow * 4 * sizeof(real));
+    real *ps1 = calloc(nrow * L, sizeof(real));
+    real *ps2 = calloc(nrow * L, sizeof(real));
+    int64_t *ips1 = calloc(nrow * L, sizeof(int64_t));
+    int64_t *ips2 = calloc(nrow * L, sizeof(int64_t));
+    real *imm = calloc(nrow * L, sizeof(real));
+    for (size_t i = 0; i < nrow; i++)
+    {
+        real *g = geo + 4 * i;
+        g[0] = RSIN(latmin[i]);
+        g[1] = RCOS(latmin[i]);
+        g[2] = RSIN(latmax[i]);
+        g[3] = RCOS(latmax[i]);
+        leg_prepare(g[1], dm, nmax, ps1 + i * L, ips1 + i * L);
+        leg_prepare(g[3], dm, nmax, ps2 + i * L, ips2 + i * L);
+        cell_imm(nmax, latmin[i], latmax[i], g[0], g[1], g[2], g[3],
+                 ps1 + i * L, ips1 + i * L, ps2 + i * L, ips2 + i * L, gm,
+                 imm + i * L);
+    }
+#pragma omp parallel
+    {
+        real *anm = calloc(nmax + 2, sizeof(real));
+        real *bnm = calloc(nmax + 2, sizeof(real));
+#pragma omp for schedule(dynamic)
+        for (unsigned long m = 0; m <= nmax; m++)
+        {
+            leg_anm_bnm(nmax, m, r, ri, anm, bnm);
+            real *cm = c + col[m], *sm = s + col[m];
+            for (size_t i = 0; i < nrow; i++)
+            {
+                const real *g = geo + 4 * i;
+                const real t1 = g[0], u1 = g[1], t2 = g[2], u2 = g[3];
+                if (polar_thr >= 0.0 &&
+                    (real)polar_thr < (real)m - (real)nmax * u1)
+                    continue;
+                const real ap = amp[i * L + m], am = amm[i * L + m];
+                const real bp = bmp[i * L + m], bm = bmm[i * L + m];
+                if (m == 0)
+                {
+                    real p0a = 1, p0b = 1, p1a = t1, p1b = t2;
+                    cm[0] += (t2 - t1) * ap;
+                    int even = 0;
+                    for (unsigned long n = 1; n <= nmax; n++, even = !even)
+                    {
+                        real p2a = en[n + 1] * (t1 * p1a) - fn[n + 1] * p0a;
+                        real p2b = en[n + 1] * (t2 * p1b) - fn[n + 1] * p0b;
+                        real in0 = ri[2 * n + 1] * ((p2b - p0b) - (p2a - p0a));
+                        cm[n] += in0 * (even ? ap : am);
+                        p0a = p1a;
+                        p1a = p2a;
+                        p0b = p1b;
+                        p1b = p2b;
+                    }
+                    continue;
+                }
+                xrec_t s1, s2;
+                real q1 = xrec_sectorial(&s1, ps1 + i * L, ips1 + i * L, m);
+                real q2 = xrec_sectorial(&s2, ps2 + i * L, ips2 + i * L, m);
+                real inm0 = imm[i * L + m];
+                cm[0] += inm0 * ap;
+                sm[0] += inm0 * bp;
+                if (m == nmax)
+                    continue;
+                real pm1 = q1, pm2 = q2;
+                q1 = xrec_semisectorial(&s1, t1, anm[m + 1]);
+                q2 = xrec_semisectorial(&s2, t2, anm[m + 1]);
+                real inm1 = -((anm[m + 1] / (real)(m + 2)) *
+                              ((u2 * u2) * pm2 - (u1 * u1) * pm1));
+                cm[1] += inm1 * am;
+                sm[1] += inm1 * bm;
+                int even = 1;
+                for (unsigned long n = m + 2; n <= nmax; n++, even = !even)
+                {
+                    real pa = q1, pb = q2;
+                    q1 = xrec_tesseral(&s1, t1, anm[n], bnm[n]);
+                    q2 = xrec_tesseral(&s2, t2, anm[n], bnm[n]);
+                    real inm2 = (hm[n] * bnm[n]) * inm0 -
+                                (anm[n] / (real)(n + 1)) *
+                                ((u2 * u2) * pb - (u1 * u1) * pa);
+                    inm0 = inm1;
+                    inm1 = inm2;
+                    cm[n - m] += inm2 * (even ? ap : am);
+                    sm[n - m] += inm2 * (even ? bp : bm);
+                }
+            }
+        }
+        free(anm);
+        free(bnm);
+    }
+    free(r);
+    free(ri);
+    free(dm);
+    free(en);
+    free(fn);
+    free(gm);
+    free(hm);
+    free(col);
+    free(geo);
+    free(ps1);
+    free(ps2);
+    free(ips1);
+    free(ips2);
+    free(imm);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Quadrature grids                                                          */
 /* ------------------------------------------------------------------------ */
 /* Gauss--Legendre latitudes and weights, src/crd/crd_point_gl_chunk.c:122-173.

@@ -9,6 +9,9 @@ Restated reference drivers (CHarm 0.4.9):
   shs_point        src/shs/shs_point.c:26-129, shs_point_grd.c:97-1076,
                    shs_point_sctr.c:86-728, shs_point_gradn.c:32-165
   sha_point        src/sha/sha_point.c:124-1125
+  shs_cell         src/shs/shs_cell.c:22-121, shs_cell_grd.c:42-884,
+                   shs_cell_sctr.c, shs_grd_fft_lc.c:73-118, shs_grd_lr.c:68-99
+  sha_cell         src/sha/sha_cell.c:37-1487
   gl, dh1, dh2     src/crd/crd_point_gl_chunk.c, crd_point_dh_chunk.c
 The longitude sums use numpy's FFT (the role FFTW plays in CHarm) on grids
 where CHarm uses FFT, and direct sums elsewhere.
@@ -50,6 +53,13 @@ def lib(prec="d"):
         fn.restype = None
         fn = getattr(L, "orc_%s_sha_contract" % prec)
         fn.argtypes = [ul, sz, p, p, p, p, p, p, p]
+        fn.restype = None
+        fn = getattr(L, "orc_%s_cell_lumped" % prec)
+        fn.argtypes = [ul, ul, p, p, sz, p, p, p, p, p, ct.c_double, p, p,
+                       p, p]
+        fn.restype = None
+        fn = getattr(L, "orc_%s_cell_contract" % prec)
+        fn.argtypes = [ul, sz, p, p, p, p, p, p, ct.c_double, p, p]
         fn.restype = None
         fn = getattr(L, "orc_%s_gl" % prec)
         fn.argtypes = [ul, p, p]
@@ -555,3 +565,322 @@ def shs_point_quad_grid(ptype, nmax, shc_nmax, mu_q, r_q, c_q, s_q, rgrid_q,
         if mi >= 0 and mi < nlat:
             f[mi * nlon:(mi + 1) * nlon] = fs[k * nlon:(k + 1) * nlon]
     return q_to_dd(f)
+
+
+# ---------------------------------------------------------------------------
+# Block-mean values in cells (charm_cell, src/crd/crd.h.in:339-409)
+# ---------------------------------------------------------------------------
+CELL_GRID, CELL_SCATTERED = -2, -1
+SHA_CELL_AQ = 0
+POLAR_OFF = -1.0
+
+
+class Cell:
+    def __init__(self, ctype, latmin, latmax, lonmin, lonmax, r):
+        self.type = ctype
+        self.latmin = np.ascontiguousarray(latmin, np.float64).reshape(-1)
+        self.latmax = np.ascontiguousarray(latmax, np.float64).reshape(-1)
+        self.lonmin = np.ascontiguousarray(lonmin, np.float64).reshape(-1)
+        self.lonmax = np.ascontiguousarray(lonmax, np.float64).reshape(-1)
+        self.r = np.ascontiguousarray(r, np.float64).reshape(-1)
+
+    @property
+    def nlat(self):
+        return self.latmin.size
+
+    @property
+    def nlon(self):
+        return self.lonmin.size
+
+    @property
+    def ncell(self):
+        return self.nlat if self.type == CELL_SCATTERED else self.nlat * self.nlon
+
+
+def generate_cell(ctype, nlat, nlon, r, lat_rng, lon_rng):
+    """tests/generate_cell.c:18-56: cells of equal size from the north pole
+    down lat_rng and from longitude 0 east lon_rng."""
+    l = np.arange(nlat, dtype=np.float64)
+    latmin = PI_2 - ((l + 1.0) / float(nlat)) * lat_rng
+    latmax = PI_2 - (l / float(nlat)) * lat_rng
+    k = np.arange(nlon, dtype=np.float64)
+    lonmin = (k / float(nlon)) * lon_rng
+    lonmax = ((k + 1.0) / float(nlon)) * lon_rng
+    return Cell(ctype, latmin, latmax, lonmin, lonmax, np.full(nlat, r))
+
+
+def arr_chck_lin_incr(arr, eps):
+    """src/misc/misc_arr_chck_lin_incr.c with first = 0, every_nth = 1:
+    0 if the array increases with a constant step."""
+    n = len(arr)
+    if n < 2:
+        return 0
+    if not nearly_equal(arr[0], float(np.min(arr)), eps):
+        return 1
+    step = arr[1] - arr[0]
+    if step <= 0.0:
+        return 1
+    for j in range(1, n):
+        if not nearly_equal(step, arr[j] - arr[j - 1], eps):
+            return 1
+    return 0
+
+
+def cell_check_grd_lons(cell):
+    """src/shs/shs_cell_check_grd_lons.c:14-85; returns deltalon."""
+    if cell.nlon > 1:
+        if arr_chck_lin_incr(cell.lonmin, THRESHOLD2):
+            raise ValueError("lonmin is not linearly increasing")
+        if arr_chck_lin_incr(cell.lonmax, THRESHOLD2):
+            raise ValueError("lonmax is not linearly increasing")
+        if not nearly_equal(cell.lonmin[1] - cell.lonmin[0],
+                            cell.lonmax[1] - cell.lonmax[0], THRESHOLD2):
+            raise ValueError("lonmin and lonmax steps differ")
+        return cell.lonmin[1] - cell.lonmin[0]
+    return cell.lonmax[0] - cell.lonmin[0]
+
+
+def crd_check_cells(cell):
+    """src/crd/crd_check_cells.c:14-40"""
+    if np.any(cell.latmax <= cell.latmin):
+        raise ValueError("latmin must be smaller than latmax")
+    if np.any(cell.lonmin >= cell.lonmax):
+        raise ValueError("lonmin must be smaller than lonmax")
+
+
+def cell_fft_applicable(cell, nmax):
+    """src/shs/shs_grd_cell_fft_check.c:17-60"""
+    if cell.nlon <= 1:
+        return False
+    return ((cell.nlon - 1) // 2 >= nmax
+            and nearly_equal(cell.lonmin[0], 0.0, THRESHOLD)
+            and nearly_equal(cell.lonmax[-1], 2.0 * PI, THRESHOLD)
+            and nearly_equal(cell.lonmin[1], cell.lonmax[0], THRESHOLD))
+
+
+def cell_grid_rows(cell):
+    """Rows, mirrors and symmetry flags of a cell grid:
+    shs_cell_grd.c:52-110 with crd_grd_check_symm.c for cell grids."""
+    nlat = cell.nlat
+    even = nlat % 2 == 0
+    symm = nlat > 1
+    for i in range(nlat):
+        if not nearly_equal(cell.latmin[i], -cell.latmax[nlat - i - 1],
+                            THRESHOLD2):
+            symm = False
+            break
+    nlatdo = (nlat + 1 - int(even)) // 2 if symm else nlat
+    rows, mirrors, flags = [], [], []
+    for ipv in range(nlatdo):
+        s = 1 if symm and not ((not even) and ipv == nlatdo - 1) else 0
+        rows.append(ipv)
+        mirrors.append(nlat - ipv - 1 if s else -1)
+        flags.append(s)
+    return np.array(rows), np.array(mirrors), np.array(flags, np.int32)
+
+
+def cell_lumped(shc, nmax, latmin, latmax, rr, rr2, symm, polar_thr=POLAR_OFF,
+                prec="d"):
+    nrow = len(latmin)
+    L = nmax + 1
+    out = [np.zeros((nrow, L)) for _ in range(4)]
+    getattr(lib(prec), "orc_%s_cell_lumped" % prec)(
+        nmax, shc.nmax, _ptr(shc.c), _ptr(shc.s), nrow,
+        _ptr(np.ascontiguousarray(latmin, np.float64)),
+        _ptr(np.ascontiguousarray(latmax, np.float64)),
+        _ptr(np.ascontiguousarray(rr, np.float64)),
+        _ptr(np.ascontiguousarray(rr2, np.float64)),
+        _ptr(np.ascontiguousarray(symm, np.int32)), float(polar_thr),
+        *[_ptr(o) for o in out])
+    return out
+
+
+def cell_lon_factors(nmax, dlon):
+    """(sm, cm) of shs_grd_fft_lc.c:79-97: the longitude integrals of one
+    cell of width dlon starting at its lonmin."""
+    L = nmax + 1
+    sm = np.empty(L)
+    cm = np.empty(L)
+    sm[0], cm[0] = dlon, 0.0
+    for m in range(1, L):
+        mr = float(m)
+        cm[m] = (math.cos(mr * dlon) - 1.0) / mr
+        sm[m] = math.sin(mr * dlon) / mr
+    return sm, cm
+
+
+def cell_m2sm2dl(nmax, dlon):
+    """(2 / m) sin(dlon / (2 / m)), m2sm2dl of shs_grd_lr.c:76-84 and
+    shs_cell_sctr.c (dlon at m = 0)."""
+    L = nmax + 1
+    out = np.empty(L)
+    out[0] = dlon
+    for m in range(1, L):
+        m2 = 2.0 / float(m)
+        out[m] = m2 * math.sin(dlon / m2)
+    return out
+
+
+def shs_cell(cell, shc, nmax, polar_thr=POLAR_OFF):
+    """charm_shs_cell restated; returns the block means (ncell,)."""
+    if nmax > shc.nmax:
+        raise ValueError("nmax > shcs->nmax")
+    if cell.ncell == 0:
+        return np.zeros(0)
+    mur = shc.mu / shc.r
+    L = nmax + 1
+    if cell.type == CELL_SCATTERED:
+        if cell.nlat != cell.nlon:
+            raise ValueError("nlat != nlon for scattered cells")
+        crd_check_cells(cell)
+        n = cell.nlat
+        rr = shc.r / cell.r
+        a, b, _, _ = cell_lumped(shc, nmax, cell.latmin, cell.latmax, rr,
+                                 rr, np.zeros(n, np.int32), polar_thr)
+        f = np.zeros(n)
+        for i in range(n):
+            dl = cell.lonmax[i] - cell.lonmin[i]
+            w = cell_m2sm2dl(nmax, dl)
+            ml = (np.arange(L, dtype=np.float64) / 2.0) * (cell.lonmin[i] +
+                                                          cell.lonmax[i])
+            fi = np.sum((a[i] * w) * np.cos(ml) + (b[i] * w) * np.sin(ml))
+            dsigma = (math.sin(cell.latmax[i]) - math.sin(cell.latmin[i])) * dl
+            f[i] = mur * (fi / dsigma)
+        return f
+    if cell.type != CELL_GRID:
+        raise ValueError("unsupported cell type")
+    rows, mirrors, flags = cell_grid_rows(cell)
+    dlon = cell_check_grd_lons(cell)
+    use_fft = cell_fft_applicable(cell, nmax)
+    crd_check_cells(cell)
+    rr = shc.r / cell.r[rows]
+    rr2 = np.array([shc.r / cell.r[mm] if mm >= 0 else 0.0 for mm in mirrors])
+    a, b, a2, b2 = cell_lumped(shc, nmax, cell.latmin[rows],
+                               cell.latmax[rows], rr, rr2, flags, polar_thr)
+    nlat, nlon = cell.nlat, cell.nlon
+    if use_fft:
+        sm, cm = cell_lon_factors(nmax, dlon)
+        c = np.full(L, 0.5)
+        c[0] = 1.0
+
+        def lon_sum(a_, b_):
+            nfc = nlon // 2 + 1
+            fc = np.zeros((a_.shape[0], nfc), dtype=np.complex128)
+            fc[:, :L] = ((a_ * sm - b_ * cm) * c) - 1j * ((a_ * cm + b_ * sm) * c)
+            return np.fft.irfft(fc, n=nlon, axis=-1) * nlon
+    else:
+        w = cell_m2sm2dl(nmax, dlon)
+        lon0 = (cell.lonmin[0] + cell.lonmax[0]) / 2.0
+        lons = lon0 + np.arange(nlon) * dlon
+
+        def lon_sum(a_, b_):
+            return lon_synthesis_direct(a_ * w, b_ * w, lons, 1.0)
+    fn = lon_sum(a, b)
+    fs = lon_sum(a2, b2)
+    f = np.zeros((nlat, nlon))
+    for k, (i, mi) in enumerate(zip(rows, mirrors)):
+        dsigma = (math.sin(cell.latmax[i]) - math.sin(cell.latmin[i])) * dlon
+        cc = mur / dsigma
+        f[i] = cc * fn[k]
+        if mi >= 0:
+            f[mi] = cc * fs[k]
+    return f.reshape(-1)
+
+
+def sha_cell(cell, f, nmax, mu, r, shc_nmax=None, polar_thr=POLAR_OFF):
+    """charm_sha_cell with CHARM_SHA_CELL_AQ restated
+    (src/sha/sha_cell.c:37-1487); returns an Shc of degree shc_nmax."""
+    shc_nmax = nmax if shc_nmax is None else shc_nmax
+    out = Shc(shc_nmax, mu, r)
+    if cell.type != CELL_GRID:
+        raise ValueError("unsupported cell type for analysis")
+    if nmax > shc_nmax:
+        raise ValueError("nmax > shcs->nmax")
+    if cell.ncell == 0:
+        return out
+    r0 = cell.r[0]
+    for x in cell.r[1:]:
+        if not nearly_equal(x, r0, THRESHOLD):
+            raise ValueError("all radii must be equal")
+    nlat, nlon = cell.nlat, cell.nlon
+    if not nearly_equal(cell.latmax[0], PI_2, THRESHOLD):
+        raise ValueError("latmax[0] must be pi/2")
+    if nlat < nmax + 1:
+        raise ValueError("not enough latitudes")
+    if not nearly_equal(cell.latmin[-1], -PI_2, THRESHOLD):
+        raise ValueError("latmin[-1] must be -pi/2")
+    for i in range(nlat - 1):
+        if not nearly_equal(cell.latmin[i], cell.latmax[i + 1], THRESHOLD):
+            raise ValueError("cells not aligned in latitude")
+    even = nlat % 2 == 0
+    symm = nlat > 1
+    for i in range(nlat):
+        if not nearly_equal(cell.latmin[i], -cell.latmax[nlat - i - 1],
+                            THRESHOLD2):
+            symm = False
+            break
+    if nlon < 2 * nmax + 1:
+        raise ValueError("not enough longitudes")
+    if not nearly_equal(cell.lonmin[0], 0.0, THRESHOLD):
+        raise ValueError("lonmin[0] must be 0")
+    if not nearly_equal(cell.lonmax[-1], 2.0 * PI, THRESHOLD):
+        raise ValueError("lonmax[-1] must be 2 pi")
+    dlon = cell_check_grd_lons(cell)
+    if nlon > 1 and not nearly_equal(cell.lonmin[1], cell.lonmax[0],
+                                     THRESHOLD):
+        raise ValueError("cells not aligned in longitude")
+    crd_check_cells(cell)
+    nlatdo = ((nlat // 2) if even else (nlat + 1) // 2) if symm else nlat
+    rows = np.arange(nlatdo)
+    flags = np.array([1 if symm and not ((not even) and i == nlatdo - 1)
+                      else 0 for i in rows], np.int32)
+    mirrors = np.where(flags == 1, nlat - 1 - rows, -1)
+    L = nmax + 1
+    F = np.fft.rfft(np.asarray(f, np.float64).reshape(nlat, nlon), axis=1)
+    a = F[rows, :L].real
+    b = -F[rows, :L].imag
+    a2 = np.zeros_like(a)
+    b2 = np.zeros_like(b)
+    for k, mi in enumerate(mirrors):
+        if mi >= 0:
+            a2[k] = F[mi, :L].real
+            b2[k] = -F[mi, :L].imag
+    sy = flags[:, None].astype(np.float64)
+    sm, cm = cell_lon_factors(nmax, dlon)
+    ap, am_ = a + sy * a2, a - sy * a2
+    bp, bm_ = b + sy * b2, b - sy * b2
+    amp = np.ascontiguousarray(ap * sm + bp * cm)
+    amm = np.ascontiguousarray(am_ * sm + bm_ * cm)
+    bmp = np.ascontiguousarray(bp * sm - ap * cm)
+    bmm = np.ascontiguousarray(bm_ * sm - am_ * cm)
+    # m = 0: (a +- a2) dlon (sha_cell.c:797-803)
+    amp[:, 0] = ap[:, 0] * dlon
+    amm[:, 0] = am_[:, 0] * dlon
+    bmp[:, 0] = 0.0
+    bmm[:, 0] = 0.0
+    T = L * (L + 1) // 2
+    cc = np.zeros(T)
+    ss = np.zeros(T)
+    lib("d").orc_d_cell_contract(
+        nmax, nlatdo, _ptr(np.ascontiguousarray(cell.latmin[rows])),
+        _ptr(np.ascontiguousarray(cell.latmax[rows])), _ptr(amp), _ptr(amm),
+        _ptr(bmp), _ptr(bmm), float(polar_thr), _ptr(cc), _ptr(ss))
+    c2 = 1.0 / (4.0 * PI) * (r0 / mu)
+    col_src = tri_col0(nmax)
+    col_dst = tri_col0(shc_nmax)
+    for m in range(L):
+        out.c[col_dst[m]:col_dst[m] + L - m] = c2 * cc[col_src[m]:col_src[m] + L - m]
+        out.s[col_dst[m]:col_dst[m] + L - m] = c2 * ss[col_src[m]:col_src[m] + L - m]
+    if not nearly_equal(r, r0, THRESHOLD):
+        r_ratio = r0 / r
+        tmp = np.empty(shc_nmax + 1)
+        tmp[0] = 1.0
+        tmp2 = r_ratio
+        for n in range(1, shc_nmax + 1):
+            tmp[n] = tmp2
+            tmp2 *= r_ratio
+        for m in range(shc_nmax + 1):
+            sl = slice(col_dst[m], col_dst[m] + shc_nmax + 1 - m)
+            out.c[sl] *= tmp[m:]
+            out.s[sl] *= tmp[m:]
+    return out

@@ -8,6 +8,10 @@ this writes, so the GPU machine never needs the reference tree.
 Sources (CHarm 0.4.9):
   data/tests/{double,quad}/shs_p_*.txt   point synthesis golden outputs
                                           (tests/check_shs_point_all.c)
+  data/tests/{double,quad}/shs_c_nx*.txt cell synthesis golden outputs
+                                          (tests/check_shs_cell.c)
+  data/tests/{double,quad}/sha_c_nx*.txt cell analysis golden outputs
+                                          (tests/check_sha_cell.c)
   data/tests/{double,quad}/crd_*.txt     GL/DH grid nodes and weights
                                           (tests/check_crd_point_quad.c)
   data/input/EGM96-degree10-mtx.txt      input coefficients of those tests
@@ -49,7 +53,7 @@ def pack(path, table):
                         offsets=offsets, data=data)
 
 
-HOT = re.compile(r"^(shs_p_|crd_nx).*\.txt$")
+HOT = re.compile(r"^(shs_p_|shs_c_nx|sha_c_nx|crd_nx).*\.txt$")
 GRAD_SUFFIX = re.compile(r"_(x|y|z|xx|xy|xz|yy|yz|zz|guru\d+)\.txt$")
 
 

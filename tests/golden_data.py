@@ -279,3 +279,100 @@ def shs_cases(families=("pot", "grad1", "grad2", "guru"), subsets=(
                                             lat0_shift=0.001 if s == 0 else 0.0,
                                             golden_names=names, eps=eps))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Cells (block-mean values)
+# ---------------------------------------------------------------------------
+CELL_GRID, CELL_SCATTERED = -2, -1
+
+
+def generate_cell(nlat, nlon, r, lat_rng, lon_rng):
+    """tests/generate_cell.c:18-56 -> (latmin, latmax, lonmin, lonmax, r)."""
+    l = np.arange(nlat, dtype=np.float64)
+    latmin = PI_2 - ((l + 1.0) / float(nlat)) * lat_rng
+    latmax = PI_2 - (l / float(nlat)) * lat_rng
+    k = np.arange(nlon, dtype=np.float64)
+    lonmin = (k / float(nlon)) * lon_rng
+    lonmax = ((k + 1.0) / float(nlon)) * lon_rng
+    return latmin, latmax, lonmin, lonmax, np.full(nlat, float(r))
+
+
+@dataclass
+class CellCase:
+    """One cell synthesis (or synthesis + analysis) of CHarm's test-suite."""
+    name: str
+    ctype: int
+    nmax: int
+    cell: tuple                # (latmin, latmax, lonmin, lonmax, r)
+    golden_names: list = field(default_factory=list)
+    eps: float = 0.0
+
+
+def shs_cell_cases():
+    """tests/check_shs_cell.c:50-185: custom cell grids (PSLR when the
+    cells span pi in longitude, FFT when 2 pi; symmetric and with the first
+    cell moved by 0.001) and scattered cells, nmax 0..4, r = R and R + 1 km;
+    tolerance threshold2."""
+    out = []
+    R = test_coefficients()[2]
+    nlats = [1, 1, 3, 10]
+    nlons = [1, 2, 8, 22]
+    for nmax in range(5):
+        for i in range(4):
+            for fft in range(2):
+                if fft == 1 and ((nlons[i] - 1) // 2 < nmax or nlons[i] < 2):
+                    continue
+                for s in range(2):
+                    if nlats[i] == 1 and s == 1:
+                        continue
+                    for d in range(2):
+                        cl = generate_cell(nlats[i], nlons[i], R + 1000.0 * d,
+                                           PI, PI if fft == 0 else 2.0 * PI)
+                        if s == 0:
+                            cl[1][0] -= 0.001
+                        nm = "shs_c_nx%d_n%d_dr%d_fft%d_s%d" % (nmax, i, d,
+                                                               fft, s)
+                        out.append(CellCase(nm, CELL_GRID, nmax, cl, [nm],
+                                            THRESHOLD2))
+    nlats = [1, 2, 3, 4, 5, 6, 7, 8, 9, 20, 30, 31]
+    for nmax in range(5):
+        for i in range(12):
+            for d in range(2):
+                cl = generate_cell(nlats[i], nlats[i], R + 1000.0 * d, PI,
+                                   2.0 * PI)
+                nm = "shs_c_nx%d_n%d_dr%d_sctr" % (nmax, i, d)
+                out.append(CellCase(nm, CELL_SCATTERED, nmax, cl, [nm],
+                                    THRESHOLD2))
+    return out
+
+
+def sha_cell_cases():
+    """tests/check_sha_cell.c:50-160: synthesis then analysis (approximate
+    quadrature) on cell grids spanning the sphere; the non-symmetric
+    variant moves the boundary between the first two cell rows by 0.001;
+    golden C and S triangles, tolerance 10 threshold2."""
+    out = []
+    R = test_coefficients()[2]
+    nlats = [1, 1, 3, 10]
+    nlons = [1, 2, 8, 22]
+    for nmax in range(5):
+        for i in range(4):
+            for s in range(2):
+                if nlats[i] == 1 and s == 1:
+                    continue
+                if nlats[i] >= nmax + 1 and s == 0 and nmax == 0:
+                    continue
+                for d in range(2):
+                    if nlats[i] < nmax + 1:
+                        continue
+                    cl = generate_cell(nlats[i], nlons[i], R + 1000.0 * d, PI,
+                                       2.0 * PI)
+                    if s == 0:
+                        cl[0][0] += 0.001
+                        cl[1][1] += 0.001
+                    stem = "sha_c_nx%d_n%d_dr%d_s%d" % (nmax, i, d, s)
+                    out.append(CellCase(stem, CELL_GRID, nmax, cl,
+                                        [stem + "_c", stem + "_s"],
+                                        10.0 * THRESHOLD2))
+    return out

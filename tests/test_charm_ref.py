@@ -167,6 +167,52 @@ def test_oracle_port_against_charm_nmax360(C):
     assert coef_rel_rms(ref.c, ref.s, cr, sr) <= 5e-14
 
 
+@needs_d
+def test_oracle_cells_against_charm(C):
+    """The oracle's cell synthesis and analysis against CHarm's own
+    charm_shs_cell / charm_sha_cell at nmax 120: a 1-degree cell grid of
+    the whole sphere above it (FFT synthesis, approximate-quadrature
+    analysis), a regional non-symmetric grid (PSLR path) and scattered
+    cells of random size and height."""
+    from charm_b200.workloads import coef_rel_rms, kaula, rel_rms
+    N = 120
+    c, s = kaula(N, 1200)
+    shc_c = C.shc(N, GM, R, c, s)
+    shc_o = orc.Shc(N, GM, R, c, s)
+    # whole sphere, 180 x 360 one-degree cells at r = R + 3 km
+    lat_e = np.deg2rad(np.linspace(90.0, -90.0, 181))
+    lon_e = np.deg2rad(np.linspace(0.0, 360.0, 361))
+    lon_e[-1] = 2.0 * np.pi
+    args = (lat_e[1:], lat_e[:-1], lon_e[:-1], lon_e[1:], np.full(180, R + 3e3))
+    cc = C.cell(orc.CELL_GRID, *args)
+    co = orc.Cell(orc.CELL_GRID, *args)
+    f = C.shs_cell(cc, shc_c, N, 180 * 360)
+    fo = orc.shs_cell(co, shc_o, N)
+    assert rel_rms(fo, f) <= 1e-14
+    cr, sr = C.sha_cell(cc, f, N, GM, R)
+    out = orc.sha_cell(co, f, N, GM, R)
+    assert coef_rel_rms(out.c, out.s, cr, sr) <= 1e-13
+    # regional grid (longitudes span 60 degrees: no FFT), not symmetric
+    lat_e = np.deg2rad(np.linspace(50.0, 10.0, 41))
+    lon_e = np.deg2rad(np.linspace(0.0, 60.0, 121))
+    args = (lat_e[1:], lat_e[:-1], lon_e[:-1], lon_e[1:], np.full(40, R))
+    f = C.shs_cell(C.cell(orc.CELL_GRID, *args), shc_c, N, 40 * 120)
+    fo = orc.shs_cell(orc.Cell(orc.CELL_GRID, *args), shc_o, N)
+    assert rel_rms(fo, f) <= 1e-14
+    # scattered cells
+    rng = np.random.default_rng(77)
+    n = 400
+    lat0 = np.arcsin(rng.uniform(-0.98, 0.98, n))
+    dlat = np.deg2rad(rng.uniform(0.1, 2.0, n))
+    lon0 = rng.uniform(0.0, 2.0 * np.pi, n)
+    dlon = np.deg2rad(rng.uniform(0.1, 2.0, n))
+    args = (lat0 - dlat / 2, lat0 + dlat / 2, lon0, lon0 + dlon,
+            R + rng.uniform(0.0, 9000.0, n))
+    f = C.shs_cell(C.cell(orc.CELL_SCATTERED, *args), shc_c, N, n)
+    fo = orc.shs_cell(orc.Cell(orc.CELL_SCATTERED, *args), shc_o, N)
+    assert rel_rms(fo, f) <= 1e-14
+
+
 @needs_q
 def test_charm_quad_golden():
     """CHarm's quad build against its quad golden files of grid synthesis
