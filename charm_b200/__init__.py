@@ -1,5 +1,5 @@
-"""charm_b200: CHarm's point spherical-harmonic synthesis and analysis on
-NVIDIA B200 (sm_100a).
+"""charm_b200: CHarm's point and cell (block-mean) spherical-harmonic
+synthesis and analysis on NVIDIA B200 (sm_100a).
 
 The C ABI lives in libcharm.so (include/charm_b200.h); this package exposes
 it to Python with PyHarm's names (see charm_b200.pyharm).  The library is
@@ -10,7 +10,9 @@ synthetic inputs) needs no library.
 _PYHARM = ("CHarmError", "GRID", "GRID_DH1", "GRID_DH2", "GRID_GL",
            "SCATTERED", "PointGrid", "PointGridDH1", "PointGridDH2",
            "PointGridGL", "PointSctr", "Shc", "sha_point", "shs_point",
-           "shs_point_grad1", "shs_point_grad2", "shs_point_guru")
+           "shs_point_grad1", "shs_point_grad2", "shs_point_guru",
+           "CELL_GRID", "CELL_SCATTERED", "SHA_CELL_AQ", "CellGrid",
+           "CellSctr", "shs_cell", "sha_cell")
 
 __all__ = list(_PYHARM) + ["LIB_PATH"]
 

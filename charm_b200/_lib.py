@@ -1,6 +1,7 @@
 """Loads libcharm.so (this package's CUDA build of CHarm's point synthesis
 and analysis) and mirrors the ctypes layouts PyHarm uses for it
-(wrap/pyharm/_err.py:29-35, crd.py:48-56, shc.py:68-75 of CHarm 0.4.9).
+(wrap/pyharm/_err.py:29-35, crd.py:48-56, shc.py:68-75 of CHarm 0.4.9;
+the cell layout of src/crd/crd.h.in:339-409).
 
 There is no CPU fallback: if the library is missing, importing fails with
 an error that says how to build it.
@@ -53,6 +54,19 @@ class _Shc(ct.Structure):
                 ("distributed", ct.c_bool)]
 
 
+class _Cell(ct.Structure):
+    _fields_ = [("type", _ct_int),
+                ("nlat", _ct_size_t),
+                ("nlon", _ct_size_t),
+                ("ncell", _ct_size_t),
+                ("latmin", ct.POINTER(_ct_flt)),
+                ("latmax", ct.POINTER(_ct_flt)),
+                ("lonmin", ct.POINTER(_ct_flt)),
+                ("lonmax", ct.POINTER(_ct_flt)),
+                ("r", ct.POINTER(_ct_flt)),
+                ("owner", ct.c_bool)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -89,6 +103,14 @@ def _load():
         "charm_shs_point_guru": ([P(_Point), P(_Shc), UL, ct.c_uint,
                                   ct.c_uint, ct.c_uint, P(D), P(_Err)], None),
         "charm_sha_point": ([P(_Point), P(D), UL, P(_Shc), P(_Err)], None),
+        "charm_crd_cell_malloc": ([_ct_int, SZ, SZ], P(_Cell)),
+        "charm_crd_cell_calloc": ([_ct_int, SZ, SZ], P(_Cell)),
+        "charm_crd_cell_init": ([_ct_int, SZ, SZ, P(D), P(D), P(D), P(D),
+                                 P(D)], P(_Cell)),
+        "charm_crd_cell_free": ([P(_Cell)], None),
+        "charm_shs_cell": ([P(_Cell), P(_Shc), UL, P(D), P(_Err)], None),
+        "charm_sha_cell": ([P(_Cell), P(D), UL, _ct_int, P(_Shc), P(_Err)],
+                           None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -343,6 +343,115 @@ charm_point *charm_crd_point_dh2(unsigned long nmax, double r)
 }
 
 // ---------------------------------------------------------------------------
+// Cells, src/crd/crd_cell_alloc.c, crd_cell_init.c, crd_cell_free.c,
+// crd_cell_check_inputs.c
+// ---------------------------------------------------------------------------
+static bool is_cell_type(int t)
+{
+    return t == CHARM_CRD_CELL_GRID || t == CHARM_CRD_CELL_SCATTERED;
+}
+
+charm_cell *charm_crd_cell_init(int type, size_t nlat, size_t nlon,
+                                double *latmin, double *latmax,
+                                double *lonmin, double *lonmax, double *r)
+{
+    if (!is_cell_type(type))
+        return NULL;
+    if (type == CHARM_CRD_CELL_SCATTERED && nlat != nlon)
+        return NULL;
+    charm_cell *c = (charm_cell *)malloc(sizeof(charm_cell));
+    if (!c)
+        return NULL;
+    c->latmin = c->latmax = c->lonmin = c->lonmax = c->r = NULL;
+    if (nlat > 0)
+    {
+        c->latmin = latmin;
+        c->latmax = latmax;
+        c->r = r;
+    }
+    if (nlon > 0)
+    {
+        c->lonmin = lonmin;
+        c->lonmax = lonmax;
+    }
+    c->nlat = nlat;
+    c->nlon = nlon;
+    c->ncell = type == CHARM_CRD_CELL_SCATTERED ? nlat : nlat * nlon;
+    c->type = type;
+    c->owner = 0;
+    return c;
+}
+
+static charm_cell *cell_alloc(int type, size_t nlat, size_t nlon, bool zero)
+{
+    if (!is_cell_type(type))
+        return NULL;
+    if (type == CHARM_CRD_CELL_SCATTERED && nlat != nlon)
+        return NULL;
+    double *latmin = NULL, *latmax = NULL, *lonmin = NULL, *lonmax = NULL;
+    double *r = NULL;
+    auto al = [&](size_t n) -> double * {
+        return zero ? (double *)calloc(n, sizeof(double))
+                    : (double *)malloc(n * sizeof(double));
+    };
+    charm_cell *c = NULL;
+    if (nlat > 0)
+    {
+        latmin = al(nlat);
+        latmax = al(nlat);
+        r = al(nlat);
+        if (!latmin || !latmax || !r)
+            goto FAIL;
+    }
+    if (nlon > 0)
+    {
+        lonmin = al(nlon);
+        lonmax = al(nlon);
+        if (!lonmin || !lonmax)
+            goto FAIL;
+    }
+    c = charm_crd_cell_init(type, nlat, nlon, latmin, latmax, lonmin, lonmax,
+                            r);
+    if (!c)
+        goto FAIL;
+    c->owner = 1;
+    return c;
+FAIL:
+    free(latmin);
+    free(latmax);
+    free(lonmin);
+    free(lonmax);
+    free(r);
+    free(c);
+    return NULL;
+}
+
+charm_cell *charm_crd_cell_malloc(int type, size_t nlat, size_t nlon)
+{
+    return cell_alloc(type, nlat, nlon, false);
+}
+
+charm_cell *charm_crd_cell_calloc(int type, size_t nlat, size_t nlon)
+{
+    return cell_alloc(type, nlat, nlon, true);
+}
+
+void charm_crd_cell_free(charm_cell *cell)
+{
+    if (!cell)
+        return;
+    if (cell->owner)
+    {
+        free(cell->latmin);
+        free(cell->latmax);
+        free(cell->lonmin);
+        free(cell->lonmax);
+        free(cell->r);
+    }
+    free(cell);
+}
+
+// ---------------------------------------------------------------------------
 // Coefficients, src/shc/shc_alloc.c, shc_init.c, shc_init_chunk.c,
 // shc_free.c
 // ---------------------------------------------------------------------------
@@ -596,6 +705,95 @@ void charm_sha_point(const charm_point *pnt, const double *f,
     report(err, __func__, cb::sha_point(pnt, f, nmax, shcs));
 }
 
+// ---------------------------------------------------------------------------
+// Cells: src/shs/shs_cell.c:22-121, src/sha/sha_cell.c:37-100
+// ---------------------------------------------------------------------------
+static bool check_nmax_cell(const charm_shc *shcs, unsigned long nmax,
+                            charm_err *err, const char *what)
+{
+    if (nmax > shcs->nmax)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg,
+                 "Maximum harmonic degree of the %s (\"nmax\") cannot be "
+                 "larger than maximum harmonic degree of spherical harmonic "
+                 "coefficients (\"shcs->nmax\").",
+                 what);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return false;
+    }
+    return true;
+}
+
+static bool check_type_shs_cell(const charm_cell *cell, charm_err *err)
+{
+    if (cell->type == CHARM_CRD_CELL_SCATTERED)
+    {
+        if (cell->nlat != cell->nlon)
+        {
+            SET_ERR(err, CHARM_EFUNCARG,
+                    "The number of latitudes and longitudes in the \"cell\" "
+                    "structure must be the same in order to perform "
+                    "cell-wise spherical harmonic synthesis.");
+            return false;
+        }
+        return true;
+    }
+    if (cell->type != CHARM_CRD_CELL_GRID)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"cell->type\" for spherical harmonic synthesis "
+                "of block-mean values in cells.");
+        return false;
+    }
+    return true;
+}
+
+void charm_shs_cell(const charm_cell *cell, const charm_shc *shcs,
+                    unsigned long nmax, double *f, charm_err *err)
+{
+    if (!check_nmax_cell(shcs, nmax, err, "synthesis"))
+        return;
+    if (cell->ncell == 0)
+        return;
+    if (!check_type_shs_cell(cell, err))
+        return;
+    report(err, __func__, cb::shs_cell(cell, shcs, nmax, f));
+}
+
+static bool check_sha_cell(const charm_cell *cell, int method,
+                           charm_err *err)
+{
+    if (method != CHARM_SHA_CELL_AQ)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"method\" of spherical harmonic analysis of "
+                "block-mean data values.");
+        return false;
+    }
+    if (cell->type != CHARM_CRD_CELL_GRID)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Unsupported \"cell->type\" for spherical harmonic analysis "
+                "of block-mean data values.");
+        return false;
+    }
+    return true;
+}
+
+void charm_sha_cell(const charm_cell *cell, const double *f,
+                    unsigned long nmax, int method, charm_shc *shcs,
+                    charm_err *err)
+{
+    if (!check_sha_cell(cell, method, err))
+        return;
+    if (!check_nmax_cell(shcs, nmax, err, "analysis"))
+        return;
+    if (cell->ncell == 0)
+        return;
+    report(err, __func__, cb::sha_cell(cell, f, nmax, shcs));
+}
+
 } // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -631,6 +829,44 @@ void charm_b200_shs_point_dev(const charm_point *pnt, unsigned long shc_nmax,
                              kgrad ? kgrad : (int)dr,
                              kgrad ? kgrad : (int)dlat,
                              kgrad ? kgrad : (int)dlon, d_f));
+}
+
+void charm_b200_shs_cell_dev(const charm_cell *cell, unsigned long shc_nmax,
+                             double mu, double r, const double *d_c,
+                             const double *d_s, unsigned long nmax,
+                             double *d_f, charm_err *err)
+{
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (cell->ncell == 0)
+        return;
+    if (!check_type_shs_cell(cell, err))
+        return;
+    report(err, __func__,
+           cb::shs_cell_dev(cell, shc_nmax, mu, r, d_c, d_s, nmax, d_f));
+}
+
+void charm_b200_sha_cell_dev(const charm_cell *cell, const double *d_f,
+                             unsigned long nmax, double mu, double r,
+                             unsigned long shc_nmax, double *d_c,
+                             double *d_s, charm_err *err)
+{
+    if (!check_sha_cell(cell, CHARM_SHA_CELL_AQ, err))
+        return;
+    if (nmax > shc_nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"nmax\" cannot be larger than \"shc_nmax\".");
+        return;
+    }
+    if (cell->ncell == 0)
+        return;
+    report(err, __func__,
+           cb::sha_cell_dev(cell, d_f, nmax, mu, r, shc_nmax, d_c, d_s));
 }
 
 void charm_b200_sha_point_dev(const charm_point *pnt, const double *d_f,

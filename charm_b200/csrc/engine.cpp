@@ -92,6 +92,7 @@ struct Context
     long long tab_nmax = -1;     // recurrence tables of this maximum degree
     long long tab32_nmax = -1;   // single-precision tables of this degree
     long long tcp_nmax = -1;     // padded ct_n rows of the tensor-core path
+    long long cell_nmax = -1;    // per-degree tables of the cell kernels
     // stream capture into a CUDA graph (batch_graph_create): host
     // synchronisations are skipped, small host uploads go through pinned
     // buffers owned by the graph
@@ -2874,6 +2875,640 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
 }
 
 // ---------------------------------------------------------------------------
+// Cells: block means (cell.cu)
+// ---------------------------------------------------------------------------
+// src/misc/misc_arr_chck_lin_incr.c with first = 0, every_nth = 1: the
+// array starts at its minimum and increases by one positive step
+bool lin_incr(const double *a, size_t n, double eps)
+{
+    if (n < 2)
+        return true;
+    double mn = a[0];
+    for (size_t j = 1; j < n; j++)
+        mn = std::min(mn, a[j]);
+    if (!nearly_equal(a[0], mn, eps))
+        return false;
+    const double step = a[1] - a[0];
+    if (step <= 0.0)
+        return false;
+    for (size_t j = 1; j < n; j++)
+        if (!nearly_equal(step, a[j] - a[j - 1], eps))
+            return false;
+    return true;
+}
+
+// src/crd/crd_check_cells.c:14-40
+Status check_cells(const charm_cell *cell)
+{
+    Status st;
+    for (size_t i = 0; i < cell->nlat; i++)
+        if (cell->latmax[i] <= cell->latmin[i])
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "Minimum cell latitudes must be smaller than maximum "
+                     "cell latitudes.";
+            return st;
+        }
+    for (size_t j = 0; j < cell->nlon; j++)
+        if (cell->lonmin[j] >= cell->lonmax[j])
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "Minimum cell longitudes must be smaller than maximum "
+                     "cell longitudes.";
+            return st;
+        }
+    return st;
+}
+
+// src/shs/shs_cell_check_grd_lons.c:14-85: constant steps of lonmin and
+// lonmax, equal to each other; returns the step (the cell width)
+Status cell_grd_lons(const charm_cell *cell, double *dlon)
+{
+    Status st;
+    const double thr2 = charm_glob_threshold2;
+    if (cell->nlon > 1)
+    {
+        if (!lin_incr(cell->lonmin, cell->nlon, thr2))
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "\"cell->lonmin\" is not a linearly increasing array of "
+                     "cells within the \"threshold2\".";
+            return st;
+        }
+        if (!lin_incr(cell->lonmax, cell->nlon, thr2))
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "\"cell->lonmax\" is not a linearly increasing array of "
+                     "cells within the \"threshold2\".";
+            return st;
+        }
+        if (!nearly_equal(cell->lonmin[1] - cell->lonmin[0],
+                          cell->lonmax[1] - cell->lonmax[0], thr2))
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "The difference \"cell->lonmin[1] - cell->lonmin[0]\" "
+                     "has to be equal to \"cell->lonmax[1] - "
+                     "cell->lonmax[0]\".";
+            return st;
+        }
+        *dlon = cell->lonmin[1] - cell->lonmin[0];
+    }
+    else
+        *dlon = cell->lonmax[0] - cell->lonmin[0];
+    return st;
+}
+
+struct CellTabs
+{
+    double2 *hn = nullptr;
+    double4 *zn = nullptr;
+    double *gm = nullptr;
+};
+
+// Per-degree tables of the cell kernels, built once per maximum degree:
+// (h_n, 1 / (n + 1)) and g_n of src/leg/leg_func_gm_hm.c:14-45, and the
+// un-normalised zonal recurrence (e_n+1, f_n+1) of src/leg/leg_pol_en_fn.c
+// with 1 / sqrt(2n + 1).
+Status cell_tables(Context &c, long long nmax, CellTabs *ct)
+{
+    Status st;
+    const size_t L = (size_t)nmax + 1;
+    CB_TRY(dbuf(c, "cell_hn", L, &ct->hn));
+    CB_TRY(dbuf(c, "cell_zn", L, &ct->zn));
+    CB_TRY(dbuf(c, "cell_gm", L, &ct->gm));
+    if (c.cell_nmax == nmax)
+        return st;
+    std::vector<double> r, ri, dmh;
+    host_r_ri_dm(nmax, r, ri, dmh);
+    std::vector<double2> hn(L);
+    std::vector<double4> zn(L);
+    std::vector<double> gm(L, 0.0);
+    for (long long n = 0; n <= nmax; n++)
+    {
+        hn[n] = make_double2((double)(n - 2) / (double)(n + 1),
+                             1.0 / (double)(n + 1));
+        if (n == 0)
+            zn[n] = make_double4(0.0, 0.0, 0.0, 0.0);
+        else
+        {
+            const long long k = n + 1;
+            zn[n] = make_double4((double)(2 * k - 1) / (double)k,
+                                 (double)(k - 1) / (double)k, ri[2 * n + 1],
+                                 0.0);
+        }
+        if (n >= 3)
+            gm[n] = 1.0 / (double)(2 * n + 2) * r[n] * r[2 * n + 1] *
+                    r[2 * n - 1] * ri[n - 1];
+    }
+    CB_CUDA(cudaMemcpyAsync(ct->hn, hn.data(), L * sizeof(double2),
+                            cudaMemcpyHostToDevice, c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(ct->zn, zn.data(), L * sizeof(double4),
+                            cudaMemcpyHostToDevice, c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(ct->gm, gm.data(), L * sizeof(double),
+                            cudaMemcpyHostToDevice, c.stream), st);
+    // the host vectors must outlive the copies
+    CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    c.cell_nmax = nmax;
+    return st;
+}
+
+// Cell-row pairs of a grid (shs_cell_grd.c:52-110 with crd_grd_check_symm.c
+// for cell grids; sha_cell.c:140-205 picks nlatdo the same way): rows
+// 0..nlatdo-1, each with its mirror nlat-1-i when the grid is symmetric,
+// except the middle row of an odd grid.  A mirror with another radius gets
+// a pair of its own (the rows of a pair share the radius ratio).
+void cell_pairs(const charm_cell *cell, bool split_radii, Pairs &P)
+{
+    const size_t nlat = cell->nlat;
+    const bool even = nlat % 2 == 0;
+    bool symm = nlat > 1;
+    for (size_t i = 0; i < nlat && symm; i++)
+        if (!nearly_equal(cell->latmin[i], -cell->latmax[nlat - i - 1],
+                          charm_glob_threshold2))
+            symm = false;
+    const size_t nlatdo = symm ? (nlat + 1 - (even ? 1 : 0)) / 2 : nlat;
+    P.row_n.clear();
+    P.row_s.clear();
+    std::vector<int> extra;
+    for (size_t i = 0; i < nlatdo; i++)
+    {
+        const bool s = symm && !(!even && i == nlatdo - 1);
+        int mi = s ? (int)(nlat - 1 - i) : -1;
+        if (mi >= 0 && split_radii && cell->r[mi] != cell->r[i])
+        {
+            extra.push_back(mi);
+            mi = -1;
+        }
+        P.row_n.push_back((int)i);
+        P.row_s.push_back(mi);
+    }
+    for (int e : extra)
+    {
+        P.row_n.push_back(e);
+        P.row_s.push_back(-1);
+    }
+}
+
+// Geometry [8][np] of the pairs (CellArgs::geo) with the block-mean scale
+// mur / ((sin latmax - sin latmin) dlon) of each pair's northern row
+// (src/shs/shs_grd_fft.c:83-92 uses it for the mirror row too)
+Status cell_geometry(Context &c, const charm_cell *cell, const Pairs &P,
+                     double R, bool rr, double mur, double dlon, double **dgeo,
+                     int **drows)
+{
+    Status st;
+    const int np = (int)P.row_n.size();
+    const size_t bytes = (size_t)np * (8 * 8 + 2 * 4);
+    void *hp = nullptr;
+    CB_TRY(pinned(c, bytes, &hp));
+    double *h = static_cast<double *>(hp);
+    int *hr = reinterpret_cast<int *>(h + 8 * (size_t)np);
+    for (int p = 0; p < np; p++)
+    {
+        const int i = P.row_n[p];
+        const double la1 = cell->latmin[i], la2 = cell->latmax[i];
+        const double t1 = std::sin(la1), t2 = std::sin(la2);
+        h[0 * np + p] = t1;
+        h[1 * np + p] = std::cos(la1);
+        h[2 * np + p] = t2;
+        h[3 * np + p] = std::cos(la2);
+        h[4 * np + p] = rr ? R / cell->r[i] : 1.0;
+        h[5 * np + p] = mur / ((t2 - t1) * dlon);
+        h[6 * np + p] = la1;
+        h[7 * np + p] = la2;
+        hr[p] = P.row_n[p];
+        hr[np + p] = P.row_s[p];
+    }
+    void *d = nullptr;
+    CB_TRY(buf(c, "geo", bytes, &d));
+    CB_CUDA(cudaMemcpyAsync(d, hp, bytes, cudaMemcpyHostToDevice, c.stream),
+            st);
+    *dgeo = static_cast<double *>(d);
+    *drows = reinterpret_cast<int *>(*dgeo + 8 * (size_t)np);
+    return st;
+}
+
+Status shs_cell_grid(Context &c, const charm_cell *cell, const CoefIn &in,
+                     unsigned long nmax, double *f_host, double *d_f)
+{
+    Status st;
+    const double thr = charm_glob_threshold;
+    const size_t nlat = cell->nlat, nlon = cell->nlon;
+    double dlon = 0.0;
+    CB_TRY(cell_grd_lons(cell, &dlon));
+    // src/shs/shs_grd_cell_fft_check.c:17-60
+    const bool use_fft =
+        nlon > 1 && (nlon - 1) / 2 >= nmax &&
+        nearly_equal(cell->lonmin[0], 0.0, thr) &&
+        nearly_equal(cell->lonmax[nlon - 1], 2.0 * PI, thr) &&
+        nearly_equal(cell->lonmin[1], cell->lonmax[0], thr);
+    CB_TRY(check_cells(cell));
+
+    // radius ratios R / r (shs_cell_grd.c:650-668); exactly 1 when r == R
+    bool rr = false;
+    for (size_t i = 0; i < nlat; i++)
+        rr |= cell->r[i] != in.r;
+    Pairs P;
+    cell_pairs(cell, rr, P);
+    const int np = (int)P.row_n.size();
+    double *dgeo = nullptr;
+    int *drows = nullptr;
+    CB_TRY(cell_geometry(c, cell, P, in.r, rr, in.mu / in.r, dlon, &dgeo,
+                         &drows));
+
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
+    CellTabs ctab;
+    CB_TRY(cell_tables(c, (long long)nmax, &ctab));
+    double2 *dcs = nullptr;
+    CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
+    double *imm = nullptr;
+    CB_TRY(dbuf(c, "cell_imm", (size_t)np * (nmax + 1), &imm));
+
+    const int ldf = use_fft ? (int)(nlon / 2 + 1) : (int)(nmax + 1);
+    double2 *lc = nullptr;
+    CB_TRY(dbuf(c, "lumped", (size_t)nlat * ldf, &lc));
+    double *fg = d_f;
+    double *f_dev_unaligned = nullptr;
+    if (fg && use_fft && nlon % 2 == 0 &&
+        reinterpret_cast<uintptr_t>(fg) % 16 != 0)
+    {
+        f_dev_unaligned = fg;
+        fg = nullptr;
+    }
+    if (!fg)
+        CB_TRY(dbuf(c, "fgrid", nlat * nlon, &fg));
+    const RfftArgs *rf = nullptr, *rfq = nullptr;
+    if (use_fft)
+    {
+        CB_TRY(row_fft(c, (long long)nlon, &rf));
+        CB_TRY(row_fft_quarter(c, (long long)nlon, rf, &rfq));
+    }
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+
+    CellArgs A{};
+    A.nmax = (long long)nmax;
+    A.npairs = np;
+    A.ntiles = (np + 31) / 32;
+    A.nitems = (long long)(nmax + 1) * A.ntiles;
+    A.tb = tab.tb;
+    A.tc = tab.tc;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
+    A.dm = tab.dm;
+    A.gm = ctab.gm;
+    A.cs = dcs;
+    A.hn = ctab.hn;
+    A.zn = ctab.zn;
+    A.geo = dgeo;
+    A.imm = imm;
+    A.row_n = drows;
+    A.row_s = drows + np;
+    A.dlon = dlon;
+    A.fft = use_fft ? 1 : 0;
+    A.ldf = ldf;
+    A.out = lc;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_cell_imm(A, c.stream), st);
+    }
+    {
+        const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                                  (long long)c.num_sms * 8);
+        Scope sc(c, TIMER_SHS);
+        CB_CUDA(launch_shs_cell(A, rr, std::max(grid, 1), c.stream), st);
+    }
+    if (rf)
+    {
+        RfftArgs R = *synth_plan(rf, rfq, (long long)nmax);
+        R.nrows = (long long)nlat;
+        R.x = fg;
+        R.ldx = (long long)nlon;
+        R.X = lc;
+        R.ldX = ldf;
+        R.kmax = (int)nmax;
+        Scope sc(c, TIMER_FFT);
+        CB_CUDA(launch_rfft(R, true, c.stream), st);
+    }
+    else
+    {
+        // sums at the cell centres lon0 + j dlon (shs_grd_lr.c:145-190)
+        std::vector<double> lon(nlon);
+        const double lon0 = (cell->lonmin[0] + cell->lonmax[0]) / 2.0;
+        for (size_t j = 0; j < nlon; j++)
+            lon[j] = lon0 + (double)j * dlon;
+        double *dlon_arr = nullptr;
+        CB_TRY(dbuf(c, "lon", nlon, &dlon_arr));
+        CB_CUDA(cudaMemcpyAsync(dlon_arr, lon.data(), nlon * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        {
+            Scope sc(c, TIMER_LON);
+            CB_CUDA(launch_lon_direct(1, (int)nlat, (int)nlon,
+                                      (long long)nmax, lc, ldf, dlon_arr, fg,
+                                      c.stream), st);
+        }
+        // lon must outlive the copy
+        CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    }
+    if (f_dev_unaligned)
+        CB_CUDA(cudaMemcpyAsync(f_dev_unaligned, fg, nlat * nlon * 8,
+                                cudaMemcpyDeviceToDevice, c.stream), st);
+    if (!d_f)
+        CB_CUDA(cudaMemcpyAsync(f_host, fg, nlat * nlon * 8,
+                                cudaMemcpyDeviceToHost, c.stream), st);
+    return finish(c, d_status);
+}
+
+// src/shs/shs_cell_sctr.c: one cell per (latmin, latmax, lonmin, lonmax, r)
+Status shs_cell_sctr(Context &c, const charm_cell *cell, const CoefIn &in,
+                     unsigned long nmax, double *f_host, double *d_f)
+{
+    Status st;
+    CB_TRY(check_cells(cell));
+    const size_t n = cell->ncell;
+    bool rr = false;
+    for (size_t i = 0; i < n; i++)
+        rr |= cell->r[i] != in.r;
+    Pairs P;
+    for (size_t i = 0; i < n; i++)
+    {
+        P.row_n.push_back((int)i);
+        P.row_s.push_back(-1);
+    }
+    double *dgeo = nullptr;
+    int *drows = nullptr;
+    CB_TRY(cell_geometry(c, cell, P, in.r, rr, in.mu / in.r, 1.0, &dgeo,
+                         &drows));
+    std::vector<double> lh(2 * n);
+    for (size_t i = 0; i < n; i++)
+    {
+        lh[i] = cell->lonmin[i] + cell->lonmax[i];
+        lh[n + i] = cell->lonmax[i] - cell->lonmin[i];
+    }
+    double *dl = nullptr;
+    CB_TRY(dbuf(c, "cell_lon", 2 * n, &dl));
+    CB_CUDA(cudaMemcpyAsync(dl, lh.data(), 2 * n * 8, cudaMemcpyHostToDevice,
+                            c.stream), st);
+
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
+    CellTabs ctab;
+    CB_TRY(cell_tables(c, (long long)nmax, &ctab));
+    double2 *dcs = nullptr;
+    CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
+    double *fo = d_f;
+    if (!fo)
+        CB_TRY(dbuf(c, "fgrid", n, &fo));
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+
+    CellArgs A{};
+    A.nmax = (long long)nmax;
+    A.npairs = (int)n;
+    A.ntiles = (int)((n + 31) / 32);
+    A.nitems = A.ntiles;
+    A.tb = tab.tb;
+    A.tc = tab.tc;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
+    A.dm = tab.dm;
+    A.gm = ctab.gm;
+    A.cs = dcs;
+    A.hn = ctab.hn;
+    A.zn = ctab.zn;
+    A.geo = dgeo;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    A.lonsum = dl;
+    A.dlonc = dl + n;
+    A.fout = fo;
+    A.mur = in.mu / in.r;
+    {
+        const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                                  (long long)c.num_sms * 8);
+        Scope sc(c, TIMER_SCTR);
+        CB_CUDA(launch_shs_cell_sctr(A, rr, std::max(grid, 1), c.stream), st);
+    }
+    if (!d_f)
+        CB_CUDA(cudaMemcpyAsync(f_host, fo, n * 8, cudaMemcpyDeviceToHost,
+                                c.stream), st);
+    // lh must outlive its copy: finish() synchronises
+    return finish(c, d_status);
+}
+
+// src/sha/sha_cell.c:37-1487 (CHARM_SHA_CELL_AQ)
+Status sha_cell_grid(Context &c, const charm_cell *cell, const double *f_host,
+                     const double *d_fin, unsigned long nmax, double mu,
+                     double R, unsigned long shc_nmax, double *const *hc,
+                     double *const *hs, double *d_c, double *d_s)
+{
+    Status st;
+    const double thr = charm_glob_threshold;
+    const size_t nlat = cell->nlat, nlon = cell->nlon;
+    auto fail = [&](const char *msg) {
+        st.code = CHARM_EFUNCARG;
+        st.msg = msg;
+        return st;
+    };
+    const double r0 = cell->r[0];
+    for (size_t i = 1; i < nlat; i++)
+        if (!nearly_equal(cell->r[i], r0, thr))
+            return fail("All spherical radii in \"cell->r\" must be equal.");
+    if (!nearly_equal(cell->latmax[0], PI / 2.0, thr))
+        return fail("\"cell->latmax[0]\" has to be equal to \"PI / 2.0\" "
+                    "within the \"threshold\".");
+    if (nlat < nmax + 1)
+        return fail("Not enough data in the latitudinal direction.  The "
+                    "required minimum is \"nmax + 1\".");
+    if (!nearly_equal(cell->latmin[nlat - 1], -PI / 2.0, thr))
+        return fail("\"cell->latmin[cell->nlat - 1]\" has to be equal to "
+                    "\"-PI / 2.0\" within the \"threshold\".");
+    for (size_t i = 0; i + 1 < nlat; i++)
+        if (!nearly_equal(cell->latmin[i], cell->latmax[i + 1], thr))
+            return fail("The grid cells are not nicely aligned in the "
+                        "latitudinal direction.  It must hold that "
+                        "\"cell->latmin[i] == cell->latmax[i + 1]\" for all "
+                        "\"i = 0, 1, ..., cell->nlat - 2\" with "
+                        "\"cell->nlat > 1\".");
+    if (nlon < 2 * nmax + 1)
+        return fail("Not enough data in the longitudinal direction.  The "
+                    "required minimum is \"2 * nmax + 1\".");
+    if (!nearly_equal(cell->lonmin[0], 0.0, thr))
+        return fail("\"cell->lonmin[0]\" has to be equal to \"0.0\" within "
+                    "the \"threshold\".");
+    if (!nearly_equal(cell->lonmax[nlon - 1], 2.0 * PI, thr))
+        return fail("\"cell->lonmax[cell->nlon - 1]\" has to be equal to "
+                    "\"2.0 * PI\" within the \"threshold\".");
+    double dlon = 0.0;
+    CB_TRY(cell_grd_lons(cell, &dlon));
+    if (nlon > 1 && !nearly_equal(cell->lonmin[1], cell->lonmax[0], thr))
+        return fail("The grid cells are not nicely aligned in the "
+                    "longitudinal direction.  It must hold that "
+                    "\"cell->lonmin[j + 1] == cell->lonmax[j]\" for all "
+                    "\"j = 0, 1, ..., cell->nlon - 2\" with "
+                    "\"cell->nlon > 1\".");
+    CB_TRY(check_cells(cell));
+
+    Pairs P;
+    cell_pairs(cell, false, P);
+    const int np = (int)P.row_n.size();
+    double *dgeo = nullptr;
+    int *drows = nullptr;
+    CB_TRY(cell_geometry(c, cell, P, R, false, 1.0, dlon, &dgeo, &drows));
+    Tabs tab;
+    CB_TRY(tables(c, (long long)nmax, &tab));
+    CellTabs ctab;
+    CB_TRY(cell_tables(c, (long long)nmax, &ctab));
+    double *imm = nullptr;
+    CB_TRY(dbuf(c, "cell_imm", (size_t)np * (nmax + 1), &imm));
+
+    // block means on the device and r2c along the rows
+    const double *fg = d_fin;
+    if (!fg || reinterpret_cast<uintptr_t>(fg) % 16 != 0)
+    {
+        double *fdev = nullptr;
+        CB_TRY(dbuf(c, "fgrid", nlat * nlon, &fdev));
+        if (fg)
+            CB_CUDA(cudaMemcpyAsync(fdev, fg, nlat * nlon * 8,
+                                    cudaMemcpyDeviceToDevice, c.stream), st);
+        else
+            CB_CUDA(cudaMemcpyAsync(fdev, f_host, nlat * nlon * 8,
+                                    cudaMemcpyHostToDevice, c.stream), st);
+        fg = fdev;
+    }
+    const int ldF = (int)(nlon / 2 + 1);
+    double2 *F = nullptr;
+    CB_TRY(dbuf(c, "lumped", nlat * (size_t)ldF, &F));
+    // even rows of 64 cells or more: the forward row transform of rfft.cu;
+    // odd and short rows: the direct DFT
+    const RfftArgs *rf = nullptr;
+    if (nlon % 2 == 0 && nlon >= 64)
+        CB_TRY(row_fft(c, (long long)nlon, &rf));
+    {
+        Scope sc(c, TIMER_FFT);
+        if (rf)
+        {
+            RfftArgs Rg = *rf;
+            Rg.nrows = (long long)nlat;
+            Rg.x = const_cast<double *>(fg);
+            Rg.ldx = (long long)nlon;
+            Rg.X = F;
+            Rg.ldX = ldF;
+            Rg.kmax = (int)nmax;
+            CB_CUDA(launch_rfft(Rg, false, c.stream), st);
+        }
+        else
+            CB_CUDA(launch_dft_rows_fwd((long long)nlat, (long long)nlon,
+                                        (int)nmax, fg, (long long)nlon, F,
+                                        ldF, c.stream), st);
+    }
+
+    unsigned *d_status;
+    unsigned long long *d_counter;
+    CB_TRY(status_words(c, &d_status, &d_counter));
+    const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
+    const int ntiles = (np + 31) / 32;
+    const long long slots = (long long)c.num_sms * 8 * 4;
+    long long G = std::max<long long>(1, (2 * slots + nmax) / (nmax + 1));
+    G = std::min<long long>(G, ntiles);
+    const int tpg = (int)((ntiles + G - 1) / G);
+    G = (ntiles + tpg - 1) / tpg;
+    double2 *part = nullptr;
+    CB_TRY(dbuf(c, "sha_part", (size_t)G * T, &part));
+
+    CellArgs A{};
+    A.nmax = (long long)nmax;
+    A.npairs = np;
+    A.ntiles = ntiles;
+    A.ngroups = (int)G;
+    A.tiles_per_group = tpg;
+    A.nitems = (long long)(nmax + 1) * G;
+    A.tb = tab.tb;
+    A.tc = tab.tc;
+    A.tmul = tab.tmul;
+    A.ldmul = tab.ldmul;
+    A.sg = tab.sg;
+    A.dm = tab.dm;
+    A.gm = ctab.gm;
+    A.hn = ctab.hn;
+    A.zn = ctab.zn;
+    A.geo = dgeo;
+    A.imm = imm;
+    A.row_n = drows;
+    A.row_s = drows + np;
+    A.dlon = dlon;
+    A.polar_thr = polar_threshold(nmax);
+    A.counter = d_counter;
+    A.status = d_status;
+    A.F = F;
+    A.ldF = ldF;
+    A.part = part;
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_cell_imm(A, c.stream), st);
+    }
+    {
+        const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
+                                                  (long long)c.num_sms * 8);
+        Scope sc(c, TIMER_SHA);
+        CB_CUDA(launch_sha_cell(A, std::max(grid, 1), c.stream), st);
+    }
+
+    // 1 / (4 pi) r0 / mu and the rescaling from r0 to R
+    // (sha_cell.c:1420-1480, src/shc/shc_rescale.c)
+    const unsigned long sn = shc_nmax;
+    double *dres = nullptr;
+    std::vector<double> res;
+    if (!nearly_equal(R, r0, thr))
+    {
+        const double r_ratio = r0 / R;
+        res.resize(sn + 1);
+        double tmp2 = r_ratio;
+        res[0] = 1.0;
+        for (unsigned long n = 1; n <= sn; n++)
+        {
+            res[n] = tmp2;
+            tmp2 *= r_ratio;
+        }
+        CB_TRY(dbuf(c, "sha_rescale", sn + 1, &dres));
+        CB_CUDA(cudaMemcpyAsync(dres, res.data(), (sn + 1) * 8,
+                                cudaMemcpyHostToDevice, c.stream), st);
+    }
+    const long long Ts = (long long)(sn + 1) * (sn + 2) / 2;
+    double *oc = d_c, *os = d_s;
+    if (!oc)
+    {
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "shc_out", (size_t)(2 * Ts), &dout));
+        oc = dout;
+        os = dout + Ts;
+    }
+    {
+        Scope sc(c, TIMER_PREP);
+        CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T,
+                                  part, tab.tc, dres,
+                                  1.0 / (4.0 * PI) * (r0 / mu), oc, os,
+                                  c.stream),
+                st);
+    }
+    if (!d_c)
+    {
+        CB_TRY(download_tri(c, oc, sn, hc));
+        CB_TRY(download_tri(c, os, sn, hs));
+    }
+    return finish(c, d_status);
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free analysis (charm_b200_sha_point_dev_static)
 // ---------------------------------------------------------------------------
 // The same kernels as sha_grid with the row transform of rfft.cu, every
@@ -3255,6 +3890,58 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_grid(g_ctx, pnt, nullptr, d_f, nmax, mu, r, shc_nmax, nullptr,
                     nullptr, d_c, d_s);
+}
+
+Status shs_cell(const charm_cell *cell, const charm_shc *shcs,
+                unsigned long nmax, double *f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    CoefIn in;
+    in.nmax = shcs->nmax;
+    in.mu = shcs->mu;
+    in.r = shcs->r;
+    in.hc = shcs->c;
+    in.hs = shcs->s;
+    if (cell->type == CHARM_CRD_CELL_SCATTERED)
+        return shs_cell_sctr(g_ctx, cell, in, nmax, f, nullptr);
+    return shs_cell_grid(g_ctx, cell, in, nmax, f, nullptr);
+}
+
+Status shs_cell_dev(const charm_cell *cell, unsigned long shc_nmax,
+                    double mu, double r, const double *d_c, const double *d_s,
+                    unsigned long nmax, double *d_f)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    CoefIn in;
+    in.nmax = shc_nmax;
+    in.mu = mu;
+    in.r = r;
+    in.dc = d_c;
+    in.ds = d_s;
+    if (cell->type == CHARM_CRD_CELL_SCATTERED)
+        return shs_cell_sctr(g_ctx, cell, in, nmax, nullptr, d_f);
+    return shs_cell_grid(g_ctx, cell, in, nmax, nullptr, d_f);
+}
+
+Status sha_cell(const charm_cell *cell, const double *f, unsigned long nmax,
+                charm_shc *shcs)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_cell_grid(g_ctx, cell, f, nullptr, nmax, shcs->mu, shcs->r,
+                         shcs->nmax, shcs->c, shcs->s, nullptr, nullptr);
+}
+
+Status sha_cell_dev(const charm_cell *cell, const double *d_f,
+                    unsigned long nmax, double mu, double r,
+                    unsigned long shc_nmax, double *d_c, double *d_s)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return sha_cell_grid(g_ctx, cell, nullptr, d_f, nmax, mu, r, shc_nmax,
+                         nullptr, nullptr, d_c, d_s);
 }
 
 Status sha_point_dev_band(const charm_point *pnt, const double *d_f,

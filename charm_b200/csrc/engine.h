@@ -59,6 +59,19 @@ Status sha_point_dev(const charm_point *pnt, const double *d_f,
 // One latitude band of a sharded analysis: the contribution of the
 // latitude pairs [pair0, pair1) of the grid's pairing to the coefficients
 // (linear in the grid, so the bands' outputs sum to sha_point_dev's).
+// Block means in cells (cell.cu): host arrays (charm_shs_cell,
+// charm_sha_cell) or device arrays.  Callers have done CHarm's checks that
+// precede the dispatch (nmax against shcs->nmax, zero cells, cell type).
+Status shs_cell(const charm_cell *cell, const charm_shc *shcs,
+                unsigned long nmax, double *f);
+Status shs_cell_dev(const charm_cell *cell, unsigned long shc_nmax,
+                    double mu, double r, const double *d_c, const double *d_s,
+                    unsigned long nmax, double *d_f);
+Status sha_cell(const charm_cell *cell, const double *f, unsigned long nmax,
+                charm_shc *shcs);
+Status sha_cell_dev(const charm_cell *cell, const double *d_f,
+                    unsigned long nmax, double mu, double r,
+                    unsigned long shc_nmax, double *d_c, double *d_s);
 Status sha_point_dev_band(const charm_point *pnt, const double *d_f,
                           unsigned long nmax, double mu, double r,
                           unsigned long shc_nmax, int pair0, int pair1,

@@ -117,6 +117,53 @@ struct ShaGridArgs
     double *out_c, *out_s;
 };
 
+// Block-mean values in cells (cell.cu).  Grid synthesis and analysis run
+// over pairs of cell rows (a northern row and its mirror [-latmax,
+// -latmin], or a row alone); scattered synthesis over single cells.
+struct CellArgs
+{
+    long long nmax;
+    int npairs;            // cell-row pairs (grids) or cells (scattered)
+    int ntiles;            // tiles of 32 pairs
+    long long nitems;      // work items of this launch
+    const double2 *tb;     // (beta_n, e_n / a_n) per (n, m), order-major
+    const double *tc;      // ct_n per (n, m)
+    const double *tmul;    // chunk entry multipliers [m][chunk]
+    int ldmul;
+    const double *sg;      // per m: (S_m 2^g_0, g_0)
+    const double *dm;      // sectorial factors d_m (leg_func_dm.c)
+    const double *gm;      // g_m of the I_mm recurrence (leg_func_gm_hm.c)
+    const double2 *cs;     // (ct C_nm, ct S_nm); synthesis only
+    const double2 *hn;     // per n: (h_n, 1 / (n + 1))
+    const double4 *zn;     // per n >= 1: (e_n+1, f_n+1, 1 / sqrt(2n + 1), 0)
+                           // of the un-normalised zonal recurrence
+    const double *geo;     // [8][npairs]: sin, cos of latmin; sin, cos of
+                           // latmax; R / r; block-mean scale mu / (R dA);
+                           // latmin; latmax
+    double *imm;           // [npairs][nmax + 1] I_mm in real units
+    const int *row_n;      // output row of the pair's northern cell row
+    const int *row_s;      // row of its mirror, or -1
+    double dlon;           // longitude step (= cell width) of a grid
+    int fft;               // 1: FFTW c2r packing with (sm, cm); 0: (2/m)
+                           // sin(m dlon / 2) for sums at cell centres
+    int ldf;               // leading dimension of out (double2)
+    double2 *out;          // lumped coefficients [nlat][ldf]
+    double polar_thr;      // polar optimisation threshold, < 0 when off
+    unsigned long long *counter;
+    unsigned *status;
+    // analysis: r2c rows and the group partial sums
+    const double2 *F;
+    int ldF;
+    double2 *part;         // [ngroups][T] in J~ units
+    int ngroups;
+    int tiles_per_group;
+    // scattered cells
+    const double *lonsum;  // lonmin + lonmax per cell
+    const double *dlonc;   // lonmax - lonmin per cell
+    double *fout;          // block means per cell
+    double mur;            // mu / R
+};
+
 // Scattered-point synthesis (sctr.cu).
 struct SctrArgs
 {
@@ -282,6 +329,16 @@ cudaError_t launch_fp64_probe(long long iters, int blocks, int threads,
                               double *sink, cudaStream_t st);
 cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
                         bool rr, int K, int grid, cudaStream_t st);
+cudaError_t launch_cell_imm(const CellArgs &A, cudaStream_t st);
+cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
+                            cudaStream_t st);
+cudaError_t launch_sha_cell(const CellArgs &A, int grid, cudaStream_t st);
+cudaError_t launch_shs_cell_sctr(const CellArgs &A, bool rr, int grid,
+                                 cudaStream_t st);
+// unnormalised forward DFT X[row][k], k <= kmax, of rows of any length
+cudaError_t launch_dft_rows_fwd(long long nrows, long long L, int kmax,
+                                const double *x, long long ldx, double2 *X,
+                                int ldX, cudaStream_t st);
 cudaError_t launch_rfft_w4(int H, double2 *w4, cudaStream_t st);
 cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
                                double2 *ht, double2 *bh, cudaStream_t st);

@@ -5,7 +5,9 @@ modules for the point path (wrap/pyharm/shs.py:27-190, sha.py:36-103,
 crd.py, shc.py): ``Shc``, ``PointGridGL``, ``PointGridDH1``,
 ``PointGridDH2``, ``PointGrid``, ``PointSctr``, ``shs_point``,
 ``shs_point_grad1``, ``shs_point_grad2``, ``shs_point_guru`` and
-``sha_point``.  Arrays are numpy float64 and stay owned by Python; the C
+``sha_point``; for block means in cells ``CellGrid``, ``CellSctr``,
+``shs_cell`` and ``sha_cell`` (wrap/pyharm/crd.py cell classes, shs.py
+shs_cell, sha.py sha_cell).  Arrays are numpy float64 and stay owned by Python; the C
 structures point into them.  Errors reported through charm_err raise
 CHarmError.
 """
@@ -13,9 +15,11 @@ import ctypes as ct
 
 import numpy as np
 
-from ._lib import _libcharm, _Err, _Point, _Shc
+from ._lib import _libcharm, _Cell, _Err, _Point, _Shc
 
 SCATTERED, GRID, GRID_GL, GRID_DH1, GRID_DH2 = 1, 2, 3, 4, 5
+CELL_GRID, CELL_SCATTERED = -2, -1
+SHA_CELL_AQ = 0
 MU = 1.0
 R = 1.0
 
@@ -218,4 +222,70 @@ def sha_point(pnt, f, nmax, mu=MU, r=R):
     with _ErrGuard() as err:
         _libcharm.charm_sha_point(pnt._Point, _dptr(f), int(nmax), shcs._Shc,
                                   err)
+    return shcs
+
+
+# ---------------------------------------------------------------------------
+# Cells (wrap/pyharm/crd.py CellGrid / CellSctr, shs.py shs_cell, sha.py
+# sha_cell)
+# ---------------------------------------------------------------------------
+class _CellBase:
+    def _from_arrays(self, ctype, latmin, latmax, lonmin, lonmax, r):
+        self.type = ctype
+        self.latmin = np.ascontiguousarray(latmin, np.float64)
+        self.latmax = np.ascontiguousarray(latmax, np.float64)
+        self.lonmin = np.ascontiguousarray(lonmin, np.float64)
+        self.lonmax = np.ascontiguousarray(lonmax, np.float64)
+        self.r = np.ascontiguousarray(r, np.float64)
+        ptr = _libcharm.charm_crd_cell_init(
+            ctype, self.latmin.size, self.lonmin.size, _dptr(self.latmin),
+            _dptr(self.latmax), _dptr(self.lonmin), _dptr(self.lonmax),
+            _dptr(self.r))
+        if not ptr:
+            raise CHarmError("charm_crd_cell_init failed")
+        self._Cell = ptr
+
+    @property
+    def ncell(self):
+        return self._Cell.contents.ncell
+
+    def __del__(self):
+        if getattr(self, "_Cell", None):
+            _libcharm.charm_crd_cell_free(self._Cell)
+            self._Cell = None
+
+
+class CellGrid(_CellBase):
+    """Grid of cells: latitude bands [latmin[i], latmax[i]] at radius r[i]
+    times longitude bands [lonmin[j], lonmax[j]]."""
+
+    def __init__(self, latmin, latmax, lonmin, lonmax, r):
+        self._from_arrays(CELL_GRID, latmin, latmax, lonmin, lonmax, r)
+
+
+class CellSctr(_CellBase):
+    """Scattered cells: cell i is [latmin[i], latmax[i]] x [lonmin[i],
+    lonmax[i]] at radius r[i]."""
+
+    def __init__(self, latmin, latmax, lonmin, lonmax, r):
+        self._from_arrays(CELL_SCATTERED, latmin, latmax, lonmin, lonmax, r)
+
+
+def shs_cell(cell, shcs, nmax):
+    if cell.type == CELL_SCATTERED:
+        f = np.zeros(cell.latmin.size)
+    else:
+        f = np.zeros((cell.latmin.size, cell.lonmin.size))
+    with _ErrGuard() as err:
+        _libcharm.charm_shs_cell(cell._Cell, shcs._Shc, int(nmax), _dptr(f),
+                                 err)
+    return f
+
+
+def sha_cell(cell, f, nmax, method=SHA_CELL_AQ, mu=MU, r=R):
+    shcs = Shc(nmax, mu, r)
+    f = np.ascontiguousarray(f, np.float64)
+    with _ErrGuard() as err:
+        _libcharm.charm_sha_cell(cell._Cell, _dptr(f), int(nmax), int(method),
+                                 shcs._Shc, err)
     return shcs

@@ -136,6 +136,43 @@ CHARM_EXTERN void CHARM_CDECL charm_crd_point_dh2_shape(unsigned long nmax,
                                                         size_t *nlat,
                                                         size_t *nlon);
 
+/* Cells: src/crd/crd.h.in:339-409 (struct), :702-846 (functions).
+ * Block-mean values over latitude-longitude cells: a grid (latmin, latmax
+ * and r per cell row, lonmin and lonmax per cell column, f[i * nlon + j])
+ * or scattered cells (nlat == nlon == ncell, all five arrays per cell). */
+typedef struct
+{
+    int type;
+    size_t nlat;
+    size_t nlon;
+    size_t ncell;
+    double *latmin;
+    double *latmax;
+    double *lonmin;
+    double *lonmax;
+    double *r;
+    _Bool owner;
+} charm_cell;
+
+/* crd.h.in:761-846 (src/crd/crd_cell_alloc.c, crd_cell_init.c,
+ * crd_cell_free.c): NULL for an unsupported type, for scattered cells with
+ * nlat != nlon, or when memory runs out */
+CHARM_EXTERN charm_cell * CHARM_CDECL charm_crd_cell_malloc(int type,
+                                                            size_t nlat,
+                                                            size_t nlon);
+CHARM_EXTERN charm_cell * CHARM_CDECL charm_crd_cell_calloc(int type,
+                                                            size_t nlat,
+                                                            size_t nlon);
+CHARM_EXTERN charm_cell * CHARM_CDECL charm_crd_cell_init(int type,
+                                                          size_t nlat,
+                                                          size_t nlon,
+                                                          double *latmin,
+                                                          double *latmax,
+                                                          double *lonmin,
+                                                          double *lonmax,
+                                                          double *r);
+CHARM_EXTERN void CHARM_CDECL charm_crd_cell_free(charm_cell *cell);
+
 /* ------------------------------------------------------------------------- */
 /* Spherical harmonic coefficients: src/shc/shc.h.in:139-381 (struct)         */
 /* ------------------------------------------------------------------------- */
@@ -189,6 +226,16 @@ CHARM_EXTERN void CHARM_CDECL charm_shs_point_guru(const charm_point *pnt,
                                                    double *f,
                                                    charm_err *err);
 
+/* Block means in cells: src/shs/shs.h.in:603-609 (src/shs/shs_cell.c).  A
+ * grid of cells takes the FFT along its rows when its cells cover the
+ * parallels from 0 to 2 pi with (nlon - 1) / 2 >= nmax, else sums at the
+ * cell centres; scattered cells need nlat == nlon. */
+CHARM_EXTERN void CHARM_CDECL charm_shs_cell(const charm_cell *cell,
+                                             const charm_shc *shcs,
+                                             unsigned long nmax,
+                                             double *f,
+                                             charm_err *err);
+
 /* ------------------------------------------------------------------------- */
 /* Analysis: src/sha/sha.h.in:164-169                                         */
 /* ------------------------------------------------------------------------- */
@@ -197,6 +244,20 @@ CHARM_EXTERN void CHARM_CDECL charm_sha_point(const charm_point *pnt,
                                               unsigned long nmax,
                                               charm_shc *shcs,
                                               charm_err *err);
+
+/* Analysis of block means on a cell grid covering the sphere:
+ * src/sha/sha.h.in:50-59 (method), :315-320 (src/sha/sha_cell.c).  The
+ * only method is the approximate quadrature CHARM_SHA_CELL_AQ. */
+enum
+{
+    CHARM_SHA_CELL_AQ
+};
+CHARM_EXTERN void CHARM_CDECL charm_sha_cell(const charm_cell *cell,
+                                             const double *f,
+                                             unsigned long nmax,
+                                             int method,
+                                             charm_shc *shcs,
+                                             charm_err *err);
 
 /* ------------------------------------------------------------------------- */
 /* Runtime globals: src/glob/glob.h.in:66-241 (values glob.c:16-23)            */
@@ -220,6 +281,19 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_dev(
     const charm_point *pnt, unsigned long shc_nmax, double mu, double r,
     const double *d_c, const double *d_s, unsigned long nmax, int kgrad,
     unsigned dr, unsigned dlat, unsigned dlon, double *d_f, charm_err *err);
+
+/* Cell synthesis and analysis with the coefficient triangles, the block
+ * means and the output in device memory (layouts as for
+ * charm_b200_shs_point_dev and charm_b200_sha_point_dev); cell stays in
+ * host memory.  Checks and errors as charm_shs_cell / charm_sha_cell. */
+CHARM_EXTERN void CHARM_CDECL charm_b200_shs_cell_dev(
+    const charm_cell *cell, unsigned long shc_nmax, double mu, double r,
+    const double *d_c, const double *d_s, unsigned long nmax, double *d_f,
+    charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_b200_sha_cell_dev(
+    const charm_cell *cell, const double *d_f, unsigned long nmax, double mu,
+    double r, unsigned long shc_nmax, double *d_c, double *d_s,
+    charm_err *err);
 
 /* Analysis with the grid values (d_f, nlat x nlon) and the output triangles
  * (degree shc_nmax, zero above nmax) in device memory; the coefficients

@@ -149,6 +149,38 @@ def test_argument_errors_without_gpu():
     assert cb.shs_point(z, shc, 4).size == 0
 
 
+def test_cell_constructors_and_errors_without_gpu():
+    """charm_cell layout and constructors (src/crd/crd.h.in:339-409,
+    crd_cell_alloc.c, crd_cell_init.c) and the argument checks that
+    charm_shs_cell / charm_sha_cell make before any GPU work
+    (src/shs/shs_cell.c:22-121, src/sha/sha_cell.c:37-100)."""
+    import charm_b200 as cb
+    from charm_b200._lib import _Cell, _libcharm
+    assert _Cell.latmin.offset == 32 and _Cell.r.offset == 64
+    assert _Cell.owner.offset == 72
+    c = _libcharm.charm_crd_cell_calloc(cb.CELL_GRID, 3, 5)
+    assert c and c.contents.ncell == 15 and c.contents.owner
+    _libcharm.charm_crd_cell_free(c)
+    c = _libcharm.charm_crd_cell_malloc(cb.CELL_SCATTERED, 4, 4)
+    assert c and c.contents.ncell == 4
+    _libcharm.charm_crd_cell_free(c)
+    assert not _libcharm.charm_crd_cell_calloc(cb.CELL_SCATTERED, 3, 4)
+    assert not _libcharm.charm_crd_cell_calloc(cb.GRID, 3, 4)
+    shc = cb.Shc(4, 1.0, 1.0)
+    cg = cb.CellGrid([0.1], [0.2], [0.0], [1.0], [1.0])
+    with pytest.raises(cb.CHarmError, match="cannot be larger"):
+        cb.shs_cell(cg, shc, 5)
+    with pytest.raises(cb.CHarmError, match="Unsupported .method."):
+        cb.sha_cell(cg, np.zeros(1), 2, method=7)
+    cs = cb.CellSctr([0.1], [0.2], [0.0], [1.0], [1.0])
+    with pytest.raises(cb.CHarmError, match="Unsupported .cell->type."):
+        cb.sha_cell(cs, np.zeros(1), 2)
+    # zero cells are a valid no-op (shs_cell.c:63-64)
+    z = cb.CellSctr(np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0),
+                    np.zeros(0))
+    assert cb.shs_cell(z, shc, 4).size == 0
+
+
 def test_err_object_lifecycle():
     from charm_b200._lib import _libcharm
     e = _libcharm.charm_err_init()

