@@ -54,11 +54,12 @@ def parse():
     ap.add_argument("--no-n10800", action="store_true",
                     help="skip the nmax 10800 round trip")
     ap.add_argument("--workload", default="roundtrip",
-                    choices=["roundtrip", "sctr-cg", "batch"],
+                    choices=["roundtrip", "sctr-cg", "batch", "cells"],
                     help="sctr-cg: scattered synthesis + adjoint + CGLS fit "
                          "(nmax 2160); batch: 64 coefficient sets with ten "
-                         "quantities each on DH grids; instead of the grid "
-                         "round trip")
+                         "quantities each on DH grids; cells: block-mean "
+                         "synthesis and analysis on 2191 x 4382 cells; "
+                         "instead of the grid round trip")
     ap.add_argument("--npoint", type=int, default=10_000_000)
     ap.add_argument("--cg-iters", type=int, default=20)
     ap.add_argument("--no-batch-dh", action="store_true",
@@ -69,6 +70,8 @@ def parse():
                     help="points of the scattered section of the default "
                          "line (the full workload: --workload sctr-cg)")
     ap.add_argument("--sctr-iters", type=int, default=2)
+    ap.add_argument("--no-cells", action="store_true",
+                    help="skip the block-mean (cell) synthesis and analysis")
     return ap.parse_args()
 
 
@@ -377,6 +380,7 @@ def run_ours(args):
     n360 = nmax360_round_trip()
     bdh = None if args.no_batch_dh else batch_dh(single_calls=False)
     sct = None if args.no_sctr else scattered(args.sctr_points, args.sctr_iters)
+    cel = None if args.no_cells else cells()
 
     if rank != 0:
         if dist is not None:
@@ -475,6 +479,8 @@ def run_ours(args):
         line["batch_dh"] = bdh
     if sct is not None:
         line["scattered"] = sct
+    if cel is not None:
+        line["cells"] = cel
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, c, s)
     print(json.dumps(line), flush=True)
@@ -986,6 +992,141 @@ def nmax360_round_trip(steps=10):
     return out
 
 
+def cells(steps=5, oracle_rows=3):
+    """Block means on the whole-sphere grid of 2191 x 4382 cells at nmax
+    2190 (the cells of the GL round trip's resolution, r = R, Kaula seed
+    2000): cell synthesis and approximate-quadrature analysis through the
+    device entry points, per-kernel times, FP64 pipe fractions, the
+    synthesis against the oracle on a few rows, and CHarm's own time and
+    coefficients for the same calls on the host cores."""
+    import torch
+    import charm_b200 as cb
+    from charm_b200._lib import _libcharm as L
+    from charm_b200.workloads import GM, R_EARTH, coef_rel_rms, kaula, rel_rms
+    from oracle import charm_ref, orc
+    N = 2190
+    nlat, nlon = N + 1, 2 * (N + 1)
+    lat_e = np.linspace(np.pi / 2, -np.pi / 2, nlat + 1)
+    lat_e[0], lat_e[-1] = np.pi / 2, -np.pi / 2
+    lon_e = np.arange(nlon + 1) * (2.0 * np.pi / nlon)
+    args = (lat_e[1:], lat_e[:-1], lon_e[:-1], lon_e[1:], np.full(nlat, R_EARTH))
+    cl = cb.CellGrid(*args)
+    c, s = kaula(N, 2000)
+    T = c.size
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_c = torch.from_numpy(c).to(dev)
+    d_s = torch.from_numpy(s).to(dev)
+    d_f = torch.empty(nlat * nlon, dtype=torch.float64, device=dev)
+    o_c = torch.empty_like(d_c)
+    o_s = torch.empty_like(d_s)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    P = ct.c_void_p
+    L.charm_b200_shs_cell_dev.argtypes = [P, ct.c_ulong, ct.c_double,
+                                          ct.c_double, P, P, ct.c_ulong, P, P]
+    L.charm_b200_sha_cell_dev.argtypes = [P, P, ct.c_ulong, ct.c_double,
+                                          ct.c_double, ct.c_ulong, P, P, P]
+    L.charm_b200_stream.restype = ct.c_void_p
+    L.charm_b200_timing.argtypes = [ct.c_int]
+    L.charm_b200_timing_read.argtypes = [
+        ct.POINTER(ct.c_double), ct.POINTER(ct.c_ulonglong), ct.c_int,
+        ct.POINTER(ct.c_ulonglong), ct.POINTER(ct.c_ulonglong)]
+    L.charm_b200_fp64_peak_tflops.restype = ct.c_double
+    err = L.charm_err_init()
+    stream = torch.cuda.ExternalStream(L.charm_b200_stream())
+
+    def check():
+        if not L.charm_err_isempty(err):
+            raise RuntimeError(ct.string_at(err.contents.msg).decode())
+
+    def shs():
+        L.charm_b200_shs_cell_dev(ct.cast(cl._Cell, P), N, GM, R_EARTH,
+                                  d_c.data_ptr(), d_s.data_ptr(), N,
+                                  d_f.data_ptr(), ct.cast(err, P))
+        check()
+
+    def sha():
+        L.charm_b200_sha_cell_dev(ct.cast(cl._Cell, P), d_f.data_ptr(), N, GM,
+                                  R_EARTH, N, o_c.data_ptr(), o_s.data_ptr(),
+                                  ct.cast(err, P))
+        check()
+
+    for _ in range(2):
+        shs()
+        sha()
+    torch.cuda.synchronize()
+    res = {}
+    for name, fn in (("shs_cell", shs), ("sha_cell", sha)):
+        L.charm_b200_timing(1)
+        tot = 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        ms = (ct.c_double * 7)()
+        cnt = (ct.c_ulonglong * 7)()
+        kl = ct.c_ulonglong()
+        fe = ct.c_ulonglong()
+        L.charm_b200_timing_read(ms, cnt, 7, ct.byref(kl), ct.byref(fe))
+        L.charm_b200_timing(0)
+        res[name] = {"ms_per_call": tot / steps,
+                     "legendre_ms": (ms[0] + ms[1]) / steps,
+                     "fft_ms": ms[3] / steps,
+                     "prep_ms": ms[5] / steps}
+    f = d_f.cpu().numpy().reshape(nlat, nlon)
+    cg, sg = o_c.cpu().numpy(), o_s.cpu().numpy()
+    L.charm_err_free(err)
+    peak = L.charm_b200_fp64_peak_tflops()
+    units = T * ((nlat + 1) // 2)
+    # FP64 instructions per (n, m, cell-row pair): two boundary recurrences
+    # (DMUL + DFMA each), the integral (h beta, 2 DMUL + 2 DFMA) and two
+    # DFMA sums in synthesis; in analysis the sums are two DMUL into the
+    # transpose plus two DADD of the reduction
+    for name, ipu in (("shs_cell", 11.0), ("sha_cell", 13.0)):
+        k = res[name]
+        k["fp64_instr_per_unit"] = ipu
+        k["fp64_pipe_frac"] = (units * ipu / (k["legendre_ms"] * 1e-3) /
+                               (peak * 1e12 / 2.0)) if peak > 0 else None
+    # the synthesis against the oracle on a few rows (a grid of those rows)
+    rows = np.linspace(0, nlat - 1, oracle_rows).astype(int)
+    sub = (args[0][rows], args[1][rows], args[2], args[3], args[4][rows])
+    fo = orc.shs_cell(orc.Cell(orc.CELL_GRID, *sub), orc.Shc(N, GM, R_EARTH, c, s),
+                      N).reshape(rows.size, nlon)
+    f00 = GM / R_EARTH
+    out = {"workload": "block means on 2191 x 4382 whole-sphere cells, "
+                       "nmax 2190, r = R, Kaula seed 2000",
+           "steps": steps, "units_n_m_pair": units,
+           "shs_cell": res["shs_cell"], "sha_cell": res["sha_cell"],
+           "shs_rel_rms_vs_oracle_rows": rel_rms(f[rows], fo),
+           "shs_signal_rel_rms_vs_oracle_rows": rel_rms(f[rows] - f00, fo - f00),
+           "oracle_rows": [int(r) for r in rows],
+           "aq_round_trip_rel_rms_vs_truth": coef_rel_rms(cg, sg, c, s),
+           "dtype": "f64", "data": "synthetic (seed 2000)"}
+    try:
+        C = charm_ref.Charm("d")
+        cc = C.cell(orc.CELL_GRID, *args)
+        shc = C.shc(N, GM, R_EARTH, c, s)
+        t0 = time.perf_counter()
+        fr = C.shs_cell(cc, shc, N, nlat * nlon)
+        t1 = time.perf_counter()
+        cr, sr = C.sha_cell(cc, np.ravel(f), N, GM, R_EARTH)
+        t2 = time.perf_counter()
+        out["charm_cpu"] = {"shs_cell_s": t1 - t0, "sha_cell_s": t2 - t1,
+                            "cores": host_cores(), "lib": os.path.relpath(
+                                charm_ref.lib_path("d"), ROOT)}
+        out["shs_rel_rms_vs_charm"] = rel_rms(np.ravel(f), fr)
+        out["sha_rel_rms_vs_charm"] = coef_rel_rms(cg, sg, cr, sr)
+    except (OSError, RuntimeError) as e:
+        out["charm_cpu"] = "unavailable: %s" % e
+    return out
+
+
 def batch_dh(single_calls=True, oracle_rows=6):
     """64 coefficient sets, nmax_j uniform in 90..2160 (numpy default_rng
     4999), Kaula coefficients (seeds 4000 + j), synthesised at r = R + 250 km
@@ -1019,6 +1160,26 @@ def batch_dh(single_calls=True, oracle_rows=6):
     def check():
         if not L.charm_err_isempty(err):
             raise RuntimeError(ct.string_at(err.contents.msg).decode())
+
+    # where the batched calls' time goes: one more call of each with the
+    # library's per-kernel event timing (not part of the timed calls)
+    L.charm_b200_timing.argtypes = [ct.c_int]
+    L.charm_b200_timing_read.argtypes = [
+        ct.POINTER(ct.c_double), ct.POINTER(ct.c_ulonglong), ct.c_int,
+        ct.POINTER(ct.c_ulonglong), ct.POINTER(ct.c_ulonglong)]
+    split_ms = {"fp64": [0.0] * 7, "split": [0.0] * 7}
+
+    def kernel_times(kind, call):
+        L.charm_b200_timing(1)
+        call()
+        torch.cuda.synchronize()
+        ms_ = (ct.c_double * 7)()
+        cnt_ = (ct.c_ulonglong * 7)()
+        kl_, fe_ = ct.c_ulonglong(), ct.c_ulonglong()
+        L.charm_b200_timing_read(ms_, cnt_, 7, ct.byref(kl_), ct.byref(fe_))
+        L.charm_b200_timing(0)
+        for i_ in range(7):
+            split_ms[kind][i_] += ms_[i_]
 
     h = 250e3
     names = ["V", "Vx", "Vy", "Vz", "Vxx", "Vxy", "Vxz", "Vyy", "Vyz", "Vzz"]
@@ -1062,6 +1223,9 @@ def batch_dh(single_calls=True, oracle_rows=6):
                 torch.cuda.synchronize()
                 if rep == 1:
                     t_batch += time.perf_counter() - t0
+            kernel_times("fp64", lambda: (L.charm_b200_shs_point_batch_dev(
+                ct.cast(pnt._Point, P), n, nmv, nmv, muv, R_EARTH, pc, ps, 3,
+                pf, ct.cast(err, P)), check()))
             if jmin in sel:
                 o = out[sel.index(jmin)].view(10, pnt.lat.size, pnt.lon.size)
                 probe[jmin] = (pnt, rows, o[:, rows, :].cpu().numpy())
@@ -1081,6 +1245,9 @@ def batch_dh(single_calls=True, oracle_rows=6):
                 torch.cuda.synchronize()
                 if rep == 1:
                     t_batch8 += time.perf_counter() - t0
+            kernel_times("split", lambda: (L.charm_b200_shs_point_batch_i8_dev(
+                ct.cast(pnt._Point, P), n, nmv, nmv, muv, R_EARTH, pc, ps, 3,
+                pf8, ct.cast(err, P)), check()))
             keep = torch.from_numpy(np.cos(pnt.lat) > 1e-8).cuda()
             for b in range(n):
                 a8 = out8[b].view(10, pnt.lat.size, pnt.lon.size)
@@ -1189,6 +1356,12 @@ def batch_dh(single_calls=True, oracle_rows=6):
         "split_precision_batched_10q_sets_per_s": 64.0 / t_batch8,
         "split_precision_speedup_10q": t_batch / t_batch8,
         "split_vs_fp64_rel_rms_per_component_off_poles": worst8,
+        # summed device time of the library's kernels in one more call of
+        # each batched form (events per kernel): Legendre kernels, row
+        # transforms, tables / seeds / digit preparation
+        "kernel_ms_10q": {
+            k: {"legendre": v[0], "row_transforms": v[3], "prep": v[5],
+                "tables": v[6]} for k, v in split_ms.items()},
         "units_n_m_pair": total_units,
         "potential_fp64_vs_split_precision": pot,
         "rel_rms_vs_oracle_per_component": comp,
@@ -1210,10 +1383,19 @@ def run_batch(args):
     print(json.dumps(batch_dh(single_calls=True)), flush=True)
 
 
+def run_cells(args):
+    """The cell workload alone (cells()); prints one JSON line.  One GPU."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(cells(steps=args.steps)), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "batch":
         run_batch(args)
+    elif args.workload == "cells":
+        run_cells(args)
     elif args.workload == "sctr-cg":
         run_sctr_cg(args)
     elif args.impl == "reference":

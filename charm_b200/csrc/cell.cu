@@ -53,9 +53,13 @@ constexpr int CELL_WARPS = 4;
 
 // per warp: LEG_CHUNK x (tb, cs, hn) double2
 constexpr size_t CELL_STAGE_BYTES = 3 * LEG_CHUNK * sizeof(double2);
-// analysis: the staging plus the 32 x 33 transpose of the partial sums
+// analysis: the staging of (tb, hn) (no coefficients) and the 32 x 32
+// transpose of the partial sums, element (row, col) at row * 32 +
+// (col ^ row) so that neither the row-wise stores nor the column-wise
+// reads meet bank conflicts: 18 KB per warp, three blocks of four warps per
+// SM
 constexpr size_t CELL_SHA_WARP_BYTES =
-    CELL_STAGE_BYTES + 32 * 33 * sizeof(double2);
+    2 * LEG_CHUNK * sizeof(double2) + 32 * 32 * sizeof(double2);
 
 struct Stage
 {
@@ -66,6 +70,13 @@ __device__ __forceinline__ Stage warp_stage(unsigned char *base)
 {
     double2 *p = reinterpret_cast<double2 *>(base);
     return Stage{p, p + LEG_CHUNK, p + 2 * LEG_CHUNK};
+}
+
+// the analysis stage: no coefficient column
+__device__ __forceinline__ Stage warp_stage_sha(unsigned char *base)
+{
+    double2 *p = reinterpret_cast<double2 *>(base);
+    return Stage{p, nullptr, p + LEG_CHUNK};
 }
 
 // Stages chunk j of order m: entries n = m + 64 j + i, i < cnt, of the
@@ -84,13 +95,15 @@ __device__ __forceinline__ void stage_chunk(const Stage &S, const CellArgs &A,
         if (i < cnt)
         {
             S.tb[i] = A.tb[c0 + off + i];
-            S.cs[i] = A.cs ? A.cs[c0 + off + i] : make_double2(0.0, 0.0);
+            if (S.cs)
+                S.cs[i] = A.cs[c0 + off + i];
             S.hn[i] = A.hn[m + off + i];
         }
         else
         {
             S.tb[i] = make_double2(0.0, 0.0);
-            S.cs[i] = make_double2(0.0, 0.0);
+            if (S.cs)
+                S.cs[i] = make_double2(0.0, 0.0);
             S.hn[i] = make_double2(0.0, 0.0);
         }
     }
@@ -202,65 +215,79 @@ __device__ __forceinline__ void lon_factors(long long m, double dlon,
 // ---------------------------------------------------------------------------
 // I_mm of every cell-row pair (sectorial integrals, sha_cell.c:586-660)
 // ---------------------------------------------------------------------------
-// One thread per pair walks m = 1..nmax with CHarm's sectorial sequence
-// (src/leg/leg_func_prepare.c: P_11 = sqrt(3) u, P_m+1,m+1 = (d_m u) P_mm,
-// X-number exponent carried separately) at both boundaries.
-__global__ void k_cell_imm(CellArgs A)
+// Two steps.  k_cell_imm_q: one thread per (order, pair) evaluates
+// q_m = (t2 P_mm(t2) - t1 P_mm(t1)) / (m + 1) from the sectorial seeds of
+// leg.cuh (P_mm = S_m u^m, S_m = sqrt(3) prod d_k, src/leg/
+// leg_func_prepare.c; below the double range it is zero, as CHarm's
+// X-numbers convert).  k_cell_imm_rec: one thread per pair runs the
+// recurrence over the orders, I_mm = g_m I_m-2,m-2 + q_m, from the closed
+// forms of I_11 and I_22, in place.  imm is order-major ([m][pair]), so
+// that the writes and the reads by the warps of one order are coalesced.
+__global__ void k_cell_imm_q(CellArgs A)
+{
+    const int np = A.npairs;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= A.nmax * (long long)np)
+        return;
+    const long long m = 1 + idx / np;
+    const int p = (int)(idx % np);
+    const double t1 = A.geo[0 * np + p], u1 = A.geo[1 * np + p];
+    const double t2 = A.geo[2 * np + p], u2 = A.geo[3 * np + p];
+    const double sigma = A.sg[2 * m];
+    const int g0 = (int)A.sg[2 * m + 1];
+    double x1, x2;
+    int e1, e2;
+    leg_seed(sigma, u1, 1.0, false, m, 0, x1, e1);
+    leg_seed(sigma, u2, 1.0, false, m, 0, x2, e2);
+    const double p1 = scalbn(x1, e1 - g0), p2 = scalbn(x2, e2 - g0);
+    A.imm[(size_t)m * np + p] = A.hn[m].y * (t2 * p2 - t1 * p1);
+}
+
+__global__ void k_cell_imm_rec(CellArgs A)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= A.npairs)
+    const int np = A.npairs;
+    if (p >= np)
         return;
     const long long N = A.nmax;
-    const double BIG = 0x1p960, BIGI = 0x1p-960;
-    const double BIGS = 0x1p480, BIGSI = 0x1p-480;
     const double ROOT3 = 1.73205080756887729353;
     const double PI_2 = 1.57079632679489661923;
-    const double t1 = A.geo[0 * A.npairs + p], u1 = A.geo[1 * A.npairs + p];
-    const double t2 = A.geo[2 * A.npairs + p], u2 = A.geo[3 * A.npairs + p];
-    const double la1 = A.geo[6 * A.npairs + p], la2 = A.geo[7 * A.npairs + p];
-    double *out = A.imm + (size_t)p * (size_t)(N + 1);
-    out[0] = 0.0;
-    double x1 = ROOT3 * u1, x2 = ROOT3 * u2;
-    int e1 = 0, e2 = 0;
-    auto x2f = [&](double x, int e) {
-        return e == 0 ? x : (e < -1 ? 0.0 : (e < 0 ? x * BIGI : x * BIG));
-    };
-    auto norm = [&](double &x, int &e) {
-        const double w = fabs(x);
-        if (w >= BIGS)
-        {
-            x *= BIGI;
-            e += 1;
-        }
-        else if (w < BIGSI)
-        {
-            x *= BIG;
-            e -= 1;
-        }
-    };
-    double im2 = 0.0, im1 = 0.0;   // I_m-2,m-2, I_m-1,m-1
-    for (long long m = 1; m <= N; m++)
+    const double t1 = A.geo[0 * np + p], u1 = A.geo[1 * np + p];
+    const double t2 = A.geo[2 * np + p], u2 = A.geo[3 * np + p];
+    const double la1 = A.geo[6 * np + p], la2 = A.geo[7 * np + p];
+    double *io = A.imm + p;
+    io[0] = 0.0;
+    // the closed forms of CHarm (shs_cell_kernel.c:229-262)
+    double im2 = (ROOT3 / 2.0) * ((t2 * u2 - (PI_2 - la2)) -
+                                  (t1 * u1 - (PI_2 - la1)));
+    io[(size_t)np] = im2;
+    if (N < 2)
+        return;
+    double im1 = (3.87298334620741688518 / 6.0) *
+                 (t2 * (3.0 - t2 * t2) - t1 * (3.0 - t1 * t1));
+    io[2 * (size_t)np] = im1;
+    constexpr int B = 8;
+    for (long long m0 = 3; m0 <= N; m0 += B)
     {
-        if (m > 1)
+        double q[B], gv[B];
+#pragma unroll
+        for (int b = 0; b < B; b++)
         {
-            x1 = (A.dm[m - 1] * u1) * x1;
-            x2 = (A.dm[m - 1] * u2) * x2;
-            norm(x1, e1);
-            norm(x2, e2);
+            const long long m = m0 + b;
+            q[b] = m <= N ? io[(size_t)m * np] : 0.0;
+            gv[b] = m <= N ? __ldg(&A.gm[m]) : 0.0;
         }
-        const double p1 = x2f(x1, e1), p2 = x2f(x2, e2);
-        double v;
-        if (m == 1)
-            v = (ROOT3 / 2.0) * ((t2 * u2 - (PI_2 - la2)) -
-                                 (t1 * u1 - (PI_2 - la1)));
-        else if (m == 2)
-            v = (3.87298334620741688518 / 6.0) *
-                (t2 * (3.0 - t2 * t2) - t1 * (3.0 - t1 * t1));
-        else
-            v = A.gm[m] * im2 + (1.0 / (double)(m + 1)) * (t2 * p2 - t1 * p1);
-        out[m] = v;
-        im2 = im1;
-        im1 = v;
+#pragma unroll
+        for (int b = 0; b < B; b++)
+        {
+            const long long m = m0 + b;
+            if (m > N)
+                break;
+            const double v = fma(gv[b], im2, q[b]);
+            io[(size_t)m * np] = v;
+            im2 = im1;
+            im1 = v;
+        }
     }
 }
 
@@ -352,7 +379,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell(CellArgs A)
             const double sigma = A.sg[2 * m];
             const int g0 = (int)A.sg[2 * m + 1];
             cell_seed(R, sigma, g0, u1, u2, m,
-                      valid ? A.imm[(size_t)p * (size_t)(N + 1) + m] : 0.0);
+                      valid ? A.imm[(size_t)m * np + p] : 0.0);
             bool any_scaled = __any_sync(0xffffffffu, (R.E1 | R.E2) != 0);
             for (int j = 0; j < nchunks; j++)
             {
@@ -442,19 +469,24 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell(CellArgs A)
 // ---------------------------------------------------------------------------
 // Grid analysis (approximate quadrature): partial sums per group of tiles
 // ---------------------------------------------------------------------------
-// Work item = (order m, group g of tiles); lane = pair of cell rows.  Every
-// 32 degrees the warp transposes its lane values through shared memory so
-// that lane l holds the warp total of degree n0 + l, added to the group's
-// partial column (the warp owns it); k_sha_reduce sums the groups in fixed
-// order and applies ct_n, the 1 / (4 pi) r / mu factor and the rescaling.
-__global__ void __launch_bounds__(CELL_WARPS * 32, 2) k_sha_cell(CellArgs A)
+// Work item = (order m, group g of tiles of 32 K pairs); each lane carries K
+// pairs of cell rows and forms, per degree, the sum over them of
+// J~_n {amp, bmp}^(n+m parity).  Every 32 degrees the warp transposes its
+// lane values through shared memory so that lane l holds the warp total of
+// degree n0 + l, added to the group's partial column (the warp owns it);
+// k_sha_reduce sums the groups in fixed order and applies ct_n, the
+// 1 / (4 pi) r / mu factor and the rescaling.
+template <int K>
+__global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
+    k_sha_cell(CellArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = threadIdx.x >> 5;
     unsigned char *wbase = smem_raw + (size_t)warp * CELL_SHA_WARP_BYTES;
-    const Stage S = warp_stage(wbase);
-    double2 *red = reinterpret_cast<double2 *>(wbase + CELL_STAGE_BYTES);
+    const Stage S = warp_stage_sha(wbase);
+    double2 *red = reinterpret_cast<double2 *>(
+        wbase + 2 * LEG_CHUNK * sizeof(double2));
     const long long N = A.nmax;
     const int np = A.npairs;
     const long long T = tri_size(N);
@@ -481,66 +513,80 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, 2) k_sha_cell(CellArgs A)
 
         for (int tile = tile0; tile < tile1; tile++)
         {
-            const int p = tile * 32 + (int)lane;
-            const bool valid = p < np;
-            CellRec R;
-            R.t1 = valid ? A.geo[0 * np + p] : 0.0;
-            const double u1 = valid ? A.geo[1 * np + p] : 1.0;
-            R.t2 = valid ? A.geo[2 * np + p] : 0.0;
-            const double u2 = valid ? A.geo[3 * np + p] : 1.0;
-            R.u1s = u1 * u1;
-            R.u2s = u2 * u2;
-            const bool skip_lane =
-                !valid || (A.polar_thr >= 0.0 &&
-                           A.polar_thr < (double)m - (double)N * u1);
-            if (__all_sync(0xffffffffu, skip_lane))
+            CellRec R[K];
+            double amp[K], amm[K], bmp[K], bmm[K];
+            double p0a[K], p0b[K], p1a[K], p1b[K];
+            bool all_skip = true, any_scaled = false;
+#pragma unroll
+            for (int k = 0; k < K; k++)
+            {
+                const int p = tile * (32 * K) + k * 32 + (int)lane;
+                const bool valid = p < np;
+                R[k].t1 = valid ? A.geo[0 * np + p] : 0.0;
+                const double u1 = valid ? A.geo[1 * np + p] : 1.0;
+                R[k].t2 = valid ? A.geo[2 * np + p] : 0.0;
+                const double u2 = valid ? A.geo[3 * np + p] : 1.0;
+                R[k].u1s = u1 * u1;
+                R[k].u2s = u2 * u2;
+                const bool skip_lane =
+                    !valid || (A.polar_thr >= 0.0 &&
+                               A.polar_thr < (double)m - (double)N * u1);
+                all_skip &= skip_lane;
+                // amplitudes of the order (sha_cell.c:790-840): the r2c
+                // sums a = Re F, b = -Im F of the row and of its mirror,
+                // combined with the longitude integrals
+                amp[k] = amm[k] = bmp[k] = bmm[k] = 0.0;
+                if (!skip_lane)
+                {
+                    const double2 Fn = A.F[(size_t)A.row_n[p] * A.ldF + m];
+                    double a = Fn.x, b = -Fn.y, a2 = 0.0, b2 = 0.0;
+                    if (A.row_s[p] >= 0)
+                    {
+                        const double2 Fs =
+                            A.F[(size_t)A.row_s[p] * A.ldF + m];
+                        a2 = Fs.x;
+                        b2 = -Fs.y;
+                    }
+                    const double ap = a + a2, am = a - a2;
+                    const double bp = b + b2, bm = b - b2;
+                    if (m == 0)
+                    {
+                        amp[k] = ap * A.dlon;
+                        amm[k] = am * A.dlon;
+                    }
+                    else
+                    {
+                        amp[k] = ap * sm + bp * cm;
+                        amm[k] = am * sm + bm * cm;
+                        bmp[k] = bp * sm - ap * cm;
+                        bmm[k] = bm * sm - am * cm;
+                    }
+                }
+                p0a[k] = p0b[k] = 1.0;
+                p1a[k] = R[k].t1;
+                p1b[k] = R[k].t2;
+                if (m > 0)
+                {
+                    cell_seed(R[k], A.sg[2 * m], (int)A.sg[2 * m + 1], u1, u2,
+                              m, valid ? A.imm[(size_t)m * np + p] : 0.0);
+                    any_scaled |= (R[k].E1 | R[k].E2) != 0;
+                }
+            }
+            if (__all_sync(0xffffffffu, all_skip))
                 continue;
-            // amplitudes of the order (sha_cell.c:790-840): the r2c sums
-            // a = Re F, b = -Im F of the row and of its mirror, combined
-            // with the longitude integrals
-            double amp = 0.0, amm = 0.0, bmp = 0.0, bmm = 0.0;
-            if (!skip_lane)
-            {
-                const double2 Fn = A.F[(size_t)A.row_n[p] * A.ldF + m];
-                double a = Fn.x, b = -Fn.y, a2 = 0.0, b2 = 0.0;
-                if (A.row_s[p] >= 0)
-                {
-                    const double2 Fs = A.F[(size_t)A.row_s[p] * A.ldF + m];
-                    a2 = Fs.x;
-                    b2 = -Fs.y;
-                }
-                const double ap = a + a2, am = a - a2;
-                const double bp = b + b2, bm = b - b2;
-                if (m == 0)
-                {
-                    amp = ap * A.dlon;
-                    amm = am * A.dlon;
-                }
-                else
-                {
-                    amp = ap * sm + bp * cm;
-                    amm = am * sm + bm * cm;
-                    bmp = bp * sm - ap * cm;
-                    bmm = bm * sm - am * cm;
-                }
-            }
-            bool any_scaled = false;
-            double p0a = 1.0, p0b = 1.0, p1a = R.t1, p1b = R.t2;
-            if (m > 0)
-            {
-                cell_seed(R, A.sg[2 * m], (int)A.sg[2 * m + 1], u1, u2, m,
-                          valid ? A.imm[(size_t)p * (size_t)(N + 1) + m]
-                                : 0.0);
-                any_scaled = __any_sync(0xffffffffu, (R.E1 | R.E2) != 0);
-            }
-            double2 *redl = red + lane;
+            any_scaled = __any_sync(0xffffffffu, any_scaled);
             for (int j = 0; j < nchunks; j++)
             {
                 const int cnt = (int)min((long long)LEG_CHUNK,
                                          ncol - (long long)j * LEG_CHUNK);
                 stage_chunk(S, A, c0, m, j, cnt, lane);
                 if (j > 0 && m > 0)
-                    R.scale(A.tmul[(size_t)m * A.ldmul + j]);
+                {
+                    const double mul = A.tmul[(size_t)m * A.ldmul + j];
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        R[k].scale(mul);
+                }
                 for (int half = 0; half < 2; half++)
                 {
                     const int ib = 32 * half;
@@ -556,51 +602,75 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, 2) k_sha_cell(CellArgs A)
                     for (int jj = 0; jj < 32; jj++)
                     {
                         const int i = ib + jj;
-                        const long long k = (long long)j * LEG_CHUNK + i;
-                        double v = 0.0;
+                        const long long kk = (long long)j * LEG_CHUNK + i;
+                        const bool odd = (jj & 1) != 0;
+                        double vc = 0.0, vs = 0.0;
                         if (i < cnt)
                         {
                             if (m == 0)
                             {
-                                double in0;
-                                if (k == 0)
-                                    in0 = R.t2 - R.t1;
-                                else
+                                const double rct = 1.0 / A.tc[c0 + kk];
+                                const double4 z =
+                                    kk > 0 ? A.zn[kk]
+                                           : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+                                for (int k = 0; k < K; k++)
                                 {
-                                    const double4 z = A.zn[k];
-                                    const double p2a =
-                                        z.x * (R.t1 * p1a) - z.y * p0a;
-                                    const double p2b =
-                                        z.x * (R.t2 * p1b) - z.y * p0b;
-                                    in0 = z.z * ((p2b - p0b) - (p2a - p0a));
-                                    p0a = p1a;
-                                    p1a = p2a;
-                                    p0b = p1b;
-                                    p1b = p2b;
+                                    double in0;
+                                    if (kk == 0)
+                                        in0 = R[k].t2 - R[k].t1;
+                                    else
+                                    {
+                                        const double p2a =
+                                            z.x * (R[k].t1 * p1a[k]) -
+                                            z.y * p0a[k];
+                                        const double p2b =
+                                            z.x * (R[k].t2 * p1b[k]) -
+                                            z.y * p0b[k];
+                                        in0 = z.z * ((p2b - p0b[k]) -
+                                                     (p2a - p0a[k]));
+                                        p0a[k] = p1a[k];
+                                        p1a[k] = p2a;
+                                        p0b[k] = p1b[k];
+                                        p1b[k] = p2b;
+                                    }
+                                    const double v = in0 * rct;
+                                    vc = fma(v, odd ? amm[k] : amp[k], vc);
                                 }
-                                v = in0 / A.tc[c0 + k];
                             }
-                            else if (k == 0)
-                                v = R.J1;
+                            else if (kk == 0)
+                            {
+#pragma unroll
+                                for (int k = 0; k < K; k++)
+                                {
+                                    vc = fma(R[k].J1, amp[k], vc);
+                                    vs = fma(R[k].J1, bmp[k], vs);
+                                }
+                            }
                             else
                             {
                                 const double beta = S.tb[i].x;
                                 const double2 h = S.hn[i];
-                                v = R.step(beta, h.x * beta, h.y);
+                                const double hb = h.x * beta;
+#pragma unroll
+                                for (int k = 0; k < K; k++)
+                                {
+                                    const double v = R[k].step(beta, hb, h.y);
+                                    vc = fma(v, odd ? amm[k] : amp[k], vc);
+                                    vs = fma(v, odd ? bmm[k] : bmp[k], vs);
+                                }
                             }
                         }
-                        const bool odd = (jj & 1) != 0;
-                        redl[jj * 33] = make_double2(v * (odd ? amm : amp),
-                                                     v * (odd ? bmm : bmp));
+                        red[jj * 32 + ((int)lane ^ jj)] = make_double2(vc, vs);
                     }
                     __syncwarp();
-                    const double2 *row = red + lane * 33;
+                    const double2 *row = red + lane * 32;
                     double oc0 = 0.0, os0 = 0.0, oc1 = 0.0, os1 = 0.0;
 #pragma unroll
                     for (int q = 0; q < 32; q += 2)
                     {
-                        const double2 a = row[q];
-                        const double2 b = row[q + 1];
+                        const double2 a = row[q ^ (int)lane];
+                        const double2 b = row[(q + 1) ^ (int)lane];
                         oc0 += a.x;
                         os0 += a.y;
                         oc1 += b.x;
@@ -614,7 +684,13 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, 2) k_sha_cell(CellArgs A)
                                           : make_double2(outc, outs);
                 }
                 if (m > 0 && any_scaled)
-                    any_scaled = __any_sync(0xffffffffu, R.fixup());
+                {
+                    bool still = false;
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        still |= R[k].fixup();
+                    any_scaled = __any_sync(0xffffffffu, still);
+                }
             }
             stored = true;
         }
@@ -866,8 +942,11 @@ cudaError_t launch_cell_imm(const CellArgs &A, cudaStream_t st)
 {
     if (A.npairs <= 0 || A.nmax < 1)
         return cudaSuccess;
-    const int threads = 64;
-    k_cell_imm<<<(A.npairs + threads - 1) / threads, threads, 0, st>>>(A);
+    const long long total = A.nmax * (long long)A.npairs;
+    k_cell_imm_q<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(A);
+    const int threads = 32;
+    k_cell_imm_rec<<<(A.npairs + threads - 1) / threads, threads, 0, st>>>(
+        A);
     return cudaGetLastError();
 }
 
@@ -882,20 +961,27 @@ cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
     return cudaGetLastError();
 }
 
-cudaError_t launch_sha_cell(const CellArgs &A, int grid, cudaStream_t st)
+cudaError_t launch_sha_cell(const CellArgs &A, int K, int grid,
+                            cudaStream_t st)
 {
     const size_t smem = CELL_WARPS * CELL_SHA_WARP_BYTES;
     static bool attr_set = false;
     if (!attr_set)
     {
-        cudaError_t e = cudaFuncSetAttribute(
-            k_sha_cell, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int)smem);
-        if (e != cudaSuccess)
-            return e;
+        for (const void *f : {(const void *)k_sha_cell<1>,
+                              (const void *)k_sha_cell<2>})
+        {
+            cudaError_t e = cudaFuncSetAttribute(
+                f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess)
+                return e;
+        }
         attr_set = true;
     }
-    k_sha_cell<<<grid, CELL_WARPS * 32, smem, st>>>(A);
+    if (K == 2)
+        k_sha_cell<2><<<grid, CELL_WARPS * 32, smem, st>>>(A);
+    else
+        k_sha_cell<1><<<grid, CELL_WARPS * 32, smem, st>>>(A);
     return cudaGetLastError();
 }
 

@@ -3416,7 +3416,9 @@ Status sha_cell_grid(Context &c, const charm_cell *cell, const double *f_host,
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
     const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
-    const int ntiles = (np + 31) / 32;
+    // two cell-row pairs per lane once there are enough of them
+    const int K = np >= 512 ? 2 : 1;
+    const int ntiles = (np + 32 * K - 1) / (32 * K);
     const long long slots = (long long)c.num_sms * 8 * 4;
     long long G = std::max<long long>(1, (2 * slots + nmax) / (nmax + 1));
     G = std::min<long long>(G, ntiles);
@@ -3460,7 +3462,7 @@ Status sha_cell_grid(Context &c, const charm_cell *cell, const double *f_host,
         const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                                   (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
-        CB_CUDA(launch_sha_cell(A, std::max(grid, 1), c.stream), st);
+        CB_CUDA(launch_sha_cell(A, K, std::max(grid, 1), c.stream), st);
     }
 
     // 1 / (4 pi) r0 / mu and the rescaling from r0 to R

@@ -140,7 +140,7 @@ struct CellArgs
     const double *geo;     // [8][npairs]: sin, cos of latmin; sin, cos of
                            // latmax; R / r; block-mean scale mu / (R dA);
                            // latmin; latmax
-    double *imm;           // [npairs][nmax + 1] I_mm in real units
+    double *imm;           // [nmax + 1][npairs] I_mm in real units
     const int *row_n;      // output row of the pair's northern cell row
     const int *row_s;      // row of its mirror, or -1
     double dlon;           // longitude step (= cell width) of a grid
@@ -332,7 +332,9 @@ cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
 cudaError_t launch_cell_imm(const CellArgs &A, cudaStream_t st);
 cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
                             cudaStream_t st);
-cudaError_t launch_sha_cell(const CellArgs &A, int grid, cudaStream_t st);
+// K cell-row pairs per lane (1 or 2); A.ntiles counts tiles of 32 K pairs
+cudaError_t launch_sha_cell(const CellArgs &A, int K, int grid,
+                            cudaStream_t st);
 cudaError_t launch_shs_cell_sctr(const CellArgs &A, bool rr, int grid,
                                  cudaStream_t st);
 // unnormalised forward DFT X[row][k], k <= kmax, of rows of any length
