@@ -706,6 +706,139 @@ void charm_sha_point(const charm_point *pnt, const double *f,
 }
 
 // ---------------------------------------------------------------------------
+// Coefficient files in CHarm's binary format: src/shc/shc_read_bin.c:18-256,
+// src/shc/shc_write_bin.c:18-187 (same checks, messages and return values)
+// ---------------------------------------------------------------------------
+unsigned long charm_shc_read_bin(const char *pathname, unsigned long nmax,
+                                 charm_shc *shcs, charm_err *err)
+{
+    const bool nmax_only = nmax == CHARM_SHC_NMAX_MODEL && shcs == NULL;
+    FILE *fp = fopen(pathname, "rb");
+    if (!fp)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg, "Couldn't open \"%s\".", pathname);
+        SET_ERR(err, CHARM_EFILEIO, msg);
+        return CHARM_SHC_NMAX_ERROR;
+    }
+    unsigned long nmax_file = CHARM_SHC_NMAX_ERROR;
+    double mu = 0.0, r = 0.0;
+    if (fread(&nmax_file, sizeof nmax_file, 1, fp) != 1)
+    {
+        SET_ERR(err, CHARM_EFILEIO,
+                "Failed to read the maximum harmonic degree.");
+        goto EXIT;
+    }
+    if (nmax_only)
+        goto EXIT;
+    if (fread(&mu, sizeof mu, 1, fp) != 1)
+    {
+        SET_ERR(err, CHARM_EFILEIO, "Failed to read the scaling parameter.");
+        goto EXIT;
+    }
+    if (fread(&r, sizeof r, 1, fp) != 1)
+    {
+        SET_ERR(err, CHARM_EFILEIO,
+                "Failed to read the radius of the reference sphere.");
+        goto EXIT;
+    }
+    if (nmax > nmax_file)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Not enough coefficients in the input file for the maximum "
+                "harmonic degree \"nmax\".");
+        goto EXIT;
+    }
+    if (shcs->nmax < nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Too low maximum degree \"shcs->nmax\" to read coefficients "
+                "up to degree \"nmax\".");
+        goto EXIT;
+    }
+    shcs->mu = mu;
+    shcs->r = r;
+    memset(shcs->c[0], 0, shcs->nc * sizeof(double));
+    memset(shcs->s[0], 0, shcs->ns * sizeof(double));
+    for (int part = 0; part < 2; part++)
+    {
+        // column m of the file holds nmax_file + 1 - m values; the first
+        // nmax + 1 - m of the columns m <= nmax are kept
+        bool ok = true;
+        for (unsigned long m = 0; ok && m <= nmax_file; m++)
+        {
+            const long len = (long)(nmax_file + 1 - m);
+            if (m <= nmax)
+            {
+                double *col = part ? shcs->s[m] : shcs->c[m];
+                const size_t nread = (size_t)(nmax + 1 - m);
+                ok = fread(col, sizeof(double), nread, fp) == nread &&
+                     fseek(fp, (len - (long)nread) * (long)sizeof(double),
+                           SEEK_CUR) == 0;
+            }
+            else
+                ok = fseek(fp, len * (long)sizeof(double), SEEK_CUR) == 0;
+        }
+        if (!ok)
+        {
+            SET_ERR(err, CHARM_EFILEIO,
+                    part ? "Failed to read the \"S\" coefficients."
+                         : "Failed to read the \"C\" coefficients.");
+            goto EXIT;
+        }
+    }
+EXIT:
+    fclose(fp);
+    return nmax_file;
+}
+
+void charm_shc_write_bin(const charm_shc *shcs, unsigned long nmax,
+                         const char *pathname, charm_err *err)
+{
+    FILE *fp = fopen(pathname, "wb");
+    if (!fp)
+    {
+        char msg[CHARM_ERR_MAX_MSG];
+        snprintf(msg, sizeof msg, "Couldn't create \"%s\".", pathname);
+        SET_ERR(err, CHARM_EFILEIO, msg);
+        return;
+    }
+    if (nmax > shcs->nmax)
+        SET_ERR(err, CHARM_EFUNCARG,
+                "Not enough coefficients in \"shcs\" to write up to degree "
+                "\"nmax\".");
+    else if (fwrite(&nmax, sizeof nmax, 1, fp) != 1)
+        SET_ERR(err, CHARM_EFILEIO,
+                "Failed to write the maximum harmonic degree.");
+    else if (fwrite(&shcs->mu, sizeof(double), 1, fp) != 1)
+        SET_ERR(err, CHARM_EFILEIO, "Failed to write the scaling parameter.");
+    else if (fwrite(&shcs->r, sizeof(double), 1, fp) != 1)
+        SET_ERR(err, CHARM_EFILEIO,
+                "Failed to write the radius of the reference sphere.");
+    else
+    {
+        for (int part = 0; part < 2; part++)
+        {
+            bool ok = true;
+            for (unsigned long m = 0; ok && m <= nmax; m++)
+            {
+                const double *col = part ? shcs->s[m] : shcs->c[m];
+                const size_t n = (size_t)(nmax + 1 - m);
+                ok = fwrite(col, sizeof(double), n, fp) == n;
+            }
+            if (!ok)
+            {
+                SET_ERR(err, CHARM_EFILEIO,
+                        part ? "Failed to write the \"S\" coefficients)."
+                             : "Failed to write the \"C\" coefficients).");
+                break;
+            }
+        }
+    }
+    fclose(fp);
+}
+
+// ---------------------------------------------------------------------------
 // Cells: src/shs/shs_cell.c:22-121, src/sha/sha_cell.c:37-100
 // ---------------------------------------------------------------------------
 static bool check_nmax_cell(const charm_shc *shcs, unsigned long nmax,
@@ -829,6 +962,19 @@ void charm_b200_shs_point_dev(const charm_point *pnt, unsigned long shc_nmax,
                              kgrad ? kgrad : (int)dr,
                              kgrad ? kgrad : (int)dlat,
                              kgrad ? kgrad : (int)dlon, d_f));
+}
+
+unsigned long charm_b200_shc_read_bin_dev(const char *pathname,
+                                          unsigned long nmax,
+                                          unsigned long shc_nmax, double *d_c,
+                                          double *d_s, double *mu, double *r,
+                                          charm_err *err)
+{
+    unsigned long nmax_file = CHARM_SHC_NMAX_ERROR;
+    cb::Status st = cb::shc_read_bin_dev(pathname, nmax, shc_nmax, d_c, d_s,
+                                         mu, r, &nmax_file);
+    report(err, __func__, st);
+    return st.ok() ? nmax_file : CHARM_SHC_NMAX_ERROR;
 }
 
 void charm_b200_shs_cell_dev(const charm_cell *cell, unsigned long shc_nmax,

@@ -570,46 +570,77 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                     cell_seed(R[k], A.sg[2 * m], (int)A.sg[2 * m + 1], u1, u2,
                               m, valid ? A.imm[(size_t)m * np + p] : 0.0);
                     any_scaled |= (R[k].E1 | R[k].E2) != 0;
+                    // state before degree m: (x, y) = (0, R~_mm) and
+                    // J0 = -J~_mm, so that the step of degree m with the
+                    // staged beta = -1, h = 1, 1/(n+1) = 0 yields R~_mm and
+                    // J~_mm: every degree takes the same step
+                    R[k].y1 = R[k].x1;
+                    R[k].x1 = 0.0;
+                    R[k].y2 = R[k].x2;
+                    R[k].x2 = 0.0;
+                    R[k].J0 = -R[k].J1;
+                    R[k].J1 = 0.0;
                 }
             }
             if (__all_sync(0xffffffffu, all_skip))
                 continue;
             any_scaled = __any_sync(0xffffffffu, any_scaled);
-            for (int j = 0; j < nchunks; j++)
-            {
-                const int cnt = (int)min((long long)LEG_CHUNK,
-                                         ncol - (long long)j * LEG_CHUNK);
-                stage_chunk(S, A, c0, m, j, cnt, lane);
-                if (j > 0 && m > 0)
-                {
-                    const double mul = A.tmul[(size_t)m * A.ldmul + j];
+            // lane partial sums of degree jj of a 32-degree block: row jj,
+            // column lane of the swizzled transpose
+            auto put = [&](int jj, double vc, double vs) {
+                red[jj * 32 + ((int)lane ^ jj)] = make_double2(vc, vs);
+            };
+            // lane l: the warp total of degree n0 + l added to the group's
+            // running column (loaded before the block, so that its latency
+            // hides behind the block)
+            auto flush = [&](long long i_l, double2 prev) {
+                __syncwarp();
+                const double2 *row = red + lane * 32;
+                double oc0 = 0.0, os0 = 0.0, oc1 = 0.0, os1 = 0.0;
 #pragma unroll
-                    for (int k = 0; k < K; k++)
-                        R[k].scale(mul);
-                }
-                for (int half = 0; half < 2; half++)
+                for (int q = 0; q < 32; q += 2)
                 {
-                    const int ib = 32 * half;
-                    if (ib >= cnt)
-                        break;
-                    // the group's running sum of degree n0 + lane, loaded
-                    // now so that its latency hides behind the block
-                    const long long i_l = (long long)j * LEG_CHUNK + ib + lane;
-                    double2 prev = make_double2(0.0, 0.0);
-                    if (stored && i_l < ncol)
-                        prev = col[i_l];
-#pragma unroll 4
-                    for (int jj = 0; jj < 32; jj++)
+                    const double2 a = row[q ^ (int)lane];
+                    const double2 b = row[(q + 1) ^ (int)lane];
+                    oc0 += a.x;
+                    os0 += a.y;
+                    oc1 += b.x;
+                    os1 += b.y;
+                }
+                __syncwarp();
+                const double outc = oc0 + oc1, outs = os0 + os1;
+                if (i_l < ncol)
+                    col[i_l] = stored ? make_double2(prev.x + outc,
+                                                     prev.y + outs)
+                                      : make_double2(outc, outs);
+            };
+            if (m == 0)
+            {
+                // zonal: un-normalised polynomials (sha_cell.c:880-960);
+                // the partial sums carry I_n0 / ct_n (k_sha_reduce applies
+                // ct_n)
+                for (int j = 0; j < nchunks; j++)
+                {
+                    const int cnt = (int)min((long long)LEG_CHUNK,
+                                             ncol - (long long)j * LEG_CHUNK);
+                    for (int half = 0; half < 2; half++)
                     {
-                        const int i = ib + jj;
-                        const long long kk = (long long)j * LEG_CHUNK + i;
-                        const bool odd = (jj & 1) != 0;
-                        double vc = 0.0, vs = 0.0;
-                        if (i < cnt)
+                        const int ib = 32 * half;
+                        if (ib >= cnt)
+                            break;
+                        const long long i_l =
+                            (long long)j * LEG_CHUNK + ib + lane;
+                        double2 prev = make_double2(0.0, 0.0);
+                        if (stored && i_l < ncol)
+                            prev = col[i_l];
+                        for (int jj = 0; jj < 32; jj++)
                         {
-                            if (m == 0)
+                            const long long kk =
+                                (long long)j * LEG_CHUNK + ib + jj;
+                            double vc = 0.0;
+                            if (kk < ncol)
                             {
-                                const double rct = 1.0 / A.tc[c0 + kk];
+                                const double rct = 1.0 / A.tc[kk];
                                 const double4 z =
                                     kk > 0 ? A.zn[kk]
                                            : make_double4(0.0, 0.0, 0.0, 0.0);
@@ -634,56 +665,72 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                                         p0b[k] = p1b[k];
                                         p1b[k] = p2b;
                                     }
-                                    const double v = in0 * rct;
-                                    vc = fma(v, odd ? amm[k] : amp[k], vc);
+                                    vc = fma(in0 * rct,
+                                             (kk & 1) ? amm[k] : amp[k], vc);
                                 }
                             }
-                            else if (kk == 0)
-                            {
-#pragma unroll
-                                for (int k = 0; k < K; k++)
-                                {
-                                    vc = fma(R[k].J1, amp[k], vc);
-                                    vs = fma(R[k].J1, bmp[k], vs);
-                                }
-                            }
-                            else
-                            {
-                                const double beta = S.tb[i].x;
-                                const double2 h = S.hn[i];
-                                const double hb = h.x * beta;
-#pragma unroll
-                                for (int k = 0; k < K; k++)
-                                {
-                                    const double v = R[k].step(beta, hb, h.y);
-                                    vc = fma(v, odd ? amm[k] : amp[k], vc);
-                                    vs = fma(v, odd ? bmm[k] : bmp[k], vs);
-                                }
-                            }
+                            put(jj, vc, 0.0);
                         }
-                        red[jj * 32 + ((int)lane ^ jj)] = make_double2(vc, vs);
+                        flush(i_l, prev);
                     }
-                    __syncwarp();
-                    const double2 *row = red + lane * 32;
-                    double oc0 = 0.0, os0 = 0.0, oc1 = 0.0, os1 = 0.0;
-#pragma unroll
-                    for (int q = 0; q < 32; q += 2)
-                    {
-                        const double2 a = row[q ^ (int)lane];
-                        const double2 b = row[(q + 1) ^ (int)lane];
-                        oc0 += a.x;
-                        os0 += a.y;
-                        oc1 += b.x;
-                        os1 += b.y;
-                    }
-                    __syncwarp();
-                    const double outc = oc0 + oc1, outs = os0 + os1;
-                    if (i_l < ncol)
-                        col[i_l] = stored ? make_double2(prev.x + outc,
-                                                         prev.y + outs)
-                                          : make_double2(outc, outs);
                 }
-                if (m > 0 && any_scaled)
+                stored = true;
+                continue;
+            }
+            for (int j = 0; j < nchunks; j++)
+            {
+                const int cnt = (int)min((long long)LEG_CHUNK,
+                                         ncol - (long long)j * LEG_CHUNK);
+                stage_chunk(S, A, c0, m, j, cnt, lane);
+                if (j == 0)
+                {
+                    // the seed step (see above)
+                    if (lane == 0)
+                    {
+                        S.tb[0].x = -1.0;
+                        S.hn[0] = make_double2(1.0, 0.0);
+                    }
+                    __syncwarp();
+                }
+                else
+                {
+                    const double mul = A.tmul[(size_t)m * A.ldmul + j];
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        R[k].scale(mul);
+                }
+                for (int half = 0; half < 2; half++)
+                {
+                    const int ib = 32 * half;
+                    if (ib >= cnt)
+                        break;
+                    const long long i_l = (long long)j * LEG_CHUNK + ib + lane;
+                    double2 prev = make_double2(0.0, 0.0);
+                    if (stored && i_l < ncol)
+                        prev = col[i_l];
+                    // degrees beyond nmax read beta = h = 1/(n+1) = 0 and
+                    // contribute J = 0
+#pragma unroll 4
+                    for (int jj = 0; jj < 32; jj++)
+                    {
+                        const int i = ib + jj;
+                        const double beta = S.tb[i].x;
+                        const double2 h = S.hn[i];
+                        const double hb = h.x * beta;
+                        const bool odd = (jj & 1) != 0;
+                        double vc = 0.0, vs = 0.0;
+#pragma unroll
+                        for (int k = 0; k < K; k++)
+                        {
+                            const double v = R[k].step(beta, hb, h.y);
+                            vc = fma(v, odd ? amm[k] : amp[k], vc);
+                            vs = fma(v, odd ? bmm[k] : bmp[k], vs);
+                        }
+                        put(jj, vc, vs);
+                    }
+                    flush(i_l, prev);
+                }
+                if (any_scaled)
                 {
                     bool still = false;
 #pragma unroll

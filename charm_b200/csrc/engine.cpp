@@ -2708,7 +2708,6 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                                                 G >= 3 ? 3 : 2, bands)
                                    : 1;
     bool ordered = false;
-    bool fused = false;   // the analysis kernel reduced the groups itself
     if (nband > 1)
     {
         // orders of the last band in up to four bands of about equal
@@ -2826,27 +2825,6 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         }
         else
             CB_TRY(rows_fft(0, (int)nlat));
-        // one launch over all groups: the last group of each order to
-        // finish sums the order's partial columns (no separate reduction
-        // pass over the partial sums)
-        unsigned *mcount = nullptr;
-        CB_TRY(dbuf(c, "sha_mcount", (size_t)nmax + 1, &mcount));
-        CB_CUDA(cudaMemsetAsync(mcount, 0, ((size_t)nmax + 1) * sizeof(unsigned),
-                                c.stream), st);
-        if (sn > nmax)
-        {
-            const size_t Tn = (size_t)(sn + 1) * (sn + 2) / 2;
-            CB_CUDA(cudaMemsetAsync(oc, 0, Tn * 8, c.stream), st);
-            CB_CUDA(cudaMemsetAsync(os, 0, Tn * 8, c.stream), st);
-        }
-        A.m_count = mcount;
-        A.tc = tab.tc;
-        A.rescale = dres;
-        A.scale = 1.0;
-        A.shc_nmax = (long long)sn;
-        A.out_c = oc;
-        A.out_s = os;
-        fused = true;
         int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                             (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
@@ -2858,7 +2836,6 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
         CB_CUDA(cudaStreamSynchronize(c.copy_stream), st);
         return finish(c, d_status);
     }
-    if (!fused)
     {
         Scope sc(c, TIMER_PREP);
         CB_CUDA(launch_sha_reduce((long long)nmax, (long long)sn, (int)G, T,
@@ -3511,6 +3488,146 @@ Status sha_cell_grid(Context &c, const charm_cell *cell, const double *f_host,
 }
 
 // ---------------------------------------------------------------------------
+// Coefficient files streamed to the device
+// ---------------------------------------------------------------------------
+// A binary coefficient file (src/shc/shc_read_bin.c layout) into device
+// triangles of degree shc_nmax.  The destination of a range of orders is
+// contiguous in the order-major triangle, so each chunk of orders is laid
+// out in a page-locked buffer exactly as on the device (the file's first
+// nmax + 1 - m values of column m, zeros up to shc_nmax) and copied with one
+// call; two buffers alternate, so that reading chunk k + 1 from the file
+// overlaps the copy of chunk k.
+Status shc_read_bin_dev_impl(Context &c, const char *path, unsigned long nmax,
+                             unsigned long shc_nmax, double *d_c, double *d_s,
+                             double *mu, double *r, unsigned long *nmax_file)
+{
+    Status st;
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp)
+    {
+        st.code = CHARM_EFILEIO;
+        st.msg = std::string("Couldn't open \"") + path + "\".";
+        return st;
+    }
+    struct Closer
+    {
+        FILE *f;
+        ~Closer() { std::fclose(f); }
+    } closer{fp};
+    unsigned long nf = 0;
+    double hdr[2];
+    if (std::fread(&nf, sizeof nf, 1, fp) != 1 ||
+        std::fread(hdr, sizeof(double), 2, fp) != 2)
+    {
+        st.code = CHARM_EFILEIO;
+        st.msg = "Failed to read the header of the coefficient file.";
+        return st;
+    }
+    if (nmax > nf)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "Not enough coefficients in the input file for the maximum "
+                 "harmonic degree \"nmax\".";
+        return st;
+    }
+    if (nmax > shc_nmax)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "\"nmax\" cannot be larger than \"shc_nmax\".";
+        return st;
+    }
+    *nmax_file = nf;
+    *mu = hdr[0];
+    *r = hdr[1];
+    constexpr size_t CHUNK = 4u << 20;   // doubles per buffer (32 MB)
+    void *hp = nullptr;
+    CB_TRY(pinned(c, 2 * CHUNK * sizeof(double), &hp));
+    double *buf[2] = {static_cast<double *>(hp),
+                      static_cast<double *>(hp) + CHUNK};
+    // the copy stream starts after the work already on the stream (buffers
+    // the caller may still read)
+    CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
+    CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+    bool used[2] = {false, false};
+    int nb = 0;
+    for (int part = 0; part < 2; part++)
+    {
+        double *dst = part ? d_s : d_c;
+        long long m = 0;
+        while (m <= (long long)shc_nmax)
+        {
+            // orders [m, m1) of this chunk
+            long long m1 = m;
+            size_t len = 0;
+            while (m1 <= (long long)shc_nmax &&
+                   (len == 0 || len + (size_t)(shc_nmax + 1 - m1) <= CHUNK))
+            {
+                len += (size_t)(shc_nmax + 1 - m1);
+                m1++;
+            }
+            if (len > CHUNK)
+            {
+                st.code = CHARM_EFUNCARG;
+                st.msg = "A coefficient column exceeds the staging buffer.";
+                return st;
+            }
+            const int b = nb & 1;
+            if (used[b])
+                CB_CUDA(cudaEventSynchronize(c.band_ev[b]), st);
+            double *h = buf[b];
+            size_t o = 0;
+            for (long long mm = m; mm < m1; mm++)
+            {
+                const size_t col = (size_t)(shc_nmax + 1 - mm);
+                size_t got = 0;
+                if (mm <= (long long)nmax)
+                {
+                    got = (size_t)(nmax + 1 - mm);
+                    if (std::fread(h + o, sizeof(double), got, fp) != got ||
+                        (nf > nmax &&
+                         std::fseek(fp, (long)((nf - nmax) * sizeof(double)),
+                                    SEEK_CUR) != 0))
+                    {
+                        st.code = CHARM_EFILEIO;
+                        st.msg = part ? "Failed to read the \"S\" coefficients."
+                                      : "Failed to read the \"C\" coefficients.";
+                        return st;
+                    }
+                }
+                std::memset(h + o + got, 0, (col - got) * sizeof(double));
+                o += col;
+            }
+            CB_CUDA(cudaMemcpyAsync(dst + tri_start((long long)shc_nmax, m), h,
+                                    len * sizeof(double),
+                                    cudaMemcpyHostToDevice, c.copy_stream),
+                    st);
+            CB_CUDA(cudaEventRecord(c.band_ev[b], c.copy_stream), st);
+            used[b] = true;
+            nb++;
+            m = m1;
+        }
+        // the file position of the next part: the rest of this part's
+        // columns (the file's columns m hold nf + 1 - m values; the loop
+        // read the first nmax + 1 - m of the columns m <= nmax)
+        if (part == 0)
+        {
+            const long long Tf = (long long)(nf + 1) * (nf + 2) / 2;
+            const long off = (long)(sizeof(unsigned long) +
+                                    2 * sizeof(double) +
+                                    (size_t)Tf * sizeof(double));
+            if (std::fseek(fp, off, SEEK_SET) != 0)
+            {
+                st.code = CHARM_EFILEIO;
+                st.msg = "Failed to read the \"S\" coefficients.";
+                return st;
+            }
+        }
+    }
+    CB_CUDA(cudaStreamSynchronize(c.copy_stream), st);
+    return st;
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free analysis (charm_b200_sha_point_dev_static)
 // ---------------------------------------------------------------------------
 // The same kernels as sha_grid with the row transform of rfft.cu, every
@@ -3944,6 +4061,16 @@ Status sha_cell_dev(const charm_cell *cell, const double *d_f,
     CB_TRY(init(g_ctx));
     return sha_cell_grid(g_ctx, cell, nullptr, d_f, nmax, mu, r, shc_nmax,
                          nullptr, nullptr, d_c, d_s);
+}
+
+Status shc_read_bin_dev(const char *path, unsigned long nmax,
+                        unsigned long shc_nmax, double *d_c, double *d_s,
+                        double *mu, double *r, unsigned long *nmax_file)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return shc_read_bin_dev_impl(g_ctx, path, nmax, shc_nmax, d_c, d_s, mu, r,
+                                 nmax_file);
 }
 
 Status sha_point_dev_band(const charm_point *pnt, const double *d_f,

@@ -72,6 +72,11 @@ Status sha_cell(const charm_cell *cell, const double *f, unsigned long nmax,
 Status sha_cell_dev(const charm_cell *cell, const double *d_f,
                     unsigned long nmax, double mu, double r,
                     unsigned long shc_nmax, double *d_c, double *d_s);
+// A coefficient file in CHarm's binary format streamed into device
+// triangles of degree shc_nmax (charm_b200_shc_read_bin_dev).
+Status shc_read_bin_dev(const char *path, unsigned long nmax,
+                        unsigned long shc_nmax, double *d_c, double *d_s,
+                        double *mu, double *r, unsigned long *nmax_file);
 Status sha_point_dev_band(const charm_point *pnt, const double *d_f,
                           unsigned long nmax, double mu, double r,
                           unsigned long shc_nmax, int pair0, int pair1,

@@ -102,19 +102,6 @@ struct ShaGridArgs
     const double *r;       // radius per point (read when r != R)
     const double *g;       // weight of each point's value
     double R;              // reference radius of the coefficients
-    // Reduction of the groups by the last arriving work item of an order
-    // (instead of k_sha_reduce): with m_count non-null, every item adds 1
-    // to m_count[m] once its partial column is written; the item that
-    // completes the order sums the groups' columns in group order, applies
-    // ct_n * scale * rescale[n] and writes degrees m..nmax of order m into
-    // out_c, out_s (triangles of degree shc_nmax; the caller zeroes the
-    // rest).  Requires group0 == 0 and all groups in this launch.
-    unsigned *m_count;
-    const double *tc;
-    const double *rescale;
-    double scale;
-    long long shc_nmax;
-    double *out_c, *out_s;
 };
 
 // Block-mean values in cells (cell.cu).  Grid synthesis and analysis run

@@ -378,46 +378,6 @@ __global__ void __launch_bounds__(128, sha_min_blocks(K)) k_sha_grid(ShaGridArgs
             for (long long n = m + lane; n <= N; n += 32)
                 col[n - m] = make_double2(0.0, 0.0);
         }
-        if (A.m_count)
-        {
-            // the last of the order's groups reduces it (release: the
-            // column is visible before the count; acquire: the other
-            // groups' columns are read from L2, past this SM's L1)
-            __threadfence();
-            __syncwarp();
-            unsigned prev = 0;
-            if (lane == 0)
-                prev = atomicAdd(&A.m_count[m], 1u);
-            prev = __shfl_sync(0xffffffffu, prev, 0);
-            if (prev == (unsigned)A.ngroups - 1)
-            {
-                __threadfence();
-                const double2 *p0 = A.part + c0;
-                const long long d0 = tri_col0(A.shc_nmax, m);
-                for (long long n = m + lane; n <= N; n += 32)
-                {
-                    double vc = 0.0, vs = 0.0;
-                    for (int gg = 0; gg < A.ngroups; gg++)
-                    {
-                        const double2 v =
-                            __ldcg(p0 + (size_t)gg * (size_t)tri_size(N) +
-                                   (n - m));
-                        vc += v.x;
-                        vs += v.y;
-                    }
-                    double k = A.tc[c0 + n - m] * A.scale;
-                    vc *= k;
-                    vs *= k;
-                    if (A.rescale)
-                    {
-                        vc *= A.rescale[n];
-                        vs *= A.rescale[n];
-                    }
-                    A.out_c[d0 + n - m] = vc;
-                    A.out_s[d0 + n - m] = vs;
-                }
-            }
-        }
     }
 }
 

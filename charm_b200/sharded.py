@@ -28,7 +28,7 @@ import numpy as np
 from .replicas import split_range
 
 __all__ = ["grid_pairs", "band_rows", "sharded_synthesis",
-           "sharded_analysis", "gpu_engine"]
+           "sharded_analysis", "gpu_engine", "coefficients_from_file"]
 
 
 def _dist():
@@ -94,6 +94,65 @@ def sharded_analysis(npairs, analyse_band, group=None):
         dist.all_reduce(c, group=group)
         dist.all_reduce(s, group=group)
     return c, s
+
+
+def coefficients_from_file(path, nmax, device, group=None):
+    """(c, s, mu, r) of a coefficient file in CHarm's binary format
+    (charm_shc_read_bin), read by rank 0 and broadcast to every rank of the
+    group: c, s are order-major triangles of degree nmax on `device`.  On a
+    CUDA device rank 0 streams the file straight into device memory
+    (charm_b200_shc_read_bin_dev: chunks of orders through page-locked
+    buffers, the disk reads overlapping the copies); on the CPU it reads
+    the host triangles with charm_shc_read_bin."""
+    import torch
+    from . import pyharm
+    from ._lib import _libcharm as L
+    dist = _dist()
+    rank, _ = _rank_world(group)
+    T = (int(nmax) + 1) * (int(nmax) + 2) // 2
+    c = torch.zeros(T, dtype=torch.float64, device=device)
+    s = torch.zeros(T, dtype=torch.float64, device=device)
+    # mu, r and 1 when rank 0 read the file (every rank learns of a failed
+    # read before it waits for the triangles)
+    hdr = torch.zeros(3, dtype=torch.float64, device=device)
+    msg = None
+    if rank == 0:
+        err = L.charm_err_init()
+        if torch.device(device).type == "cuda":
+            P = ct.c_void_p
+            L.charm_b200_shc_read_bin_dev.restype = ct.c_ulong
+            L.charm_b200_shc_read_bin_dev.argtypes = [
+                ct.c_char_p, ct.c_ulong, ct.c_ulong, P, P,
+                ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), P]
+            mu, r = ct.c_double(), ct.c_double()
+            L.charm_b200_shc_read_bin_dev(str(path).encode(), int(nmax),
+                                          int(nmax), c.data_ptr(),
+                                          s.data_ptr(), ct.byref(mu),
+                                          ct.byref(r), ct.cast(err, P))
+            hdr[0], hdr[1] = mu.value, r.value
+        else:
+            L.charm_shc_read_bin.restype = ct.c_ulong
+            L.charm_shc_read_bin.argtypes = [ct.c_char_p, ct.c_ulong,
+                                             ct.c_void_p, ct.c_void_p]
+            shc = pyharm.Shc(int(nmax), 1.0, 1.0)
+            L.charm_shc_read_bin(str(path).encode(), int(nmax),
+                                 ct.cast(shc._Shc, ct.c_void_p),
+                                 ct.cast(err, ct.c_void_p))
+            c.copy_(torch.from_numpy(shc.c))
+            s.copy_(torch.from_numpy(shc.s))
+            hdr[0], hdr[1] = shc.mu, shc.r
+        if not L.charm_err_isempty(err):
+            msg = ct.string_at(err.contents.msg).decode()
+        L.charm_err_free(err)
+        hdr[2] = 0.0 if msg else 1.0
+    if dist is not None:
+        dist.broadcast(hdr, src=0, group=group)
+    if float(hdr[2]) != 1.0:
+        raise pyharm.CHarmError(msg or "rank 0 failed to read %s" % path)
+    if dist is not None:
+        dist.broadcast(c, src=0, group=group)
+        dist.broadcast(s, src=0, group=group)
+    return c, s, float(hdr[0]), float(hdr[1])
 
 
 def gpu_engine(pnt, nmax, mu, r):

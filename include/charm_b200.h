@@ -17,6 +17,7 @@
 #define CHARM_B200_H
 
 #include <stddef.h>
+#include <limits.h>
 
 #ifdef __cplusplus
 /* C's _Bool and C++'s bool share size and representation on the supported
@@ -199,6 +200,24 @@ CHARM_EXTERN charm_shc * CHARM_CDECL charm_shc_init(unsigned long nmax,
                                                     double *c, double *s);
 CHARM_EXTERN void CHARM_CDECL charm_shc_free(charm_shc *shcs);
 
+/* Coefficient files in CHarm's binary format: src/shc/shc.h.in:98-108
+ * (constants), :628-722 (charm_shc_read_bin), the writer's counterpart
+ * (src/shc/shc_write_bin.c).  The file holds nmax (unsigned long), mu, r
+ * (double) and the order-major columns of C, then of S, column m with
+ * nmax + 1 - m values.  nmax = CHARM_SHC_NMAX_MODEL with shcs = NULL only
+ * reads the file's maximum degree, which every successful call returns;
+ * CHARM_SHC_NMAX_ERROR on error. */
+#define CHARM_SHC_NMAX_MODEL (ULONG_MAX - 1UL)
+#define CHARM_SHC_NMAX_ERROR (ULONG_MAX)
+CHARM_EXTERN unsigned long CHARM_CDECL charm_shc_read_bin(const char *pathname,
+                                                          unsigned long nmax,
+                                                          charm_shc *shcs,
+                                                          charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_shc_write_bin(const charm_shc *shcs,
+                                                  unsigned long nmax,
+                                                  const char *pathname,
+                                                  charm_err *err);
+
 /* ------------------------------------------------------------------------- */
 /* Synthesis: src/shs/shs.h.in:168-173, :239-244, :344-349, :428-435          */
 /* ------------------------------------------------------------------------- */
@@ -294,6 +313,17 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_sha_cell_dev(
     const charm_cell *cell, const double *d_f, unsigned long nmax, double mu,
     double r, unsigned long shc_nmax, double *d_c, double *d_s,
     charm_err *err);
+
+/* A binary coefficient file (charm_shc_read_bin's format) streamed into
+ * device triangles d_c, d_s of degree shc_nmax (CHarm's order-major layout,
+ * zero above nmax): the columns are read in chunks into two page-locked
+ * buffers, each chunk copied to the device while the next one is read.
+ * *mu and *r receive the file's values.  Returns the file's maximum degree,
+ * or CHARM_SHC_NMAX_ERROR with err set (file I/O: CHARM_EFILEIO; nmax above
+ * the file's or above shc_nmax: CHARM_EFUNCARG). */
+CHARM_EXTERN unsigned long CHARM_CDECL charm_b200_shc_read_bin_dev(
+    const char *pathname, unsigned long nmax, unsigned long shc_nmax,
+    double *d_c, double *d_s, double *mu, double *r, charm_err *err);
 
 /* Analysis with the grid values (d_f, nlat x nlon) and the output triangles
  * (degree shc_nmax, zero above nmax) in device memory; the coefficients

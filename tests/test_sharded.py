@@ -104,3 +104,68 @@ def test_two_gloo_ranks_shard_latitude_bands():
         flat = sorted(r for rows in all_rows for r in rows)
         assert flat == list(range(nlat))       # every row exactly once
         assert npairs == (nlat + 1) // 2
+
+
+def _file_worker(rank, world, port, path, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                      RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+    from charm_b200.sharded import coefficients_from_file
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        c, s, mu, r = coefficients_from_file(path, 30, "cpu")
+        # a failed read on rank 0 reaches every rank as an error
+        try:
+            coefficients_from_file(path + ".missing", 30, "cpu")
+            failed = False
+        except Exception:
+            failed = True
+        q.put((rank, c.numpy().copy(), s.numpy().copy(), mu, r, failed))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_coefficients_from_file(tmp_path):
+    """A binary coefficient file read by rank 0 and broadcast: every rank
+    holds rank 0's triangles (the file's first 30 degrees), mu and r."""
+    import ctypes as ct
+    import charm_b200.pyharm as ph
+    from charm_b200._lib import _libcharm as L
+    nmax = 40
+    T = (nmax + 1) * (nmax + 2) // 2
+    rng = np.random.default_rng(3)
+    c = rng.standard_normal(T)
+    s = rng.standard_normal(T)
+    s[:nmax + 1] = 0.0
+    shc = ph.Shc(nmax, 3.986e14, 6378136.3, c, s)
+    path = str(tmp_path / "m.shcs")
+    L.charm_shc_write_bin.argtypes = [ct.c_void_p, ct.c_ulong, ct.c_char_p,
+                                      ct.c_void_p]
+    err = L.charm_err_init()
+    L.charm_shc_write_bin(ct.cast(shc._Shc, ct.c_void_p), nmax, path.encode(),
+                          ct.cast(err, ct.c_void_p))
+    assert L.charm_err_isempty(err)
+    L.charm_err_free(err)
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_file_worker, args=(r, world, port, path, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=180) for _ in range(world)),
+                 key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    want_c = np.concatenate([c[m * (2 * nmax + 3 - m) // 2:
+                               m * (2 * nmax + 3 - m) // 2 + 31 - m]
+                             for m in range(31)])
+    for rank, rc, rs, mu, r, failed in res:
+        assert np.array_equal(rc, want_c)
+        assert mu == 3.986e14 and r == 6378136.3
+        assert failed
+    assert np.array_equal(res[0][2], res[1][2])
