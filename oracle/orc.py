@@ -884,3 +884,83 @@ def sha_cell(cell, f, nmax, mu, r, shc_nmax=None, polar_thr=POLAR_OFF):
             out.c[sl] *= tmp[m:]
             out.s[sl] *= tmp[m:]
     return out
+
+
+# ---------------------------------------------------------------------------
+# Spectral gravity forward modelling, global variant
+# (src/gfm/gfm_sgfm.c with SGFM_GLOBAL, gfm_global_density_*.c)
+# ---------------------------------------------------------------------------
+def global_vnmc(nmax, p, i, c):
+    """gfm_sgfm.c global_vnmc: c * binomial-type factor of degree n."""
+    out = np.zeros(nmax + 1)
+    pr = float(p)
+    for n in range(nmax + 1):
+        npip3 = float(n + i + 3)
+        snpi = npip3 / pr
+        for pt in range(1, p):
+            snpi *= (npip3 - float(pt)) / (pr - float(pt))
+        snpi *= 2.0 / ((2.0 * float(n) + 1.0) * npip3)
+        out[n] = c * snpi
+    return out
+
+
+def gfm_global(shape, shape_nmax, R, density, density_nmax, G, mass, pmin,
+               pmax, nmax_pot, const_density=None):
+    """The potential coefficients of charm_gfm_global_density_3d (density:
+    list of Shc, density_nmax: list), _lateral (one density) or _const
+    (const_density, density None).  Returns an Shc of degree nmax_pot with
+    mu = G mass and r = R."""
+    out = Shc(nmax_pot, G * mass, R)
+    if const_density is None:
+        imax = len(density) - 1
+        # get_max_nmax(density_nmax, density_order): the first
+        # density_order entries (gfm_sgfm.c)
+        dmax = density_nmax[0]
+        for k in range(1, imax):
+            dmax = max(dmax, density_nmax[k])
+    else:
+        imax = 0
+        dmax = 0
+    c = (2.0 * PI * R ** 3) / mass
+    if const_density is not None:
+        c *= const_density
+    col_pot = tri_col0(nmax_pot)
+    for p in range(pmin, pmax + 1):
+        nmaxp = p * shape_nmax + dmax
+        thr = min(nmaxp, nmax_pot)
+        g = gl(nmaxp, 1.0)
+        fshape = shs_point(g, shape, shape_nmax)[0] - R
+        Ri = 1.0
+        for i in range(imax + 1):
+            s_ij = fshape / R
+            sp = s_ij.copy()
+            for _ in range(2, p + 1):
+                sp = sp * s_ij
+            if const_density is None:
+                rho = shs_point(g, density[i], density_nmax[i])[0]
+                rho = rho * (sp * Ri)
+                Ri *= R
+            else:
+                rho = sp
+            a = sha_point(g, rho.reshape(g.nlat, g.nlon), thr, 1.0, 1.0)
+            v = global_vnmc(thr, p, i, c)
+            col = tri_col0(thr)
+            for m in range(thr + 1):
+                sl = slice(col[m], col[m] + thr + 1 - m)
+                dl = slice(col_pot[m], col_pot[m] + thr + 1 - m)
+                out.c[dl] += a.c[sl] * v[m:]
+                out.s[dl] += a.s[sl] * v[m:]
+    return out
+
+
+def shc_da(shc, nmax):
+    """src/shc/shc_da.c: degree amplitudes sqrt(sum_m C_nm^2 + S_nm^2)."""
+    col = tri_col0(shc.nmax)
+    out = np.zeros(nmax + 1)
+    for n in range(nmax + 1):
+        v = 0.0
+        for m in range(n + 1):
+            i = col[m] + n - m
+            v += shc.c[i] * shc.c[i] + shc.s[i] * shc.s[i]
+        out[n] = math.sqrt(v)
+    return out

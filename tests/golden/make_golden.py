@@ -14,8 +14,14 @@ Sources (CHarm 0.4.9):
                                           (tests/check_sha_cell.c)
   data/tests/{double,quad}/crd_*.txt     GL/DH grid nodes and weights
                                           (tests/check_crd_point_quad.c)
+  data/tests/double/gfm_sgfm_g_*.txt     degree amplitudes of the global
+                                          gravity forward modelling tests
+                                          (tests/check_gfm_sgfm_all.c.in)
   data/input/EGM96-degree10-mtx.txt      input coefficients of those tests
                                           (tests/parameters.h:46-48)
+  data/input/MoonTopo2600p_to10-tbl.txt, the lunar shape and density
+  data/input/moon-rho{0,1}_to10.tbl      inputs of the gfm tests
+                                          (tests/parameters.h:298-306)
 
 Outputs:
   charm_golden_double.npz  every hot-path golden file as float64
@@ -53,7 +59,7 @@ def pack(path, table):
                         offsets=offsets, data=data)
 
 
-HOT = re.compile(r"^(shs_p_|shs_c_nx|sha_c_nx|crd_nx).*\.txt$")
+HOT = re.compile(r"^(shs_p_|shs_c_nx|sha_c_nx|crd_nx|gfm_sgfm_g_).*\.txt$")
 GRAD_SUFFIX = re.compile(r"_(x|y|z|xx|xy|xz|yy|yz|zz|guru\d+)\.txt$")
 
 
@@ -113,6 +119,30 @@ def main():
         nmax=np.array(nmax), mu=np.array(float(mu_s)), r=np.array(float(r_s)),
         mu_q=np.array(dd(mu_s)), r_q=np.array(dd(r_s)),
         c=c, s=s, c_q=cq, s_q=sq)
+    # the gfm tests' inputs in the "tbl" layout
+    # (src/shc/shc_read_tbl.c: "nmax mu r", then lines "n m C S")
+    moon = {}
+    for key, name in (("shape", "MoonTopo2600p_to10-tbl.txt"),
+                      ("rho0", "moon-rho0_to10.tbl"),
+                      ("rho1", "moon-rho1_to10.tbl")):
+        with open(os.path.join(ref, "data/input", name)) as fh:
+            toks = fh.read().split()
+        nm = int(toks[0])
+        T = (nm + 1) * (nm + 2) // 2
+        cc = np.zeros(T)
+        ss = np.zeros(T)
+        vals = toks[3:]
+        for k in range(0, len(vals), 4):
+            n, m = int(vals[k]), int(vals[k + 1])
+            i = m * (2 * nm + 3 - m) // 2 + n - m
+            cc[i] = float(vals[k + 2])
+            ss[i] = float(vals[k + 3])
+        moon[key + "_nmax"] = np.array(nm)
+        moon[key + "_mu"] = np.array(float(toks[1]))
+        moon[key + "_r"] = np.array(float(toks[2]))
+        moon[key + "_c"] = cc
+        moon[key + "_s"] = ss
+    np.savez_compressed(os.path.join(here, "moon_gfm_inputs.npz"), **moon)
     print(len(dbl), "double files;", len(quad), "quad files")
 
 
