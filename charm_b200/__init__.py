@@ -12,7 +12,8 @@ _PYHARM = ("CHarmError", "GRID", "GRID_DH1", "GRID_DH2", "GRID_GL",
            "PointGridGL", "PointSctr", "Shc", "sha_point", "shs_point",
            "shs_point_grad1", "shs_point_grad2", "shs_point_guru",
            "CELL_GRID", "CELL_SCATTERED", "SHA_CELL_AQ", "CellGrid",
-           "CellSctr", "shs_cell", "sha_cell")
+           "CellSctr", "shs_cell", "sha_cell", "gfm_global_density_3d",
+           "gfm_global_density_lateral", "gfm_global_density_const")
 
 __all__ = list(_PYHARM) + ["LIB_PATH"]
 

@@ -111,6 +111,16 @@ def _load():
         "charm_shs_cell": ([P(_Cell), P(_Shc), UL, P(D), P(_Err)], None),
         "charm_sha_cell": ([P(_Cell), P(D), UL, _ct_int, P(_Shc), P(_Err)],
                            None),
+        "charm_gfm_global_density_3d": (
+            [P(_Shc), UL, D, P(P(_Shc)), P(UL), ct.c_uint, D, D, ct.c_uint,
+             ct.c_uint, UL, ct.c_char_p, ct.c_char_p, ct.c_char_p, P(_Shc),
+             P(_Err)], None),
+        "charm_gfm_global_density_lateral": (
+            [P(_Shc), UL, D, P(_Shc), UL, D, D, ct.c_uint, ct.c_uint, UL,
+             ct.c_char_p, ct.c_char_p, ct.c_char_p, P(_Shc), P(_Err)], None),
+        "charm_gfm_global_density_const": (
+            [P(_Shc), UL, D, D, D, D, ct.c_uint, ct.c_uint, UL, ct.c_char_p,
+             ct.c_char_p, ct.c_char_p, P(_Shc), P(_Err)], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -25,7 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-ccbin", HOST_CXX,
           "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "--expt-relaxed-constexpr"]
 
-SOURCES = ["tables.cu", "shs_grid.cu", "sha_grid.cu", "sctr.cu", "crd.cu", "probe.cu", "rfft.cu", "sha_static.cu", "f32.cu", "shs_tc.cu", "cell.cu",
+SOURCES = ["tables.cu", "shs_grid.cu", "sha_grid.cu", "sctr.cu", "crd.cu", "probe.cu", "rfft.cu", "sha_static.cu", "f32.cu", "shs_tc.cu", "cell.cu", "gfm.cu",
            "engine.cpp", "capi.cpp"]
 
 

@@ -839,6 +839,215 @@ void charm_shc_write_bin(const charm_shc *shcs, unsigned long nmax,
 }
 
 // ---------------------------------------------------------------------------
+// Global spectral gravity forward modelling: src/gfm/gfm_sgfm.c (checks in
+// CHarm's order and wording), gfm_global_density_lateral.c,
+// gfm_global_density_3d.c, gfm_global_density_const.c
+// ---------------------------------------------------------------------------
+static void gfm_run(const charm_shc *shape_shcs, unsigned long shape_nmax,
+                    double R, charm_shc **density_shcs,
+                    unsigned long *density_nmax, unsigned density_order,
+                    double rho, double G, double mass, unsigned pmin,
+                    unsigned pmax, unsigned long nmax_pot,
+                    const char *hro_path, const char *pot_path,
+                    const char *fmt, charm_shc *pot, charm_err *err,
+                    const char *func)
+{
+    char msg[CHARM_ERR_MAX_MSG];
+    const double thr = charm_glob_threshold;
+    if (shape_nmax > shape_shcs->nmax)
+    {
+        snprintf(msg, sizeof msg,
+                 "\"shape_nmax\" is \"%lu\", but it cannot be larger than "
+                 "\"shape_shcs->nmax = %lu\".",
+                 shape_nmax, shape_shcs->nmax);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (!nearly_equal(shape_shcs->mu, 1.0, thr))
+    {
+        snprintf(msg, sizeof msg,
+                 "\"shape_shcs->mu\" is \"%0.16e\", but it has to be \"1.0\".",
+                 shape_shcs->mu);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (!nearly_equal(shape_shcs->r, 1.0, thr))
+    {
+        snprintf(msg, sizeof msg,
+                 "\"shape_shcs->r\" is \"%0.16e\", but it has to be \"1.0\".",
+                 shape_shcs->r);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (R <= 0.0)
+    {
+        snprintf(msg, sizeof msg,
+                 "\"shape_ref_radius\" is \"%0.16e\", but it has to be "
+                 "positive.", R);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (nearly_equal(mass, 0.0, thr))
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "\"mass\" cannot be zero.");
+        return;
+    }
+    // src/gfm/gfm_check_p.c
+    if (pmin < 1 || pmax < 1)
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "Topography power must be positive.");
+        return;
+    }
+    if (pmin > pmax)
+    {
+        snprintf(msg, sizeof msg,
+                 "\"shape_power_min\" is \"%u\", but it cannot be larger than "
+                 "\"shape_power_max = %u\".", pmin, pmax);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    for (unsigned i = 0; density_shcs && i <= density_order; i++)
+    {
+        if (density_nmax[i] > density_shcs[i]->nmax)
+        {
+            snprintf(msg, sizeof msg,
+                     "\"density_nmax[%u]\" is \"%lu\", but it cannot be larger "
+                     "than \"density_shcs[%u]->nmax = %lu\".",
+                     i, density_nmax[i], i, density_shcs[i]->nmax);
+            SET_ERR(err, CHARM_EFUNCARG, msg);
+            return;
+        }
+        if (!nearly_equal(density_shcs[i]->mu, 1.0, thr))
+        {
+            snprintf(msg, sizeof msg,
+                     "\"density_shcs[%u]->mu\" is \"%0.16e\", but it has to "
+                     "be \"1.0\".", i, density_shcs[i]->mu);
+            SET_ERR(err, CHARM_EFUNCARG, msg);
+            return;
+        }
+        if (!nearly_equal(density_shcs[i]->r, 1.0, thr))
+        {
+            snprintf(msg, sizeof msg,
+                     "\"density_shcs[%u]->r\" is \"%0.16e\", but it has to "
+                     "be \"1.0\".", i, density_shcs[i]->r);
+            SET_ERR(err, CHARM_EFUNCARG, msg);
+            return;
+        }
+    }
+    if (pot && nmax_pot > pot->nmax)
+    {
+        snprintf(msg, sizeof msg,
+                 "\"potential_shcs_nmax\" is \"%lu\", but it cannot be larger "
+                 "than \"potential_shcs->nmax = %lu\".", nmax_pot, pot->nmax);
+        SET_ERR(err, CHARM_EFUNCARG, msg);
+        return;
+    }
+    if (hro_path || pot_path)
+    {
+        if (!fmt || (strcmp(fmt, "bin") && strcmp(fmt, "mtx") &&
+                     strcmp(fmt, "tbl") && strcmp(fmt, "dov")))
+        {
+            SET_ERR(err, CHARM_EFUNCARG,
+                    "Unsupported value of \"shcs_file_format\".");
+            return;
+        }
+        if (strcmp(fmt, "bin"))
+        {
+            SET_ERR(err, CHARM_EFUNCARG,
+                    "This library exports the partial coefficients in the "
+                    "\"bin\" format only.");
+            return;
+        }
+    }
+    cb::GfmArgs g{};
+    g.shape = shape_shcs;
+    g.shape_nmax = shape_nmax;
+    g.R = R;
+    g.density = density_shcs;
+    g.density_nmax = density_nmax;
+    g.density_order = density_order;
+    g.rho = rho;
+    g.G = G;
+    g.mass = mass;
+    g.pmin = pmin;
+    g.pmax = pmax;
+    g.nmax_pot = nmax_pot;
+    g.hro_path = hro_path;
+    g.pot_path = pot_path;
+    g.pot = pot;
+    report(err, func, cb::gfm_global(g));
+}
+
+void charm_gfm_global_density_3d(const charm_shc *shape_shcs,
+                                 unsigned long shape_nmax,
+                                 double shape_radius_ref,
+                                 charm_shc **density_shcs,
+                                 unsigned long *density_nmax,
+                                 unsigned density_order, double grav_const,
+                                 double mass, unsigned shape_power_min,
+                                 unsigned shape_power_max,
+                                 unsigned long potential_shcs_nmax,
+                                 const char *shape_density_shcs_path,
+                                 const char *potential_shcs_path,
+                                 const char *shcs_file_format,
+                                 charm_shc *potential_shcs, charm_err *err)
+{
+    gfm_run(shape_shcs, shape_nmax, shape_radius_ref, density_shcs,
+            density_nmax, density_order, 0.0, grav_const, mass,
+            shape_power_min, shape_power_max, potential_shcs_nmax,
+            shape_density_shcs_path, potential_shcs_path, shcs_file_format,
+            potential_shcs, err, __func__);
+}
+
+void charm_gfm_global_density_lateral(
+    const charm_shc *shape_shcs, unsigned long shape_nmax,
+    double shape_radius_ref, charm_shc *density_shcs,
+    unsigned long density_nmax, double grav_const, double mass,
+    unsigned shape_power_min, unsigned shape_power_max,
+    unsigned long potential_shcs_nmax, const char *shape_density_shcs_path,
+    const char *potential_shcs_path, const char *shcs_file_format,
+    charm_shc *potential_shcs, charm_err *err)
+{
+    // src/gfm/gfm_global_density_lateral.c:30-60
+    if (density_nmax > density_shcs->nmax)
+    {
+        SET_ERR(err, CHARM_EFUNCARG,
+                "\"density_nmax\" cannot be larger than "
+                "\"density_shcs->nmax\".");
+        return;
+    }
+    if (!nearly_equal(density_shcs->mu, 1.0, charm_glob_threshold))
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "\"density_shcs->mu\" have to be \"1.0\".");
+        return;
+    }
+    if (!nearly_equal(density_shcs->r, 1.0, charm_glob_threshold))
+    {
+        SET_ERR(err, CHARM_EFUNCARG, "\"density_shcs->r\" have to be \"1.0\".");
+        return;
+    }
+    gfm_run(shape_shcs, shape_nmax, shape_radius_ref, &density_shcs,
+            &density_nmax, 0, 0.0, grav_const, mass, shape_power_min,
+            shape_power_max, potential_shcs_nmax, shape_density_shcs_path,
+            potential_shcs_path, shcs_file_format, potential_shcs, err,
+            __func__);
+}
+
+void charm_gfm_global_density_const(
+    const charm_shc *shape_shcs, unsigned long shape_nmax,
+    double shape_radius_ref, double density, double grav_const, double mass,
+    unsigned shape_power_min, unsigned shape_power_max,
+    unsigned long potential_shcs_nmax, const char *shape_shcs_path,
+    const char *potential_shcs_path, const char *shcs_file_format,
+    charm_shc *potential_shcs, charm_err *err)
+{
+    gfm_run(shape_shcs, shape_nmax, shape_radius_ref, nullptr, nullptr, 0,
+            density, grav_const, mass, shape_power_min, shape_power_max,
+            potential_shcs_nmax, shape_shcs_path, potential_shcs_path,
+            shcs_file_format, potential_shcs, err, __func__);
+}
+
+// ---------------------------------------------------------------------------
 // Cells: src/shs/shs_cell.c:22-121, src/sha/sha_cell.c:37-100
 // ---------------------------------------------------------------------------
 static bool check_nmax_cell(const charm_shc *shcs, unsigned long nmax,

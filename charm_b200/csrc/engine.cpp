@@ -3628,6 +3628,205 @@ Status shc_read_bin_dev_impl(Context &c, const char *path, unsigned long nmax,
 }
 
 // ---------------------------------------------------------------------------
+// Spectral gravity forward modelling, global (src/gfm/gfm_sgfm.c)
+// ---------------------------------------------------------------------------
+// gfm_sgfm.c global_vnmc: c times the degree factor of power p and density
+// order i, in CHarm's order of operations
+void gfm_vnmc(unsigned long nmax, unsigned p, unsigned i, double cc,
+              std::vector<double> &v)
+{
+    v.assign(nmax + 1, 0.0);
+    const double pr = (double)p;
+    for (unsigned long n = 0; n <= nmax; n++)
+    {
+        const double npip3 = (double)(n + i + 3);
+        double snpi = npip3 / pr;
+        for (unsigned pt = 1; pt < p; pt++)
+            snpi *= (npip3 - (double)pt) / (pr - (double)pt);
+        snpi *= 2.0 / ((2.0 * (double)n + 1.0) * npip3);
+        v[n] = cc * snpi;
+    }
+}
+
+// Writes the degree-n triangles (c, s) on the device as a binary
+// coefficient file path-p<P>-i<I>.shcs (gfm_sgfm.c export_shcs_powers with
+// the "bin" format).
+Status gfm_export(Context &c, const double *dc, const double *ds,
+                  unsigned long n, double mu, double r, const char *path,
+                  unsigned p, unsigned pmax, unsigned i, unsigned imax)
+{
+    Status st;
+    auto digits = [](unsigned x) {
+        return x > 0 ? (int)std::ceil(std::log10((double)x)) : 1;
+    };
+    char name[CHARM_ERR_MAX_FILE];
+    const int ret = std::snprintf(name, sizeof name, "%s-p%0*u-i%0*u.shcs",
+                                  path, digits(pmax), p, digits(imax), i);
+    if (ret <= 0 || (size_t)ret >= sizeof name)
+    {
+        st.code = CHARM_EFUNCARG;
+        st.msg = "Too small string buffer for the output file name.";
+        return st;
+    }
+    const size_t T = (size_t)(n + 1) * (n + 2) / 2;
+    std::vector<double> hc(T), hs(T);
+    CB_CUDA(cudaMemcpyAsync(hc.data(), dc, T * 8, cudaMemcpyDeviceToHost,
+                            c.stream), st);
+    CB_CUDA(cudaMemcpyAsync(hs.data(), ds, T * 8, cudaMemcpyDeviceToHost,
+                            c.stream), st);
+    CB_CUDA(cudaStreamSynchronize(c.stream), st);
+    FILE *fp = std::fopen(name, "wb");
+    if (!fp)
+    {
+        st.code = CHARM_EFILEIO;
+        st.msg = std::string("Couldn't create \"") + name + "\".";
+        return st;
+    }
+    const bool ok = std::fwrite(&n, sizeof n, 1, fp) == 1 &&
+                    std::fwrite(&mu, 8, 1, fp) == 1 &&
+                    std::fwrite(&r, 8, 1, fp) == 1 &&
+                    std::fwrite(hc.data(), 8, T, fp) == T &&
+                    std::fwrite(hs.data(), 8, T, fp) == T;
+    std::fclose(fp);
+    if (!ok)
+    {
+        st.code = CHARM_EFILEIO;
+        st.msg = std::string("Failed to write \"") + name + "\".";
+    }
+    return st;
+}
+
+Status gfm_global_impl(Context &c, const GfmArgs &g)
+{
+    Status st;
+    const bool rho_const = g.density == nullptr;
+    const unsigned imax = rho_const ? 0u : g.density_order;
+    // get_max_nmax(density_nmax, density_order) of gfm_sgfm.c: the largest
+    // of the first density_order entries (the first entry when 0)
+    unsigned long dmax = 0;
+    if (!rho_const)
+    {
+        dmax = g.density_nmax[0];
+        for (unsigned k = 1; k < g.density_order; k++)
+            dmax = std::max(dmax, g.density_nmax[k]);
+    }
+    double cc = (2.0 * PI * std::pow(g.R, 3)) / g.mass;
+    if (rho_const)
+        cc *= g.rho;
+    const double gm = g.G * g.mass;
+    const unsigned long np = g.nmax_pot;
+    const size_t Tp = (size_t)(np + 1) * (np + 2) / 2;
+
+    // inputs and the potential accumulators on the device
+    const unsigned long sn = g.shape->nmax;
+    const size_t Tsh = (size_t)(sn + 1) * (sn + 2) / 2;
+    double *dshape = nullptr;
+    CB_TRY(dbuf(c, "gfm_shape_tri", 2 * Tsh, &dshape));
+    CB_TRY(upload_tri(c, g.shape->c, sn, dshape));
+    CB_TRY(upload_tri(c, g.shape->s, sn, dshape + Tsh));
+    std::vector<double *> ddens(imax + 1, nullptr);
+    for (unsigned i = 0; !rho_const && i <= imax; i++)
+    {
+        const unsigned long dn = g.density[i]->nmax;
+        const size_t Td = (size_t)(dn + 1) * (dn + 2) / 2;
+        CB_TRY(dbuf(c, "gfm_dens_tri" + std::to_string(i), 2 * Td,
+                    &ddens[i]));
+        CB_TRY(upload_tri(c, g.density[i]->c, dn, ddens[i]));
+        CB_TRY(upload_tri(c, g.density[i]->s, dn, ddens[i] + Td));
+    }
+    double *dpot = nullptr;
+    if (g.pot)
+    {
+        CB_TRY(dbuf(c, "gfm_pot", 2 * Tp, &dpot));
+        CB_CUDA(cudaMemsetAsync(dpot, 0, 2 * Tp * 8, c.stream), st);
+    }
+    std::vector<double> v;
+    for (unsigned p = g.pmin; p <= g.pmax; p++)
+    {
+        const unsigned long nmaxp = p * g.shape_nmax + dmax;
+        const unsigned long thr = nmaxp > np ? np : nmaxp;
+        charm_point *grd = charm_crd_point_gl(nmaxp, 1.0);
+        if (!grd)
+        {
+            st.code = CHARM_EFUNCARG;
+            st.msg = "Failed to compute the Gauss--Legendre grid.";
+            return st;
+        }
+        struct Free
+        {
+            charm_point *q;
+            ~Free() { charm_crd_point_free(q); }
+        } fr{grd};
+        const size_t npt = grd->npoint;
+        double *fshape = nullptr, *frho = nullptr;
+        CB_TRY(dbuf(c, "gfm_f_shape", npt, &fshape));
+        CB_TRY(dbuf(c, "gfm_f_rho", npt, &frho));
+        CoefIn shin;
+        shin.nmax = sn;
+        shin.mu = 1.0;
+        shin.r = 1.0;
+        shin.dc = dshape;
+        shin.ds = dshape + Tsh;
+        CB_TRY(shs_grid(c, grd, shin, g.shape_nmax, 0, 0, 0, 0, nullptr,
+                        fshape));
+        const size_t Ta = (size_t)(thr + 1) * (thr + 2) / 2;
+        double *da = nullptr;
+        CB_TRY(dbuf(c, "gfm_a", 2 * Ta, &da));
+        double *dv = nullptr;
+        CB_TRY(dbuf(c, "gfm_v", thr + 1, &dv));
+        double Ri = 1.0;
+        for (unsigned i = 0; i <= imax; i++)
+        {
+            if (!rho_const)
+            {
+                const unsigned long dn = g.density[i]->nmax;
+                const size_t Td = (size_t)(dn + 1) * (dn + 2) / 2;
+                CoefIn din;
+                din.nmax = dn;
+                din.mu = 1.0;
+                din.r = 1.0;
+                din.dc = ddens[i];
+                din.ds = ddens[i] + Td;
+                CB_TRY(shs_grid(c, grd, din, g.density_nmax[i], 0, 0, 0, 0,
+                                nullptr, frho));
+                CB_CUDA(launch_gfm_power(npt, fshape, g.R, p, Ri, frho,
+                                         nullptr, c.stream), st);
+                Ri *= g.R;
+            }
+            else
+                CB_CUDA(launch_gfm_power(npt, fshape, g.R, p, 1.0, nullptr,
+                                         frho, c.stream), st);
+            CB_TRY(sha_grid(c, grd, nullptr, frho, thr, 1.0, 1.0, thr,
+                            nullptr, nullptr, da, da + Ta));
+            if (g.hro_path)
+                CB_TRY(gfm_export(c, da, da + Ta, thr, 1.0, 1.0, g.hro_path,
+                                  p, g.pmax, i, imax));
+            gfm_vnmc(thr, p, i, cc, v);
+            CB_CUDA(cudaMemcpyAsync(dv, v.data(), (thr + 1) * 8,
+                                    cudaMemcpyHostToDevice, c.stream), st);
+            CB_CUDA(launch_gfm_accum((long long)thr, (long long)np, dv, da,
+                                     da + Ta, dpot, dpot ? dpot + Tp : nullptr,
+                                     g.pot_path != nullptr, c.stream),
+                    st);
+            if (g.pot_path)
+                CB_TRY(gfm_export(c, da, da + Ta, thr, gm, g.R, g.pot_path, p,
+                                  g.pmax, i, imax));
+            // v must outlive its copy
+            CB_CUDA(cudaStreamSynchronize(c.stream), st);
+        }
+    }
+    if (g.pot)
+    {
+        CB_TRY(download_tri(c, dpot, np, g.pot->c));
+        CB_TRY(download_tri(c, dpot + Tp, np, g.pot->s));
+        CB_CUDA(cudaStreamSynchronize(c.stream), st);
+        g.pot->mu = gm;
+        g.pot->r = g.R;
+    }
+    return st;
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free analysis (charm_b200_sha_point_dev_static)
 // ---------------------------------------------------------------------------
 // The same kernels as sha_grid with the row transform of rfft.cu, every
@@ -4071,6 +4270,13 @@ Status shc_read_bin_dev(const char *path, unsigned long nmax,
     CB_TRY(init(g_ctx));
     return shc_read_bin_dev_impl(g_ctx, path, nmax, shc_nmax, d_c, d_s, mu, r,
                                  nmax_file);
+}
+
+Status gfm_global(const GfmArgs &g)
+{
+    std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
+    CB_TRY(init(g_ctx));
+    return gfm_global_impl(g_ctx, g);
 }
 
 Status sha_point_dev_band(const charm_point *pnt, const double *d_f,

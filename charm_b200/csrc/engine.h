@@ -72,6 +72,25 @@ Status sha_cell(const charm_cell *cell, const double *f, unsigned long nmax,
 Status sha_cell_dev(const charm_cell *cell, const double *d_f,
                     unsigned long nmax, double mu, double r,
                     unsigned long shc_nmax, double *d_c, double *d_s);
+// Global spectral gravity forward modelling (src/gfm/gfm_sgfm.c,
+// SGFM_GLOBAL): density null for a constant density rho; the callers have
+// made CHarm's checks.  Exports go to binary coefficient files.
+struct GfmArgs
+{
+    const charm_shc *shape;
+    unsigned long shape_nmax;
+    double R;
+    charm_shc *const *density;
+    const unsigned long *density_nmax;
+    unsigned density_order;
+    double rho;
+    double G, mass;
+    unsigned pmin, pmax;
+    unsigned long nmax_pot;
+    const char *hro_path, *pot_path;
+    charm_shc *pot;
+};
+Status gfm_global(const GfmArgs &g);
 // A coefficient file in CHarm's binary format streamed into device
 // triangles of degree shc_nmax (charm_b200_shc_read_bin_dev).
 Status shc_read_bin_dev(const char *path, unsigned long nmax,

@@ -328,6 +328,13 @@ cudaError_t launch_shs_cell_sctr(const CellArgs &A, bool rr, int grid,
 cudaError_t launch_dft_rows_fwd(long long nrows, long long L, int kmax,
                                 const double *x, long long ldx, double2 *X,
                                 int ldX, cudaStream_t st);
+// global spectral gravity forward modelling (gfm.cu)
+cudaError_t launch_gfm_power(size_t n, const double *shape, double R,
+                             unsigned p, double Ri, double *rho, double *out,
+                             cudaStream_t st);
+cudaError_t launch_gfm_accum(long long na, long long np, const double *v,
+                             double *ac, double *as, double *pc, double *ps,
+                             bool scaled, cudaStream_t st);
 cudaError_t launch_rfft_w4(int H, double2 *w4, cudaStream_t st);
 cudaError_t launch_rfft_tables(RfftArgs &A, double2 *tw, double2 *w,
                                double2 *ht, double2 *bh, cudaStream_t st);

@@ -289,3 +289,64 @@ def sha_cell(cell, f, nmax, method=SHA_CELL_AQ, mu=MU, r=R):
         _libcharm.charm_sha_cell(cell._Cell, _dptr(f), int(nmax), int(method),
                                  shcs._Shc, err)
     return shcs
+
+
+# ---------------------------------------------------------------------------
+# Global spectral gravity forward modelling (wrap/pyharm/gfm.py
+# global_density_3d, global_density_lateral, global_density_const)
+# ---------------------------------------------------------------------------
+def _enc(x):
+    return None if x is None else str(x).encode()
+
+
+def gfm_global_density_3d(shape_shcs, shape_nmax, shape_radius_ref,
+                          density_shcs, density_nmax, density_order,
+                          grav_const, mass, shape_power_min, shape_power_max,
+                          potential_shcs_nmax, shape_density_shcs_path=None,
+                          potential_shcs_path=None, shcs_file_format="bin"):
+    pot = Shc(potential_shcs_nmax, 1.0, 1.0)
+    n = int(density_order) + 1
+    arr = (ct.POINTER(_Shc) * n)(*[d._Shc for d in density_shcs[:n]])
+    nm = (ct.c_ulong * n)(*[int(x) for x in density_nmax[:n]])
+    with _ErrGuard() as err:
+        _libcharm.charm_gfm_global_density_3d(
+            shape_shcs._Shc, int(shape_nmax), float(shape_radius_ref), arr,
+            nm, int(density_order), float(grav_const), float(mass),
+            int(shape_power_min), int(shape_power_max),
+            int(potential_shcs_nmax), _enc(shape_density_shcs_path),
+            _enc(potential_shcs_path), _enc(shcs_file_format), pot._Shc, err)
+    return pot
+
+
+def gfm_global_density_lateral(shape_shcs, shape_nmax, shape_radius_ref,
+                               density_shcs, density_nmax, grav_const, mass,
+                               shape_power_min, shape_power_max,
+                               potential_shcs_nmax,
+                               shape_density_shcs_path=None,
+                               potential_shcs_path=None,
+                               shcs_file_format="bin"):
+    pot = Shc(potential_shcs_nmax, 1.0, 1.0)
+    with _ErrGuard() as err:
+        _libcharm.charm_gfm_global_density_lateral(
+            shape_shcs._Shc, int(shape_nmax), float(shape_radius_ref),
+            density_shcs._Shc, int(density_nmax), float(grav_const),
+            float(mass), int(shape_power_min), int(shape_power_max),
+            int(potential_shcs_nmax), _enc(shape_density_shcs_path),
+            _enc(potential_shcs_path), _enc(shcs_file_format), pot._Shc, err)
+    return pot
+
+
+def gfm_global_density_const(shape_shcs, shape_nmax, shape_radius_ref,
+                             density, grav_const, mass, shape_power_min,
+                             shape_power_max, potential_shcs_nmax,
+                             shape_shcs_path=None, potential_shcs_path=None,
+                             shcs_file_format="bin"):
+    pot = Shc(potential_shcs_nmax, 1.0, 1.0)
+    with _ErrGuard() as err:
+        _libcharm.charm_gfm_global_density_const(
+            shape_shcs._Shc, int(shape_nmax), float(shape_radius_ref),
+            float(density), float(grav_const), float(mass),
+            int(shape_power_min), int(shape_power_max),
+            int(potential_shcs_nmax), _enc(shape_shcs_path),
+            _enc(potential_shcs_path), _enc(shcs_file_format), pot._Shc, err)
+    return pot

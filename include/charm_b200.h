@@ -279,6 +279,40 @@ CHARM_EXTERN void CHARM_CDECL charm_sha_cell(const charm_cell *cell,
                                              charm_err *err);
 
 /* ------------------------------------------------------------------------- */
+/* Global spectral gravity forward modelling: src/gfm/gfm.h.in:223-320        */
+/* (src/gfm/gfm_sgfm.c).  Masses between the sphere of radius                */
+/* shape_radius_ref and the surface given by shape_shcs, with a density      */
+/* polynomial in the radius whose coefficients density_shcs[0..order] vary   */
+/* laterally (3d), one lateral density (lateral) or a constant (const); the  */
+/* shape-density functions of topography powers shape_power_min..max are    */
+/* synthesised, multiplied and analysed on Gauss--Legendre grids on the GPU. */
+/* The optional exports of partial coefficients take the "bin" format.      */
+/* ------------------------------------------------------------------------- */
+CHARM_EXTERN void CHARM_CDECL charm_gfm_global_density_3d(
+    const charm_shc *shape_shcs, unsigned long shape_nmax,
+    double shape_radius_ref, charm_shc **density_shcs,
+    unsigned long *density_nmax, unsigned density_order, double grav_const,
+    double mass, unsigned shape_power_min, unsigned shape_power_max,
+    unsigned long potential_shcs_nmax, const char *shape_density_shcs_path,
+    const char *potential_shcs_path, const char *shcs_file_format,
+    charm_shc *potential_shcs, charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_gfm_global_density_lateral(
+    const charm_shc *shape_shcs, unsigned long shape_nmax,
+    double shape_radius_ref, charm_shc *density_shcs,
+    unsigned long density_nmax, double grav_const, double mass,
+    unsigned shape_power_min, unsigned shape_power_max,
+    unsigned long potential_shcs_nmax, const char *shape_density_shcs_path,
+    const char *potential_shcs_path, const char *shcs_file_format,
+    charm_shc *potential_shcs, charm_err *err);
+CHARM_EXTERN void CHARM_CDECL charm_gfm_global_density_const(
+    const charm_shc *shape_shcs, unsigned long shape_nmax,
+    double shape_radius_ref, double density, double grav_const, double mass,
+    unsigned shape_power_min, unsigned shape_power_max,
+    unsigned long potential_shcs_nmax, const char *shape_shcs_path,
+    const char *potential_shcs_path, const char *shcs_file_format,
+    charm_shc *potential_shcs, charm_err *err);
+
+/* ------------------------------------------------------------------------- */
 /* Runtime globals: src/glob/glob.h.in:66-241 (values glob.c:16-23)            */
 /* ------------------------------------------------------------------------- */
 CHARM_EXTERN extern double charm_glob_threshold;
