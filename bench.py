@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--sctr-iters", type=int, default=2)
     ap.add_argument("--no-cells", action="store_true",
                     help="skip the block-mean (cell) synthesis and analysis")
+    ap.add_argument("--no-gfm", action="store_true",
+                    help="skip the global gravity forward modelling section")
     return ap.parse_args()
 
 
@@ -381,6 +383,7 @@ def run_ours(args):
     bdh = None if args.no_batch_dh else batch_dh(single_calls=False)
     sct = None if args.no_sctr else scattered(args.sctr_points, args.sctr_iters)
     cel = None if args.no_cells else cells()
+    gfmr = None if args.no_gfm else gfm()
 
     if rank != 0:
         if dist is not None:
@@ -481,6 +484,8 @@ def run_ours(args):
         line["scattered"] = sct
     if cel is not None:
         line["cells"] = cel
+    if gfmr is not None:
+        line["gfm"] = gfmr
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, c, s)
     print(json.dumps(line), flush=True)
@@ -1123,6 +1128,82 @@ def cells(steps=5, oracle_rows=3):
         out["shs_rel_rms_vs_charm"] = rel_rms(np.ravel(f), fr)
         out["sha_rel_rms_vs_charm"] = coef_rel_rms(cg, sg, cr, sr)
     except (OSError, RuntimeError) as e:
+        out["charm_cpu"] = "unavailable: %s" % e
+    return out
+
+
+def gfm(steps=2):
+    """Global spectral gravity forward modelling of a synthetic body:
+    shape of degree 360 (lunar radius, Kaula-like relief), a density
+    polynomial of order 1 (coefficients of degree 180 and 90), topography
+    powers 1..5, potential to degree 720 (Gauss--Legendre grids up to nmax
+    1980).  GPU time per call (wall clock, the call returns after its
+    streams are idle), the potential's agreement with CHarm's own
+    charm_gfm_global_density_3d, and CHarm's time on the host cores."""
+    import torch
+    import charm_b200 as cb
+    from charm_b200.workloads import coef_rel_rms
+    from oracle import charm_ref
+    R = 1728000.0
+    G, M = 6.67430e-11, 7.346e22
+
+    def body(nmax, seed, relief, c00):
+        rng = np.random.default_rng(seed)
+        T = (nmax + 1) * (nmax + 2) // 2
+        n = np.concatenate([np.arange(m, nmax + 1) for m in range(nmax + 1)])
+        sig = relief / (1.0 + n) ** 2
+        c = rng.standard_normal(T) * sig
+        s = rng.standard_normal(T) * sig
+        s[:nmax + 1] = 0.0
+        c[0] = c00
+        return c, s
+    shape = body(360, 61, 3000.0, R + 1700.0)
+    dens = [body(180, 62, 80.0, 2500.0), body(90, 63, 1e-6, -2e-5)]
+    args_s = (360, 1.0, 1.0) + shape
+    sh = cb.Shc(*args_s)
+    ds = [cb.Shc(180, 1.0, 1.0, *dens[0]), cb.Shc(90, 1.0, 1.0, *dens[1])]
+
+    def call():
+        return cb.gfm_global_density_3d(sh, 360, R, ds, [180, 90], 1, G, M, 1,
+                                        5, 720)
+    pot = call()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        pot = call()
+        ts.append(time.perf_counter() - t0)
+    out = {"workload": "global gravity forward modelling: shape nmax 360, "
+                       "density order 1 (nmax 180, 90), powers 1..5, "
+                       "potential nmax 720 (GL grids up to nmax 1980)",
+           "gpu_s": float(np.median(ts)), "steps": steps,
+           "data": "synthetic (seeds 61-63)"}
+    try:
+        C = charm_ref.Charm("d")
+        P = ct.POINTER
+        fn = C.fn("gfm_global_density_3d")
+        fn.argtypes = [P(C.Shc), ct.c_ulong, ct.c_double, P(P(C.Shc)),
+                       P(ct.c_ulong), ct.c_uint, ct.c_double, ct.c_double,
+                       ct.c_uint, ct.c_uint, ct.c_ulong, ct.c_char_p,
+                       ct.c_char_p, ct.c_char_p, P(C.Shc), P(C.Err)]
+        fn.restype = None
+        csh = C.shc(*args_s)
+        cds = [C.shc(180, 1.0, 1.0, *dens[0]), C.shc(90, 1.0, 1.0, *dens[1])]
+        arr = (P(C.Shc) * 2)(*[d.ptr for d in cds])
+        nm = (ct.c_ulong * 2)(180, 90)
+        T = 721 * 722 // 2
+        cpot = C.shc(720, 1.0, 1.0, np.zeros(T), np.zeros(T))
+        t0 = time.perf_counter()
+        fn(csh.ptr, 360, R, arr, nm, 1, G, M, 1, 5, 720, None, None, None,
+           cpot.ptr, C.err)
+        t1 = time.perf_counter()
+        C.check()
+        out["charm_cpu"] = {"s": t1 - t0, "cores": host_cores(),
+                            "lib": os.path.relpath(charm_ref.lib_path("d"),
+                                                   ROOT)}
+        out["potential_rel_rms_vs_charm"] = coef_rel_rms(
+            pot.c, pot.s, cpot.keep[0], cpot.keep[1])
+    except (OSError, RuntimeError, AttributeError) as e:
         out["charm_cpu"] = "unavailable: %s" % e
     return out
 
