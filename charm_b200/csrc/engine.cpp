@@ -3740,7 +3740,42 @@ Status gfm_global_impl(Context &c, const GfmArgs &g)
         CB_TRY(dbuf(c, "gfm_pot", 2 * Tp, &dpot));
         CB_CUDA(cudaMemsetAsync(dpot, 0, 2 * Tp * 8, c.stream), st);
     }
-    std::vector<double> v;
+    // the degree factors of every (power, density order), uploaded once
+    const unsigned npow = g.pmax - g.pmin + 1;
+    const size_t nv = (size_t)npow * (imax + 1) * (np + 1);
+    std::vector<double> vh(nv, 0.0), v;
+    for (unsigned p = g.pmin; p <= g.pmax; p++)
+        for (unsigned i = 0; i <= imax; i++)
+        {
+            const unsigned long nmaxp = p * g.shape_nmax + dmax;
+            gfm_vnmc(nmaxp > np ? np : nmaxp, p, i, cc, v);
+            std::copy(v.begin(), v.end(),
+                      vh.begin() + ((size_t)(p - g.pmin) * (imax + 1) + i) *
+                                       (np + 1));
+        }
+    double *dv = nullptr;
+    CB_TRY(dbuf(c, "gfm_v", nv, &dv));
+    CB_CUDA(cudaMemcpyAsync(dv, vh.data(), nv * 8, cudaMemcpyHostToDevice,
+                            c.stream), st);
+    // (a pageable source: the copy has read vh when the call returns)
+
+    // The shape and the densities of one power share its grid: one batched
+    // synthesis forms all of them (sets of their own degrees, one launch)
+    // when their grids and lumped coefficients (about as large again) fit
+    // the budget (default: a quarter of the free
+    // device memory; CHARM_B200_GFM_BATCH_BYTES overrides it, 0 turns the
+    // batching off), otherwise one synthesis per set.
+    const size_t nsets = 1 + (rho_const ? 0 : imax + 1);
+    size_t budget = 0;
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+            budget = fr / 4;
+        cudaGetLastError();
+        const char *e = std::getenv("CHARM_B200_GFM_BATCH_BYTES");
+        if (e && *e)
+            budget = (size_t)std::strtoull(e, nullptr, 10);
+    }
     for (unsigned p = g.pmin; p <= g.pmax; p++)
     {
         const unsigned long nmaxp = p * g.shape_nmax + dmax;
@@ -3758,61 +3793,72 @@ Status gfm_global_impl(Context &c, const GfmArgs &g)
             ~Free() { charm_crd_point_free(q); }
         } fr{grd};
         const size_t npt = grd->npoint;
-        double *fshape = nullptr, *frho = nullptr;
-        CB_TRY(dbuf(c, "gfm_f_shape", npt, &fshape));
-        CB_TRY(dbuf(c, "gfm_f_rho", npt, &frho));
-        CoefIn shin;
-        shin.nmax = sn;
-        shin.mu = 1.0;
-        shin.r = 1.0;
-        shin.dc = dshape;
-        shin.ds = dshape + Tsh;
-        CB_TRY(shs_grid(c, grd, shin, g.shape_nmax, 0, 0, 0, 0, nullptr,
-                        fshape));
+        // fields: [0] the shape, [1 + i] density i (or, for a constant
+        // density, [1] the power of the shape)
+        std::vector<double *> fld(std::max<size_t>(nsets, 2), nullptr);
+        for (size_t k = 0; k < fld.size(); k++)
+            CB_TRY(dbuf(c, "gfm_f" + std::to_string(k), npt, &fld[k]));
+        std::vector<unsigned long> nm_v(nsets), sn_v(nsets);
+        std::vector<double> mu_v(nsets, 1.0);
+        std::vector<const double *> dc_v(nsets), ds_v(nsets);
+        nm_v[0] = g.shape_nmax;
+        sn_v[0] = sn;
+        dc_v[0] = dshape;
+        ds_v[0] = dshape + Tsh;
+        for (unsigned i = 0; !rho_const && i <= imax; i++)
+        {
+            const unsigned long dn = g.density[i]->nmax;
+            nm_v[1 + i] = g.density_nmax[i];
+            sn_v[1 + i] = dn;
+            dc_v[1 + i] = ddens[i];
+            ds_v[1 + i] = ddens[i] + (size_t)(dn + 1) * (dn + 2) / 2;
+        }
+        if (nsets > 1 && nsets * npt * 16 <= budget)
+            CB_TRY(shs_batch(c, grd, nsets, nm_v.data(), sn_v.data(),
+                             mu_v.data(), 1.0, dc_v.data(), ds_v.data(), 0,
+                             fld.data()));
+        else
+            for (size_t k = 0; k < nsets; k++)
+            {
+                CoefIn in;
+                in.nmax = sn_v[k];
+                in.mu = 1.0;
+                in.r = 1.0;
+                in.dc = dc_v[k];
+                in.ds = ds_v[k];
+                CB_TRY(shs_grid(c, grd, in, nm_v[k], 0, 0, 0, 0, nullptr,
+                                fld[k]));
+            }
         const size_t Ta = (size_t)(thr + 1) * (thr + 2) / 2;
         double *da = nullptr;
         CB_TRY(dbuf(c, "gfm_a", 2 * Ta, &da));
-        double *dv = nullptr;
-        CB_TRY(dbuf(c, "gfm_v", thr + 1, &dv));
         double Ri = 1.0;
         for (unsigned i = 0; i <= imax; i++)
         {
+            double *frho = fld[1 + i];
             if (!rho_const)
             {
-                const unsigned long dn = g.density[i]->nmax;
-                const size_t Td = (size_t)(dn + 1) * (dn + 2) / 2;
-                CoefIn din;
-                din.nmax = dn;
-                din.mu = 1.0;
-                din.r = 1.0;
-                din.dc = ddens[i];
-                din.ds = ddens[i] + Td;
-                CB_TRY(shs_grid(c, grd, din, g.density_nmax[i], 0, 0, 0, 0,
-                                nullptr, frho));
-                CB_CUDA(launch_gfm_power(npt, fshape, g.R, p, Ri, frho,
+                CB_CUDA(launch_gfm_power(npt, fld[0], g.R, p, Ri, frho,
                                          nullptr, c.stream), st);
                 Ri *= g.R;
             }
             else
-                CB_CUDA(launch_gfm_power(npt, fshape, g.R, p, 1.0, nullptr,
+                CB_CUDA(launch_gfm_power(npt, fld[0], g.R, p, 1.0, nullptr,
                                          frho, c.stream), st);
             CB_TRY(sha_grid(c, grd, nullptr, frho, thr, 1.0, 1.0, thr,
                             nullptr, nullptr, da, da + Ta));
             if (g.hro_path)
                 CB_TRY(gfm_export(c, da, da + Ta, thr, 1.0, 1.0, g.hro_path,
                                   p, g.pmax, i, imax));
-            gfm_vnmc(thr, p, i, cc, v);
-            CB_CUDA(cudaMemcpyAsync(dv, v.data(), (thr + 1) * 8,
-                                    cudaMemcpyHostToDevice, c.stream), st);
-            CB_CUDA(launch_gfm_accum((long long)thr, (long long)np, dv, da,
+            const double *dvi =
+                dv + ((size_t)(p - g.pmin) * (imax + 1) + i) * (np + 1);
+            CB_CUDA(launch_gfm_accum((long long)thr, (long long)np, dvi, da,
                                      da + Ta, dpot, dpot ? dpot + Tp : nullptr,
                                      g.pot_path != nullptr, c.stream),
                     st);
             if (g.pot_path)
                 CB_TRY(gfm_export(c, da, da + Ta, thr, gm, g.R, g.pot_path, p,
                                   g.pmax, i, imax));
-            // v must outlive its copy
-            CB_CUDA(cudaStreamSynchronize(c.stream), st);
         }
     }
     if (g.pot)

@@ -108,17 +108,51 @@ def test_gfm_global_vs_oracle_and_exports(cb, tmp_path):
     assert files == ["pot-p%d-i%d.shcs" % (p, i) for p in range(1, 6)
                      for i in range(2)]
     for name in files:
-        part = cb.Shc(150, 1.0, 1.0)
+        # the contribution of power p is analysed to degree
+        # min(p shape_nmax + density_nmax, potential degree), and written
+        # at that degree (gfm_sgfm.c export_shcs_powers writes shcs->nmax)
+        p = int(name.split("-p")[1].split("-")[0])
+        d = min(40 * p + 20, 150)
+        part = cb.Shc(d, 1.0, 1.0)
         err = L.charm_err_init()
-        n = L.charm_shc_read_bin(str(tmp_path / name).encode(), 150,
+        n = L.charm_shc_read_bin(str(tmp_path / name).encode(), d,
                                  ct.cast(part._Shc, ct.c_void_p),
                                  ct.cast(err, ct.c_void_p))
-        assert L.charm_err_isempty(err) and n == 150
+        assert L.charm_err_isempty(err) and n == d
         L.charm_err_free(err)
-        total_c += part.c
-        total_s += part.s
+        assert part.mu == pot.mu and part.r == pot.r
+        for m in range(d + 1):
+            a0 = m * (d + 1) - m * (m - 1) // 2
+            b0 = m * 151 - m * (m - 1) // 2
+            total_c[b0:b0 + d + 1 - m] += part.c[a0:a0 + d + 1 - m]
+            total_s[b0:b0 + d + 1 - m] += part.s[a0:a0 + d + 1 - m]
     assert coef_rel_rms(total_c, total_s, pot.c, pot.s) <= 1e-14
     del acc
+
+
+def test_gfm_batched_synthesis_matches_per_set(cb, monkeypatch):
+    """The shape and the densities of a power synthesised in one batched
+    launch against one synthesis per set (the batching budget set to 0):
+    the same potential to rounding."""
+    R = 1728000.0
+    c, s = random_body(30, 7, R, 3000.0)
+    shape = cb.Shc(30, 1.0, 1.0, c, s)
+    dens = []
+    for k, nm in enumerate((25, 12, 8)):
+        dc, ds = random_body(nm, 20 + k, 0.0, 50.0)
+        dc[0] = (2600.0, -2e-4, 1e-10)[k]
+        dens.append(cb.Shc(nm, 1.0, 1.0, dc, ds))
+    args = (shape, 30, R, dens, [25, 12, 8], 2, GRAV_CONST, MOON_MASS, 1, 4,
+            120)
+    monkeypatch.delenv("CHARM_B200_GFM_BATCH_BYTES", raising=False)
+    batched = cb.gfm_global_density_3d(*args)
+    monkeypatch.setenv("CHARM_B200_GFM_BATCH_BYTES", "0")
+    single = cb.gfm_global_density_3d(*args)
+    assert coef_rel_rms(batched.c, batched.s, single.c, single.s) <= 1e-14
+    ref = orc.gfm_global(orc.Shc(30, 1.0, 1.0, c, s), 30, R,
+                         [orc.Shc(d.nmax, 1.0, 1.0, d.c, d.s) for d in dens],
+                         [25, 12, 8], GRAV_CONST, MOON_MASS, 1, 4, 120)
+    assert coef_rel_rms(batched.c, batched.s, ref.c, ref.s) <= 1e-12
 
 
 def test_gfm_argument_errors(cb):
