@@ -5,8 +5,9 @@
 // calls copy their grids and coefficients in bands there, ordered against
 // the kernels by events), grow-only device buffers, cached recurrence
 // tables per maximum degree, cached row-transform plans (rfft.cu, every
-// row length up to 147456 points; no library FFT) and a pinned staging
-// area for the small per-call arrays.
+// row length up to 147456 points; no library FFT), a pinned staging
+// area for the small per-call arrays and a ring of pinned buffers through
+// which host threads copy pageable host arrays.
 // Calls are serialised by a mutex.  Every call ends with a synchronisation
 // of its streams and a check of the device status word written by the
 // kernels.
@@ -14,14 +15,19 @@
 
 #include <cuda_runtime.h>
 
+#include <sched.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <array>
 #include <cfloat>
 #include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -89,7 +95,20 @@ struct Context
     std::map<std::string, DevBuf> bufs;
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
-    long long tab_nmax = -1;     // recurrence tables of this maximum degree
+    // ring of page-locked buffers for copies of pageable host arrays
+    // (stage_h2d / stage_d2h); ring_ev[b] marks the last copy on buffer b
+    void *ring[4] = {};
+    cudaEvent_t ring_ev[4] = {};
+    // recurrence tables of two maximum degrees (a least-recently-used pair
+    // of slots, so that calls alternating between two degrees, e.g. a
+    // synthesis and an analysis of another degree, rebuild nothing)
+    long long tab_nmax[2] = {-1, -1};
+    unsigned long long tab_used[2] = {0, 0};
+    unsigned long long tab_clock = 0;
+    // bumped whenever a cached device buffer is (re)allocated or a cached
+    // table is rewritten: a captured graph reads these by address, so it
+    // replays only while the epoch it was made in lasts
+    unsigned long long epoch = 0;
     long long tab32_nmax = -1;   // single-precision tables of this degree
     long long tcp_nmax = -1;     // padded ct_n rows of the tensor-core path
     long long cell_nmax = -1;    // per-degree tables of the cell kernels
@@ -276,6 +295,7 @@ Status buf(Context &c, const std::string &name, size_t bytes, void **out)
             b.bytes = 0;
         }
         size_t want = std::max<size_t>(bytes, 256);
+        c.epoch++;
         cudaError_t e = cudaMalloc(&b.p, want);
         if (e != cudaSuccess)
         {
@@ -327,6 +347,213 @@ Status pinned(Context &c, size_t bytes, void **out)
         c.pinned_bytes = want;
     }
     *out = c.pinned;
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// Pageable host arrays
+// ---------------------------------------------------------------------------
+// A copy between pageable host memory and the device runs through the
+// driver's own staging, serially and at a fraction of the page-locked rate
+// (numpy arrays, as PyHarm passes them, are pageable).  Such arrays are
+// copied here through a ring of page-locked buffers instead: host threads
+// copy chunk i between the caller's array and a ring buffer while the copy
+// engine moves chunk i - 1.
+
+constexpr int RING_N = 4;
+constexpr size_t RING_CHUNK = (size_t)8 << 20;
+
+// Host threads that copy one block of memory together: the caller takes
+// the first slice and the workers the others.
+class CopyPool
+{
+  public:
+    explicit CopyPool(int workers) : n_(workers)
+    {
+        for (int k = 0; k < n_; k++)
+            std::thread([this, k] { run(k + 1); }).detach();
+    }
+
+    void copy(void *dst, const void *src, size_t bytes)
+    {
+        if (n_ == 0 || bytes < ((size_t)1 << 20))
+        {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            dst_ = static_cast<char *>(dst);
+            src_ = static_cast<const char *>(src);
+            bytes_ = bytes;
+            pending_ = n_;
+            gen_++;
+        }
+        go_.notify_all();
+        slice(0, dst_, src_, bytes);
+        std::unique_lock<std::mutex> l(mu_);
+        done_.wait(l, [this] { return pending_ == 0; });
+    }
+
+  private:
+    void slice(int k, char *d, const char *s, size_t bytes) const
+    {
+        const size_t parts = (size_t)n_ + 1;
+        size_t a = (bytes * k / parts) & ~(size_t)63;
+        size_t b = k + 1 == (int)parts ? bytes
+                                       : (bytes * (k + 1) / parts) & ~(size_t)63;
+        if (b > a)
+            std::memcpy(d + a, s + a, b - a);
+    }
+
+    void run(int k)
+    {
+        unsigned long seen = 0;
+        for (;;)
+        {
+            char *d;
+            const char *s;
+            size_t bytes;
+            {
+                std::unique_lock<std::mutex> l(mu_);
+                go_.wait(l, [&] { return gen_ != seen; });
+                seen = gen_;
+                d = dst_;
+                s = src_;
+                bytes = bytes_;
+            }
+            slice(k, d, s, bytes);
+            std::lock_guard<std::mutex> l(mu_);
+            if (--pending_ == 0)
+                done_.notify_one();
+        }
+    }
+
+    const int n_;
+    std::mutex mu_;
+    std::condition_variable go_, done_;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t bytes_ = 0;
+    unsigned long gen_ = 0;
+    int pending_ = 0;
+};
+
+// The pool of this process (made again in a forked child, which has none
+// of the parent's threads): one worker per usable core beyond the
+// caller's, at most seven.
+CopyPool &copy_pool()
+{
+    static CopyPool *pool = nullptr;
+    static pid_t owner = 0;
+    if (!pool || owner != getpid())
+    {
+        int ncpu = 1;
+        cpu_set_t set;
+        if (sched_getaffinity(0, sizeof(set), &set) == 0)
+            ncpu = CPU_COUNT(&set);
+        pool = new CopyPool(std::max(0, std::min(7, ncpu - 1)));
+        owner = getpid();
+    }
+    return *pool;
+}
+
+bool is_pageable(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+Status ring_ready(Context &c)
+{
+    Status st;
+    for (int b = 0; b < RING_N; b++)
+    {
+        if (!c.ring[b])
+            CB_CUDA(cudaMallocHost(&c.ring[b], RING_CHUNK), st);
+        if (!c.ring_ev[b])
+            CB_CUDA(cudaEventCreateWithFlags(&c.ring_ev[b],
+                                             cudaEventDisableTiming), st);
+    }
+    return st;
+}
+
+// Host to device on the compute stream; a pageable source is read through
+// the ring (the caller may change it once this returns).
+Status stage_h2d(Context &c, void *dst, const void *src, size_t bytes)
+{
+    Status st;
+    if (bytes == 0)
+        return st;
+    if (!is_pageable(src))
+    {
+        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice,
+                                c.stream), st);
+        return st;
+    }
+    CB_TRY(ring_ready(c));
+    char *d = static_cast<char *>(dst);
+    const char *s = static_cast<const char *>(src);
+    for (size_t off = 0, i = 0; off < bytes; off += RING_CHUNK, i++)
+    {
+        const int b = (int)(i % RING_N);
+        const size_t len = std::min(RING_CHUNK, bytes - off);
+        // the buffer's previous copy has read it
+        CB_CUDA(cudaEventSynchronize(c.ring_ev[b]), st);
+        copy_pool().copy(c.ring[b], s + off, len);
+        CB_CUDA(cudaMemcpyAsync(d + off, c.ring[b], len,
+                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_CUDA(cudaEventRecord(c.ring_ev[b], c.stream), st);
+    }
+    return st;
+}
+
+// Device to host after the work already on the compute stream; returns
+// when the host array holds the data.  A pageable destination is written
+// through the ring.
+Status stage_d2h(Context &c, void *dst, const void *src, size_t bytes)
+{
+    Status st;
+    if (bytes == 0)
+        return st;
+    if (!is_pageable(dst))
+    {
+        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost,
+                                c.stream), st);
+        CB_CUDA(cudaStreamSynchronize(c.stream), st);
+        return st;
+    }
+    CB_TRY(ring_ready(c));
+    char *d = static_cast<char *>(dst);
+    const char *s = static_cast<const char *>(src);
+    const size_t nch = (bytes + RING_CHUNK - 1) / RING_CHUNK;
+    auto issue = [&](size_t i) -> Status {
+        Status s2;
+        const int b = (int)(i % RING_N);
+        const size_t off = i * RING_CHUNK;
+        CB_CUDA(cudaMemcpyAsync(c.ring[b], s + off,
+                                std::min(RING_CHUNK, bytes - off),
+                                cudaMemcpyDeviceToHost, c.stream), s2);
+        CB_CUDA(cudaEventRecord(c.ring_ev[b], c.stream), s2);
+        return s2;
+    };
+    for (size_t i = 0; i < std::min<size_t>(RING_N, nch); i++)
+        CB_TRY(issue(i));
+    for (size_t i = 0; i < nch; i++)
+    {
+        const int b = (int)(i % RING_N);
+        const size_t off = i * RING_CHUNK;
+        CB_CUDA(cudaEventSynchronize(c.ring_ev[b]), st);
+        copy_pool().copy(d + off, c.ring[b],
+                         std::min(RING_CHUNK, bytes - off));
+        if (i + RING_N < nch)
+            CB_TRY(issue(i + RING_N));
+    }
     return st;
 }
 
@@ -400,13 +627,23 @@ Status tables(Context &c, long long nmax, Tabs *tab)
     Status st;
     long long T = (nmax + 1) * (nmax + 2) / 2;
     tab->ldmul = (int)((nmax + 1 + 63) / 64);
-    CB_TRY(dbuf(c, "tab_b", (size_t)T, &tab->tb));
-    CB_TRY(dbuf(c, "tab_c", (size_t)T, &tab->tc));
-    CB_TRY(dbuf(c, "tab_mul", (size_t)(nmax + 1) * tab->ldmul, &tab->tmul));
-    CB_TRY(dbuf(c, "tab_sg", (size_t)(2 * (nmax + 1)), &tab->sg));
-    CB_TRY(dbuf(c, "tab_dm", (size_t)(nmax + 1), &tab->dm));
-    if (c.tab_nmax == nmax)
+    int slot = c.tab_nmax[0] == nmax ? 0 : (c.tab_nmax[1] == nmax ? 1 : -1);
+    const bool hit = slot >= 0;
+    if (!hit)
+        slot = c.tab_used[0] <= c.tab_used[1] ? 0 : 1;
+    c.tab_used[slot] = ++c.tab_clock;
+    const std::string sfx = slot ? "#1" : "";
+    CB_TRY(dbuf(c, "tab_b" + sfx, (size_t)T, &tab->tb));
+    CB_TRY(dbuf(c, "tab_c" + sfx, (size_t)T, &tab->tc));
+    CB_TRY(dbuf(c, "tab_mul" + sfx, (size_t)(nmax + 1) * tab->ldmul,
+                &tab->tmul));
+    CB_TRY(dbuf(c, "tab_sg" + sfx, (size_t)(2 * (nmax + 1)), &tab->sg));
+    CB_TRY(dbuf(c, "tab_dm" + sfx, (size_t)(nmax + 1), &tab->dm));
+    if (hit)
         return st;
+    // the slot is rewritten: invalid until the rebuild below completes
+    c.tab_nmax[slot] = -1;
+    c.epoch++;
     std::vector<double> r, ri, dmh;
     host_r_ri_dm(nmax, r, ri, dmh);
     std::vector<double> smm(nmax + 1);
@@ -430,7 +667,7 @@ Status tables(Context &c, long long nmax, Tabs *tab)
     }
     // the host vectors must outlive the copies
     CB_CUDA(cudaStreamSynchronize(c.stream), st);
-    c.tab_nmax = nmax;
+    c.tab_nmax[slot] = nmax;
     return st;
 }
 
@@ -1899,6 +2136,7 @@ Status shs_batch_tc(Context &c, const charm_point *pnt, size_t nsets,
     double *ctp = btp + (size_t)(N + 1) * ld;
     if (c.tcp_nmax != (long long)N)
     {
+        c.epoch++;
         Scope sc(c, TIMER_TABLES);
         CB_CUDA(launch_tc_ctab((long long)N, ld, tab.tb, tab.tc, btp, ctp,
                                c.stream), st);
@@ -4200,22 +4438,65 @@ Status sha_point_dev_static_impl(Context &c, const charm_point *pnt,
 // ---------------------------------------------------------------------------
 // Public engine entry points
 // ---------------------------------------------------------------------------
+// A coefficient triangle whose columns lie contiguously in pageable host
+// memory (null otherwise).
+const double *pageable_tri(double *const *cols, unsigned long nmax)
+{
+    const double *base = contiguous_tri(cols, nmax);
+    return (base && is_pageable(base)) ? base : nullptr;
+}
+
 Status shs_point(const charm_point *pnt, const charm_shc *shcs,
                  unsigned long nmax, int kgrad, int dr, int dlat, int dlon,
                  double **f)
 {
     std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
-    CB_TRY(init(g_ctx));
+    Context &c = g_ctx;
+    CB_TRY(init(c));
     CoefIn in;
     in.nmax = shcs->nmax;
     in.mu = shcs->mu;
     in.r = shcs->r;
     in.hc = shcs->c;
     in.hs = shcs->s;
-    if (pnt->type == CHARM_CRD_POINT_SCATTERED)
-        return shs_sctr(g_ctx, pnt, in, nmax, kgrad, dr, dlat, dlon, f,
-                        nullptr);
-    return shs_grid(g_ctx, pnt, in, nmax, kgrad, dr, dlat, dlon, f, nullptr);
+    const bool sctr = pnt->type == CHARM_CRD_POINT_SCATTERED;
+    // pageable host arrays: the coefficients uploaded and the output
+    // downloaded through the ring, the transform on device arrays
+    double mur;
+    int dorder, npar;
+    mur_dorder(in.mu, in.r, kgrad, dr, dlat, dlon, &mur, &dorder, &npar);
+    const double *pc = pageable_tri(shcs->c, shcs->nmax);
+    const double *ps = pageable_tri(shcs->s, shcs->nmax);
+    bool pf = false;
+    for (int q = 0; q < npar && pnt->npoint > 0; q++)
+        pf = pf || is_pageable(f[q]);
+    if (pc && ps)
+    {
+        const size_t Ts = (size_t)(shcs->nmax + 1) * (shcs->nmax + 2) / 2;
+        double *raw = nullptr;
+        CB_TRY(dbuf(c, "stage_shc", 2 * Ts, &raw));
+        CB_TRY(stage_h2d(c, raw, pc, Ts * 8));
+        CB_TRY(stage_h2d(c, raw + Ts, ps, Ts * 8));
+        in.hc = in.hs = nullptr;
+        in.dc = raw;
+        in.ds = raw + Ts;
+    }
+    if (pf)
+    {
+        const size_t np = pnt->npoint;
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "stage_out", (size_t)npar * np, &dout));
+        CB_TRY(sctr ? shs_sctr(c, pnt, in, nmax, kgrad, dr, dlat, dlon,
+                               nullptr, dout)
+                    : shs_grid(c, pnt, in, nmax, kgrad, dr, dlat, dlon,
+                               nullptr, dout));
+        for (int q = 0; q < npar; q++)
+            CB_TRY(stage_d2h(c, f[q], dout + (size_t)q * np, np * 8));
+        return Status{};
+    }
+    if (sctr)
+        return shs_sctr(c, pnt, in, nmax, kgrad, dr, dlat, dlon, f, nullptr);
+    return shs_grid(c, pnt, in, nmax, kgrad, dr, dlat, dlon, f, nullptr);
 }
 
 Status shs_point_dev(const charm_point *pnt, unsigned long shc_nmax,
@@ -4241,8 +4522,34 @@ Status sha_point(const charm_point *pnt, const double *f, unsigned long nmax,
                  charm_shc *shcs)
 {
     std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
-    CB_TRY(init(g_ctx));
-    return sha_grid(g_ctx, pnt, f, nullptr, nmax, shcs->mu, shcs->r,
+    Context &c = g_ctx;
+    CB_TRY(init(c));
+    // pageable host arrays: the grid uploaded and the coefficients
+    // downloaded through the ring, the analysis on device arrays
+    const bool pf = pnt->npoint > 0 && is_pageable(f);
+    const double *pc = pageable_tri(shcs->c, shcs->nmax);
+    const double *ps = pageable_tri(shcs->s, shcs->nmax);
+    const double *din = nullptr;
+    if (pf)
+    {
+        double *d = nullptr;
+        CB_TRY(dbuf(c, "stage_in", pnt->npoint, &d));
+        CB_TRY(stage_h2d(c, d, f, pnt->npoint * 8));
+        din = d;
+    }
+    if (pc && ps)
+    {
+        const size_t Ts = (size_t)(shcs->nmax + 1) * (shcs->nmax + 2) / 2;
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "stage_shc", 2 * Ts, &dout));
+        CB_TRY(sha_grid(c, pnt, din ? nullptr : f, din, nmax, shcs->mu,
+                        shcs->r, shcs->nmax, nullptr, nullptr, dout,
+                        dout + Ts));
+        CB_TRY(stage_d2h(c, const_cast<double *>(pc), dout, Ts * 8));
+        CB_TRY(stage_d2h(c, const_cast<double *>(ps), dout + Ts, Ts * 8));
+        return Status{};
+    }
+    return sha_grid(c, pnt, din ? nullptr : f, din, nmax, shcs->mu, shcs->r,
                     shcs->nmax, shcs->c, shcs->s, nullptr, nullptr);
 }
 
@@ -4260,16 +4567,40 @@ Status shs_cell(const charm_cell *cell, const charm_shc *shcs,
                 unsigned long nmax, double *f)
 {
     std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
-    CB_TRY(init(g_ctx));
+    Context &c = g_ctx;
+    CB_TRY(init(c));
     CoefIn in;
     in.nmax = shcs->nmax;
     in.mu = shcs->mu;
     in.r = shcs->r;
     in.hc = shcs->c;
     in.hs = shcs->s;
-    if (cell->type == CHARM_CRD_CELL_SCATTERED)
-        return shs_cell_sctr(g_ctx, cell, in, nmax, f, nullptr);
-    return shs_cell_grid(g_ctx, cell, in, nmax, f, nullptr);
+    const bool sctr = cell->type == CHARM_CRD_CELL_SCATTERED;
+    // pageable host arrays through the ring, as shs_point
+    const double *pc = pageable_tri(shcs->c, shcs->nmax);
+    const double *ps = pageable_tri(shcs->s, shcs->nmax);
+    if (pc && ps)
+    {
+        const size_t Ts = (size_t)(shcs->nmax + 1) * (shcs->nmax + 2) / 2;
+        double *raw = nullptr;
+        CB_TRY(dbuf(c, "stage_shc", 2 * Ts, &raw));
+        CB_TRY(stage_h2d(c, raw, pc, Ts * 8));
+        CB_TRY(stage_h2d(c, raw + Ts, ps, Ts * 8));
+        in.hc = in.hs = nullptr;
+        in.dc = raw;
+        in.ds = raw + Ts;
+    }
+    if (cell->ncell > 0 && is_pageable(f))
+    {
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "stage_out", cell->ncell, &dout));
+        CB_TRY(sctr ? shs_cell_sctr(c, cell, in, nmax, nullptr, dout)
+                    : shs_cell_grid(c, cell, in, nmax, nullptr, dout));
+        return stage_d2h(c, f, dout, cell->ncell * 8);
+    }
+    if (sctr)
+        return shs_cell_sctr(c, cell, in, nmax, f, nullptr);
+    return shs_cell_grid(c, cell, in, nmax, f, nullptr);
 }
 
 Status shs_cell_dev(const charm_cell *cell, unsigned long shc_nmax,
@@ -4293,9 +4624,33 @@ Status sha_cell(const charm_cell *cell, const double *f, unsigned long nmax,
                 charm_shc *shcs)
 {
     std::lock_guard<std::recursive_mutex> lock(g_ctx.mtx);
-    CB_TRY(init(g_ctx));
-    return sha_cell_grid(g_ctx, cell, f, nullptr, nmax, shcs->mu, shcs->r,
-                         shcs->nmax, shcs->c, shcs->s, nullptr, nullptr);
+    Context &c = g_ctx;
+    CB_TRY(init(c));
+    // pageable host arrays through the ring, as sha_point
+    const double *din = nullptr;
+    if (cell->ncell > 0 && is_pageable(f))
+    {
+        double *d = nullptr;
+        CB_TRY(dbuf(c, "stage_in", cell->ncell, &d));
+        CB_TRY(stage_h2d(c, d, f, cell->ncell * 8));
+        din = d;
+    }
+    const double *pc = pageable_tri(shcs->c, shcs->nmax);
+    const double *ps = pageable_tri(shcs->s, shcs->nmax);
+    if (pc && ps)
+    {
+        const size_t Ts = (size_t)(shcs->nmax + 1) * (shcs->nmax + 2) / 2;
+        double *dout = nullptr;
+        CB_TRY(dbuf(c, "stage_shc", 2 * Ts, &dout));
+        CB_TRY(sha_cell_grid(c, cell, din ? nullptr : f, din, nmax, shcs->mu,
+                             shcs->r, shcs->nmax, nullptr, nullptr, dout,
+                             dout + Ts));
+        CB_TRY(stage_d2h(c, const_cast<double *>(pc), dout, Ts * 8));
+        return stage_d2h(c, const_cast<double *>(ps), dout + Ts, Ts * 8);
+    }
+    return sha_cell_grid(c, cell, din ? nullptr : f, din, nmax, shcs->mu,
+                         shcs->r, shcs->nmax, shcs->c, shcs->s, nullptr,
+                         nullptr);
 }
 
 Status sha_cell_dev(const charm_cell *cell, const double *d_f,
@@ -4371,6 +4726,7 @@ struct BatchGraph
 {
     cudaGraphExec_t exec = nullptr;
     std::vector<void *> pins;
+    unsigned long long epoch = 0;  // the context's epoch at capture
 };
 
 Status batch_graph_create(const charm_point *pnt, size_t nsets,
@@ -4443,6 +4799,7 @@ Status batch_graph_create(const charm_point *pnt, size_t nsets,
         return st;
     }
     G->pins.swap(pins);
+    G->epoch = c.epoch;
     *out = G;
     return st;
 }
@@ -4453,6 +4810,17 @@ Status batch_graph_launch(void *h)
     Context &c = g_ctx;
     Status st;
     BatchGraph *G = static_cast<BatchGraph *>(h);
+    if (G->epoch != c.epoch)
+    {
+        // a call since the capture reallocated or rewrote buffers or
+        // tables the graph reads: replaying it would touch freed or other
+        // memory
+        st.code = CHARM_EFUNCARG;
+        st.msg = "the library's cached buffers or tables changed since this "
+                 "graph was captured (a call with other sizes ran in "
+                 "between); capture the graph again";
+        return st;
+    }
     CB_CUDA(cudaGraphLaunch(G->exec, c.stream), st);
     c.launches++;
     void *p = nullptr;
@@ -4557,14 +4925,10 @@ Status shs_point_f32_host(const charm_point *pnt, unsigned long shc_nmax,
     CB_TRY(dbuf(cx, "f32h_c", T, &dc));
     CB_TRY(dbuf(cx, "f32h_s", T, &ds));
     CB_TRY(dbuf(cx, "f32h_f", npt, &df));
-    CB_CUDA(cudaMemcpyAsync(dc, c, T * 4, cudaMemcpyHostToDevice, cx.stream),
-            st);
-    CB_CUDA(cudaMemcpyAsync(ds, s, T * 4, cudaMemcpyHostToDevice, cx.stream),
-            st);
+    CB_TRY(stage_h2d(cx, dc, c, T * 4));
+    CB_TRY(stage_h2d(cx, ds, s, T * 4));
     CB_TRY(shs_grid_f32(cx, pnt, shc_nmax, mu, r, dc, ds, nmax, df));
-    CB_CUDA(cudaMemcpyAsync(f, df, npt * 4, cudaMemcpyDeviceToHost,
-                            cx.stream), st);
-    CB_CUDA(cudaStreamSynchronize(cx.stream), st);
+    CB_TRY(stage_d2h(cx, f, df, npt * 4));
     return st;
 }
 
@@ -4582,14 +4946,10 @@ Status sha_point_f32_host(const charm_point *pnt, const float *f,
     CB_TRY(dbuf(cx, "f32h_c", T, &dc));
     CB_TRY(dbuf(cx, "f32h_s", T, &ds));
     CB_TRY(dbuf(cx, "f32h_f", npt, &df));
-    CB_CUDA(cudaMemcpyAsync(df, f, npt * 4, cudaMemcpyHostToDevice,
-                            cx.stream), st);
+    CB_TRY(stage_h2d(cx, df, f, npt * 4));
     CB_TRY(sha_grid_f32(cx, pnt, df, nmax, mu, r, shc_nmax, dc, ds));
-    CB_CUDA(cudaMemcpyAsync(c, dc, T * 4, cudaMemcpyDeviceToHost, cx.stream),
-            st);
-    CB_CUDA(cudaMemcpyAsync(s, ds, T * 4, cudaMemcpyDeviceToHost, cx.stream),
-            st);
-    CB_CUDA(cudaStreamSynchronize(cx.stream), st);
+    CB_TRY(stage_d2h(cx, c, dc, T * 4));
+    CB_TRY(stage_d2h(cx, s, ds, T * 4));
     return st;
 }
 
@@ -4740,7 +5100,16 @@ void shutdown()
     if (c.h_status)
         cudaFreeHost(c.h_status);
     c.h_status = nullptr;
-    c.tab_nmax = -1;
+    for (int b = 0; b < RING_N; b++)
+    {
+        if (c.ring[b])
+            cudaFreeHost(c.ring[b]);
+        c.ring[b] = nullptr;
+        if (c.ring_ev[b])
+            cudaEventDestroy(c.ring_ev[b]);
+        c.ring_ev[b] = nullptr;
+    }
+    c.tab_nmax[0] = c.tab_nmax[1] = -1;
     c.ready = false;
 }
 

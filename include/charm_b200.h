@@ -391,7 +391,11 @@ CHARM_EXTERN void CHARM_CDECL charm_b200_shs_point_batch_dev(
  * charm_b200_graph_launch replays the whole call (every launch, copy and
  * row transform of it) on the same device buffers, whose contents the
  * caller may change between launches, and reports the kernels' status;
- * charm_b200_graph_free releases the graph. */
+ * charm_b200_graph_free releases the graph.  The graph also reads the
+ * library's own cached buffers and tables by address: a launch after a
+ * call that reallocated or rewrote them (larger sizes, another maximum
+ * degree) is refused with CHARM_EFUNCARG, and the graph must be captured
+ * again. */
 CHARM_EXTERN void *CHARM_CDECL charm_b200_shs_point_batch_graph(
     const charm_point *pnt, size_t nsets, const unsigned long *nmax,
     const unsigned long *shc_nmax, const double *mu, double r,

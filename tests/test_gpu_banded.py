@@ -1,4 +1,5 @@
-"""Host-array entry points with the grid copied in bands: charm_shs_point
+"""Host-array entry points with page-locked host arrays, the grid copied in
+bands: charm_shs_point
 copies the rows of each band of latitude tiles to the host while the next
 band is synthesised, charm_sha_point copies band b while band b - 1 is
 transformed and analysed, and copies the coefficients to the host in bands
@@ -6,7 +7,9 @@ of orders while the last band is analysed.  Synthesis work items compute the
 same sums as in one launch, so the grids equal those of the device-array
 entry point bit for bit.  The analysis of a host grid adds its partial sums
 in groups of single latitude tiles (the device-array entry point in larger
-groups), so its coefficients agree to rounding: 1e-14 relative RMS."""
+groups), so its coefficients agree to rounding: 1e-14 relative RMS.
+(Pageable host arrays take the ring of page-locked buffers instead:
+tests/test_gpu_pageable.py.)"""
 import ctypes as ct
 
 import numpy as np
@@ -61,6 +64,35 @@ def device_sha(env, p, f, N):
     return oc.cpu().numpy(), os_.cpu().numpy()
 
 
+def pinned_round_trip(env, p, c, s, N, analyse):
+    """charm_shs_point (and charm_sha_point of its grid) with page-locked
+    host arrays: the banded paths."""
+    torch, cb, L = env
+    P = ct.POINTER(ct.c_double)
+    T = (N + 1) * (N + 2) // 2
+    hc = torch.from_numpy(c).pin_memory()
+    hs = torch.from_numpy(s).pin_memory()
+    hf = torch.empty(p.lat.size * p.lon.size, dtype=torch.float64).pin_memory()
+    oc = torch.zeros(T, dtype=torch.float64).pin_memory()
+    os_ = torch.zeros(T, dtype=torch.float64).pin_memory()
+    shc_in = L.charm_shc_init(N, GM, R_EARTH, ct.cast(hc.data_ptr(), P),
+                              ct.cast(hs.data_ptr(), P))
+    shc_out = L.charm_shc_init(N, GM, R_EARTH, ct.cast(oc.data_ptr(), P),
+                               ct.cast(os_.data_ptr(), P))
+    err = L.charm_err_init()
+    L.charm_shs_point(p._Point, shc_in, N, ct.cast(hf.data_ptr(), P), err)
+    assert L.charm_err_isempty(err)
+    if analyse:
+        L.charm_sha_point(p._Point, ct.cast(hf.data_ptr(), P), N, shc_out,
+                          err)
+        assert L.charm_err_isempty(err)
+    L.charm_err_free(err)
+    L.charm_shc_free(shc_in)
+    L.charm_shc_free(shc_out)
+    return (hf.numpy().reshape(p.lat.size, p.lon.size).copy(),
+            oc.numpy().copy(), os_.numpy().copy())
+
+
 @pytest.mark.parametrize("grid,N,h", [("GL", 2190, 0.0), ("GL", 601, 0.0),
                                       ("DH1", 800, 0.0), ("DH2", 700, 3e4)])
 def test_host_paths_equal_device_paths(env, grid, N, h):
@@ -69,18 +101,16 @@ def test_host_paths_equal_device_paths(env, grid, N, h):
             "DH2": cb.PointGridDH2}[grid]
     p = ctor(N, R_EARTH + h)
     c, s = kaula(N, 880 + N)
-    shc = cb.Shc(N, GM, R_EARTH, c, s)
-    f_host = cb.shs_point(p, shc, N)
+    f_host, hc, hs = pinned_round_trip(env, p, c, s, N, h == 0.0)
     f_dev = device_shs(env, p, c, s, N)
     assert np.array_equal(f_host, f_dev)
     if h == 0.0:
-        out = cb.sha_point(p, f_host, N, GM, R_EARTH)
         oc, os_ = device_sha(env, p, f_host, N)
-        assert coef_rel_rms(out.c, out.s, oc, os_) <= 1e-14
+        assert coef_rel_rms(hc, hs, oc, os_) <= 1e-14
         # every coefficient, not only the RMS
         scale = np.max(np.abs(np.concatenate([oc, os_])))
-        assert np.max(np.abs(out.c - oc)) <= 1e-13 * scale
-        assert np.max(np.abs(out.s - os_)) <= 1e-13 * scale
+        assert np.max(np.abs(hc - oc)) <= 1e-13 * scale
+        assert np.max(np.abs(hs - os_)) <= 1e-13 * scale
 
 
 class ScatteredShc:
@@ -117,15 +147,19 @@ def test_repeated_calls_and_scattered_columns(env):
     p = cb.PointGridGL(N, R_EARTH)
     c, s = kaula(N, 777)
     f_dev = device_shs(env, p, c, s, N)
-    shc = cb.Shc(N, GM, R_EARTH, c, s)
     for _ in range(3):
-        assert np.array_equal(cb.shs_point(p, shc, N), f_dev)
+        assert np.array_equal(pinned_round_trip(env, p, c, s, N, False)[0],
+                              f_dev)
     sc = ScatteredShc(N, c, s)
-    f = np.empty(p.lat.size * p.lon.size)
+    # page-locked grids (the banded paths), coefficient columns in
+    # pageable arrays of their own
+    f = torch.empty(p.lat.size * p.lon.size,
+                    dtype=torch.float64).pin_memory().numpy()
     P = ct.POINTER(ct.c_double)
     oc, os_ = device_sha(env, p, f_dev, N)
     out = ScatteredShc(N, np.zeros_like(c), np.zeros_like(s))
-    fd = np.ascontiguousarray(f_dev).ravel()
+    fd = torch.from_numpy(np.ascontiguousarray(f_dev).ravel()).pin_memory()
+    fd = fd.numpy()
     for _ in range(2):
         err = L.charm_err_init()
         L.charm_shs_point(p._Point, sc.ptr, N, f.ctypes.data_as(P), err)

@@ -100,3 +100,41 @@ def test_graph_replays_the_call(env, split, kgrad):
     finally:
         L.charm_b200_graph_free(g)
         L.charm_err_free(err)
+
+
+def test_graph_refuses_replay_after_buffers_changed(env):
+    """A call with larger sizes between capture and replay reallocates the
+    library's cached buffers the graph reads by address: the replay is
+    refused with an error (no kernel touches freed memory), and a graph
+    captured again replays."""
+    torch, cb, L = env
+    P = ct.c_void_p
+    pnt = cb.PointGridGL(150, R_EARTH)
+    b = Batch(env, pnt, [150, 90], 1, 1400)
+    err = L.charm_err_init()
+    args = (ct.cast(pnt._Point, P), b.n, b.nm, b.nm, b.mu, R_EARTH, b.pc, b.ps,
+            0, b.pf)
+    g = L.charm_b200_shs_point_batch_graph(*args, 0, ct.cast(err, P))
+    check(L, err)
+    L.charm_b200_graph_launch(g, ct.cast(err, P))
+    check(L, err)
+    ref = b.outputs()
+    # a larger synthesis in between: grows the cached buffers
+    big = cb.PointGridGL(1200, R_EARTH)
+    c, s = kaula(1200, 1401)
+    cb.shs_point(big, cb.Shc(1200, GM, R_EARTH, c, s), 1200)
+    L.charm_b200_graph_launch(g, ct.cast(err, P))
+    assert not L.charm_err_isempty(err)
+    assert b"capture the graph again" in ct.string_at(err.contents.msg)
+    L.charm_err_reset(err)
+    L.charm_b200_graph_free(g)
+    g = L.charm_b200_shs_point_batch_graph(*args, 0, ct.cast(err, P))
+    check(L, err)
+    for t in b.f:
+        t.fill_(np.nan)
+    L.charm_b200_graph_launch(g, ct.cast(err, P))
+    check(L, err)
+    for a, r in zip(b.outputs(), ref):
+        assert np.array_equal(a, r)
+    L.charm_b200_graph_free(g)
+    L.charm_err_free(err)
