@@ -76,6 +76,8 @@ struct DevBuf
     size_t bytes = 0;
 };
 
+constexpr int TAB_SLOTS = 3;
+
 struct Context
 {
     bool ready = false;
@@ -99,11 +101,12 @@ struct Context
     // (stage_h2d / stage_d2h); ring_ev[b] marks the last copy on buffer b
     void *ring[4] = {};
     cudaEvent_t ring_ev[4] = {};
-    // recurrence tables of two maximum degrees (a least-recently-used pair
-    // of slots, so that calls alternating between two degrees, e.g. a
-    // synthesis and an analysis of another degree, rebuild nothing)
-    long long tab_nmax[2] = {-1, -1};
-    unsigned long long tab_used[2] = {0, 0};
+    // recurrence tables of up to TAB_SLOTS maximum degrees (least recently
+    // used slot rewritten), so that calls alternating between a few
+    // degrees, e.g. syntheses and analyses of other degrees, rebuild
+    // nothing
+    long long tab_nmax[TAB_SLOTS] = {-1, -1, -1};
+    unsigned long long tab_used[TAB_SLOTS] = {};
     unsigned long long tab_clock = 0;
     // bumped whenever a cached device buffer is (re)allocated or a cached
     // table is rewritten: a captured graph reads these by address, so it
@@ -123,6 +126,11 @@ struct Context
     std::map<std::tuple<int, int, int, int, long long, int>,
              std::pair<int, std::vector<std::pair<int, float>>>>
         tuned;
+    // quadrature nodes and weights by (grid type, nmax), host copies of
+    // the last few grids built (they are deterministic; forward modelling
+    // builds the same grids at every call)
+    std::map<std::pair<int, unsigned long>, std::vector<double>> nodes;
+    std::vector<std::pair<int, unsigned long>> nodes_order;
     std::map<long long, RfftArgs> rffts;   // row transforms by row length
     std::map<long long, void *> rfft_mem;  // their tables
     std::recursive_mutex mtx;
@@ -627,12 +635,20 @@ Status tables(Context &c, long long nmax, Tabs *tab)
     Status st;
     long long T = (nmax + 1) * (nmax + 2) / 2;
     tab->ldmul = (int)((nmax + 1 + 63) / 64);
-    int slot = c.tab_nmax[0] == nmax ? 0 : (c.tab_nmax[1] == nmax ? 1 : -1);
+    int slot = -1;
+    for (int k = 0; k < TAB_SLOTS; k++)
+        if (c.tab_nmax[k] == nmax)
+            slot = k;
     const bool hit = slot >= 0;
     if (!hit)
-        slot = c.tab_used[0] <= c.tab_used[1] ? 0 : 1;
+    {
+        slot = 0;
+        for (int k = 1; k < TAB_SLOTS; k++)
+            if (c.tab_used[k] < c.tab_used[slot])
+                slot = k;
+    }
     c.tab_used[slot] = ++c.tab_clock;
-    const std::string sfx = slot ? "#1" : "";
+    const std::string sfx = slot ? "#" + std::to_string(slot) : "";
     CB_TRY(dbuf(c, "tab_b" + sfx, (size_t)T, &tab->tb));
     CB_TRY(dbuf(c, "tab_c" + sfx, (size_t)T, &tab->tc));
     CB_TRY(dbuf(c, "tab_mul" + sfx, (size_t)(nmax + 1) * tab->ldmul,
@@ -4990,6 +5006,14 @@ Status quad_nodes(int type, unsigned long nmax, double *lat, double *w)
     CB_TRY(init(c));
     Status st;
     size_t nlat = type == CHARM_CRD_POINT_GRID_GL ? nmax + 1 : 2 * (nmax + 1);
+    const auto key = std::make_pair(type, nmax);
+    auto hit = c.nodes.find(key);
+    if (hit != c.nodes.end())
+    {
+        std::memcpy(lat, hit->second.data(), nlat * 8);
+        std::memcpy(w, hit->second.data() + nlat, nlat * 8);
+        return st;
+    }
     double *d = nullptr;
     CB_TRY(dbuf(c, "crd", 2 * nlat, &d));
     CB_CUDA(cudaMemsetAsync(d, 0, 2 * nlat * 8, c.stream), st);
@@ -5012,6 +5036,20 @@ Status quad_nodes(int type, unsigned long nmax, double *lat, double *w)
         st.msg = "Error in computing latitudes of the Gauss--Legendre grid.  "
                  "Either the maximum number of iterations was exceeded or at "
                  "least one latitude was detected to be not a real number.";
+    if (st.ok())
+    {
+        // keep the eight most recent grids
+        if (c.nodes_order.size() >= 8)
+        {
+            c.nodes.erase(c.nodes_order.front());
+            c.nodes_order.erase(c.nodes_order.begin());
+        }
+        std::vector<double> v(2 * nlat);
+        std::memcpy(v.data(), lat, nlat * 8);
+        std::memcpy(v.data() + nlat, w, nlat * 8);
+        c.nodes.emplace(key, std::move(v));
+        c.nodes_order.push_back(key);
+    }
     return st;
 }
 
@@ -5109,7 +5147,10 @@ void shutdown()
             cudaEventDestroy(c.ring_ev[b]);
         c.ring_ev[b] = nullptr;
     }
-    c.tab_nmax[0] = c.tab_nmax[1] = -1;
+    for (int k = 0; k < TAB_SLOTS; k++)
+        c.tab_nmax[k] = -1;
+    c.nodes.clear();
+    c.nodes_order.clear();
     c.ready = false;
 }
 
