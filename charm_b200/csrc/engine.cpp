@@ -77,6 +77,12 @@ struct DevBuf
 };
 
 constexpr int TAB_SLOTS = 3;
+// bands of the host-array calls' copies (at most 6 of each kind)
+constexpr int SHS_LAT_BANDS = 3;   // synthesis: grid rows down
+constexpr int SHA_LAT_BANDS = 3;   // analysis: grid rows up
+constexpr int SHS_ORD_BANDS = 4;   // synthesis: coefficients up
+constexpr int SHA_ORD_BANDS = 4;   // analysis: coefficients down
+constexpr int EV_LAT0 = 0, EV_ORD0 = 6, EV_START = 15;
 
 struct Context
 {
@@ -88,10 +94,10 @@ struct Context
     // `stream` (events order the two)
     cudaStream_t copy_stream = nullptr;
     // events between the compute and copy streams of the banded host-array
-    // calls: 0..2 the bands of latitude tiles (grid_bands gives at most
-    // three), 3..6 the bands of orders (at most four), 7 the start of the
-    // copy stream after the work already on the compute stream
-    cudaEvent_t band_ev[8] = {};
+    // calls: EV_LAT0.. the bands of latitude tiles, EV_ORD0.. the bands of
+    // orders, EV_START the start of the copy stream after the work already
+    // on the compute stream
+    cudaEvent_t band_ev[16] = {};
     // page-locked copy of the device status word read at the end of a call
     unsigned *h_status = nullptr;
     std::map<std::string, DevBuf> bufs;
@@ -1608,7 +1614,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
     std::vector<std::array<int, 6>> bands;
     const int nband =
         (!d_f && rf) ? grid_bands(P, (int)nlat, ntiles, 32 * K,
-                                  ntiles >= 6 ? 3 : 2, bands)
+                                  ntiles >= 6 ? SHS_LAT_BANDS : 2, bands)
                      : 1;
     if (coef_later && nband <= 1)
     {
@@ -1627,24 +1633,25 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
         CB_TRY(dbuf(c, "band_counters", 16, &bcnt));
         CB_CUDA(cudaMemsetAsync(bcnt, 0, 16 * sizeof(unsigned long long),
                                 c.stream), st);
-        // orders in up to four bands of about equal numbers of coefficients
+        // orders in up to SHS_ORD_BANDS bands of about equal numbers of
+        // coefficients
         std::vector<long long> mb{0};
         if (coef_later)
         {
             const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
-            for (int k = 1; k < 4; k++)
+            for (int k = 1; k < SHS_ORD_BANDS; k++)
             {
                 long long m = mb.back();
                 while (m <= (long long)nmax &&
-                       tri_start((long long)nmax, m) < k * T / 4)
+                       tri_start((long long)nmax, m) < k * T / SHS_ORD_BANDS)
                     m++;
                 if (m > mb.back() && m <= (long long)nmax)
                     mb.push_back(m);
             }
             // the copy stream starts after everything before it on the
             // stream; band k of the orders: copy (copy stream), then scale
-            CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
-            CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+            CB_CUDA(cudaEventRecord(c.band_ev[EV_START], c.stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[EV_START], 0), st);
         }
         mb.push_back((long long)nmax + 1);
         const int nob = (int)mb.size() - 1;
@@ -1655,7 +1662,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
                                          mb[k + 1], c.copy_stream));
                 CB_TRY(upload_tri_orders(in.hs, in.nmax, raw + Ts, mb[k],
                                          mb[k + 1], c.copy_stream));
-                CB_CUDA(cudaEventRecord(c.band_ev[3 + k], c.copy_stream),
+                CB_CUDA(cudaEventRecord(c.band_ev[EV_ORD0 + k], c.copy_stream),
                         st);
             }
         for (int b = 0; b < nband; b++)
@@ -1668,7 +1675,7 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
             {
                 if (split)
                 {
-                    CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[3 + k],
+                    CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[EV_ORD0 + k],
                                                 0),
                             st);
                     Scope sc(c, TIMER_PREP);
@@ -1708,8 +1715,10 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
                     Scope sc(c, TIMER_FFT);
                     CB_CUDA(launch_rfft(R, true, c.stream), st);
                 }
-            CB_CUDA(cudaEventRecord(c.band_ev[b], c.stream), st);
-            CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[b], 0), st);
+            CB_CUDA(cudaEventRecord(c.band_ev[EV_LAT0 + b], c.stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[EV_LAT0 + b],
+                                        0),
+                    st);
             for (int q = 0; q < npar; q++)
                 for (int h = 0; h < 2; h++)
                 {
@@ -2959,17 +2968,18 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
     std::vector<std::array<int, 6>> bands;
     const int nband = (fdev && rf) ? grid_bands(P, (int)nlat, (int)G,
                                                 32 * K * tpg,
-                                                G >= 3 ? 3 : 2, bands)
+                                                G >= 3 ? SHA_LAT_BANDS : 2,
+                                                bands)
                                    : 1;
     bool ordered = false;
     if (nband > 1)
     {
-        // orders of the last band in up to four bands of about equal
-        // numbers of coefficients
+        // orders of the last band in up to SHA_ORD_BANDS bands of about
+        // equal numbers of coefficients
         std::vector<long long> mb{0};
         if (!d_c)
         {
-            const int nob = 4;
+            const int nob = SHA_ORD_BANDS;
             for (int k = 1; k < nob; k++)
             {
                 long long m = mb.back();
@@ -2988,8 +2998,8 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                                 c.stream), st);
         // the copy stream starts after everything before it on the stream
         // (buffers in use by an earlier call)
-        CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
-        CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+        CB_CUDA(cudaEventRecord(c.band_ev[EV_START], c.stream), st);
+        CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[EV_START], 0), st);
         for (int b = 0; b < nband; b++)
         {
             const auto &bd = bands[b];
@@ -3004,8 +3014,9 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                                             c.copy_stream),
                             st);
             }
-            CB_CUDA(cudaEventRecord(c.band_ev[b], c.copy_stream), st);
-            CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[b], 0), st);
+            CB_CUDA(cudaEventRecord(c.band_ev[EV_LAT0 + b], c.copy_stream), st);
+            CB_CUDA(cudaStreamWaitEvent(c.stream, c.band_ev[EV_LAT0 + b], 0),
+                    st);
             for (int h = 0; h < 2; h++)
             {
                 const int r0 = bd[2 + 2 * h], r1 = bd[3 + 2 * h];
@@ -3042,7 +3053,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                                 part, tab.tc, dres, 1.0, oc, os, mb[k], m_hi,
                                 c.stream),
                             st);
-                    CB_CUDA(cudaEventRecord(c.band_ev[3 + k], c.stream), st);
+                    CB_CUDA(cudaEventRecord(c.band_ev[EV_ORD0 + k], c.stream), st);
                 }
             }
             if (split)
@@ -3055,7 +3066,7 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                     const long long m_hi =
                         k == nob - 1 ? (long long)sn + 1 : mb[k + 1];
                     CB_CUDA(cudaStreamWaitEvent(c.copy_stream,
-                                                c.band_ev[3 + k], 0),
+                                                c.band_ev[EV_ORD0 + k], 0),
                             st);
                     CB_TRY(download_tri_orders(oc, sn, hc, mb[k], m_hi,
                                                c.copy_stream));
@@ -3800,8 +3811,8 @@ Status shc_read_bin_dev_impl(Context &c, const char *path, unsigned long nmax,
                       static_cast<double *>(hp) + CHUNK};
     // the copy stream starts after the work already on the stream (buffers
     // the caller may still read)
-    CB_CUDA(cudaEventRecord(c.band_ev[7], c.stream), st);
-    CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[7], 0), st);
+    CB_CUDA(cudaEventRecord(c.band_ev[EV_START], c.stream), st);
+    CB_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_ev[EV_START], 0), st);
     bool used[2] = {false, false};
     int nb = 0;
     for (int part = 0; part < 2; part++)
