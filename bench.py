@@ -1090,10 +1090,10 @@ def cells(steps=5, oracle_rows=3):
     peak = L.charm_b200_fp64_peak_tflops()
     units = T * ((nlat + 1) // 2)
     # FP64 instructions per (n, m, cell-row pair): two boundary recurrences
-    # (DMUL + DFMA each), the integral (h beta, 2 DMUL + 2 DFMA) and two
-    # DFMA sums in synthesis; in analysis the sums are two DMUL into the
-    # transpose plus two DADD of the reduction
-    for name, ipu in (("shs_cell", 11.0), ("sha_cell", 13.0)):
+    # (DMUL + DFMA each), the integral (2 DMUL + 2 DFMA; h_n beta_n comes
+    # staged) and two DFMA sums; the analysis adds the reduction of the
+    # lane sums (two DADD per lane and degree for two pairs per lane)
+    for name, ipu in (("shs_cell", 10.0), ("sha_cell", 11.0)):
         k = res[name]
         k["fp64_instr_per_unit"] = ipu
         k["fp64_pipe_frac"] = (units * ipu / (k["legendre_ms"] * 1e-3) /

@@ -80,8 +80,8 @@ __device__ __forceinline__ Stage warp_stage_sha(unsigned char *base)
 }
 
 // Stages chunk j of order m: entries n = m + 64 j + i, i < cnt, of the
-// order's column (tb, cs) and of the per-degree table hn.  The warp reads
-// the stage only after the __syncwarp that ends this function.
+// order's column (tb, cs) and (h_n beta_n, 1 / (n + 1)) in hn.  The warp
+// reads the stage only after the __syncwarp that ends this function.
 __device__ __forceinline__ void stage_chunk(const Stage &S, const CellArgs &A,
                                             long long c0, long long m, int j,
                                             int cnt, unsigned lane)
@@ -94,10 +94,14 @@ __device__ __forceinline__ void stage_chunk(const Stage &S, const CellArgs &A,
         const int i = (int)lane + 32 * h;
         if (i < cnt)
         {
-            S.tb[i] = A.tb[c0 + off + i];
+            const double2 b = A.tb[c0 + off + i];
+            const double2 h = A.hn[m + off + i];
+            S.tb[i] = b;
             if (S.cs)
                 S.cs[i] = A.cs[c0 + off + i];
-            S.hn[i] = A.hn[m + off + i];
+            // h_n beta_n formed once here instead of by every lane per
+            // degree
+            S.hn[i] = make_double2(h.x * b.x, h.y);
         }
         else
         {
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell(CellArgs A)
                 auto one = [&](int i, bool odd) {
                     const double beta = S.tb[i].x;
                     const double2 h = S.hn[i];
-                    const double J = R.step(beta, h.x * beta, h.y);
+                    const double J = R.step(beta, h.x, h.y);
                     const double v = RR ? J * rn : J;
                     if (RR)
                         rn *= rho;
@@ -572,7 +576,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                     any_scaled |= (R[k].E1 | R[k].E2) != 0;
                     // state before degree m: (x, y) = (0, R~_mm) and
                     // J0 = -J~_mm, so that the step of degree m with the
-                    // staged beta = -1, h = 1, 1/(n+1) = 0 yields R~_mm and
+                    // staged beta = -1, h beta = -1, 1/(n+1) = 0 yields R~_mm and
                     // J~_mm: every degree takes the same step
                     R[k].y1 = R[k].x1;
                     R[k].x1 = 0.0;
@@ -688,7 +692,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                     if (lane == 0)
                     {
                         S.tb[0].x = -1.0;
-                        S.hn[0] = make_double2(1.0, 0.0);
+                        S.hn[0] = make_double2(-1.0, 0.0);   // h beta, 0
                     }
                     __syncwarp();
                 }
@@ -716,7 +720,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                         const int i = ib + jj;
                         const double beta = S.tb[i].x;
                         const double2 h = S.hn[i];
-                        const double hb = h.x * beta;
+                        const double hb = h.x;
                         const bool odd = (jj & 1) != 0;
                         double vc = 0.0, vs = 0.0;
 #pragma unroll
@@ -894,7 +898,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell_sctr(CellArgs A)
                     {
                         const double beta = S.tb[i].x;
                         const double2 h = S.hn[i];
-                        const double J = R.step(beta, h.x * beta, h.y);
+                        const double J = R.step(beta, h.x, h.y);
                         const double v = RR ? J * rn : J;
                         if (RR)
                             rn *= rho;

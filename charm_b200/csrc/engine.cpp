@@ -78,8 +78,8 @@ struct DevBuf
 
 constexpr int TAB_SLOTS = 3;
 // bands of the host-array calls' copies (at most 6 of each kind)
-constexpr int SHS_LAT_BANDS = 3;   // synthesis: grid rows down
-constexpr int SHA_LAT_BANDS = 3;   // analysis: grid rows up
+constexpr int SHS_LAT_BANDS = 4;   // synthesis: grid rows down
+constexpr int SHA_LAT_BANDS = 4;   // analysis: grid rows up
 constexpr int SHS_ORD_BANDS = 4;   // synthesis: coefficients up
 constexpr int SHA_ORD_BANDS = 4;   // analysis: coefficients down
 constexpr int EV_LAT0 = 0, EV_ORD0 = 6, EV_START = 15;
