@@ -163,6 +163,39 @@ struct CellRec
     }
 };
 
+// One degree of two adjacent cell rows r0 (above) and r1 (below) whose
+// common boundary, r0's lower and r1's upper, is carried once, by r0
+// (r1's boundary-2 state is not advanced): three boundary recurrences
+// instead of four and one product w x of the common boundary for both
+// integrals.  r0's value rounds as CellRec::step; r1's difference of
+// boundary terms is formed from the rounded common product.
+__device__ __forceinline__ void step_shared(CellRec &r0, CellRec &r1,
+                                            double beta, double hb,
+                                            double inv, double &v0,
+                                            double &v1)
+{
+    const double q = r0.w1 * r0.x1;
+    const double d0 = fma(r0.w2, r0.x2, -q);
+    const double d1 = fma(-r1.w1, r1.x1, q);
+    const double J0 = fma(hb, r0.J0, -(d0 * inv));
+    const double J1 = fma(hb, r1.J0, -(d1 * inv));
+    r0.J0 = r0.J1;
+    r0.J1 = J0;
+    r1.J0 = r1.J1;
+    r1.J1 = J1;
+    const double za = fma(r0.t1, r0.x1, -(beta * r0.y1));
+    r0.y1 = r0.x1;
+    r0.x1 = za;
+    const double zb = fma(r0.t2, r0.x2, -(beta * r0.y2));
+    r0.y2 = r0.x2;
+    r0.x2 = zb;
+    const double zc = fma(r1.t1, r1.x1, -(beta * r1.y1));
+    r1.y1 = r1.x1;
+    r1.x1 = zc;
+    v0 = J0;
+    v1 = J1;
+}
+
 // Seeds of order m >= 1 at one cell row: R~_mm at both boundaries and
 // J~_mm = I_mm 2^g0 (I_mm in real units from imm).
 __device__ __forceinline__ void cell_seed(CellRec &R, double sigma, int g0,
@@ -480,10 +513,11 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell(CellArgs A)
 // degree n0 + l, added to the group's partial column (the warp owns it);
 // k_sha_reduce sums the groups in fixed order and applies ct_n, the
 // 1 / (4 pi) r / mu factor and the rescaling.
-template <int K>
+template <int K, bool SH>
 __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
     k_sha_cell(CellArgs A)
 {
+    static_assert(!SH || K == 2, "shared boundaries pair two rows");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31u;
     const unsigned warp = threadIdx.x >> 5;
@@ -524,7 +558,9 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
 #pragma unroll
             for (int k = 0; k < K; k++)
             {
-                const int p = tile * (32 * K) + k * 32 + (int)lane;
+                // with shared boundaries a lane takes two adjacent pairs
+                const int p = SH ? tile * 64 + 2 * (int)lane + k
+                                 : tile * (32 * K) + k * 32 + (int)lane;
                 const bool valid = p < np;
                 R[k].t1 = valid ? A.geo[0 * np + p] : 0.0;
                 const double u1 = valid ? A.geo[1 * np + p] : 1.0;
@@ -584,6 +620,9 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                     R[k].x2 = 0.0;
                     R[k].J0 = -R[k].J1;
                     R[k].J1 = 0.0;
+                    // the common boundary is renormalised through r0
+                    if (SH && k == 1)
+                        R[k].E2 = 0;
                 }
             }
             if (__all_sync(0xffffffffu, all_skip))
@@ -723,12 +762,24 @@ __global__ void __launch_bounds__(CELL_WARPS * 32, K == 1 ? 3 : 2)
                         const double hb = h.x;
                         const bool odd = (jj & 1) != 0;
                         double vc = 0.0, vs = 0.0;
-#pragma unroll
-                        for (int k = 0; k < K; k++)
+                        if constexpr (SH)
                         {
-                            const double v = R[k].step(beta, hb, h.y);
-                            vc = fma(v, odd ? amm[k] : amp[k], vc);
-                            vs = fma(v, odd ? bmm[k] : bmp[k], vs);
+                            double v0, v1;
+                            step_shared(R[0], R[K - 1], beta, hb, h.y, v0, v1);
+                            vc = fma(v0, odd ? amm[0] : amp[0], vc);
+                            vs = fma(v0, odd ? bmm[0] : bmp[0], vs);
+                            vc = fma(v1, odd ? amm[K - 1] : amp[K - 1], vc);
+                            vs = fma(v1, odd ? bmm[K - 1] : bmp[K - 1], vs);
+                        }
+                        else
+                        {
+#pragma unroll
+                            for (int k = 0; k < K; k++)
+                            {
+                                const double v = R[k].step(beta, hb, h.y);
+                                vc = fma(v, odd ? amm[k] : amp[k], vc);
+                                vs = fma(v, odd ? bmm[k] : bmp[k], vs);
+                            }
                         }
                         put(jj, vc, vs);
                     }
@@ -1012,15 +1063,16 @@ cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
     return cudaGetLastError();
 }
 
-cudaError_t launch_sha_cell(const CellArgs &A, int K, int grid,
+cudaError_t launch_sha_cell(const CellArgs &A, int K, bool shared, int grid,
                             cudaStream_t st)
 {
     const size_t smem = CELL_WARPS * CELL_SHA_WARP_BYTES;
     static bool attr_set = false;
     if (!attr_set)
     {
-        for (const void *f : {(const void *)k_sha_cell<1>,
-                              (const void *)k_sha_cell<2>})
+        for (const void *f : {(const void *)k_sha_cell<1, false>,
+                              (const void *)k_sha_cell<2, false>,
+                              (const void *)k_sha_cell<2, true>})
         {
             cudaError_t e = cudaFuncSetAttribute(
                 f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1029,10 +1081,12 @@ cudaError_t launch_sha_cell(const CellArgs &A, int K, int grid,
         }
         attr_set = true;
     }
-    if (K == 2)
-        k_sha_cell<2><<<grid, CELL_WARPS * 32, smem, st>>>(A);
+    if (K == 2 && shared)
+        k_sha_cell<2, true><<<grid, CELL_WARPS * 32, smem, st>>>(A);
+    else if (K == 2)
+        k_sha_cell<2, false><<<grid, CELL_WARPS * 32, smem, st>>>(A);
     else
-        k_sha_cell<1><<<grid, CELL_WARPS * 32, smem, st>>>(A);
+        k_sha_cell<1, false><<<grid, CELL_WARPS * 32, smem, st>>>(A);
     return cudaGetLastError();
 }
 

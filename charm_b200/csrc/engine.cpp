@@ -3658,8 +3658,13 @@ Status sha_cell_grid(Context &c, const charm_cell *cell, const double *f_host,
     unsigned long long *d_counter;
     CB_TRY(status_words(c, &d_status, &d_counter));
     const long long T = (long long)(nmax + 1) * (nmax + 2) / 2;
-    // two cell-row pairs per lane once there are enough of them
+    // two cell-row pairs per lane once there are enough of them; adjacent
+    // ones (pairs 2l, 2l + 1) when each such pair of rows shares a
+    // boundary, which the kernel then carries once
     const int K = np >= 512 ? 2 : 1;
+    bool shared = K == 2;
+    for (int p = 0; shared && p + 1 < np; p += 2)
+        shared = cell->latmin[P.row_n[p]] == cell->latmax[P.row_n[p + 1]];
     const int ntiles = (np + 32 * K - 1) / (32 * K);
     const long long slots = (long long)c.num_sms * 8 * 4;
     long long G = std::max<long long>(1, (2 * slots + nmax) / (nmax + 1));
@@ -3704,7 +3709,8 @@ Status sha_cell_grid(Context &c, const charm_cell *cell, const double *f_host,
         const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                                   (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHA);
-        CB_CUDA(launch_sha_cell(A, K, std::max(grid, 1), c.stream), st);
+        CB_CUDA(launch_sha_cell(A, K, shared, std::max(grid, 1), c.stream),
+                st);
     }
 
     // 1 / (4 pi) r0 / mu and the rescaling from r0 to R

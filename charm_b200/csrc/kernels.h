@@ -320,7 +320,9 @@ cudaError_t launch_cell_imm(const CellArgs &A, cudaStream_t st);
 cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
                             cudaStream_t st);
 // K cell-row pairs per lane (1 or 2); A.ntiles counts tiles of 32 K pairs
-cudaError_t launch_sha_cell(const CellArgs &A, int K, int grid,
+// shared: pairs 2l and 2l + 1 are adjacent cell rows (the lower boundary
+// of the first is the upper one of the second); K must be 2
+cudaError_t launch_sha_cell(const CellArgs &A, int K, bool shared, int grid,
                             cudaStream_t st);
 cudaError_t launch_shs_cell_sctr(const CellArgs &A, bool rr, int grid,
                                  cudaStream_t st);
