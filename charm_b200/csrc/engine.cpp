@@ -497,17 +497,25 @@ Status ring_ready(Context &c)
     return st;
 }
 
-// Host to device on the compute stream; a pageable source is read through
-// the ring (the caller may change it once this returns).
-Status stage_h2d(Context &c, void *dst, const void *src, size_t bytes)
+// Host to device on stream q (the compute stream when null); a pageable
+// source is read through the ring (the caller may change it once this
+// returns).  `pageable` < 0 asks the driver about src; callers that copy
+// one array in several pieces decide once, for the whole array, and pass
+// 0 or 1.
+Status stage_h2d(Context &c, void *dst, const void *src, size_t bytes,
+                 cudaStream_t q = nullptr, int pageable = -1)
 {
     Status st;
+    if (!q)
+        q = c.stream;
     if (bytes == 0)
         return st;
-    if (!is_pageable(src))
+    if (pageable < 0)
+        pageable = is_pageable(src) ? 1 : 0;
+    if (!pageable)
     {
-        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice,
-                                c.stream), st);
+        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, q),
+                st);
         return st;
     }
     CB_TRY(ring_ready(c));
@@ -521,25 +529,30 @@ Status stage_h2d(Context &c, void *dst, const void *src, size_t bytes)
         CB_CUDA(cudaEventSynchronize(c.ring_ev[b]), st);
         copy_pool().copy(c.ring[b], s + off, len);
         CB_CUDA(cudaMemcpyAsync(d + off, c.ring[b], len,
-                                cudaMemcpyHostToDevice, c.stream), st);
-        CB_CUDA(cudaEventRecord(c.ring_ev[b], c.stream), st);
+                                cudaMemcpyHostToDevice, q), st);
+        CB_CUDA(cudaEventRecord(c.ring_ev[b], q), st);
     }
     return st;
 }
 
-// Device to host after the work already on the compute stream; returns
-// when the host array holds the data.  A pageable destination is written
-// through the ring.
-Status stage_d2h(Context &c, void *dst, const void *src, size_t bytes)
+// Device to host after the work already on stream q (the compute stream
+// when null); returns when the host array holds the data.  A pageable
+// destination is written through the ring.
+Status stage_d2h(Context &c, void *dst, const void *src, size_t bytes,
+                 cudaStream_t q = nullptr, int pageable = -1)
 {
     Status st;
+    if (!q)
+        q = c.stream;
     if (bytes == 0)
         return st;
-    if (!is_pageable(dst))
+    if (pageable < 0)
+        pageable = is_pageable(dst) ? 1 : 0;
+    if (!pageable)
     {
-        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost,
-                                c.stream), st);
-        CB_CUDA(cudaStreamSynchronize(c.stream), st);
+        CB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, q),
+                st);
+        CB_CUDA(cudaStreamSynchronize(q), st);
         return st;
     }
     CB_TRY(ring_ready(c));
@@ -550,10 +563,13 @@ Status stage_d2h(Context &c, void *dst, const void *src, size_t bytes)
         Status s2;
         const int b = (int)(i % RING_N);
         const size_t off = i * RING_CHUNK;
+        // an earlier copy out of this buffer, possibly on another stream,
+        // has read it
+        CB_CUDA(cudaStreamWaitEvent(q, c.ring_ev[b], 0), s2);
         CB_CUDA(cudaMemcpyAsync(c.ring[b], s + off,
                                 std::min(RING_CHUNK, bytes - off),
-                                cudaMemcpyDeviceToHost, c.stream), s2);
-        CB_CUDA(cudaEventRecord(c.ring_ev[b], c.stream), s2);
+                                cudaMemcpyDeviceToHost, q), s2);
+        CB_CUDA(cudaEventRecord(c.ring_ev[b], q), s2);
         return s2;
     };
     for (size_t i = 0; i < std::min<size_t>(RING_N, nch); i++)
@@ -972,11 +988,7 @@ Status upload_tri(Context &c, double *const *cols, unsigned long shc_nmax,
     const double *base = contiguous_tri(cols, shc_nmax);
     size_t T = (size_t)(shc_nmax + 1) * (shc_nmax + 2) / 2;
     if (base)
-    {
-        CB_CUDA(cudaMemcpyAsync(dst, base, T * 8, cudaMemcpyHostToDevice,
-                                c.stream), st);
-        return st;
-    }
+        return stage_h2d(c, dst, base, T * 8);
     size_t idx = 0;
     for (unsigned long m = 0; m <= shc_nmax; m++)
     {
@@ -996,9 +1008,16 @@ Status download_tri(Context &c, const double *src, unsigned long shc_nmax,
     size_t T = (size_t)(shc_nmax + 1) * (shc_nmax + 2) / 2;
     if (base)
     {
-        CB_CUDA(cudaMemcpyAsync(const_cast<double *>(base), src, T * 8,
-                                cudaMemcpyDeviceToHost, c.stream), st);
-        return st;
+        // a page-locked destination is copied asynchronously (the call's
+        // final synchronisation waits for it); a pageable one through the
+        // ring, which returns when the copy is done
+        if (!is_pageable(base))
+        {
+            CB_CUDA(cudaMemcpyAsync(const_cast<double *>(base), src, T * 8,
+                                    cudaMemcpyDeviceToHost, c.stream), st);
+            return st;
+        }
+        return stage_d2h(c, const_cast<double *>(base), src, T * 8);
     }
     size_t idx = 0;
     for (unsigned long m = 0; m <= shc_nmax; m++)
@@ -1019,10 +1038,11 @@ long long tri_start(long long N, long long m)
 }
 
 // The columns m_lo <= m < m_hi of a charm_shc's host columns into a device
-// triangle of degree shc_nmax, on stream st.
-Status upload_tri_orders(double *const *cols, unsigned long shc_nmax,
-                         double *dst, long long m_lo, long long m_hi,
-                         cudaStream_t st)
+// triangle of degree shc_nmax, on stream st (pg: the host triangle is
+// pageable, copied through the ring).
+Status upload_tri_orders(Context &c, double *const *cols,
+                         unsigned long shc_nmax, double *dst, long long m_lo,
+                         long long m_hi, cudaStream_t st, int pg)
 {
     Status s2;
     if (m_hi <= m_lo)
@@ -1032,10 +1052,8 @@ Status upload_tri_orders(double *const *cols, unsigned long shc_nmax,
     if (base)
     {
         const long long i0 = tri_start(N, m_lo), i1 = tri_start(N, m_hi);
-        CB_CUDA(cudaMemcpyAsync(dst + i0, base + i0, (size_t)(i1 - i0) * 8,
-                                cudaMemcpyHostToDevice, st),
-                s2);
-        return s2;
+        return stage_h2d(c, dst + i0, base + i0, (size_t)(i1 - i0) * 8, st,
+                         pg);
     }
     for (long long m = m_lo; m < m_hi; m++)
         CB_CUDA(cudaMemcpyAsync(dst + tri_start(N, m), cols[m],
@@ -1046,10 +1064,12 @@ Status upload_tri_orders(double *const *cols, unsigned long shc_nmax,
 }
 
 // The columns m_lo <= m < m_hi of a device triangle of degree shc_nmax into
-// a charm_shc's host columns, on stream st.
-Status download_tri_orders(const double *src, unsigned long shc_nmax,
-                           double *const *cols, long long m_lo,
-                           long long m_hi, cudaStream_t st)
+// a charm_shc's host columns, on stream st (pg: the host triangle is
+// pageable, copied through the ring).
+Status download_tri_orders(Context &c, const double *src,
+                           unsigned long shc_nmax, double *const *cols,
+                           long long m_lo, long long m_hi, cudaStream_t st,
+                           int pg)
 {
     Status s2;
     if (m_hi <= m_lo)
@@ -1059,11 +1079,17 @@ Status download_tri_orders(const double *src, unsigned long shc_nmax,
     if (base)
     {
         const long long i0 = tri_start(N, m_lo), i1 = tri_start(N, m_hi);
-        CB_CUDA(cudaMemcpyAsync(const_cast<double *>(base) + i0, src + i0,
-                                (size_t)(i1 - i0) * 8, cudaMemcpyDeviceToHost,
-                                st),
-                s2);
-        return s2;
+        double *dst = const_cast<double *>(base) + i0;
+        // page-locked: asynchronous on st; pageable: through the ring,
+        // done when this returns
+        if (!pg)
+        {
+            CB_CUDA(cudaMemcpyAsync(dst, src + i0, (size_t)(i1 - i0) * 8,
+                                    cudaMemcpyDeviceToHost, st),
+                    s2);
+            return s2;
+        }
+        return stage_d2h(c, dst, src + i0, (size_t)(i1 - i0) * 8, st, 1);
     }
     for (long long m = m_lo; m < m_hi; m++)
         CB_CUDA(cudaMemcpyAsync(cols[m], src + tri_start(N, m),
@@ -1658,10 +1684,10 @@ Status shs_grid(Context &c, const charm_point *pnt, const CoefIn &in,
         if (coef_later)
             for (int k = 0; k < nob; k++)
             {
-                CB_TRY(upload_tri_orders(in.hc, in.nmax, raw, mb[k],
-                                         mb[k + 1], c.copy_stream));
-                CB_TRY(upload_tri_orders(in.hs, in.nmax, raw + Ts, mb[k],
-                                         mb[k + 1], c.copy_stream));
+                CB_TRY(upload_tri_orders(c, in.hc, in.nmax, raw, mb[k],
+                                         mb[k + 1], c.copy_stream, 0));
+                CB_TRY(upload_tri_orders(c, in.hs, in.nmax, raw + Ts, mb[k],
+                                         mb[k + 1], c.copy_stream, 0));
                 CB_CUDA(cudaEventRecord(c.band_ev[EV_ORD0 + k], c.copy_stream),
                         st);
             }
@@ -1799,13 +1825,10 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
     CB_TRY(coef_to_device(c, in, nmax, tab, &dcs));
     double *dpts = nullptr;
     CB_TRY(dbuf(c, "sctr_pts", 3 * npt, &dpts));
-    CB_CUDA(cudaMemcpyAsync(dpts, pnt->lat, npt * 8, cudaMemcpyHostToDevice,
-                            c.stream), st);
-    CB_CUDA(cudaMemcpyAsync(dpts + npt, pnt->lon, npt * 8,
-                            cudaMemcpyHostToDevice, c.stream), st);
+    CB_TRY(stage_h2d(c, dpts, pnt->lat, npt * 8));
+    CB_TRY(stage_h2d(c, dpts + npt, pnt->lon, npt * 8));
     if (!r_eq)
-        CB_CUDA(cudaMemcpyAsync(dpts + 2 * npt, pnt->r, npt * 8,
-                                cudaMemcpyHostToDevice, c.stream), st);
+        CB_TRY(stage_h2d(c, dpts + 2 * npt, pnt->r, npt * 8));
     double *fo = d_f;
     if (!fo)
         CB_TRY(dbuf(c, "sctr_f", (size_t)npar * npt, &fo));
@@ -1842,8 +1865,14 @@ Status shs_sctr(Context &c, const charm_point *pnt, const CoefIn &in,
     }
     if (!d_f)
         for (int q = 0; q < npar; q++)
-            CB_CUDA(cudaMemcpyAsync(f[q], fo + (size_t)q * npt, npt * 8,
-                                    cudaMemcpyDeviceToHost, c.stream), st);
+        {
+            if (!is_pageable(f[q]))
+                CB_CUDA(cudaMemcpyAsync(f[q], fo + (size_t)q * npt, npt * 8,
+                                        cudaMemcpyDeviceToHost, c.stream),
+                        st);
+            else
+                CB_TRY(stage_d2h(c, f[q], fo + (size_t)q * npt, npt * 8));
+        }
     return finish(c, d_status);
 }
 
@@ -3068,10 +3097,10 @@ Status sha_grid(Context &c, const charm_point *pnt, const double *f_host,
                     CB_CUDA(cudaStreamWaitEvent(c.copy_stream,
                                                 c.band_ev[EV_ORD0 + k], 0),
                             st);
-                    CB_TRY(download_tri_orders(oc, sn, hc, mb[k], m_hi,
-                                               c.copy_stream));
-                    CB_TRY(download_tri_orders(os, sn, hs, mb[k], m_hi,
-                                               c.copy_stream));
+                    CB_TRY(download_tri_orders(c, oc, sn, hc, mb[k], m_hi,
+                                               c.copy_stream, 0));
+                    CB_TRY(download_tri_orders(c, os, sn, hs, mb[k], m_hi,
+                                               c.copy_stream, 0));
                 }
                 ordered = true;
             }
