@@ -1089,11 +1089,12 @@ def cells(steps=5, oracle_rows=3):
     L.charm_err_free(err)
     peak = L.charm_b200_fp64_peak_tflops()
     units = T * ((nlat + 1) // 2)
-    # FP64 instructions per (n, m, cell-row pair): two boundary recurrences
-    # (DMUL + DFMA each), the integral (2 DMUL + 2 DFMA; h_n beta_n comes
-    # staged) and two DFMA sums; the analysis adds the reduction of the
-    # lane sums (two DADD per lane and degree for two pairs per lane)
-    for name, ipu in (("shs_cell", 10.0), ("sha_cell", 11.0)):
+    # FP64 instructions per (n, m, cell-row pair) as ncu counts them at
+    # nmax 2190: synthesis two boundary recurrences (DMUL + DFMA each), the integral
+    # (2 DMUL + 2 DFMA; h_n beta_n comes staged) and two DFMA sums; the
+    # analysis carries the common boundary of two adjacent rows once and
+    # adds the reduction of the lane sums
+    for name, ipu in (("shs_cell", 10.5), ("sha_cell", 10.4)):
         k = res[name]
         k["fp64_instr_per_unit"] = ipu
         k["fp64_pipe_frac"] = (units * ipu / (k["legendre_ms"] * 1e-3) /
