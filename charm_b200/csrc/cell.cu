@@ -504,6 +504,233 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell(CellArgs A)
 }
 
 // ---------------------------------------------------------------------------
+// Grid synthesis, two adjacent cell-row pairs per lane
+// ---------------------------------------------------------------------------
+// Rows aligned as the analysis requires them (latmin[i] == latmax[i + 1]):
+// lane l of tile t takes the pairs 2l and 2l + 1 of the tile's 64, whose
+// common boundary (the lower one of the first, the upper one of the second)
+// is carried once (step_shared): per two pairs and degree, three boundary
+// recurrences instead of four and one product w x for both integrals.  The
+// rest is k_shs_cell's, row by row.
+template <bool RR>
+__global__ void __launch_bounds__(CELL_WARPS * 32) k_shs_cell2(CellArgs A)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned warp = threadIdx.x >> 5;
+    const Stage S = warp_stage(smem_raw + (size_t)warp * CELL_STAGE_BYTES);
+    const long long N = A.nmax;
+    const int np = A.npairs;
+
+    for (;;)
+    {
+        unsigned long long item = 0;
+        if (lane == 0)
+            item = atomicAdd(A.counter, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= (unsigned long long)A.nitems)
+            break;
+        const long long m = (long long)(item / (unsigned long long)A.ntiles);
+        const int tile = (int)(item % (unsigned long long)A.ntiles);
+        CellRec R[2];
+        int pk[2];
+        bool valid[2], skip_k[2];
+        double rho[2], rn[2], u1k[2], u2k[2];
+        double ae[2] = {0.0, 0.0}, ao[2] = {0.0, 0.0};
+        double be[2] = {0.0, 0.0}, bo[2] = {0.0, 0.0};
+        bool skip_all = true;
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+            const int p = tile * 64 + 2 * (int)lane + k;
+            pk[k] = p;
+            valid[k] = p < np;
+            R[k].t1 = valid[k] ? A.geo[0 * np + p] : 0.0;
+            u1k[k] = valid[k] ? A.geo[1 * np + p] : 1.0;
+            R[k].t2 = valid[k] ? A.geo[2 * np + p] : 0.0;
+            u2k[k] = valid[k] ? A.geo[3 * np + p] : 1.0;
+            rho[k] = (RR && valid[k]) ? A.geo[4 * np + p] : 1.0;
+            R[k].u1s = u1k[k] * u1k[k];
+            R[k].u2s = u2k[k] * u2k[k];
+            skip_k[k] = !valid[k] ||
+                        (A.polar_thr >= 0.0 &&
+                         A.polar_thr < (double)m - (double)N * u1k[k]);
+            skip_all &= skip_k[k];
+            rn[k] = RR ? ipow(rho[k], m + 1) : 1.0;
+        }
+        const bool skip = __all_sync(0xffffffffu, skip_all);
+        const long long c0 = tri_col0(N, m);
+        const long long ncol = N - m + 1;
+        const int nchunks = (int)((ncol + LEG_CHUNK - 1) / LEG_CHUNK);
+
+        if (!skip && m == 0)
+        {
+            // zonal: un-normalised polynomials (shs_cell_kernel.c:97-175),
+            // row by row
+            double p0a[2] = {1.0, 1.0}, p0b[2] = {1.0, 1.0};
+            double p1a[2] = {R[0].t1, R[1].t1}, p1b[2] = {R[0].t2, R[1].t2};
+            for (int j = 0; j < nchunks; j++)
+            {
+                const int cnt = (int)min((long long)LEG_CHUNK,
+                                         ncol - (long long)j * LEG_CHUNK);
+                stage_chunk(S, A, c0, m, j, cnt, lane);
+                for (int i = 0; i < cnt; i++)
+                {
+                    const long long n = (long long)j * LEG_CHUNK + i;
+                    const double tcn = A.tc[c0 + n];
+                    const double2 c = S.cs[i];
+#pragma unroll
+                    for (int k = 0; k < 2; k++)
+                    {
+                        double in0;
+                        if (n == 0)
+                            in0 = R[k].t2 - R[k].t1;
+                        else
+                        {
+                            const double4 z = A.zn[n];
+                            const double p2a =
+                                z.x * (R[k].t1 * p1a[k]) - z.y * p0a[k];
+                            const double p2b =
+                                z.x * (R[k].t2 * p1b[k]) - z.y * p0b[k];
+                            in0 = z.z * ((p2b - p0b[k]) - (p2a - p0a[k]));
+                            p0a[k] = p1a[k];
+                            p1a[k] = p2a;
+                            p0b[k] = p1b[k];
+                            p1b[k] = p2b;
+                        }
+                        const double v = (in0 / tcn) * rn[k];
+                        if (RR)
+                            rn[k] *= rho[k];
+                        if ((n & 1) == 0)
+                            ae[k] = fma(v, c.x, ae[k]);
+                        else
+                            ao[k] = fma(v, c.x, ao[k]);
+                    }
+                }
+            }
+        }
+        else if (!skip)
+        {
+            const double sigma = A.sg[2 * m];
+            const int g0 = (int)A.sg[2 * m + 1];
+            bool sc = false;
+#pragma unroll
+            for (int k = 0; k < 2; k++)
+            {
+                cell_seed(R[k], sigma, g0, u1k[k], u2k[k], m,
+                          valid[k] ? A.imm[(size_t)m * np + pk[k]] : 0.0);
+                sc |= (R[k].E1 | R[k].E2) != 0;
+            }
+            // the common boundary is renormalised through R[0]
+            R[1].E2 = 0;
+            bool any_scaled = __any_sync(0xffffffffu, sc);
+            for (int j = 0; j < nchunks; j++)
+            {
+                const int cnt = (int)min((long long)LEG_CHUNK,
+                                         ncol - (long long)j * LEG_CHUNK);
+                stage_chunk(S, A, c0, m, j, cnt, lane);
+                int i0 = 0;
+                if (j == 0)
+                {
+                    // n = m: the sectorial integrals
+                    const double2 c = S.cs[0];
+#pragma unroll
+                    for (int k = 0; k < 2; k++)
+                    {
+                        const double v = R[k].J1 * rn[k];
+                        if (RR)
+                            rn[k] *= rho[k];
+                        ae[k] = fma(v, c.x, ae[k]);
+                        be[k] = fma(v, c.y, be[k]);
+                    }
+                    i0 = 1;
+                }
+                else
+                {
+                    const double mul = A.tmul[(size_t)m * A.ldmul + j];
+                    R[0].scale(mul);
+                    R[1].scale(mul);
+                }
+                auto one = [&](int i, bool odd) {
+                    const double beta = S.tb[i].x;
+                    const double2 h = S.hn[i];
+                    double v[2];
+                    step_shared(R[0], R[1], beta, h.x, h.y, v[0], v[1]);
+                    const double2 c = S.cs[i];
+#pragma unroll
+                    for (int k = 0; k < 2; k++)
+                    {
+                        const double w = RR ? v[k] * rn[k] : v[k];
+                        if (RR)
+                            rn[k] *= rho[k];
+                        if (odd)
+                        {
+                            ao[k] = fma(w, c.x, ao[k]);
+                            bo[k] = fma(w, c.y, bo[k]);
+                        }
+                        else
+                        {
+                            ae[k] = fma(w, c.x, ae[k]);
+                            be[k] = fma(w, c.y, be[k]);
+                        }
+                    }
+                };
+                int i = i0;
+                if (i & 1)
+                {
+                    one(i, true);
+                    i++;
+                }
+#pragma unroll 2
+                for (; i + 1 < cnt; i += 2)
+                {
+                    one(i, false);
+                    one(i + 1, true);
+                }
+                if (i < cnt)
+                    one(i, false);
+                if (any_scaled)
+                {
+                    const bool s0 = R[0].fixup();
+                    const bool s1 = R[1].fixup();
+                    any_scaled = __any_sync(0xffffffffu, s0 || s1);
+                }
+            }
+        }
+        double sm, cm, fm;
+        lon_factors(m, A.dlon, &sm, &cm, &fm);
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+            if (skip_k[k])
+                ae[k] = ao[k] = be[k] = bo[k] = 0.0;
+            if (!valid[k])
+                continue;
+            const int p = pk[k];
+            const double sc = A.geo[5 * np + p];
+            auto put = [&](int row, double a, double b) {
+                double2 v;
+                if (A.fft)
+                {
+                    const double c = m == 0 ? 1.0 : 0.5;
+                    v.x = ((a * sm - b * cm) * c) * sc;
+                    v.y = -((a * cm + b * sm) * c) * sc;
+                }
+                else
+                {
+                    v.x = (a * fm) * sc;
+                    v.y = (b * fm) * sc;
+                }
+                A.out[(size_t)row * A.ldf + m] = v;
+            };
+            put(A.row_n[p], ae[k] + ao[k], be[k] + bo[k]);
+            if (A.row_s[p] >= 0)
+                put(A.row_s[p], ae[k] - ao[k], be[k] - bo[k]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Grid analysis (approximate quadrature): partial sums per group of tiles
 // ---------------------------------------------------------------------------
 // Work item = (order m, group g of tiles of 32 K pairs); each lane carries K
@@ -1052,11 +1279,15 @@ cudaError_t launch_cell_imm(const CellArgs &A, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
-                            cudaStream_t st)
+cudaError_t launch_shs_cell(const CellArgs &A, bool rr, bool shared,
+                            int grid, cudaStream_t st)
 {
     const size_t smem = CELL_WARPS * CELL_STAGE_BYTES;
-    if (rr)
+    if (shared && rr)
+        k_shs_cell2<true><<<grid, CELL_WARPS * 32, smem, st>>>(A);
+    else if (shared)
+        k_shs_cell2<false><<<grid, CELL_WARPS * 32, smem, st>>>(A);
+    else if (rr)
         k_shs_cell<true><<<grid, CELL_WARPS * 32, smem, st>>>(A);
     else
         k_shs_cell<false><<<grid, CELL_WARPS * 32, smem, st>>>(A);

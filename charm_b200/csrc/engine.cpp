@@ -3422,7 +3422,12 @@ Status shs_cell_grid(Context &c, const charm_cell *cell, const CoefIn &in,
     CellArgs A{};
     A.nmax = (long long)nmax;
     A.npairs = np;
-    A.ntiles = (np + 31) / 32;
+    // two adjacent pairs per lane when the rows are aligned (each pair of
+    // rows shares a boundary) and there are enough pairs
+    bool shared = np >= 512;
+    for (int p = 0; shared && p + 1 < np; p += 2)
+        shared = cell->latmin[P.row_n[p]] == cell->latmax[P.row_n[p + 1]];
+    A.ntiles = shared ? (np + 63) / 64 : (np + 31) / 32;
     A.nitems = (long long)(nmax + 1) * A.ntiles;
     A.tb = tab.tb;
     A.tc = tab.tc;
@@ -3453,7 +3458,8 @@ Status shs_cell_grid(Context &c, const charm_cell *cell, const CoefIn &in,
         const int grid = (int)std::min<long long>((A.nitems + 3) / 4,
                                                   (long long)c.num_sms * 8);
         Scope sc(c, TIMER_SHS);
-        CB_CUDA(launch_shs_cell(A, rr, std::max(grid, 1), c.stream), st);
+        CB_CUDA(launch_shs_cell(A, rr, shared, std::max(grid, 1), c.stream),
+                st);
     }
     if (rf)
     {

@@ -317,8 +317,11 @@ cudaError_t launch_fp64_probe(long long iters, int blocks, int threads,
 cudaError_t launch_sctr(const SctrArgs &A, int kgrad, int dr, int dlat,
                         bool rr, int K, int grid, cudaStream_t st);
 cudaError_t launch_cell_imm(const CellArgs &A, cudaStream_t st);
-cudaError_t launch_shs_cell(const CellArgs &A, bool rr, int grid,
-                            cudaStream_t st);
+// shared: two adjacent pairs per lane (tiles of 64 pairs, A.ntiles set
+// accordingly), rows aligned so that pair 2l's lower boundary is pair
+// 2l + 1's upper one
+cudaError_t launch_shs_cell(const CellArgs &A, bool rr, bool shared,
+                            int grid, cudaStream_t st);
 // K cell-row pairs per lane (1 or 2); A.ntiles counts tiles of 32 K pairs
 // shared: pairs 2l and 2l + 1 are adjacent cell rows (the lower boundary
 // of the first is the upper one of the second); K must be 2

@@ -72,6 +72,9 @@ def sphere_cells(nlat, nlon, r):
     (360, 361, 722, 0.0),       # odd rows: a middle row astride the equator
     (360, 362, 724, 3000.0),    # above the sphere
     (720, 721, 1442, 0.0),
+    # 513 cell-row pairs: two adjacent pairs per lane sharing a boundary
+    (1024, 1025, 2050, 3000.0),
+    (1024, 1026, 2052, 0.0),
 ])
 def test_cell_grid_sphere_vs_oracle(cb, N, nlat, nlon, dr):
     """Whole-sphere cell grids (FFT synthesis, approximate-quadrature
