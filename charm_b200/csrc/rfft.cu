@@ -817,16 +817,17 @@ struct SrcClusterDif
     int q, C, Mc, M, nz;
     __device__ __forceinline__ double2 operator()(int i) const
     {
+        // i < Mc and q < C, C a power of two: k q mod C is a mask and
+        // i q < Mc C = M needs no reduction
         double2 acc = src(i);
         for (int k = 1; k < C && k * Mc < nz; k++)
         {
-            const int kq = (k * q) % C;
+            const int kq = (k * q) & (C - 1);
             acc = add2(acc, cmul(src(i + k * Mc), __ldg(&twM[kq * Mc])));
         }
         if (q == 0)
             return acc;
-        const int e = (int)(((long long)i * q) % M);
-        return cmul(acc, __ldg(&twM[e]));
+        return cmul(acc, __ldg(&twM[i * q]));
     }
 };
 
@@ -838,10 +839,14 @@ __device__ __forceinline__ double2 cluster_v(
 {
     const int pj = pidx(t % Mc);
     double2 acc = *cl.map_shared_rank(s + pj, 0);
+    // e = qq t mod M by repeated addition (t < M)
+    int e = 0;
     for (int qq = 1; qq < C; qq++)
     {
+        e += t;
+        if (e >= M)
+            e -= M;
         const double2 u = *cl.map_shared_rank(s + pj, qq);
-        const int e = (int)(((long long)qq * t) % M);
         acc = add2(acc, cmul(u, __ldg(&twM[e])));
     }
     return acc;
