@@ -446,6 +446,8 @@ constexpr int ct_radix(int M, int p)
 {
     if (M == 4608)
         return p < 2 ? 16 : 18;
+    if (M == 6144)   // the per-CTA length of the nmax 10800 cluster plan
+        return p < 2 ? 16 : (p == 2 ? 8 : 3);
     return p < 2 ? 16 : (p == 2 ? 9 : 4);
 }
 
@@ -1001,7 +1003,7 @@ __global__ void RFFT_BOUNDS(NR) k_rfft_inv_odd(RfftArgs A)
 }
 
 // Analysis direction of a cluster plan (A.C CTAs per row, double rows).
-template <int V, int NR>
+template <int V, int NR, int MC = 0>
 __global__ void RFFT_BOUNDS(NR) k_rfftc_fwd(RfftArgs A)
 {
     namespace cg = cooperative_groups;
@@ -1013,8 +1015,17 @@ __global__ void RFFT_BOUNDS(NR) k_rfftc_fwd(RfftArgs A)
     const long long row = blockIdx.x / C;
     SrcRow src{reinterpret_cast<const double2 *>(A.x + row * A.ldx), A.w, H};
     SrcClusterDif<SrcRow> dif{src, A.twM, q, C, Mc, A.M, H};
-    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, A.bh + (size_t)q * Mc);
-    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, SrcSmem{s}, nullptr);
+    if constexpr (MC > 0)
+    {
+        // plan fixed at compile time (Mc == MC)
+        fft_ct<V, MC, 0, false>(s, A.tw, tid, dif, A.bh + (size_t)q * Mc);
+        fft_ct<V, MC, 0, false>(s, A.tw, tid, SrcSmem{s}, nullptr);
+    }
+    else
+    {
+        fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, A.bh + (size_t)q * Mc);
+        fft_m<V>(s, A.tw, Mc, A.npass, tid, T, SrcSmem{s}, nullptr);
+    }
     cl.sync();
     // this CTA's share of the half spectrum X_0..X_kmax
     const int nk = A.kmax + 1;
@@ -1039,7 +1050,7 @@ __global__ void RFFT_BOUNDS(NR) k_rfftc_fwd(RfftArgs A)
 
 // Synthesis direction of a cluster plan: rows of even length (ODD false,
 // pairs x_2t + i x_2t+1 for t < H) or of odd length H (the real part).
-template <int V, int NR, bool ODD>
+template <int V, int NR, bool ODD, int MC = 0>
 __global__ void RFFT_BOUNDS(NR) k_rfftc_inv(RfftArgs A)
 {
     namespace cg = cooperative_groups;
@@ -1059,9 +1070,17 @@ __global__ void RFFT_BOUNDS(NR) k_rfftc_inv(RfftArgs A)
     {
         SrcSpectrum src{A.X + row * A.ldX, A.w, A.ht, H, A.kmax};
         SrcClusterDif<SrcSpectrum> dif{src, A.twM, q, C, Mc, A.M, H};
-        fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif, A.bh + (size_t)q * Mc);
+        if constexpr (MC > 0)
+            fft_ct<V, MC, 0, false>(s, A.tw, tid, dif,
+                                    A.bh + (size_t)q * Mc);
+        else
+            fft_m<V>(s, A.tw, Mc, A.npass, tid, T, dif,
+                     A.bh + (size_t)q * Mc);
     }
-    fft_m<V>(s, A.tw, Mc, A.npass, tid, T, SrcSmem{s}, nullptr);
+    if constexpr (MC > 0)
+        fft_ct<V, MC, 0, false>(s, A.tw, tid, SrcSmem{s}, nullptr);
+    else
+        fft_m<V>(s, A.tw, Mc, A.npass, tid, T, SrcSmem{s}, nullptr);
     cl.sync();
     const int t0 = (int)((long long)H * q / C);
     const int t1 = (int)((long long)H * (q + 1) / C);
@@ -1211,6 +1230,8 @@ cudaError_t rfft_set_smem(size_t smem)
         (const void *)k_rfftc_fwd<16, 96>,
         (const void *)k_rfftc_inv<16, 96, false>,
         (const void *)k_rfftc_inv<16, 96, true>,
+        (const void *)k_rfftc_fwd<16, 96, 6144>,
+        (const void *)k_rfftc_inv<16, 96, false, 6144>,
         (const void *)k_rfftc_kspec<16, 96>};
     for (const void *f : fns)
     {
@@ -1222,7 +1243,9 @@ cudaError_t rfft_set_smem(size_t smem)
     // clusters of 16 CTAs (rows beyond 8 x 9216) are a non-portable size
     const void *cfns[] = {(const void *)k_rfftc_fwd<16, 96>,
                           (const void *)k_rfftc_inv<16, 96, false>,
-                          (const void *)k_rfftc_inv<16, 96, true>};
+                          (const void *)k_rfftc_inv<16, 96, true>,
+                          (const void *)k_rfftc_fwd<16, 96, 6144>,
+                          (const void *)k_rfftc_inv<16, 96, false, 6144>};
     for (const void *f : cfns)
     {
         // where refused, plans with 16 CTAs fail their occupancy check
@@ -1310,11 +1333,16 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         at[0].val.clusterDim.z = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
+        // Mc = 6144 (the nmax 10800 rows): the plan fixed at compile time
+        const bool ct = Mc == 6144;
         if (!inverse)
-            return cudaLaunchKernelEx(&cfg, k_rfftc_fwd<16, 96>, A);
+            return ct ? cudaLaunchKernelEx(&cfg, k_rfftc_fwd<16, 96, 6144>, A)
+                      : cudaLaunchKernelEx(&cfg, k_rfftc_fwd<16, 96>, A);
         if (A.odd)
             return cudaLaunchKernelEx(&cfg, k_rfftc_inv<16, 96, true>, A);
-        return cudaLaunchKernelEx(&cfg, k_rfftc_inv<16, 96, false>, A);
+        return ct ? cudaLaunchKernelEx(&cfg, k_rfftc_inv<16, 96, false, 6144>,
+                                       A)
+                  : cudaLaunchKernelEx(&cfg, k_rfftc_inv<16, 96, false>, A);
     }
     const size_t smem = rfft_smem_bytes(A.M);
     const int T = A.M / 16;
