@@ -1090,11 +1090,11 @@ def cells(steps=5, oracle_rows=3):
     peak = L.charm_b200_fp64_peak_tflops()
     units = T * ((nlat + 1) // 2)
     # FP64 instructions per (n, m, cell-row pair) as ncu counts them at
-    # nmax 2190: synthesis two boundary recurrences (DMUL + DFMA each), the integral
-    # (2 DMUL + 2 DFMA; h_n beta_n comes staged) and two DFMA sums; the
-    # analysis carries the common boundary of two adjacent rows once and
-    # adds the reduction of the lane sums
-    for name, ipu in (("shs_cell", 10.5), ("sha_cell", 10.4)):
+    # nmax 2190: the boundary recurrences (DMUL + DFMA each; two adjacent
+    # rows share one), the integral (2 DMUL + 2 DFMA; h_n beta_n comes
+    # staged) and two DFMA sums; the analysis adds the reduction of the
+    # lane sums
+    for name, ipu in (("shs_cell", 9.2), ("sha_cell", 10.4)):
         k = res[name]
         k["fp64_instr_per_unit"] = ipu
         k["fp64_pipe_frac"] = (units * ipu / (k["legendre_ms"] * 1e-3) /
