@@ -437,9 +437,13 @@ __device__ __forceinline__ void fft_m(double2 *s,
 // 9216 = 16 16 9 4 (four instead of six).  The first pass has radix 16
 // and every later stride is a multiple of 8, as the padded addressing
 // needs.
+// Compile-time plans: the radices of FFT_M pass by pass.  The first is 16
+// (the zero half of a chirped sequence is skipped there), the last even
+// (the half-output passes), and every pass keeps M / R and the stride a
+// multiple of 8 (the padded layout).
 constexpr int ct_npass(int M)
 {
-    return M == 4608 ? 3 : 4;
+    return (M == 9216 || M == 6144) ? 4 : 3;
 }
 
 constexpr int ct_radix(int M, int p)
@@ -448,7 +452,13 @@ constexpr int ct_radix(int M, int p)
         return p < 2 ? 16 : 18;
     if (M == 6144)   // the per-CTA length of the nmax 10800 cluster plan
         return p < 2 ? 16 : (p == 2 ? 8 : 3);
-    return p < 2 ? 16 : (p == 2 ? 9 : 4);
+    if (M == 1152)
+        return p == 0 ? 16 : (p == 1 ? 4 : 18);
+    if (M == 2048)
+        return p < 2 ? 16 : 8;
+    if (M == 4096)
+        return 16;
+    return p < 2 ? 16 : (p == 2 ? 9 : 4);   // 9216
 }
 
 constexpr int ct_ns(int M, int p)
@@ -1224,6 +1234,18 @@ cudaError_t rfft_set_smem(size_t smem)
         (const void *)k_rfft_inv<16, 96, false, 9216>,
         (const void *)k_rfft_fwd<16, 96, true, 9216>,
         (const void *)k_rfft_inv<16, 96, true, 9216>,
+        (const void *)k_rfft_fwd<16, 96, false, 4096>,
+        (const void *)k_rfft_inv<16, 96, false, 4096>,
+        (const void *)k_rfft_fwd<16, 96, true, 4096>,
+        (const void *)k_rfft_inv<16, 96, true, 4096>,
+        (const void *)k_rfft_fwd<16, 96, false, 2048>,
+        (const void *)k_rfft_inv<16, 96, false, 2048>,
+        (const void *)k_rfft_fwd<16, 96, true, 2048>,
+        (const void *)k_rfft_inv<16, 96, true, 2048>,
+        (const void *)k_rfft_fwd<16, 96, false, 1152>,
+        (const void *)k_rfft_inv<16, 96, false, 1152>,
+        (const void *)k_rfft_fwd<16, 96, true, 1152>,
+        (const void *)k_rfft_inv<16, 96, true, 1152>,
         (const void *)k_rfft_inv4<16, 96, 4608>,
         (const void *)k_rfft_kernel_spectrum<16, 96>,
         (const void *)k_rfft_inv_odd<16, 96>,
@@ -1386,6 +1408,12 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         go(std::integral_constant<int, 4608>{});
     else if (A.M == 9216)
         go(std::integral_constant<int, 9216>{});
+    else if (A.M == 4096)
+        go(std::integral_constant<int, 4096>{});
+    else if (A.M == 2048)
+        go(std::integral_constant<int, 2048>{});
+    else if (A.M == 1152)
+        go(std::integral_constant<int, 1152>{});
     else
         go(std::integral_constant<int, 0>{});
     return cudaGetLastError();
