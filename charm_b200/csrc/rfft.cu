@@ -437,13 +437,15 @@ __device__ __forceinline__ void fft_m(double2 *s,
 // 9216 = 16 16 9 4 (four instead of six).  The first pass has radix 16
 // and every later stride is a multiple of 8, as the padded addressing
 // needs.
-// Compile-time plans: the radices of FFT_M pass by pass.  The first is 16
+// Compile-time plans: the radices of FFT_M pass by pass (the grids' common
+// Bluestein lengths: GL rows of nmax 360, 540, 900, 1260, 1620, 1980, 2190
+// and their neighbours, DH2 rows of nmax 2190, the nmax 10800 clusters).  The first is 16
 // (the zero half of a chirped sequence is skipped there), the last even
 // (the half-output passes), and every pass keeps M / R and the stride a
 // multiple of 8 (the padded layout).
 constexpr int ct_npass(int M)
 {
-    return (M == 9216 || M == 6144) ? 4 : 3;
+    return (M == 9216 || M == 6144 || M == 3072 || M == 3456) ? 4 : 3;
 }
 
 constexpr int ct_radix(int M, int p)
@@ -452,6 +454,12 @@ constexpr int ct_radix(int M, int p)
         return p < 2 ? 16 : 18;
     if (M == 6144)   // the per-CTA length of the nmax 10800 cluster plan
         return p < 2 ? 16 : (p == 2 ? 8 : 3);
+    if (M == 768)
+        return p == 1 ? 3 : 16;
+    if (M == 3072)
+        return p == 1 ? 3 : (p == 2 ? 4 : 16);
+    if (M == 3456)
+        return p == 0 ? 16 : (p == 1 ? 3 : (p == 2 ? 9 : 8));
     if (M == 1152)
         return p == 0 ? 16 : (p == 1 ? 4 : 18);
     if (M == 2048)
@@ -1242,6 +1250,18 @@ cudaError_t rfft_set_smem(size_t smem)
         (const void *)k_rfft_inv<16, 96, false, 2048>,
         (const void *)k_rfft_fwd<16, 96, true, 2048>,
         (const void *)k_rfft_inv<16, 96, true, 2048>,
+        (const void *)k_rfft_fwd<16, 96, false, 3072>,
+        (const void *)k_rfft_inv<16, 96, false, 3072>,
+        (const void *)k_rfft_fwd<16, 96, true, 3072>,
+        (const void *)k_rfft_inv<16, 96, true, 3072>,
+        (const void *)k_rfft_fwd<16, 96, false, 3456>,
+        (const void *)k_rfft_inv<16, 96, false, 3456>,
+        (const void *)k_rfft_fwd<16, 96, true, 3456>,
+        (const void *)k_rfft_inv<16, 96, true, 3456>,
+        (const void *)k_rfft_fwd<16, 96, false, 768>,
+        (const void *)k_rfft_inv<16, 96, false, 768>,
+        (const void *)k_rfft_fwd<16, 96, true, 768>,
+        (const void *)k_rfft_inv<16, 96, true, 768>,
         (const void *)k_rfft_fwd<16, 96, false, 1152>,
         (const void *)k_rfft_inv<16, 96, false, 1152>,
         (const void *)k_rfft_fwd<16, 96, true, 1152>,
@@ -1414,6 +1434,12 @@ cudaError_t launch_rfft(const RfftArgs &A, bool inverse, cudaStream_t st)
         go(std::integral_constant<int, 2048>{});
     else if (A.M == 1152)
         go(std::integral_constant<int, 1152>{});
+    else if (A.M == 768)
+        go(std::integral_constant<int, 768>{});
+    else if (A.M == 3072)
+        go(std::integral_constant<int, 3072>{});
+    else if (A.M == 3456)
+        go(std::integral_constant<int, 3456>{});
     else
         go(std::integral_constant<int, 0>{});
     return cudaGetLastError();
