@@ -4,8 +4,12 @@
   0.6 degrees of the poles, where the sectorial terms need the scaled-seed
   path) times 64 of the 21602 GL longitudes (fixture made by
   tests/golden/make_quad_n10800.py).  The whole potential must agree to a
-  relative RMS of 1e-12, and its part without the degree-0 term to 1e-9 of
-  that part's RMS (the degree-0 term alone is 1e5 times larger).
+  relative RMS of 2e-14 (3.4e-15 on B200), and its part without the
+  degree-0 term to 1e-9 of that part's RMS (6.5e-10 on B200).  The second
+  figure is the first one rescaled: the degree-0 term alone is 1e5 times
+  larger than the rest, every partial sum carries it, so the FP64 rounding
+  of the whole value (a few 1e-15 of it) is a few 1e-10 of the signal, and
+  no FP64 evaluation of the full sum can do better.
 * SHA(SHS(c)) on the full 10801 x 21602 GL grid must return c to a
   relative RMS of 1e-12."""
 import ctypes as ct
@@ -39,7 +43,7 @@ def test_n10800_against_quad_oracle(coefs):
     c, s = coefs
     p = cb.PointGrid(lat, lon, np.full(lat.size, R_EARTH))
     f = cb.shs_point(p, cb.Shc(N, GM, R_EARTH, c, s), N)[:, idx]
-    assert rel_rms(f, ref) <= 1e-12
+    assert rel_rms(f, ref) <= 2e-14
     f00 = GM / R_EARTH
     assert rel_rms(f - f00, ref - f00) <= 1e-9
 
